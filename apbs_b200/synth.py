@@ -1,0 +1,162 @@
+"""Seeded synthetic molecules and mg-manual calculation descriptions.
+
+The benchmark configurations describe globular clusters of atoms (no public
+dataset is involved).  A cluster of ``natoms`` atoms is drawn from a seed:
+positions uniform in a ball of radius ``radius`` with a minimum pairwise
+separation (random sequential rejection), charges from
+{-1, -0.5, 0, +0.5, +1} with weights {.1, .2, .4, .2, .1} shifted so the net
+charge equals ``net_charge``, radii uniform in [1.2, 2.0] Angstrom.
+
+``mg_manual`` builds the plain-C parameter block (``pmgb_params``) that both
+the CUDA library and the CPU oracle consume, with the grid centred on the
+molecule the way ``gcent mol 1`` does (midpoint of the atom-coordinate
+bounding box, Valist_getStatistics in src/generic/valist.c).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+PMGB_MAXION = 8
+SRFM_MOL, SRFM_SMOL = 0, 1
+CHGM_SPL2 = 1
+BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS = 0, 1, 2, 4
+
+
+class PmgbParams(ctypes.Structure):
+    """Mirror of ``pmgb_params`` in include/pmgb_params.h."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("nlev", ctypes.c_int),
+        ("hx", ctypes.c_double), ("hy", ctypes.c_double), ("hz", ctypes.c_double),
+        ("center", ctypes.c_double * 3),
+        ("nonlin", ctypes.c_int), ("srfm", ctypes.c_int),
+        ("chgm", ctypes.c_int), ("bcfl", ctypes.c_int),
+        ("pdie", ctypes.c_double), ("sdie", ctypes.c_double),
+        ("srad", ctypes.c_double), ("sdens", ctypes.c_double),
+        ("temp", ctypes.c_double), ("etol", ctypes.c_double),
+        ("nion", ctypes.c_int),
+        ("ion_q", ctypes.c_double * PMGB_MAXION),
+        ("ion_conc", ctypes.c_double * PMGB_MAXION),
+        ("ion_radius", ctypes.c_double * PMGB_MAXION),
+    ]
+
+
+@dataclass
+class Molecule:
+    xyz: np.ndarray      # (n, 3) float64, Angstrom
+    charge: np.ndarray   # (n,) float64, e
+    radius: np.ndarray   # (n,) float64, Angstrom
+
+    @property
+    def natoms(self) -> int:
+        return int(self.xyz.shape[0])
+
+    def center(self) -> np.ndarray:
+        """Bounding-box midpoint of the atom coordinates (gcent mol)."""
+        return 0.5 * (self.xyz.max(axis=0) + self.xyz.min(axis=0))
+
+
+def cluster(natoms: int, radius: float, seed: int, net_charge: float = 0.0,
+            min_sep: float = 1.5, center=(0.0, 0.0, 0.0)) -> Molecule:
+    """Globular cluster by random sequential rejection inside a ball."""
+    rng = np.random.default_rng(seed)
+    cell = min_sep
+    ncell = int(np.ceil(2 * radius / cell)) + 3
+    grid: dict = {}
+    pts = np.empty((natoms, 3))
+    count = 0
+    tries = 0
+    sep2 = min_sep * min_sep
+    while count < natoms:
+        batch = rng.uniform(-radius, radius, size=(4096, 3))
+        batch = batch[np.einsum("ij,ij->i", batch, batch) <= radius * radius]
+        for p in batch:
+            tries += 1
+            c = tuple(((p + radius) / cell).astype(int) + 1)
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        lst = grid.get((c[0] + dx, c[1] + dy, c[2] + dz))
+                        if lst:
+                            for q in lst:
+                                d = p - pts[q]
+                                if d @ d < sep2:
+                                    ok = False
+                                    break
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                pts[count] = p
+                grid.setdefault(c, []).append(count)
+                count += 1
+                if count == natoms:
+                    break
+        if tries > 2000 * natoms + 100000:
+            raise RuntimeError("cluster: packing too dense for min_sep")
+    vals = np.array([-1.0, -0.5, 0.0, 0.5, 1.0])
+    q = rng.choice(vals, size=natoms, p=[0.1, 0.2, 0.4, 0.2, 0.1])
+    q = q + (net_charge - q.sum()) / natoms
+    r = rng.uniform(1.2, 2.0, size=natoms)
+    return Molecule(pts + np.asarray(center, dtype=float), q, r)
+
+
+def mgparm_nlev(n: int) -> int:
+    """Level count chosen by MGparm_check (src/generic/mgparm.c:263-330)."""
+    ti = n - 1
+    nlev = 0
+    while ti % 2 == 0 and ti > 0:
+        nlev += 1
+        ti = int(np.ceil(0.5 * ti))
+    nlev -= 1
+    if n > 65 and nlev < 4:
+        raise ValueError("dime %d needs rounding to c*2^5+1 as MGparm_check does" % n)
+    return nlev
+
+
+def mg_manual(dime, grid, center, *, npbe=False, srfm=SRFM_SMOL, bcfl=BCFL_SDH,
+              pdie=2.0, sdie=78.54, srad=1.4, sdens=10.0, temp=298.15,
+              ions=((1.0, 0.15, 2.0), (-1.0, 0.15, 2.0)), etol=0.0,
+              nlev=None) -> PmgbParams:
+    """Parameter block of one mg-manual ELEC calculation."""
+    if np.isscalar(dime):
+        dime = (int(dime),) * 3
+    if np.isscalar(grid):
+        grid = (float(grid),) * 3
+    p = PmgbParams()
+    p.nx, p.ny, p.nz = (int(d) for d in dime)
+    p.nlev = int(nlev) if nlev else min(mgparm_nlev(d) for d in dime)
+    p.hx, p.hy, p.hz = (float(h) for h in grid)
+    for i in range(3):
+        p.center[i] = float(center[i])
+    p.nonlin = 1 if npbe else 0
+    p.srfm = srfm
+    p.chgm = CHGM_SPL2
+    p.bcfl = bcfl
+    p.pdie, p.sdie, p.srad, p.sdens, p.temp = pdie, sdie, srad, sdens, temp
+    p.etol = etol
+    p.nion = len(ions)
+    for i, (qq, cc, rr) in enumerate(ions):
+        p.ion_q[i], p.ion_conc[i], p.ion_radius[i] = qq, cc, rr
+    return p
+
+
+def config0(seed: int = 0):
+    """65^3 LPBE, 500 atoms in a 12 A ball, 0.15 M 1:1 salt, spl2/smol/sdh."""
+    mol = cluster(500, 12.0, seed)
+    return mol, mg_manual(65, 0.5, mol.center())
+
+
+def config1(seed: int = 1):
+    """161^3 NPBE, 5000 atoms in a 25 A ball, net +12, 0.1 M 1:1 salt."""
+    mol = cluster(5000, 25.0, seed, net_charge=12.0)
+    return mol, mg_manual(161, 0.4, mol.center(), npbe=True,
+                          ions=((1.0, 0.1, 2.0), (-1.0, 0.1, 2.0)))

@@ -1,0 +1,71 @@
+"""ctypes binding of oracle/_ref/libapbsref.so: the reference APBS PMG path
+compiled unchanged (see oracle/Makefile).  TEST INFRASTRUCTURE ONLY."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libapbsref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.ref_pmg_run.restype = ctypes.c_int
+        _lib.ref_pmg_run.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
+                                     dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=4096):
+    """Run ctor+fillco+solve+energy of the reference on one calculation.
+
+    Returns a dict with u (nz,ny,nx), energy_kT, progress-message count,
+    residual log, phase timings and, on request, the fill maps and faces.
+    """
+    n = params.nx * params.ny * params.nz
+    u = np.zeros(n)
+    maps = np.zeros(5 * n) if want_maps else None
+    nfaces = 2 * (params.ny * params.nz + params.nx * params.nz + params.nx * params.ny)
+    faces = np.zeros(nfaces) if want_faces else None
+    out = np.zeros(16)
+    reslog = np.zeros(reslog_cap)
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(mol.charge, dtype=np.float64)
+    r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    rc = lib().ref_pmg_run(ctypes.byref(params), mol.natoms, _ptr(xyz), _ptr(q), _ptr(r),
+                           _ptr(u), _ptr(maps), _ptr(faces), _ptr(out), _ptr(reslog),
+                           reslog_cap, verbose)
+    if rc != 1:
+        raise RuntimeError("reference PMG run failed")
+    shape = (params.nz, params.ny, params.nx)
+    res = {
+        "u": u.reshape(shape),
+        "energy_kT": out[0],
+        "progress_msgs": int(out[1]),
+        "reslog": reslog[: min(int(out[2]), reslog_cap)].copy(),
+        "t_ctor": out[3], "t_fillco": out[4], "t_solve": out[5], "t_energy": out[6],
+        "qf": out[7], "diel": out[8], "qm": out[9],
+    }
+    if maps is not None:
+        m = maps.reshape(5, *shape)
+        res.update(charge=m[0], epsx=m[1], epsy=m[2], epsz=m[3], kappa=m[4])
+    if faces is not None:
+        res["faces"] = faces
+    return res

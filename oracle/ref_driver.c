@@ -1,0 +1,186 @@
+/*
+ * ref_driver.c -- runs the REFERENCE APBS PMG path (compiled unchanged from
+ * the reference sources by oracle/Makefile) on one mg-manual calculation.
+ *
+ * TEST INFRASTRUCTURE ONLY (parity checker and CPU baseline).  Built into
+ * oracle/_ref/libapbsref.so; never linked into the product library.
+ *
+ * The call sequence mirrors initMG / solveMG / setPartMG / energyMG of the
+ * reference (src/routines.c:1314-1606, 1635-1674, 1676-1724, 1726-1801) for
+ * a single non-focused mg-manual ELEC block, starting from an in-memory atom
+ * list instead of a PQR file (Valist_readPQR, src/generic/valist.c:606, is
+ * replaced by filling the Valist directly and calling Valist_getStatistics).
+ */
+#include <time.h>
+#include "apbscfg.h"
+#include "maloc/maloc.h"
+#include "generic/vhal.h"
+#include "generic/valist.h"
+#include "generic/vatom.h"
+#include "generic/vpbe.h"
+#include "generic/mgparm.h"
+#include "generic/pbeparm.h"
+#include "mg/vpmgp.h"
+#include "mg/vpmg.h"
+#include "pmgb_params.h"
+
+void oracle_shim_set_log(double *buf, int cap);
+int oracle_shim_log_count(void);
+int oracle_shim_iter_count(void);
+void oracle_shim_set_verbose(int v);
+
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static Valist *make_alist(int natoms, const double *xyz, const double *q,
+                          const double *r) {
+    int i;
+    Valist *alist = Valist_ctor();
+    alist->atoms = (Vatom *)Vmem_malloc(alist->vmem, (size_t)natoms,
+                                        sizeof(Vatom));
+    alist->number = natoms;
+    for (i = 0; i < natoms; i++) {
+        Vatom *a = &(alist->atoms[i]);
+        a->position[0] = xyz[3 * i + 0];
+        a->position[1] = xyz[3 * i + 1];
+        a->position[2] = xyz[3 * i + 2];
+        a->charge = q[i];
+        a->radius = r[i];
+        a->partID = 1.0;
+        a->epsilon = 0.0;
+        a->id = i;
+    }
+    Valist_getStatistics(alist);
+    return alist;
+}
+
+/* MGparm for an mg-manual block (fields read by Vpmgp_ctor2, vpmgp.c:93-170,
+ * and Vpmg_ctor2, vpmg.c:153-399). */
+static MGparm *make_mgparm(const pmgb_params *p) {
+    int i;
+    MGparm *mg = MGparm_ctor(MCT_MANUAL);
+    mg->dime[0] = p->nx; mg->dime[1] = p->ny; mg->dime[2] = p->nz;
+    mg->setdime = 1;
+    mg->nlev = p->nlev; mg->setnlev = 1;
+    mg->grid[0] = p->hx; mg->grid[1] = p->hy; mg->grid[2] = p->hz;
+    mg->setgrid = 1;
+    mg->glen[0] = (p->nx - 1) * p->hx;
+    mg->glen[1] = (p->ny - 1) * p->hy;
+    mg->glen[2] = (p->nz - 1) * p->hz;
+    mg->setglen = 1;
+    for (i = 0; i < 3; i++) mg->center[i] = p->center[i];
+    mg->cmeth = MCM_POINT;
+    mg->setgcent = 1;
+    mg->chgm = (Vchrg_Meth)p->chgm; mg->setchgm = 1;
+    mg->chgs = VCM_CHARGE;
+    if (p->etol > 0.0) { mg->etol = p->etol; mg->setetol = 1; }
+    mg->useAqua = 0;
+    for (i = 0; i < 6; i++) mg->partDisjOwnSide[i] = 0;
+    if (p->nonlin) {
+        mg->nonlintype = NONLIN_NPBE;
+        mg->method = VSOL_Newton;
+    } else {
+        mg->nonlintype = NONLIN_LPBE;
+        mg->method = VSOL_MG;
+    }
+    return mg;
+}
+
+/*
+ * Run ctor + fillco + solve + setPart + energy.
+ *   u      (out, optional) potential, nx*ny*nz doubles, IJK = k*nx*ny+j*nx+i
+ *   maps   (out, optional) 5*N doubles: charge, epsx, epsy, epsz, kappa
+ *   faces  (out, optional) 2*(ny*nz + nx*nz + nx*ny) doubles: gxcf slots 0,1
+ *          then gycf slots 0,1 then gzcf slots 0,1 (vpmg.h:1384-1386 layout)
+ *   out    (out) [0] energy (kT) [1] V-cycle/Newton progress messages
+ *          [2] residual-log entries [3] t_ctor [4] t_fillco [5] t_solve
+ *          [6] t_energy (seconds) [7] qf [8] diel [9] qm (kT, NPBE only)
+ *   reslog (out, optional) relative residual of every progress message
+ * Returns 1 on success (Vpmg convention), 0 on failure.
+ */
+int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
+                const double *q, const double *r, double *u, double *maps,
+                double *faces, double *out, double *reslog, int reslog_cap,
+                int verbose) {
+    int i, n, rc;
+    double t0, t1, t2, t3, t4;
+    double ionc[PMGB_MAXION], ionr[PMGB_MAXION], ionq[PMGB_MAXION];
+    double partMin[3], partMax[3];
+    Valist *alist;
+    MGparm *mg;
+    Vpbe *pbe;
+    Vpmgp *pmgp;
+    Vpmg *pmg;
+
+    oracle_shim_set_verbose(verbose);
+    oracle_shim_set_log(reslog, reslog_cap);
+    for (i = 0; i < p->nion && i < PMGB_MAXION; i++) {
+        ionc[i] = p->ion_conc[i];
+        ionr[i] = p->ion_radius[i];
+        ionq[i] = p->ion_q[i];
+    }
+    t0 = now_s();
+    alist = make_alist(natoms, xyz, q, r);
+    mg = make_mgparm(p);
+    pbe = Vpbe_ctor(alist, p->nion, ionc, ionr, ionq, p->temp, p->pdie,
+                    p->sdie, p->srad, 0, p->sdens, 0.0, 0.0, 0.0, 0.0);
+    if (pbe == VNULL) return 0;
+    pmgp = Vpmgp_ctor(mg);
+    pmgp->bcfl = (Vbcfl)p->bcfl;
+    pmgp->xcent = p->center[0];
+    pmgp->ycent = p->center[1];
+    pmgp->zcent = p->center[2];
+    pmg = Vpmg_ctor(pmgp, pbe, 0, VNULL, mg, PCE_NO);
+    t1 = now_s();
+    rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, 0.3, (Vchrg_Meth)p->chgm,
+                     0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
+                     VNULL);
+    t2 = now_s();
+    if (rc != 1) return 0;
+    n = p->nx * p->ny * p->nz;
+    if (maps) {
+        memcpy(maps + 0 * (size_t)n, pmg->charge, sizeof(double) * n);
+        memcpy(maps + 1 * (size_t)n, pmg->epsx, sizeof(double) * n);
+        memcpy(maps + 2 * (size_t)n, pmg->epsy, sizeof(double) * n);
+        memcpy(maps + 3 * (size_t)n, pmg->epsz, sizeof(double) * n);
+        memcpy(maps + 4 * (size_t)n, pmg->kappa, sizeof(double) * n);
+    }
+    if (faces) {
+        size_t fx = (size_t)p->ny * p->nz, fy = (size_t)p->nx * p->nz,
+               fz = (size_t)p->nx * p->ny;
+        memcpy(faces, pmg->gxcf, sizeof(double) * 2 * fx);
+        memcpy(faces + 2 * fx, pmg->gycf, sizeof(double) * 2 * fy);
+        memcpy(faces + 2 * fx + 2 * fy, pmg->gzcf, sizeof(double) * 2 * fz);
+    }
+    rc = Vpmg_solve(pmg);
+    t3 = now_s();
+    if (rc != 1) return 0;
+    if (u) memcpy(u, pmg->u, sizeof(double) * n);
+    for (i = 0; i < 3; i++) {
+        partMin[i] = mg->center[i] - 0.5 * mg->glen[i];
+        partMax[i] = mg->center[i] + 0.5 * mg->glen[i];
+    }
+    Vpmg_setPart(pmg, partMin, partMax, mg->partDisjOwnSide);
+    out[0] = Vpmg_energy(pmg, 1);
+    t4 = now_s();
+    out[1] = (double)oracle_shim_iter_count();
+    out[2] = (double)oracle_shim_log_count();
+    out[3] = t1 - t0;
+    out[4] = t2 - t1;
+    out[5] = t3 - t2;
+    out[6] = t4 - t3;
+    out[7] = Vpmg_qfEnergy(pmg, 1);
+    out[8] = (p->nonlin) ? Vpmg_dielEnergy(pmg, 1) : 0.0;
+    out[9] = (p->nonlin) ? Vpmg_qmEnergy(pmg, 1) : 0.0;
+    oracle_shim_set_log(VNULL, 0);
+
+    Vpmg_dtor(&pmg);
+    Vpmgp_dtor(&pmgp);
+    Vpbe_dtor(&pbe);
+    MGparm_dtor(&mg);
+    Valist_dtor(&alist);
+    return 1;
+}
