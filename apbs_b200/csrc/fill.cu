@@ -1,0 +1,492 @@
+// Coefficient-map fill of the B200 PMG solver (Vpmg_fillco,
+// src/mg/vpmg.c:5250-5414) and the sdh Dirichlet boundary values.
+//
+// Compiled with -fmad=false and written with the reference's expression
+// trees: the integer index bounds (ceil/floor of FP64 expressions) and the
+// FP64 comparisons that decide which grid points a sphere marks are then
+// identical to the reference's, so the maps are bitwise equal.
+#include "fill_kernels.cuh"
+
+namespace pmgb {
+
+// ---------------------------------------------------------------------------
+// Charge: fillcoChargeSpline2 + bspline2 (vpmg.c:5091-5248).  One thread per
+// atom, 64 scatter-adds.  FP64 atomics make the per-point accumulation order
+// run-dependent (the sum is exact to round-off either way).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double bspline2(double x) {
+  double m2m, m2, m3;
+  if ((x >= 0.0) && (x <= 2.0)) m2m = 1.0 - fabs(x - 1.0);
+  else m2m = 0.0;
+  if ((x >= 1.0) && (x <= 3.0)) m2 = 1.0 - fabs(x - 2.0);
+  else m2 = 0.0;
+  if ((x >= 0.0) && (x <= 3.0)) m3 = 0.5 * x * m2m + 0.5 * (3.0 - x) * m2;
+  else m3 = 0.0;
+  return m3;
+}
+
+__global__ void k_charge_spl2(FillGeom G, int natoms, const double* __restrict__ xyz,
+                              const double* __restrict__ q, double zmagic, double* charge) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2];
+  if ((ax <= (G.xmin[0] - hx)) || (ax >= (G.xmax[0] + hx)) || (ay <= (G.xmin[1] - hy)) ||
+      (ay >= (G.xmax[1] + hy)) || (az <= (G.xmin[2] - hz)) || (az >= (G.xmax[2] + hz)))
+    return;
+  const double px = ax - G.xmin[0], py = ay - G.xmin[1], pz = az - G.xmin[2];
+  const double c = q[a] * zmagic / (hx * hy * hz);
+  const double fi = px / hx, fj = py / hy, fk = pz / hz;
+  int ip1 = (int)ceil(fi), im1 = (int)floor(fi);
+  int jp1 = (int)ceil(fj), jm1 = (int)floor(fj);
+  int kp1 = (int)ceil(fk), km1 = (int)floor(fk);
+  int ip2 = ip1 + 1, im2 = im1 - 1, jp2 = jp1 + 1, jm2 = jm1 - 1, kp2 = kp1 + 1, km2 = km1 - 1;
+  ip2 = min(ip2, nx - 1); im2 = max(im2, 0);
+  jp2 = min(jp2, ny - 1); jm2 = max(jm2, 0);
+  kp2 = min(kp2, nz - 1); km2 = max(km2, 0);
+  for (int ii = im2; ii <= ip2; ii++) {
+    const double mx = bspline2(1.5 + ((double)ii - fi));
+    for (int jj = jm2; jj <= jp2; jj++) {
+      const double my = bspline2(1.5 + ((double)jj - fj));
+      for (int kk = km2; kk <= kp2; kk++) {
+        const double mz = bspline2(1.5 + ((double)kk - fk));
+        atomicAdd(charge + G.g.idx(ii, jj, kk), (c * mx * my * mz));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// markSphere (vpmg.c:6444-6491) for one sphere on one (possibly staggered)
+// grid, executed by the calling thread group.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double cy, double cz,
+                                                  Grid g, double hx, double hy, double hz,
+                                                  double xmin, double ymin, double zmin,
+                                                  double* array, double markVal, int lane,
+                                                  int nlanes) {
+  const double posx = cx - xmin, posy = cy - ymin, posz = cz - zmin;
+  const double rtot2 = rtot * rtot;
+  const double xr = rtot + 0.5 * hx, yr = rtot + 0.5 * hy, zr = rtot + 0.5 * hz;
+  const int imin = max(0, (int)ceil((posx - xr) / hx));
+  const int jmin = max(0, (int)ceil((posy - yr) / hy));
+  const int kmin = max(0, (int)ceil((posz - zr) / hz));
+  const int imax = min(g.nx - 1, (int)floor((posx + xr) / hx));
+  const int jmax = min(g.ny - 1, (int)floor((posy + yr) / hy));
+  const int kmax = min(g.nz - 1, (int)floor((posz + zr) / hz));
+  if (imax < imin || jmax < jmin || kmax < kmin) return;
+  const int ni = imax - imin + 1, nj = jmax - jmin + 1, nk = kmax - kmin + 1;
+  const int tot = ni * nj * nk;
+  for (int t = lane; t < tot; t += nlanes) {
+    const int kk = kmin + t % nk;
+    const int jj = jmin + (t / nk) % nj;
+    const int ii = imin + t / (nk * nj);
+    const double fi = (double)ii, fj = (double)jj, fk = (double)kk;
+    const double dx2 = (posx - hx * fi) * (posx - hx * fi);
+    const double dy2 = (posy - hy * fj) * (posy - hy * fj);
+    if ((dx2 + dy2) > rtot2) continue;
+    const double dz2 = (posz - hz * fk) * (posz - hz * fk);
+    if ((dz2 + dy2 + dx2) <= rtot2) array[g.idx(ii, jj, kk)] = markVal;
+  }
+}
+
+__global__ void k_fill_value(double* a, size_t n, double v) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x)
+    a[q] = v;
+}
+
+// Atom spheres of fillcoCoefMolDielNoSmooth (vpmg.c:4390-4446): one block per
+// atom, the three staggered dielectric grids marked with epsp.
+__global__ void k_mark_atoms_diel(FillGeom G, int natoms, const double* __restrict__ xyz,
+                                  const double* __restrict__ r, double srad, double epsp,
+                                  double* epsx, double* epsy, double* epsz) {
+  const int a = blockIdx.x;
+  if (a >= natoms) return;
+  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2], arad = r[a];
+  if ((ax <= G.xmin[0]) || (ax >= G.xmax[0]) || (ay <= G.xmin[1]) || (ay >= G.xmax[1]) ||
+      (az <= G.xmin[2]) || (az >= G.xmax[2]))
+    return;
+  if (!(arad > 1.0e-9)) return;
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx),
+                    G.xmin[1], G.xmin[2], epsx, epsp, threadIdx.x, blockDim.x);
+  mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, G.xmin[0],
+                    (G.xmin[1] + 0.5 * hy), G.xmin[2], epsy, epsp, threadIdx.x, blockDim.x);
+  mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
+                    (G.xmin[2] + 0.5 * hz), epsz, epsp, threadIdx.x, blockDim.x);
+}
+
+// Ion accessibility of fillcoCoefMolIon (vpmg.c:4237-4333).
+__global__ void k_mark_atoms_kappa(FillGeom G, int natoms, const double* __restrict__ xyz,
+                                   const double* __restrict__ r, double irad, double* kappa) {
+  const int a = blockIdx.x;
+  if (a >= natoms) return;
+  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2], arad = r[a];
+  if (!(arad > 1.0e-9)) return;
+  if ((ax < (G.xmin[0] - irad - arad)) || (ax > (G.xmax[0] + irad + arad)) ||
+      (ay < (G.xmin[1] - irad - arad)) || (ay > (G.xmax[1] + irad + arad)) ||
+      (az < (G.xmin[2] - irad - arad)) || (az > (G.xmax[2] + irad + arad)))
+    return;
+  mark_sphere_group((irad + arad), ax, ay, az, G.g, G.h[0], G.h[1], G.h[2], G.xmin[0],
+                    G.xmin[1], G.xmin[2], kappa, 0.0, threadIdx.x, blockDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// Solvent-accessible surface points (Vacc_atomSurf, src/generic/vacc.c:866-922)
+// and their exclusion test (ivdwAccExclus, vacc.c:78-128).  The candidate
+// blockers of a point come from a uniform cell grid whose cells are at least
+// (max radius + probe) wide, so the 27 cells around the point hold every atom
+// that can exclude it -- the same atoms the reference's Vclist cell holds
+// (vclist.c:231-342); the decision is an exact FP64 comparison either way.
+// ---------------------------------------------------------------------------
+__global__ void k_cell_count(CellGrid C, int natoms, const double* __restrict__ xyz,
+                             int* count, int* cell_of) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  int c[3];
+  for (int d = 0; d < 3; d++) {
+    int v = (int)floor((xyz[3 * a + d] - C.lo[d]) / C.cs);
+    c[d] = min(max(v, 0), C.n[d] - 1);
+  }
+  const int cell = (c[2] * C.n[1] + c[1]) * C.n[0] + c[0];
+  cell_of[a] = cell;
+  atomicAdd(count + cell, 1);
+}
+
+__global__ void k_scan_single(const int* count, int n, int* start) {
+  // one block: exclusive scan, serial per chunk (cell counts are small)
+  __shared__ int sums[1024];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (n + nt - 1) / nt;
+  int s = 0;
+  for (int i = t * chunk; i < min(n, (t + 1) * chunk); i++) s += count[i];
+  sums[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    int acc = 0;
+    for (int i = 0; i < nt; i++) {
+      int v = sums[i];
+      sums[i] = acc;
+      acc += v;
+    }
+  }
+  __syncthreads();
+  int acc = sums[t];
+  for (int i = t * chunk; i < min(n, (t + 1) * chunk); i++) {
+    start[i] = acc;
+    acc += count[i];
+  }
+  if (t == nt - 1) start[n] = acc;
+}
+
+__global__ void k_cell_fill(int natoms, const int* __restrict__ cell_of, int* fillpos,
+                            int* atoms_sorted) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const int p = atomicAdd(fillpos + cell_of[a], 1);
+  atoms_sorted[p] = a;
+}
+
+__global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xyz,
+                           const double* __restrict__ r, const double* __restrict__ ref,
+                           int nref, double srad, const int* __restrict__ start,
+                           const int* __restrict__ atoms_sorted, unsigned char* flags,
+                           int* npts) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (tid >= (long long)natoms * nref) return;
+  const int a = (int)(tid / nref), t = (int)(tid % nref);
+  const double arad = r[a];
+  unsigned char acc = 0;
+  if (!(arad < 1.0e-9)) {
+    const double rad = arad + srad;
+    const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
+    const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
+    const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+    int c[3];
+    const double pp[3] = {px, py, pz};
+    for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
+    acc = 1;
+    for (int dz = -1; dz <= 1 && acc; dz++)
+      for (int dy = -1; dy <= 1 && acc; dy++)
+        for (int dx = -1; dx <= 1 && acc; dx++) {
+          const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+          if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
+            continue;
+          const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
+          for (int s = start[cell]; s < start[cell + 1]; s++) {
+            const int b = atoms_sorted[s];
+            if (b == a) continue;
+            const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1],
+                         d2 = pz - xyz[3 * b + 2];
+            const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+            const double rr = r[b] + srad;
+            if (dist2 < rr * rr) {
+              acc = 0;
+              break;
+            }
+          }
+        }
+  }
+  flags[tid] = acc;
+  if (acc) atomicAdd(npts, 1);
+}
+
+// Probe spheres around accessible SAS points reset the three dielectric
+// grids to epsw (vpmg.c:4456-4496).  One warp per surface point.
+__global__ void k_sas_mark(FillGeom G, int natoms, const double* __restrict__ xyz,
+                           const double* __restrict__ r, const double* __restrict__ ref,
+                           int nref, double srad, double epsw,
+                           const unsigned char* __restrict__ flags, double* epsx, double* epsy,
+                           double* epsz) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= (long long)natoms * nref) return;
+  if (!flags[w]) return;
+  const int a = (int)(w / nref), t = (int)(w % nref);
+  const double rad = r[a] + srad;
+  const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
+  const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
+  const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
+                    G.xmin[2], epsx, epsw, lane, 32);
+  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
+                    G.xmin[2], epsy, epsw, lane, 32);
+  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
+                    (G.xmin[2] + 0.5 * hz), epsz, epsw, lane, 32);
+}
+
+// 9-point harmonic-mean smoothing, fillcoCoefMolDielSmooth (vpmg.c:4500-4628).
+// a1..a3 are the unsmoothed maps.
+__global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __restrict__ a2,
+                         const double* __restrict__ a3, double* epsx, double* epsy,
+                         double* epsz) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t n = g.n();
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
+    double frac;
+    int np;
+    frac = 1.0 / a1[q];
+    frac += 1.0 / a2[q];
+    frac += 1.0 / a3[q];
+    np = 3;
+    if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k)]; np += 1; }
+    if (k > 0) { frac += 1.0 / a3[g.idx(i, j, k - 1)]; np += 1; }
+    if (i < (nx - 1)) {
+      frac += 1.0 / a2[g.idx(i + 1, j, k)];
+      frac += 1.0 / a3[g.idx(i + 1, j, k)];
+      np += 2;
+      if (j > 0) { frac += 1.0 / a2[g.idx(i + 1, j - 1, k)]; np += 1; }
+      if (k > 0) { frac += 1.0 / a3[g.idx(i + 1, j, k - 1)]; np += 1; }
+    }
+    epsx[q] = np / frac;
+
+    frac = 1.0 / a2[q];
+    frac += 1.0 / a1[q];
+    frac += 1.0 / a3[q];
+    np = 3;
+    if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k)]; np += 1; }
+    if (k > 0) { frac += 1.0 / a3[g.idx(i, j, k - 1)]; np += 1; }
+    if (j < (ny - 1)) {
+      frac += 1.0 / a1[g.idx(i, j + 1, k)];
+      frac += 1.0 / a3[g.idx(i, j + 1, k)];
+      np += 2;
+      if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j + 1, k)]; np += 1; }
+      if (k > 0) { frac += 1.0 / a3[g.idx(i, j + 1, k - 1)]; np += 1; }
+    }
+    epsy[q] = np / frac;
+
+    frac = 1.0 / a3[q];
+    frac += 1.0 / a1[q];
+    frac += 1.0 / a2[q];
+    np = 3;
+    if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k)]; np += 1; }
+    if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k)]; np += 1; }
+    if (k < (nz - 1)) {
+      frac += 1.0 / a1[g.idx(i, j, k + 1)];
+      frac += 1.0 / a2[g.idx(i, j, k + 1)];
+      np += 2;
+      if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k + 1)]; np += 1; }
+      if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k + 1)]; np += 1; }
+    }
+    epsz[q] = np / frac;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sdh boundary (bcfl_sdh + multipolebc, vpmg.c:3369-3645).  The 13 moment
+// sums run one per thread in atom order, as the reference accumulates them.
+// ---------------------------------------------------------------------------
+__global__ void k_sdh_moments(int natoms, const double* __restrict__ xyz,
+                              const double* __restrict__ q, double cx, double cy, double cz,
+                              double* mom) {
+  const int m = threadIdx.x;  // 0 charge, 1-3 dipole, 4-12 quadrupole
+  if (m >= 13) return;
+  double acc = 0.0;
+  for (int a = 0; a < natoms; a++) {
+    const double xr = xyz[3 * a] - cx, yr = xyz[3 * a + 1] - cy, zr = xyz[3 * a + 2] - cz;
+    const double c = q[a];
+    if (m == 0) {
+      acc += c;
+    } else if (m <= 3) {
+      const double d = (m == 1) ? xr : (m == 2) ? yr : zr;
+      acc += d * c;
+    } else {
+      double tr[9];
+      tr[0] = xr * xr * c; tr[1] = xr * yr * c; tr[2] = xr * zr * c;
+      tr[3] = yr * xr * c; tr[4] = yr * yr * c; tr[5] = yr * zr * c;
+      tr[6] = zr * xr * c; tr[7] = zr * yr * c; tr[8] = zr * zr * c;
+      const double qave = (tr[0] + tr[4] + tr[8]) / 3.0;
+      const int e = m - 4;
+      const double v = (e == 0 || e == 4 || e == 8) ? (tr[e] - qave) : (tr[e]);
+      acc += 1.5 * v;
+    }
+  }
+  mom[m] = acc;
+}
+
+__device__ void multipolebc(double r, double kappa, double eps_p, double eps_w, double rad,
+                            double tsr[3]) {
+  const double eps_r = eps_w / eps_p;
+  const double r2 = r * r, r3 = r2 * r, r5 = r3 * r2;
+  tsr[0] = (1.0 / eps_w) / r;
+  tsr[1] = (1.0 / eps_w) * (-1.0) / r3;
+  tsr[2] = (1.0 / eps_w) * (3.0) / r5;
+  if (kappa < 1.0e-9) {
+    tsr[1] = (3.0 * eps_r) / (1.0 + 2.0 * eps_r) * tsr[1];
+    tsr[2] = (5.0 * eps_r) / (2.0 + 3.0 * eps_r) * tsr[2];
+  } else {
+    const double ka = kappa * rad, ka2 = ka * ka, ka3 = ka2 * ka;
+    const double kr = kappa * r, kr2 = kr * kr;
+    tsr[0] = exp(ka - kr) / (1.0 + ka) * tsr[0];
+    tsr[1] = 3.0 * eps_r * exp(ka - kr) * (1.0 + kr) * tsr[1];
+    tsr[1] = tsr[1] / (1.0 + ka + eps_r * (2.0 + 2.0 * ka + ka2));
+    tsr[2] = 5.0 * eps_r * exp(ka - kr) * (3.0 + 3.0 * kr + kr2) * tsr[2];
+    tsr[2] = tsr[2] / (6.0 + 6.0 * ka + 2.0 * ka2 + eps_r * (9.0 + 9.0 * ka + 4.0 * ka2 + ka3));
+  }
+}
+
+// One thread per face point of the three face pairs; a grid point on an edge
+// is evaluated once per face it belongs to (identical value).
+__global__ void k_sdh_faces(SdhArgs A, const double* __restrict__ mom,
+                            const double* __restrict__ xf, const double* __restrict__ yf,
+                            const double* __restrict__ zf, double* gx, double* gy, double* gz) {
+  const Grid g = A.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t fx = (size_t)ny * nz, fy = (size_t)nx * nz, fz = (size_t)nx * ny;
+  const size_t tot = 2 * (fx + fy + fz);
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < tot;
+       t += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    double* out;
+    if (t < 2 * fx) {
+      const int s = (int)(t / fx);
+      const size_t rem = t % fx;
+      k = (int)(rem / ny); j = (int)(rem % ny); i = s ? nx - 1 : 0;
+      out = gx + t;
+    } else if (t < 2 * fx + 2 * fy) {
+      const size_t u = t - 2 * fx;
+      const int s = (int)(u / fy);
+      const size_t rem = u % fy;
+      k = (int)(rem / nx); i = (int)(rem % nx); j = s ? ny - 1 : 0;
+      out = gy + u;
+    } else {
+      const size_t u = t - 2 * fx - 2 * fy;
+      const int s = (int)(u / fz);
+      const size_t rem = u % fz;
+      j = (int)(rem / nx); i = (int)(rem % nx); k = s ? nz - 1 : 0;
+      out = gz + u;
+    }
+    const double xr = xf[i] - A.center[0], yr = yf[j] - A.center[1], zr = zf[k] - A.center[2];
+    const double dist = sqrt((xr * xr) + (yr * yr) + (zr * zr));
+    double t3[3];
+    multipolebc(dist, A.xkappa, A.eps_p, A.eps_w, A.size, t3);
+    const double pre = A.pre;
+    const double sq = mom[0], ux = mom[1], uy = mom[2], uz = mom[3];
+    const double qxx = mom[4] / 3.0, qxy = mom[5] / 3.0, qxz = mom[6] / 3.0;
+    const double qyy = mom[8] / 3.0, qyz = mom[9] / 3.0, qzz = mom[12] / 3.0;
+    double val = pre * sq * t3[0];
+    val -= pre * ux * xr * t3[1];
+    val -= pre * uy * yr * t3[1];
+    val -= pre * uz * zr * t3[1];
+    val += pre * qxx * xr * xr * t3[2];
+    val += pre * qyy * yr * yr * t3[2];
+    val += pre * qzz * zr * zr * t3[2];
+    val += pre * 2.0 * qxy * xr * yr * t3[2];
+    val += pre * 2.0 * qxz * xr * zr * t3[2];
+    val += pre * 2.0 * qyz * yr * zr * t3[2];
+    *out = val;
+  }
+}
+
+// ccf = zkappa2 * kappa (Vpmg_solve, vpmg.c:436-448)
+__global__ void k_ccf(size_t n, const double* __restrict__ kappa, double zkappa2, double* ccf) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x)
+    ccf[q] = zkappa2 * kappa[q];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_fill_value(cudaStream_t s, double* a, size_t n, double v) {
+  k_fill_value<<<blocks_for(n), kThreads, 0, s>>>(a, n, v);
+}
+void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                        const double* q, double zmagic, double* charge) {
+  if (natoms <= 0) return;
+  k_charge_spl2<<<(natoms + 127) / 128, 128, 0, s>>>(G, natoms, xyz, q, zmagic, charge);
+}
+void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                            const double* r, double srad, double epsp, double* epsx,
+                            double* epsy, double* epsz) {
+  if (natoms <= 0) return;
+  k_mark_atoms_diel<<<natoms, 256, 0, s>>>(G, natoms, xyz, r, srad, epsp, epsx, epsy, epsz);
+}
+void launch_mark_atoms_kappa(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                             const double* r, double irad, double* kappa) {
+  if (natoms <= 0) return;
+  k_mark_atoms_kappa<<<natoms, 256, 0, s>>>(G, natoms, xyz, r, irad, kappa);
+}
+void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
+                       int* count, int* start, int* fillpos, int* cell_of, int* sorted) {
+  const int ncell = C.n[0] * C.n[1] * C.n[2];
+  cudaMemsetAsync(count, 0, sizeof(int) * ncell, s);
+  k_cell_count<<<(natoms + 255) / 256, 256, 0, s>>>(C, natoms, xyz, count, cell_of);
+  k_scan_single<<<1, 1024, 0, s>>>(count, ncell, start);
+  cudaMemcpyAsync(fillpos, start, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s);
+  k_cell_fill<<<(natoms + 255) / 256, 256, 0, s>>>(natoms, cell_of, fillpos, sorted);
+}
+void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
+                const double* xyz, const double* r, const double* ref, int nref, double srad,
+                double epsw, const int* start, const int* sorted, unsigned char* flags,
+                int* npts, double* epsx, double* epsy, double* epsz) {
+  const long long tot = (long long)natoms * nref;
+  if (tot <= 0) return;
+  cudaMemsetAsync(npts, 0, sizeof(int), s);
+  k_sas_test<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(C, natoms, xyz, r, ref, nref, srad,
+                                                           start, sorted, flags, npts);
+  k_sas_mark<<<(unsigned)((tot * 32 + 255) / 256), 256, 0, s>>>(
+      G, natoms, xyz, r, ref, nref, srad, epsw, flags, epsx, epsy, epsz);
+}
+void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
+                   const double* a3, double* epsx, double* epsy, double* epsz) {
+  k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, a1, a2, a3, epsx, epsy, epsz);
+}
+void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
+                const double* q, double* mom, const double* xf, const double* yf,
+                const double* zf, double* gx, double* gy, double* gz) {
+  k_sdh_moments<<<1, 32, 0, s>>>(natoms, xyz, q, A.center[0], A.center[1], A.center[2], mom);
+  const size_t tot = 2 * ((size_t)A.g.ny * A.g.nz + (size_t)A.g.nx * A.g.nz +
+                          (size_t)A.g.nx * A.g.ny);
+  k_sdh_faces<<<blocks_for(tot), kThreads, 0, s>>>(A, mom, xf, yf, zf, gx, gy, gz);
+}
+void launch_ccf(cudaStream_t s, size_t n, const double* kappa, double zkappa2, double* ccf) {
+  k_ccf<<<blocks_for(n), kThreads, 0, s>>>(n, kappa, zkappa2, ccf);
+}
+
+}  // namespace pmgb

@@ -1,0 +1,51 @@
+// Kernel declarations of the coefficient-map fill (fill.cu).
+#pragma once
+#include "common.cuh"
+
+namespace pmgb {
+
+struct FillGeom {
+  Grid g;
+  double h[3];
+  double xmin[3];
+  double xmax[3];
+};
+
+// Uniform atom cell grid used for the SAS exclusion test.
+struct CellGrid {
+  double lo[3];
+  double cs;   // cell edge >= max atom radius + probe radius
+  int n[3];
+};
+
+struct SdhArgs {
+  Grid g;
+  double center[3];  // solute centre
+  double size;       // solute radius
+  double xkappa;
+  double eps_p, eps_w;
+  double pre;        // e^2 / (4 pi eps0 kB T) * 1e10
+};
+
+void launch_fill_value(cudaStream_t s, double* a, size_t n, double v);
+void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                        const double* q, double zmagic, double* charge);
+void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                            const double* r, double srad, double epsp, double* epsx,
+                            double* epsy, double* epsz);
+void launch_mark_atoms_kappa(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                             const double* r, double irad, double* kappa);
+void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
+                       int* count, int* start, int* fillpos, int* cell_of, int* sorted);
+void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
+                const double* xyz, const double* r, const double* ref, int nref, double srad,
+                double epsw, const int* start, const int* sorted, unsigned char* flags,
+                int* npts, double* epsx, double* epsy, double* epsz);
+void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
+                   const double* a3, double* epsx, double* epsy, double* epsz);
+void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
+                const double* q, double* mom, const double* xf, const double* yf,
+                const double* zf, double* gx, double* gy, double* gz);
+void launch_ccf(cudaStream_t s, size_t n, const double* kappa, double zkappa2, double* ccf);
+
+}  // namespace pmgb

@@ -1,0 +1,1027 @@
+// Host orchestration of the B200 PMG solver and the C ABI (apbs_b200.h).
+//
+// The control flow restates the reference drivers: Vpmg_fillco
+// (src/mg/vpmg.c:5250-5414), Vpmg_solve (401-558), Vmgdriv2
+// (src/pmgc/mgdrvd.c:190-558), Vmvcs (src/pmgc/mgcsd.c:57-565), Vnewdriv2 /
+// Vnewton (src/pmgc/newdrvd.c:169-350, newtond.c:162-598) and Vpmg_energy
+// (vpmg.c:1248-1891).  All arithmetic runs in CUDA kernels; the host keeps
+// only the decisions the reference takes on scalar norms (stopping tests,
+// Newton damping), reading one scalar per decision.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "apbs_b200.h"
+#include "fill_kernels.cuh"
+#include "mg_kernels.cuh"
+#include "mixed.cuh"
+#include "solver_internal.cuh"
+
+namespace pmgb {
+
+static thread_local char g_err[512] = "";
+static thread_local long long g_launches = 0;
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+void note_launches(long long n) { g_launches += n; }
+
+}  // namespace pmgb
+
+using namespace pmgb;
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e__ = (call);                                                          \
+    if (e__ != cudaSuccess) {                                                          \
+      set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e__));  \
+      return 0;                                                                        \
+    }                                                                                  \
+  } while (0)
+
+namespace {
+
+int dalloc(double** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(double));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu doubles): %s", n, cudaGetErrorString(e));
+    *p = nullptr;
+    return 0;
+  }
+  cudaMemset(*p, 0, n * sizeof(double));
+  return 1;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+// Vpbe_ctor2 scalars (src/generic/vpbe.c:264-411) and the ion tables of
+// Vpmg_ctor2 (src/mg/vpmg.c:340-377).
+void phys_setup(pmgb_solver* s, int natoms, const double* xyz, const double* r) {
+  const pmgb_params& p = s->p;
+  const double N_A = 6.022045000e+23, e_c = 4.803242384e-10, k_B = 1.380662000e-16;
+  const double pi = 4. * atan(1.);
+  double mn[3], mx[3], radius = 0.0;
+  for (int i = 0; i < 3; i++) mn[i] = mx[i] = xyz[i];
+  for (int a = 0; a < natoms; a++)
+    for (int i = 0; i < 3; i++) {
+      double v = xyz[3 * a + i];
+      if (v < mn[i]) mn[i] = v;
+      if (v > mx[i]) mx[i] = v;
+    }
+  for (int i = 0; i < 3; i++) s->soluteCenter[i] = 0.5 * (mx[i] + mn[i]);
+  for (int a = 0; a < natoms; a++) {
+    double d0 = xyz[3 * a] - s->soluteCenter[0];
+    double d1 = xyz[3 * a + 1] - s->soluteCenter[1];
+    double d2 = xyz[3 * a + 2] - s->soluteCenter[2];
+    double dist = (d0 * d0) + (d1 * d1) + (d2 * d2);
+    dist = sqrt(dist) + r[a];
+    if (dist > radius) radius = dist;
+  }
+  s->soluteRadius = radius;
+  s->ionstr = 0.0;
+  s->maxIonRadius = 0.0;
+  for (int i = 0; i < p.nion; i++) {
+    if (p.ion_radius[i] > s->maxIonRadius) s->maxIonRadius = p.ion_radius[i];
+    s->ionstr += (0.5 * p.ion_conc[i] * (p.ion_q[i] * p.ion_q[i]));
+  }
+  if (s->ionstr == 0.) {
+    s->xkappa = 0.;
+    s->zkappa2 = 0.;
+  } else {
+    s->xkappa = sqrt(s->ionstr * 1.0e-16 *
+                     ((8.0 * pi * N_A * e_c * e_c) / (1000.0 * p.sdie * k_B * p.temp)));
+    s->zkappa2 = p.sdie * (s->xkappa * s->xkappa);
+  }
+  s->zmagic = ((4.0 * pi * e_c * e_c) / (k_B * p.temp)) * 1.0e+8;
+  const double zks2 = (s->ionstr > 0.0) ? 0.5 / s->ionstr : 0.0;
+  s->ions.nion = p.nion;
+  s->ions_e.nion = p.nion;
+  for (int i = 0; i < p.nion && i < 8; i++) {
+    s->ions.q[i] = p.ion_q[i];
+    s->ions.sconc[i] = zks2 * p.ion_conc[i];
+    s->ions_e.q[i] = p.ion_q[i];
+    s->ions_e.sconc[i] = p.ion_conc[i];
+  }
+}
+
+// Per-axis partition weights of Vpmg_setPart (src/mg/vpmg.c:627-870) for a
+// partition equal to the mg-manual domain (no neighbouring processors).
+void part_weights(int n, double h, double cent, double lo, double hi, double* w) {
+  const double small = 1.0e-12;
+  double xmin = cent - 0.5 * h * (n - 1);
+  for (int i = 0; i < n; i++) {
+    double x = i * h + xmin, ok;
+    if ((x < (hi - h / 2)) && (x > (lo + h / 2))) ok = 1.0;
+    else if (fabs(x - lo) < small) ok = 1.0;
+    else if (fabs(x - hi) < small) ok = 1.0;
+    else if ((x > (hi + h / 2)) || (x < (lo - h / 2))) ok = 0.0;
+    else if ((x < (hi + h / 2)) || (x > (lo - h / 2))) {
+      double x0 = (x - h / 2 >= lo) ? x - h / 2 : lo;
+      double x1 = (x + h / 2 <= hi) ? x + h / 2 : hi;
+      ok = fabs(x1 - x0) / h;
+      if (ok < 0.0 && fabs(ok) < small) ok = 0.0;
+      if (ok > 1.0 && fabs(ok - 1.0) < small) ok = 1.0;
+    } else ok = 0.0;
+    w[i] = ok;
+  }
+}
+
+// Reference sphere of VaccSurf_refSphere (src/generic/vacc.c:924-978), built
+// with the host libm exactly as the reference builds it.
+int ref_sphere(int npts, std::vector<double>& pts) {
+  const double pi = 3.14159265358979323846;
+  const double frac = ((double)npts) / 4.0;
+  const int ntheta = (int)floor(sqrt(pi * frac) + 0.5);
+  const double dtheta = pi / ((double)ntheta);
+  const int nphimax = 2 * ntheta;
+  pts.clear();
+  for (int it = 0; it < ntheta; it++) {
+    const double theta = dtheta * ((double)it);
+    const double st = sin(theta), ct = cos(theta);
+    const int nphi = (int)floor(st * nphimax + 0.5);
+    if (nphi != 0) {
+      const double dphi = 2 * pi / ((double)nphi);
+      for (int ip = 0; ip < nphi; ip++) {
+        const double phi = dphi * ((double)ip);
+        pts.push_back(cos(phi) * st);
+        pts.push_back(sin(phi) * st);
+        pts.push_back(ct);
+      }
+    }
+  }
+  return (int)(pts.size() / 3);
+}
+
+float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+int read_scalar(pmgb_solver* s, int slot, double* v) {
+  CK(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 1;
+}
+
+// GS27 launch shape per level (cluster of CTAs for the wavefront).
+int g_max_cluster = 0;
+
+Gs27Plan plan_for(Grid g) {
+  const int ni = std::max(g.nx, std::max(g.ny, g.nz)) - 2;
+  Gs27Plan p;
+  if (g_max_cluster == 0) g_max_cluster = mg_init();
+  if (ni >= 60) { p.cluster = g_max_cluster; p.threads = 512; }
+  else if (ni >= 28) { p.cluster = 8; p.threads = 256; }
+  else if (ni >= 12) { p.cluster = 2; p.threads = 256; }
+  else { p.cluster = 1; p.threads = 256; }
+  return p;
+}
+
+}  // namespace
+
+// ===========================================================================
+// construction
+// ===========================================================================
+extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver** out) {
+  *out = nullptr;
+  if (!params) {
+    set_error("pmgb_create: params is NULL");
+    return 0;
+  }
+  const pmgb_params& p = *params;
+  if (p.nx < 5 || p.ny < 5 || p.nz < 5 || p.nlev < 2 || p.nlev > 11) {
+    set_error("pmgb_create: unsupported grid %dx%dx%d nlev %d", p.nx, p.ny, p.nz, p.nlev);
+    return 0;
+  }
+  if (p.chgm != PMGB_CHGM_SPL2) {
+    set_error("pmgb_create: only chgm spl2 is implemented");
+    return 0;
+  }
+  if (p.nion > 8) {
+    set_error("pmgb_create: at most 8 ion species");
+    return 0;
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    set_error("pmgb_create: no CUDA device available");
+    return 0;
+  }
+  // every level must coarsen exactly (Vcorsr, src/pmgc/mgsubd.c:426-444)
+  {
+    int nx = p.nx, ny = p.ny, nz = p.nz;
+    for (int l = 1; l < p.nlev; l++) {
+      if ((nx - 1) % 2 || (ny - 1) % 2 || (nz - 1) % 2) {
+        set_error("pmgb_create: dime %d %d %d does not coarsen %d times", p.nx, p.ny, p.nz,
+                  p.nlev - 1);
+        return 0;
+      }
+      nx = (nx - 1) / 2 + 1;
+      ny = (ny - 1) / 2 + 1;
+      nz = (nz - 1) / 2 + 1;
+      if (nx < 3 || ny < 3 || nz < 3) {
+        set_error("pmgb_create: too many levels for dime %d %d %d", p.nx, p.ny, p.nz);
+        return 0;
+      }
+    }
+  }
+  pmgb_solver* s = new pmgb_solver();
+  memset(&s->st, 0, sizeof(s->st));
+  s->p = p;
+  s->precision = precision;
+  s->device = dev;
+  s->g = Grid{p.nx, p.ny, p.nz};
+  s->n = s->g.n();
+  s->mixed = nullptr;
+  if (cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("pmgb_create: stream creation failed");
+    delete s;
+    return 0;
+  }
+  s->stream = s->own_stream;
+  for (int i = 0; i < 8; i++) cudaEventCreate(&s->ev[i]);
+  const size_t n = s->n;
+  int ok = 1;
+  ok &= dalloc(&s->charge, n) && dalloc(&s->epsx, n) && dalloc(&s->epsy, n) &&
+        dalloc(&s->epsz, n) && dalloc(&s->kappa, n) && dalloc(&s->ccf, n);
+  ok &= dalloc(&s->gx, 2 * (size_t)p.ny * p.nz) && dalloc(&s->gy, 2 * (size_t)p.nx * p.nz) &&
+        dalloc(&s->gz, 2 * (size_t)p.nx * p.ny);
+  ok &= dalloc(&s->xf, p.nx) && dalloc(&s->yf, p.ny) && dalloc(&s->zf, p.nz) &&
+        dalloc(&s->wx, p.nx) && dalloc(&s->wy, p.ny) && dalloc(&s->wz, p.nz) &&
+        dalloc(&s->mom, 16);
+  ok &= dalloc(&s->tmp3, 3 * n);
+  // hierarchy (Vbuildstr, src/pmgc/mgsubd.c:261-343)
+  s->nlev = p.nlev;
+  for (int l = 0; ok && l < s->nlev; l++) {
+    Level& L = s->lev[l];
+    if (l == 0) L.g = s->g;
+    else
+      L.g = Grid{(s->lev[l - 1].g.nx - 1) / 2 + 1, (s->lev[l - 1].g.ny - 1) / 2 + 1,
+                 (s->lev[l - 1].g.nz - 1) / 2 + 1};
+    L.nop = (l == 0) ? 4 : 14;
+    const size_t nl = L.g.n();
+    for (int c = 0; c < 14; c++) L.op[c] = nullptr;
+    for (int c = 0; c < L.nop; c++) ok &= dalloc(&L.op[c], nl);
+    ok &= dalloc(&L.cc, nl) && dalloc(&L.fc, nl) && dalloc(&L.x, nl) && dalloc(&L.w0, nl);
+    ok &= dalloc(&L.cp, nl) && dalloc(&L.rhs, nl) && dalloc(&L.xt, nl);
+    s->plan[l] = plan_for(L.g);
+  }
+  ok &= dalloc(&s->w1, n) && dalloc(&s->w2, n) && dalloc(&s->w3, n);
+  ok &= dalloc(&s->nw_r0, n) && dalloc(&s->nw_ws, n) && dalloc(&s->nw_keepx, n) &&
+        dalloc(&s->nw_keepr, n);
+  ok &= dalloc(&s->part, 4 * 1184 + 64) && dalloc(&s->scal, S_COUNT);
+  if (ok) ok &= (cudaMalloc(&s->d_iters, 16 * sizeof(int)) == cudaSuccess);
+  if (ok) ok &= (cudaMalloc(&s->d_info, 16 * sizeof(int)) == cudaSuccess);
+  if (ok) ok &= (cudaMalloc(&s->d_npts, sizeof(int)) == cudaSuccess);
+  if (!ok) {
+    pmgb_destroy(s);
+    return 0;
+  }
+  // Geometry (Vpmg_fillco, vpmg.c:5332-5366) and the coordinate arrays.
+  {
+    const double xlen = (p.nx - 1) * p.hx, ylen = (p.ny - 1) * p.hy, zlen = (p.nz - 1) * p.hz;
+    s->G.g = s->g;
+    s->G.h[0] = p.hx; s->G.h[1] = p.hy; s->G.h[2] = p.hz;
+    s->G.xmin[0] = p.center[0] - (xlen / 2.0);
+    s->G.xmin[1] = p.center[1] - (ylen / 2.0);
+    s->G.xmin[2] = p.center[2] - (zlen / 2.0);
+    s->G.xmax[0] = p.center[0] + (xlen / 2.0);
+    s->G.xmax[1] = p.center[1] + (ylen / 2.0);
+    s->G.xmax[2] = p.center[2] + (zlen / 2.0);
+    std::vector<double> xf(p.nx), yf(p.ny), zf(p.nz), wx(p.nx), wy(p.ny), wz(p.nz);
+    for (int i = 0; i < p.nx; i++) xf[i] = s->G.xmin[0] + i * p.hx;
+    for (int i = 0; i < p.ny; i++) yf[i] = s->G.xmin[1] + i * p.hy;
+    for (int i = 0; i < p.nz; i++) zf[i] = s->G.xmin[2] + i * p.hz;
+    part_weights(p.nx, p.hx, p.center[0], p.center[0] - 0.5 * ((p.nx - 1) * p.hx),
+                 p.center[0] + 0.5 * ((p.nx - 1) * p.hx), wx.data());
+    part_weights(p.ny, p.hy, p.center[1], p.center[1] - 0.5 * ((p.ny - 1) * p.hy),
+                 p.center[1] + 0.5 * ((p.ny - 1) * p.hy), wy.data());
+    part_weights(p.nz, p.hz, p.center[2], p.center[2] - 0.5 * ((p.nz - 1) * p.hz),
+                 p.center[2] + 0.5 * ((p.nz - 1) * p.hz), wz.data());
+    cudaMemcpy(s->xf, xf.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->yf, yf.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->zf, zf.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->wx, wx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->wy, wy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->wz, wz.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice);
+  }
+  s->vc_exec[0] = s->vc_exec[1] = nullptr;
+  s->vc_kernels[0] = s->vc_kernels[1] = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    set_error("pmgb_create: device error during setup");
+    pmgb_destroy(s);
+    return 0;
+  }
+  *out = s;
+  return 1;
+}
+
+extern "C" int pmgb_set_stream(pmgb_solver* s, void* stream) {
+  if (!s) return 0;
+  CK(cudaStreamSynchronize(s->stream));
+  for (int m = 0; m < 2; m++)
+    if (s->vc_exec[m]) {
+      cudaGraphExecDestroy(s->vc_exec[m]);
+      s->vc_exec[m] = nullptr;
+    }
+  s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+  return 1;
+}
+
+extern "C" void pmgb_destroy(pmgb_solver* s) {
+  if (!s) return;
+  cudaStreamSynchronize(s->stream);
+  for (int m = 0; m < 2; m++)
+    if (s->vc_exec[m]) cudaGraphExecDestroy(s->vc_exec[m]);
+  if (s->mixed) mixed_destroy(s->mixed);
+  dfree(s->charge); dfree(s->epsx); dfree(s->epsy); dfree(s->epsz); dfree(s->kappa);
+  dfree(s->ccf); dfree(s->gx); dfree(s->gy); dfree(s->gz); dfree(s->xf); dfree(s->yf);
+  dfree(s->zf); dfree(s->wx); dfree(s->wy); dfree(s->wz); dfree(s->mom); dfree(s->tmp3);
+  for (int l = 0; l < s->nlev; l++) {
+    Level& L = s->lev[l];
+    for (int c = 0; c < 14; c++) dfree(L.op[c]);
+    dfree(L.cc); dfree(L.fc); dfree(L.x); dfree(L.w0); dfree(L.cp); dfree(L.rhs); dfree(L.xt);
+  }
+  dfree(s->w1); dfree(s->w2); dfree(s->w3);
+  dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
+  dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
+  dfree(s->band);
+  dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
+  dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref);
+  if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
+  for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
+  cudaStreamDestroy(s->own_stream);
+  delete s;
+}
+
+// ===========================================================================
+// fill (Vpmg_fillco)
+// ===========================================================================
+static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
+  const pmgb_params& p = s->p;
+  cudaStream_t st = s->stream;
+  const size_t n = s->n;
+  const int natoms = s->natoms;
+  phys_setup(s, natoms, h_xyz, h_r);
+  CK(cudaEventRecord(s->ev[0], st));
+  // charge (fillcoChargeSpline2)
+  CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
+  launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+  note_launches(1);
+  const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
+  int sas_pts = 0;
+  if (!islap) {
+    // dielectric (fillcoCoefMolDielNoSmooth)
+    launch_fill_value(st, s->epsx, n, p.sdie);
+    launch_fill_value(st, s->epsy, n, p.sdie);
+    launch_fill_value(st, s->epsz, n, p.sdie);
+    launch_mark_atoms_diel(st, s->G, natoms, s->d_xyz, s->d_r, p.srad, p.pdie, s->epsx,
+                           s->epsy, s->epsz);
+    note_launches(4);
+    if (p.srad > 1.0e-9) {
+      // Vacc_storeParms sphere density with the Vclist probe radius
+      const double clist_rad =
+          ((s->maxIonRadius > p.srad) ? s->maxIonRadius : p.srad) + 0.5;
+      double maxrad = 0.0, lo[3], hi[3];
+      for (int a = 0; a < natoms; a++) maxrad = std::max(maxrad, h_r[a]);
+      const double rad_total = maxrad + clist_rad;
+      const double maxarea = 4.0 * 3.14159265358979323846 * rad_total * rad_total;
+      const int nsphere = (int)ceil(maxarea * p.sdens);
+      std::vector<double> ref;
+      const int nref = ref_sphere(nsphere, ref);
+      if (nref != s->nref) {
+        dfree(s->d_ref);
+        s->d_ref = nullptr;
+        if (!dalloc(&s->d_ref, 3 * (size_t)nref)) return 0;
+        s->nref = nref;
+      }
+      CK(cudaMemcpyAsync(s->d_ref, ref.data(), sizeof(double) * 3 * nref,
+                         cudaMemcpyHostToDevice, st));
+      // atom cell grid
+      for (int d = 0; d < 3; d++) { lo[d] = 1e300; hi[d] = -1e300; }
+      for (int a = 0; a < natoms; a++)
+        for (int d = 0; d < 3; d++) {
+          lo[d] = std::min(lo[d], h_xyz[3 * a + d]);
+          hi[d] = std::max(hi[d], h_xyz[3 * a + d]);
+        }
+      CellGrid C;
+      C.cs = maxrad + p.srad + 1.0e-6;
+      int ncell = 1;
+      for (int d = 0; d < 3; d++) {
+        C.lo[d] = lo[d] - C.cs;
+        C.n[d] = (int)ceil((hi[d] - C.lo[d]) / C.cs) + 2;
+        ncell *= C.n[d];
+      }
+      if (ncell + 1 > s->ncell_alloc) {
+        dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos);
+        CK(cudaMalloc(&s->cell_count, sizeof(int) * (ncell + 1)));
+        CK(cudaMalloc(&s->cell_start, sizeof(int) * (ncell + 1)));
+        CK(cudaMalloc(&s->cell_fillpos, sizeof(int) * (ncell + 1)));
+        s->ncell_alloc = ncell + 1;
+      }
+      if (!s->cell_of) {
+        CK(cudaMalloc(&s->cell_of, sizeof(int) * std::max(natoms, 1)));
+        CK(cudaMalloc(&s->cell_sorted, sizeof(int) * std::max(natoms, 1)));
+      }
+      launch_cell_build(st, C, natoms, s->d_xyz, s->cell_count, s->cell_start,
+                        s->cell_fillpos, s->cell_of, s->cell_sorted);
+      note_launches(3);
+      const size_t nflags = (size_t)natoms * nref;
+      if (nflags > s->sas_flags_alloc) {
+        dfree(s->sas_flags);
+        CK(cudaMalloc(&s->sas_flags, nflags));
+        s->sas_flags_alloc = nflags;
+      }
+      launch_sas(st, s->G, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
+                 s->cell_start, s->cell_sorted, s->sas_flags, s->d_npts, s->epsx, s->epsy,
+                 s->epsz);
+      note_launches(2);
+      CK(cudaMemcpyAsync(&sas_pts, s->d_npts, sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    if (p.srfm == PMGB_SRFM_SMOL) {
+      CK(cudaMemcpyAsync(s->tmp3, s->epsx, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(s->tmp3 + n, s->epsy, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                         st));
+      CK(cudaMemcpyAsync(s->tmp3 + 2 * n, s->epsz, n * sizeof(double),
+                         cudaMemcpyDeviceToDevice, st));
+      launch_smooth(st, s->g, s->tmp3, s->tmp3 + n, s->tmp3 + 2 * n, s->epsx, s->epsy,
+                    s->epsz);
+      note_launches(1);
+    }
+    // ion accessibility (fillcoCoefMolIon)
+    const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
+    launch_fill_value(st, s->kappa, n, ionmask);
+    note_launches(1);
+    if (!(s->ionstr < 1.0e-12)) {
+      launch_mark_atoms_kappa(st, s->G, natoms, s->d_xyz, s->d_r, s->maxIonRadius, s->kappa);
+      note_launches(1);
+    }
+  } else {
+    launch_fill_value(st, s->kappa, n, 0.0);
+    launch_fill_value(st, s->epsx, n, p.pdie);
+    launch_fill_value(st, s->epsy, n, p.pdie);
+    launch_fill_value(st, s->epsz, n, p.pdie);
+    note_launches(4);
+  }
+  // boundary values (bcCalc)
+  CK(cudaMemsetAsync(s->gx, 0, sizeof(double) * 2 * p.ny * p.nz, st));
+  CK(cudaMemsetAsync(s->gy, 0, sizeof(double) * 2 * p.nx * p.nz, st));
+  CK(cudaMemsetAsync(s->gz, 0, sizeof(double) * 2 * p.nx * p.ny, st));
+  if (p.bcfl == PMGB_BCFL_SDH) {
+    SdhArgs A;
+    A.g = s->g;
+    for (int d = 0; d < 3; d++) A.center[d] = s->soluteCenter[d];
+    A.size = s->soluteRadius;
+    A.xkappa = s->xkappa;
+    A.eps_p = p.pdie;
+    A.eps_w = p.sdie;
+    const double pi = 3.14159265358979323846;
+    A.pre = (1.6021773e-19 * 1.6021773e-19) /
+            (4 * pi * 8.8541878e-12 * 1.3806581e-23 * p.temp);
+    A.pre = A.pre * (1.0e10);
+    launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
+               s->gz);
+    note_launches(2);
+  } else if (p.bcfl != PMGB_BCFL_ZERO) {
+    set_error("pmgb_fillco: bcfl %d not implemented (zero and sdh are)", p.bcfl);
+    return 0;
+  }
+  CK(cudaEventRecord(s->ev[1], st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  s->st.t_fill_ms = elapsed_ms(s->ev[0], s->ev[1]);
+  s->st.sas_points = sas_pts;
+  s->filled = 1;
+  s->built = 0;
+  s->solved = 0;
+  return 1;
+}
+
+extern "C" int pmgb_fillco(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
+                           const double* radius) {
+  if (!s || natoms <= 0 || !xyz || !charge || !radius) {
+    set_error("pmgb_fillco: bad arguments");
+    return 0;
+  }
+  if (natoms > s->natoms || !s->own_atoms) {
+    if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
+    s->d_xyz = s->d_q = s->d_r = nullptr;
+    if (!dalloc(&s->d_xyz, 3 * (size_t)natoms) || !dalloc(&s->d_q, natoms) ||
+        !dalloc(&s->d_r, natoms))
+      return 0;
+    s->own_atoms = 1;
+    dfree(s->cell_of); dfree(s->cell_sorted);
+    s->cell_of = s->cell_sorted = nullptr;
+  }
+  s->natoms = natoms;
+  CK(cudaMemcpyAsync(s->d_xyz, xyz, sizeof(double) * 3 * natoms, cudaMemcpyHostToDevice,
+                     s->stream));
+  CK(cudaMemcpyAsync(s->d_q, charge, sizeof(double) * natoms, cudaMemcpyHostToDevice,
+                     s->stream));
+  CK(cudaMemcpyAsync(s->d_r, radius, sizeof(double) * natoms, cudaMemcpyHostToDevice,
+                     s->stream));
+  return do_fill(s, xyz, radius);
+}
+
+extern "C" int pmgb_fillco_device(pmgb_solver* s, int natoms, const double* d_xyz,
+                                  const double* d_charge, const double* d_radius) {
+  if (!s || natoms <= 0) {
+    set_error("pmgb_fillco_device: bad arguments");
+    return 0;
+  }
+  // host copies of positions and radii for the scalar setup (bounding box,
+  // solute radius, sphere density)
+  std::vector<double> xyz(3 * (size_t)natoms), r(natoms);
+  CK(cudaMemcpy(xyz.data(), d_xyz, sizeof(double) * 3 * natoms, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(r.data(), d_radius, sizeof(double) * natoms, cudaMemcpyDeviceToHost));
+  if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
+  s->own_atoms = 0;
+  s->d_xyz = const_cast<double*>(d_xyz);
+  s->d_q = const_cast<double*>(d_charge);
+  s->d_r = const_cast<double*>(d_radius);
+  if (natoms != s->natoms) {
+    dfree(s->cell_of); dfree(s->cell_sorted);
+    s->cell_of = s->cell_sorted = nullptr;
+  }
+  s->natoms = natoms;
+  return do_fill(s, xyz.data(), r.data());
+}
+
+extern "C" int pmgb_set_coefficients(pmgb_solver* s, const double* charge, const double* epsx,
+                                     const double* epsy, const double* epsz,
+                                     const double* kappa, const double* gxcf,
+                                     const double* gycf, const double* gzcf) {
+  if (!s) return 0;
+  const size_t n = s->n;
+  const pmgb_params& p = s->p;
+  CK(cudaMemcpy(s->charge, charge, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->epsx, epsx, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->epsy, epsy, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->epsz, epsz, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->kappa, kappa, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->gx, gxcf, 2 * (size_t)p.ny * p.nz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->gy, gycf, 2 * (size_t)p.nx * p.nz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->gz, gzcf, 2 * (size_t)p.nx * p.ny * sizeof(double), cudaMemcpyHostToDevice));
+  // scalar physics without atoms: ionic strength and Debye parameters
+  double dummy_xyz[3] = {p.center[0], p.center[1], p.center[2]}, dummy_r = 0.0;
+  phys_setup(s, 1, dummy_xyz, &dummy_r);
+  s->filled = 1;
+  s->built = 0;
+  s->solved = 0;
+  return 1;
+}
+
+// ===========================================================================
+// operator build (Vbuildops ido=0,1: src/pmgc/mgsubd.c:61-259)
+// ===========================================================================
+static int build_ops(pmgb_solver* s) {
+  cudaStream_t st = s->stream;
+  const size_t n = s->n;
+  // ccf = zkappa2 * kappa, or 0 (Vpmg_solve, vpmg.c:436-448)
+  if (s->zkappa2 > 1.0e-12) launch_ccf(st, n, s->kappa, s->zkappa2, s->ccf);
+  else CK(cudaMemsetAsync(s->ccf, 0, n * sizeof(double), st));
+  Level& F = s->lev[0];
+  launch_build_fine(st, F.g, s->xf, s->yf, s->zf, s->epsx, s->epsy, s->epsz, s->ccf,
+                    s->charge, s->gx, s->gy, s->gz, F.op[OC], F.op[OE], F.op[ON], F.op[UC],
+                    F.cc, F.fc);
+  note_launches(2);
+  double** dptrs = nullptr;
+  CK(cudaMalloc(&dptrs, sizeof(double*) * 14 * s->nlev));
+  for (int l = 1; l < s->nlev; l++) {
+    Level& C = s->lev[l];
+    Level& P = s->lev[l - 1];
+    CK(cudaMemcpyAsync(dptrs + 14 * l, C.op, sizeof(double*) * 14, cudaMemcpyHostToDevice, st));
+    launch_galerkin(st, P.g, P.ops(), C.g, dptrs + 14 * l);
+    launch_restrict(st, P.g, P.cc, C.g, C.cc);
+    launch_restrict(st, P.g, P.fc, C.g, C.fc);
+    note_launches(3);
+  }
+  CK(cudaStreamSynchronize(st));
+  cudaFree(dptrs);
+  // coarsest direct solve for the linear problem (Vbuildband, buildBd.c:57-117)
+  s->mgsolv = s->p.nonlin ? 0 : 1;
+  if (s->mgsolv == 1) {
+    Level& C = s->lev[s->nlev - 1];
+    const int ex = C.g.nx - 2, exy = (C.g.nx - 2) * (C.g.ny - 2);
+    const int nb = (C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
+    const int m = exy + ex + 1, lda = m + 1;
+    if (nb != s->bn || m != s->bm) {
+      dfree(s->band);
+      s->band = nullptr;
+      if (!dalloc(&s->band, (size_t)lda * nb + nb)) return 0;
+    }
+    s->bn = nb;
+    s->bm = m;
+    s->blda = lda;
+    launch_band_build(st, C.g, C.ops(), s->band, m, lda);
+    launch_band_factor(st, s->band, nb, m, lda, s->d_info);
+    note_launches(2);
+    int info = 0;
+    CK(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (info != 0) s->mgsolv = 0;  // "Changing your mgsolv to iterative" (mgsubd.c:248-254)
+  }
+  CK(cudaGetLastError());
+  s->built = 1;
+  return 1;
+}
+
+// ===========================================================================
+// one V-cycle (body of the do-loop of Vmvcs, src/pmgc/mgcsd.c:312-562)
+// ===========================================================================
+static int vcycle_body(pmgb_solver* s, int newton) {
+  cudaStream_t st = s->stream;
+  const int nlev = s->nlev;
+  Level& F = s->lev[0];
+  auto CC = [&](int l) -> double* { return newton ? s->lev[l].cp : s->lev[l].cc; };
+  auto X = [&](int l) -> double* { return newton ? s->lev[l].xt : s->lev[l].x; };
+  double* FC0 = newton ? F.rhs : F.fc;
+  long long k = 0;
+  // nu1 = 2 pre-smoothings on the fine level, then the residual
+  for (int sw = 0; sw < 2; sw++) {
+    launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
+    launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
+    k += 2;
+  }
+  launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
+  launch_copy_interior(st, F.g, s->w1, F.w0);
+  k += 2;
+  // down
+  for (int l = 1; l < nlev; l++) {
+    Level& C = s->lev[l];
+    Level& P = s->lev[l - 1];
+    launch_restrict(st, P.g, s->w1, C.g, C.w0);
+    k++;
+    if (l != nlev - 1) {
+      launch_zero(st, X(l), C.g.n());
+      if (!launch_gs27_wave(st, C.g, C.ops(), CC(l), C.w0, X(l), s->w1, 2, 1, s->plan[l])) {
+        set_error("gs27 launch failed at level %d", l);
+        return 0;
+      }
+      k += 2;
+    }
+  }
+  // coarsest
+  {
+    Level& C = s->lev[nlev - 1];
+    if (s->mgsolv == 1) {
+      launch_band_solve(st, C.g, s->band, s->bn, s->bm, s->blda, C.w0, X(nlev - 1));
+      k++;
+    } else {
+      launch_zero(st, X(nlev - 1), C.g.n());
+      if (!launch_cg_coarse(st, C.g, C.ops(), CC(nlev - 1), C.w0, X(nlev - 1), s->w1, s->w2,
+                            s->w3, 100, 2.220446049250313e-16, s->d_iters)) {
+        set_error("coarse CG launch failed");
+        return 0;
+      }
+      k += 2;
+    }
+  }
+  // up
+  for (int l = nlev - 2; l >= 0; l--) {
+    Level& C = s->lev[l + 1];
+    Level& P = s->lev[l];
+    launch_matvec(st, C.g, C.ops(), CC(l + 1), X(l + 1), s->w2);
+    launch_dot(st, C.g, X(l + 1), C.w0, s->part, s->scal + S_XNUM_L + l);
+    launch_dot(st, C.g, X(l + 1), s->w2, s->part + 1184 * 2, s->scal + S_XDEN_L + l);
+    launch_interp_axpy(st, C.g, X(l + 1), P.g, X(l), s->scal + S_XNUM_L + l,
+                       s->scal + S_XDEN_L + l);
+    k += 6;
+    if (l == 0) {
+      for (int sw = 0; sw < 2; sw++) {
+        launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
+        launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
+        k += 2;
+      }
+    } else {
+      if (!launch_gs27_wave(st, P.g, P.ops(), CC(l), P.w0, X(l), nullptr, 2, 0, s->plan[l])) {
+        set_error("gs27 launch failed at level %d", l);
+        return 0;
+      }
+      k++;
+    }
+  }
+  // stopping test residual
+  launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
+  launch_nrm1(st, F.g, s->w1, s->part, s->scal + S_RSNRM);
+  k += 3;
+  s->vc_kernels[newton] = k;
+  return 1;
+}
+
+static int ensure_graph(pmgb_solver* s, int newton) {
+  if (s->vc_exec[newton]) return 1;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  int ok = vcycle_body(s, newton);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+  if (!ok) return 0;
+  if (e != cudaSuccess) {
+    set_error("graph capture failed: %s", cudaGetErrorString(e));
+    return 0;
+  }
+  CK(cudaGraphInstantiate(&s->vc_exec[newton], graph, 0));
+  cudaGraphDestroy(graph);
+  return 1;
+}
+
+// V-cycles until the stopping test holds (Vmvcs).  istop0: rsden = 1
+// (istop = 0, the Newton inner solve) instead of ||f||_1.
+static int vcycles(pmgb_solver* s, int newton, double errtol, int itmax, int istop0,
+                   int* iters_out) {
+  Level& F = s->lev[0];
+  double* FC0 = newton ? F.rhs : F.fc;
+  double rsden = 1.0, rsnrm;
+  if (!istop0) {
+    launch_nrm1(s->stream, F.g, FC0, s->part, s->scal + S_RSDEN);
+    note_launches(2);
+    if (!read_scalar(s, S_RSDEN, &rsden)) return 0;
+  }
+  if (rsden == 0.0) rsden = 1.0;
+  rsnrm = rsden;
+  s->reslog.push_back(rsnrm / rsden);
+  if (!ensure_graph(s, newton)) return 0;
+  int iters = 0;
+  do {
+    CK(cudaGraphLaunch(s->vc_exec[newton], s->stream));
+    note_launches(s->vc_kernels[newton]);
+    if (!read_scalar(s, S_RSNRM, &rsnrm)) return 0;
+    iters++;
+    s->st.vcycles++;
+    s->reslog.push_back(rsnrm / rsden);
+    if (!(rsnrm == rsnrm)) {
+      set_error("non-finite residual in V-cycle %d", iters);
+      return 0;
+    }
+  } while (iters < itmax && (rsnrm / rsden) > errtol);
+  s->st.rel_residual = rsnrm / rsden;
+  *iters_out = iters;
+  return 1;
+}
+
+static int nresid_norm(pmgb_solver* s, const double* x, double* r, double* out) {
+  Level& F = s->lev[0];
+  launch_nresid(s->stream, F.g, F.ops(), F.cc, F.fc, x, r, s->ions);
+  launch_nrm1(s->stream, F.g, r, s->part, s->scal + S_NRM);
+  note_launches(3);
+  return read_scalar(s, S_NRM, out);
+}
+
+// Damped inexact Newton (Vnewton, src/pmgc/newtond.c:162-548)
+static int newton(pmgb_solver* s, double errtol, int itmax) {
+  cudaStream_t st = s->stream;
+  Level& F = s->lev[0];
+  const size_t n = s->n;
+  double rsden, rsnrm, xnorm_old, xnorm_new, xnorm_med = 0.0;
+  // rsden = ||N(0)||_1
+  CK(cudaMemsetAsync(s->nw_ws, 0, n * sizeof(double), st));
+  if (!nresid_norm(s, s->nw_ws, s->nw_keepx, &rsden)) return 0;
+  if (rsden == 0.0) rsden = 1.0;
+  rsnrm = rsden;
+  s->reslog.push_back(rsnrm / rsden);
+  if (!nresid_norm(s, F.x, s->nw_r0, &xnorm_old)) return 0;
+  int iters = 0, idamp = 1;
+  for (;;) {
+    iters++;
+    // Vgetjac (newtond.c:550-598)
+    launch_copy_interior(st, F.g, s->nw_r0, F.rhs);
+    launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
+    note_launches(2);
+    for (int l = 1; l < s->nlev; l++) {
+      launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].rhs, s->lev[l].g, s->lev[l].rhs);
+      launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].cp, s->lev[l].g, s->lev[l].cp);
+      note_launches(2);
+    }
+    const double errtol_s =
+        (0.9 * xnorm_old <= 1.0 * pow(xnorm_old, 2.0)) ? 0.9 * xnorm_old : 1.0 * pow(xnorm_old, 2.0);
+    CK(cudaMemsetAsync(F.xt, 0, n * sizeof(double), st));
+    int it_s = 0;
+    if (!vcycles(s, 1, errtol_s, 1000, 1, &it_s)) return 0;
+    if (idamp == 1) {
+      double damp = 1.0;
+      int iter_d = 0, mode = 0;
+      launch_copy_interior(st, F.g, F.x, s->nw_ws);
+      launch_axpy_interior(st, F.g, nullptr, damp, F.xt, s->nw_ws);
+      note_launches(2);
+      if (!nresid_norm(s, s->nw_ws, s->nw_r0, &xnorm_new)) return 0;
+      while (iter_d < 10) {
+        if (mode == 0) {
+          if (xnorm_new < xnorm_old) mode = 1;
+        } else if (xnorm_new > xnorm_med) {
+          break;
+        }
+        launch_copy_interior(st, F.g, s->nw_ws, s->nw_keepx);
+        launch_copy_interior(st, F.g, s->nw_r0, s->nw_keepr);
+        xnorm_med = xnorm_new;
+        launch_copy_interior(st, F.g, F.x, s->nw_ws);
+        damp = damp / 2.0;
+        launch_axpy_interior(st, F.g, nullptr, damp, F.xt, s->nw_ws);
+        note_launches(4);
+        if (!nresid_norm(s, s->nw_ws, s->nw_r0, &xnorm_new)) return 0;
+        iter_d++;
+      }
+      launch_copy_interior(st, F.g, s->nw_keepx, F.x);
+      launch_copy_interior(st, F.g, s->nw_keepr, s->nw_r0);
+      note_launches(2);
+      xnorm_new = xnorm_med;
+      xnorm_old = xnorm_new;
+      if ((iter_d - 1) == 0) idamp = 0;
+    } else {
+      launch_axpy_interior(st, F.g, nullptr, 1.0, F.xt, F.x);
+      note_launches(1);
+      if (!nresid_norm(s, F.x, s->nw_r0, &xnorm_new)) return 0;
+      xnorm_old = xnorm_new;
+    }
+    rsnrm = xnorm_new;
+    s->reslog.push_back(rsnrm / rsden);
+    if ((rsnrm / rsden) <= errtol) break;
+    if (iters >= itmax) break;
+  }
+  s->st.rel_residual = rsnrm / rsden;
+  s->st.newton_iters = iters;
+  return 1;
+}
+
+extern "C" int pmgb_solve(pmgb_solver* s) {
+  if (!s) return 0;
+  if (!s->filled) {
+    set_error("pmgb_solve: call pmgb_fillco first (Vpmg_solve requires filled maps)");
+    return 0;
+  }
+  cudaStream_t st = s->stream;
+  s->reslog.clear();
+  s->st.vcycles = 0;
+  s->st.newton_iters = 0;
+  s->st.refinements = 0;
+  CK(cudaEventRecord(s->ev[2], st));
+  if (!s->built && !build_ops(s)) return 0;
+  CK(cudaEventRecord(s->ev[3], st));
+  s->st.coarse_method = s->mgsolv;
+  const double errtol = (s->p.etol > 0.0) ? s->p.etol : 1.0e-6;
+  int ok;
+  if (s->precision == PMGB_MIXED) {
+    ok = mixed_solve(s, errtol);
+  } else {
+    // u = 0 (Vazeros + VfboundPMG00, mgdrvd.c:462-483 / newdrvd.c:300)
+    CK(cudaMemsetAsync(s->lev[0].x, 0, s->n * sizeof(double), st));
+    if (!s->p.nonlin) {
+      int iters = 0;
+      ok = vcycles(s, 0, errtol, 200, 0, &iters);
+    } else {
+      ok = newton(s, errtol, 200);
+    }
+  }
+  if (!ok) return 0;
+  // restore Dirichlet values (VfboundPMG, mgdrvd.c:557)
+  launch_fbound(st, s->g, s->lev[0].x, s->gx, s->gy, s->gz);
+  note_launches(1);
+  CK(cudaEventRecord(s->ev[4], st));
+  CK(cudaStreamSynchronize(st));
+  CK(cudaGetLastError());
+  s->st.t_setup_ms = elapsed_ms(s->ev[2], s->ev[3]);
+  s->st.t_solve_ms = elapsed_ms(s->ev[3], s->ev[4]);
+  s->solved = 1;
+  return 1;
+}
+
+// Vpmg_energy (src/mg/vpmg.c:1248-1277) with extFlag = 1 and no external
+// contributions (non-focused calculation)
+extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
+  if (!s || !s->solved) {
+    set_error("pmgb_energy: no solution");
+    return 0;
+  }
+  cudaStream_t st = s->stream;
+  EnergyArgs a;
+  a.g = s->g;
+  a.u = s->lev[0].x;
+  a.charge = s->charge;
+  a.epsx = s->epsx;
+  a.epsy = s->epsy;
+  a.epsz = s->epsz;
+  a.kappa = s->kappa;
+  a.wx = s->wx;
+  a.wy = s->wy;
+  a.wz = s->wz;
+  a.hx = s->p.hx;
+  a.hy = s->p.hy;
+  a.hz = s->p.hz;
+  a.nonlin = (s->p.nonlin && s->ionstr > 0.) ? 1 : 0;
+  a.ions = s->ions_e;
+  a.zks2 = (s->ionstr > 0.0) ? 0.5 * s->zkappa2 / s->ionstr : 0.0;
+  CK(cudaEventRecord(s->ev[5], st));
+  launch_energy_sums(st, a, s->part, s->scal + S_E0);
+  note_launches(2);
+  double sums[4];
+  CK(cudaMemcpyAsync(sums, s->scal + S_E0, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(s->ev[6], st));
+  CK(cudaStreamSynchronize(st));
+  const pmgb_params& p = s->p;
+  double qf = sums[0] * p.hx * p.hy * p.hz / s->zmagic;
+  double diel = 0.0, qm = 0.0, e;
+  if (a.nonlin) {
+    diel = 0.5 * sums[1] * p.hx * p.hy * p.hz;
+    diel = diel / s->zmagic;
+    if (!(s->zkappa2 < 1.0e-9)) {
+      if (sums[3] > 0.0) {
+        set_error("pmgb_energy: clamped exponentials in the mobile-ion energy");
+        return 0;
+      }
+      qm = sums[2] * p.hx * p.hy * p.hz;
+      qm = qm / s->zmagic;
+    }
+    e = qf - diel - qm;
+  } else {
+    e = 0.5 * qf;
+  }
+  s->st.qf = qf;
+  s->st.diel = diel;
+  s->st.qm = qm;
+  s->st.energy_kT = e;
+  s->st.t_energy_ms = elapsed_ms(s->ev[5], s->ev[6]);
+  *energy_kT = e;
+  return 1;
+}
+
+extern "C" int pmgb_get_potential(pmgb_solver* s, double* u) {
+  if (!s || !s->solved || !u) {
+    set_error("pmgb_get_potential: no solution");
+    return 0;
+  }
+  CK(cudaMemcpyAsync(u, s->lev[0].x, s->n * sizeof(double), cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return 1;
+}
+
+extern "C" int pmgb_get_maps(pmgb_solver* s, double* maps, double* faces) {
+  if (!s || !s->filled) {
+    set_error("pmgb_get_maps: not filled");
+    return 0;
+  }
+  const size_t n = s->n;
+  const pmgb_params& p = s->p;
+  CK(cudaStreamSynchronize(s->stream));
+  if (maps) {
+    CK(cudaMemcpy(maps, s->charge, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(maps + n, s->epsx, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(maps + 2 * n, s->epsy, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(maps + 3 * n, s->epsz, n * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(maps + 4 * n, s->kappa, n * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  if (faces) {
+    const size_t fx = 2 * (size_t)p.ny * p.nz, fy = 2 * (size_t)p.nx * p.nz;
+    const size_t fz = 2 * (size_t)p.nx * p.ny;
+    CK(cudaMemcpy(faces, s->gx, fx * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(faces + fx, s->gy, fy * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(faces + fx + fy, s->gz, fz * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return 1;
+}
+
+extern "C" int pmgb_get_stats(pmgb_solver* s, pmgb_stats* out) {
+  if (!s || !out) return 0;
+  *out = s->st;
+  return 1;
+}
+
+extern "C" int pmgb_get_residual_history(pmgb_solver* s, double* buf, int cap) {
+  if (!s) return 0;
+  const int n = (int)s->reslog.size();
+  for (int i = 0; i < n && i < cap; i++) buf[i] = s->reslog[i];
+  return n;
+}
+
+extern "C" int pmgb_solve_molecule(const pmgb_params* params, int precision, int natoms,
+                                   const double* xyz, const double* charge,
+                                   const double* radius, double* energy_kT, double* u,
+                                   pmgb_stats* stats) {
+  pmgb_solver* s = nullptr;
+  if (!pmgb_create(params, precision, &s)) return 0;
+  int ok = pmgb_fillco(s, natoms, xyz, charge, radius) && pmgb_solve(s) &&
+           pmgb_energy(s, energy_kT);
+  if (ok && u) ok = pmgb_get_potential(s, u);
+  if (ok && stats) pmgb_get_stats(s, stats);
+  pmgb_destroy(s);
+  return ok;
+}
+
+extern "C" const char* pmgb_last_error(void) { return g_err; }
+
+extern "C" long long pmgb_launch_count(int reset) {
+  long long v = g_launches;
+  if (reset) g_launches = 0;
+  return v;
+}

@@ -1,0 +1,98 @@
+// Internal state of one PMG calculation (shared by solver.cu and mixed.cu).
+#pragma once
+#include <vector>
+
+#include "apbs_b200.h"
+#include "fill_kernels.cuh"
+#include "mg_kernels.cuh"
+
+namespace pmgb {
+struct MixedState;
+void note_launches(long long n);
+}  // namespace pmgb
+
+namespace pmgb {
+
+struct Level {
+  Grid g;
+  int nop;
+  double* op[14];
+  double* cc;
+  double* fc;
+  double* x;
+  double* w0;
+  double* cp;   // Newton: c'(u)
+  double* rhs;  // Newton: rhs
+  double* xt;   // Newton: correction
+  Op ops() const {
+    Op o;
+    for (int c = 0; c < 14; c++) o.c[c] = (c < nop) ? op[c] : nullptr;
+    o.nop = nop;
+    return o;
+  }
+};
+
+// Scalar slots in device memory.
+enum Scal { S_RSDEN = 0, S_RSNRM, S_XNUM, S_XDEN, S_NRM, S_E0, S_E1, S_E2, S_E3, S_TMP,
+            S_XNUM_L = 16, S_XDEN_L = 32, S_COUNT = 64 };
+
+}  // namespace pmgb
+
+using namespace pmgb;
+
+struct pmgb_solver {
+  // (types from namespace pmgb)
+  pmgb_params p;
+  int precision;
+  int device;
+  cudaStream_t stream;      // stream all work is issued on
+  cudaStream_t own_stream;  // created with the solver
+  size_t n;
+  Grid g;
+  // physics scalars (Vpbe_ctor2, src/generic/vpbe.c:264-450)
+  double zmagic, xkappa, zkappa2, ionstr, maxIonRadius;
+  double soluteCenter[3], soluteRadius;
+  IonTable ions;    // scaled concentrations for c(u)
+  IonTable ions_e;  // raw concentrations for the energy
+  FillGeom G;
+  // maps
+  double *charge, *epsx, *epsy, *epsz, *kappa, *ccf;
+  double *gx, *gy, *gz, *xf, *yf, *zf, *wx, *wy, *wz, *mom;
+  double* tmp3;  // 3N scratch for smoothing
+  // atoms
+  int natoms;
+  double *d_xyz, *d_q, *d_r;
+  int own_atoms;
+  // hierarchy
+  int nlev;
+  Level lev[12];
+  double *w1, *w2, *w3;
+  double *nw_r0, *nw_ws, *nw_keepx, *nw_keepr;  // Newton work vectors
+  double* part;
+  double* scal;
+  int* d_iters;
+  int* d_info;
+  // coarsest direct solve
+  int mgsolv;
+  double* band;
+  int bn, bm, blda;
+  // fill work
+  int *cell_count, *cell_start, *cell_fillpos, *cell_of, *cell_sorted;
+  int ncell_alloc;
+  unsigned char* sas_flags;
+  size_t sas_flags_alloc;
+  double* d_ref;
+  int nref;
+  int* d_npts;
+  // state
+  int filled, solved, built;
+  std::vector<double> reslog;
+  pmgb_stats st;
+  Gs27Plan plan[12];
+  cudaEvent_t ev[8];
+  // graphs of one V-cycle (linear / Newton system)
+  cudaGraphExec_t vc_exec[2];
+  long long vc_kernels[2];
+  pmgb::MixedState* mixed;
+};
+

@@ -1,0 +1,213 @@
+"""Host-side mirror of the reference Vpmg interface over the CUDA C ABI.
+
+``Vpmg`` follows the call sequence of APBS's C API for one mg-manual
+calculation (src/mg/vpmg.h):
+
+    pmg = Vpmg(params)            # Vpmg_ctor    (vpmg.h:226)
+    pmg.fillco(molecule)          # Vpmg_fillco  (vpmg.h:281)
+    pmg.solve()                   # Vpmg_solve   (vpmg.h:306)
+    e = pmg.energy()              # Vpmg_energy  (vpmg.h:334), kT
+    u = pmg.u                     # thee->u after the solve
+
+Every call goes to ``libapbs_b200.so`` (include/apbs_b200.h).  There is no
+CPU implementation behind this module: if the library or a CUDA device is
+missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .synth import PmgbParams
+
+FP64 = 0
+MIXED = 1
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")
+_lib = None
+
+
+class PmgbStats(ctypes.Structure):
+    """Mirror of ``pmgb_stats`` in include/apbs_b200.h."""
+
+    _fields_ = [
+        ("vcycles", ctypes.c_int), ("newton_iters", ctypes.c_int),
+        ("refinements", ctypes.c_int), ("coarse_method", ctypes.c_int),
+        ("rel_residual", ctypes.c_double),
+        ("t_fill_ms", ctypes.c_double), ("t_setup_ms", ctypes.c_double),
+        ("t_solve_ms", ctypes.c_double), ("t_energy_ms", ctypes.c_double),
+        ("energy_kT", ctypes.c_double), ("qf", ctypes.c_double),
+        ("diel", ctypes.c_double), ("qm", ctypes.c_double),
+        ("sas_points", ctypes.c_int), ("status", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PmgbError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the CUDA library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PmgbError("libapbs_b200.so is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        vp = ctypes.c_void_p
+        L.pmgb_create.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.pmgb_fillco.argtypes = [vp, ctypes.c_int, dp, dp, dp]
+        L.pmgb_set_stream.argtypes = [vp, vp]
+        L.pmgb_fillco_device.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+        L.pmgb_set_coefficients.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.pmgb_solve.argtypes = [vp]
+        L.pmgb_energy.argtypes = [vp, dp]
+        L.pmgb_get_potential.argtypes = [vp, dp]
+        L.pmgb_get_maps.argtypes = [vp, dp, dp]
+        L.pmgb_get_stats.argtypes = [vp, ctypes.POINTER(PmgbStats)]
+        L.pmgb_get_residual_history.argtypes = [vp, dp, ctypes.c_int]
+        L.pmgb_destroy.argtypes = [vp]
+        L.pmgb_destroy.restype = None
+        L.pmgb_solve_molecule.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp,
+                                          ctypes.POINTER(PmgbStats)]
+        L.pmgb_last_error.restype = ctypes.c_char_p
+        L.pmgb_launch_count.argtypes = [ctypes.c_int]
+        L.pmgb_launch_count.restype = ctypes.c_longlong
+        for name in ("pmgb_create", "pmgb_fillco", "pmgb_fillco_device", "pmgb_set_coefficients",
+                     "pmgb_solve", "pmgb_energy", "pmgb_get_potential", "pmgb_get_maps",
+                     "pmgb_get_stats", "pmgb_get_residual_history", "pmgb_solve_molecule",
+                     "pmgb_set_stream"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().pmgb_last_error().decode(errors="replace")
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _check(rc, what):
+    if rc != 1:
+        raise PmgbError("%s failed: %s" % (what, last_error()))
+
+
+def _atoms(mol):
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(mol.charge, dtype=np.float64)
+    r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    return xyz, q, r
+
+
+class Vpmg:
+    """One PMG calculation held on the current CUDA device."""
+
+    def __init__(self, params: PmgbParams, precision: int = FP64):
+        self.params = params
+        self.precision = precision
+        self._h = ctypes.c_void_p()
+        _check(lib().pmgb_create(ctypes.byref(params), precision, ctypes.byref(self._h)),
+               "pmgb_create")
+
+    @property
+    def shape(self):
+        p = self.params
+        return (p.nz, p.ny, p.nx)
+
+    def set_stream(self, stream_handle: int):
+        """Issue all device work on this cudaStream_t (e.g. torch stream.cuda_stream)."""
+        _check(lib().pmgb_set_stream(self._h, ctypes.c_void_p(stream_handle)), "pmgb_set_stream")
+
+    def fillco_device(self, natoms, d_xyz, d_q, d_r):
+        """Fill from atom arrays already in device memory (raw pointers)."""
+        _check(lib().pmgb_fillco_device(self._h, natoms, ctypes.c_void_p(d_xyz),
+                                        ctypes.c_void_p(d_q), ctypes.c_void_p(d_r)),
+               "pmgb_fillco_device")
+
+    def fillco(self, mol):
+        xyz, q, r = _atoms(mol)
+        self._keep = (xyz, q, r)
+        _check(lib().pmgb_fillco(self._h, mol.natoms, _dp(xyz), _dp(q), _dp(r)), "pmgb_fillco")
+
+    def set_coefficients(self, charge, epsx, epsy, epsz, kappa, faces):
+        p = self.params
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+                for a in (charge, epsx, epsy, epsz, kappa)]
+        faces = np.ascontiguousarray(faces, dtype=np.float64)
+        fx, fy = 2 * p.ny * p.nz, 2 * p.nx * p.nz
+        gx, gy, gz = faces[:fx], faces[fx:fx + fy], faces[fx + fy:]
+        self._keep = (arrs, gx, gy, gz)
+        _check(lib().pmgb_set_coefficients(self._h, *[_dp(a) for a in arrs], _dp(gx), _dp(gy),
+                                           _dp(gz)), "pmgb_set_coefficients")
+
+    def solve(self):
+        _check(lib().pmgb_solve(self._h), "pmgb_solve")
+        return 1
+
+    def energy(self) -> float:
+        e = np.zeros(1)
+        _check(lib().pmgb_energy(self._h, _dp(e)), "pmgb_energy")
+        return float(e[0])
+
+    @property
+    def u(self) -> np.ndarray:
+        out = np.empty(self.shape)
+        _check(lib().pmgb_get_potential(self._h, _dp(out)), "pmgb_get_potential")
+        return out
+
+    def maps(self):
+        p = self.params
+        n = p.nx * p.ny * p.nz
+        m = np.empty(5 * n)
+        f = np.empty(2 * (p.ny * p.nz + p.nx * p.nz + p.nx * p.ny))
+        _check(lib().pmgb_get_maps(self._h, _dp(m), _dp(f)), "pmgb_get_maps")
+        m = m.reshape(5, *self.shape)
+        return dict(charge=m[0], epsx=m[1], epsy=m[2], epsz=m[3], kappa=m[4], faces=f)
+
+    def stats(self) -> dict:
+        st = PmgbStats()
+        lib().pmgb_get_stats(self._h, ctypes.byref(st))
+        return st.as_dict()
+
+    def residual_history(self) -> np.ndarray:
+        buf = np.zeros(8192)
+        n = lib().pmgb_get_residual_history(self._h, _dp(buf), buf.size)
+        return buf[:min(n, buf.size)].copy()
+
+    def close(self):
+        if self._h:
+            lib().pmgb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def solve_molecule(params, mol, precision=FP64, want_u=False):
+    """One host-buffer call: fill + solve + energy (pmgb_solve_molecule)."""
+    xyz, q, r = _atoms(mol)
+    e = np.zeros(1)
+    u = np.empty((params.nz, params.ny, params.nx)) if want_u else None
+    st = PmgbStats()
+    _check(lib().pmgb_solve_molecule(ctypes.byref(params), precision, mol.natoms, _dp(xyz),
+                                     _dp(q), _dp(r), _dp(e), _dp(u), ctypes.byref(st)),
+           "pmgb_solve_molecule")
+    return float(e[0]), u, st.as_dict()

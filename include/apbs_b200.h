@@ -1,0 +1,126 @@
+/*
+ * apbs_b200.h -- C ABI of the B200-native PMG Poisson-Boltzmann solver.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, no C++ or torch types.
+ * Each entry point replaces one step of the reference's Vpmg C API for an
+ * mg-manual calculation (APBS 3.4.1, src/mg/vpmg.h):
+ *
+ *   pmgb_create         <- Vpmg_ctor / Vpmg_ctor2   (vpmg.h:226, 242;
+ *                                                  vpmg.c:141-399)
+ *   pmgb_fillco         <- Vpmg_fillco             (vpmg.h:281; vpmg.c:5250)
+ *   pmgb_set_coefficients  the arrays Vpmg_fillco leaves in struct sVpmg
+ *                          (charge, epsx/y/z, kappa, gxcf/gycf/gzcf,
+ *                          vpmg.h:116-193) for callers that fill on the host
+ *   pmgb_solve          <- Vpmg_solve              (vpmg.h:306; vpmg.c:401)
+ *   pmgb_energy         <- Vpmg_energy             (vpmg.h:334; vpmg.c:1248)
+ *   pmgb_get_potential  <- reading thee->u after Vpmg_solve
+ *   pmgb_destroy        <- Vpmg_dtor               (vpmg.h:260)
+ *
+ * Return convention follows Vpmg: 1 = success, 0 = failure; on failure
+ * pmgb_last_error() describes the cause.  The library never aborts the
+ * process and never falls back to a CPU path: without a usable CUDA device
+ * every entry point fails.
+ *
+ * Grid arrays are x-fastest, index (k*ny + j)*nx + i (IJK, vpmg.h:1383).
+ * Boundary faces use the reference layout: gxcf[s][k][j], gycf[s][k][i],
+ * gzcf[s][j][i], s = 0 (low face) or 1 (high face) (IJKx/IJKy/IJKz,
+ * vpmg.h:1384-1386).
+ */
+#ifndef APBS_B200_H
+#define APBS_B200_H
+
+#include <stddef.h>
+
+#include "pmgb_params.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMGB_FP64 0   /* plain FP64 PMG, drop-in for Vpmg_solve */
+#define PMGB_MIXED 1  /* FP32 V-cycles inside FP64 iterative refinement */
+
+typedef struct pmgb_solver pmgb_solver;
+
+typedef struct pmgb_stats {
+    int vcycles;          /* V-cycles executed (all Newton steps included) */
+    int newton_iters;     /* Newton iterations (NPBE), 0 for LPBE */
+    int refinements;      /* outer refinement steps (PMGB_MIXED) */
+    int coarse_method;    /* 1 band Cholesky, 0 conjugate gradients */
+    double rel_residual;  /* final relative residual of the stopping test */
+    double t_fill_ms;     /* coefficient fill, device time */
+    double t_setup_ms;    /* operator build + Galerkin + coarse factor */
+    double t_solve_ms;    /* iterations */
+    double t_energy_ms;
+    double energy_kT;     /* last pmgb_energy result */
+    double qf, diel, qm;  /* energy components (kT) */
+    int sas_points;       /* accessible surface points used by the fill */
+    int status;           /* 0 ok, nonzero: last device-side status code */
+} pmgb_stats;
+
+/* Vpmg_ctor: allocate device state for one calculation on the current CUDA
+ * device.  precision: PMGB_FP64 or PMGB_MIXED. */
+int pmgb_create(const pmgb_params *params, int precision, pmgb_solver **out);
+
+/* Run all device work of this calculation on the given CUDA stream
+ * (a cudaStream_t passed as void*; NULL restores the solver's own stream).
+ * The caller keeps ownership of the stream. */
+int pmgb_set_stream(pmgb_solver *s, void *cuda_stream);
+
+/* Vpmg_fillco: spl2 charge, molecular (mol/smol) dielectric, ion
+ * accessibility and sdh/zero boundary values, computed on the device from
+ * host atom arrays: xyz[3*natoms] (Angstrom), charge[natoms] (e),
+ * radius[natoms] (Angstrom). */
+int pmgb_fillco(pmgb_solver *s, int natoms, const double *xyz, const double *charge,
+                const double *radius);
+
+/* Same, with the atom arrays already in device memory. */
+int pmgb_fillco_device(pmgb_solver *s, int natoms, const double *d_xyz,
+                       const double *d_charge, const double *d_radius);
+
+/* Load coefficient maps produced elsewhere (host arrays of N = nx*ny*nz
+ * doubles; faces as in the header comment).  The atom list is needed only
+ * for the sdh boundary, which is given here, so this replaces the fill. */
+int pmgb_set_coefficients(pmgb_solver *s, const double *charge, const double *epsx,
+                          const double *epsy, const double *epsz, const double *kappa,
+                          const double *gxcf, const double *gycf, const double *gzcf);
+
+/* Vpmg_solve: build the operators and solve (LPBE: linear PMG; NPBE:
+ * damped inexact Newton).  The potential stays on the device. */
+int pmgb_solve(pmgb_solver *s);
+
+/* Vpmg_energy(extFlag = 1) of a non-focused calculation, in kT. */
+int pmgb_energy(pmgb_solver *s, double *energy_kT);
+
+/* Copy the potential (thee->u, Dirichlet values restored) to host memory. */
+int pmgb_get_potential(pmgb_solver *s, double *u);
+
+/* Copy the coefficient maps and faces to host memory (any pointer may be
+ * NULL): maps = charge, epsx, epsy, epsz, kappa (5*N doubles). */
+int pmgb_get_maps(pmgb_solver *s, double *maps, double *faces);
+
+int pmgb_get_stats(pmgb_solver *s, pmgb_stats *stats);
+
+/* Relative-residual history of the last solve (one entry per stopping
+ * test, as the reference's Vprtstp reports it).  Returns the count. */
+int pmgb_get_residual_history(pmgb_solver *s, double *buf, int cap);
+
+void pmgb_destroy(pmgb_solver *s);
+
+/* One call from host buffers to energy: create + fillco + solve + energy
+ * (+ optional potential copy) + destroy. */
+int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
+                        const double *xyz, const double *charge, const double *radius,
+                        double *energy_kT, double *u_or_null, pmgb_stats *stats_or_null);
+
+const char *pmgb_last_error(void);
+
+/* Number of kernel launches issued by the calling thread since the last
+ * reset (instrumentation for the benchmark). */
+long long pmgb_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APBS_B200_H */

@@ -1,0 +1,92 @@
+"""Parity of the CUDA PMG path (through the C ABI) with the reference
+compiled from source (oracle/_ref) and with the C restatement (oracle/)."""
+import numpy as np
+import pytest
+
+from apbs_b200 import synth
+from apbs_b200.vpmg import FP64, Vpmg
+from oracle import port, ref
+
+pytestmark = pytest.mark.gpu
+
+REL_U = 1e-9       # potential, relative to max |u|  (FP64 drop-in bar)
+REL_E = 1e-9       # total energy, relative
+
+
+def _checker():
+    return ref if ref.available() else port
+
+
+def _cases():
+    m0, p0 = synth.config0()
+    m1 = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
+    p1 = synth.mg_manual(65, 0.5, m1.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    m2 = synth.cluster(400, 12.0, seed=7)
+    p2 = synth.mg_manual(97, 0.4, m2.center())
+    p3 = synth.mg_manual(49, 0.8, m2.center(), srfm=synth.SRFM_MOL)
+    m4 = synth.cluster(120, 6.0, seed=11, net_charge=-2.0)
+    p4 = synth.mg_manual(33, 0.6, m4.center(), npbe=True, ions=((2, 0.05, 2.0), (-1, 0.1, 1.8)))
+    return [("config0_lpbe65", m0, p0), ("npbe65", m1, p1), ("lpbe97_band", m2, p2),
+            ("lpbe49_mol", m2, p3), ("npbe33_2to1", m4, p4)]
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("name,mol,params", CASES, ids=[c[0] for c in CASES])
+def test_fill_maps(name, mol, params):
+    want = port.fill(params, mol)
+    with Vpmg(params, FP64) as pmg:
+        pmg.fillco(mol)
+        got = pmg.maps()
+    for k in ("epsx", "epsy", "epsz", "kappa"):
+        assert np.array_equal(got[k], want[k]), k
+    # spline charges are scattered with FP64 atomics: equal to round-off
+    scale = np.abs(want["charge"]).max()
+    assert np.abs(got["charge"] - want["charge"]).max() <= 1e-14 * scale
+    # boundary values go through exp(): CUDA libdevice vs glibc, round-off apart
+    fscale = np.abs(want["faces"]).max()
+    assert np.abs(got["faces"] - want["faces"]).max() <= 1e-13 * fscale
+
+
+@pytest.mark.parametrize("name,mol,params", CASES, ids=[c[0] for c in CASES])
+def test_solve_matches_reference(name, mol, params):
+    want = _checker().run(params, mol)
+    with Vpmg(params, FP64) as pmg:
+        pmg.fillco(mol)
+        pmg.solve()
+        e = pmg.energy()
+        u = pmg.u
+        hist = pmg.residual_history()
+    scale = np.abs(want["u"]).max()
+    assert np.abs(u - want["u"]).max() <= REL_U * scale
+    assert abs(e - want["energy_kT"]) <= REL_E * abs(want["energy_kT"])
+    # same iteration history as the reference (its log has 7 digits)
+    assert len(hist) == len(want["reslog"])
+    np.testing.assert_allclose(hist, want["reslog"], rtol=2e-6)
+
+
+def test_set_coefficients_dropin():
+    """Vpmg_solve drop-in: maps filled on the host, solve on the GPU."""
+    mol, params = synth.config0()
+    want = _checker().run(params, mol, want_maps=True, want_faces=True)
+    with Vpmg(params, FP64) as pmg:
+        pmg.set_coefficients(want["charge"], want["epsx"], want["epsy"], want["epsz"],
+                             want["kappa"], want["faces"])
+        pmg.solve()
+        u = pmg.u
+    scale = np.abs(want["u"]).max()
+    assert np.abs(u - want["u"]).max() <= REL_U * scale
+
+
+def test_repeat_solve_is_deterministic():
+    mol, params = synth.config0()
+    with Vpmg(params, FP64) as pmg:
+        pmg.fillco(mol)
+        pmg.solve()
+        e1, u1 = pmg.energy(), pmg.u
+        pmg.fillco(mol)
+        pmg.solve()
+        e2, u2 = pmg.energy(), pmg.u
+    assert abs(e1 - e2) <= 1e-13 * abs(e1)
+    assert np.abs(u1 - u2).max() <= 1e-13 * np.abs(u1).max()
