@@ -321,31 +321,37 @@ __global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __
 // sdh boundary (bcfl_sdh + multipolebc, vpmg.c:3369-3645).  The 13 moment
 // sums run one per thread in atom order, as the reference accumulates them.
 // ---------------------------------------------------------------------------
-__global__ void k_sdh_moments(int natoms, const double* __restrict__ xyz,
-                              const double* __restrict__ q, double cx, double cy, double cz,
-                              double* mom) {
-  const int m = threadIdx.x;  // 0 charge, 1-3 dipole, 4-12 quadrupole
-  if (m >= 13) return;
-  double acc = 0.0;
-  for (int a = 0; a < natoms; a++) {
-    const double xr = xyz[3 * a] - cx, yr = xyz[3 * a + 1] - cy, zr = xyz[3 * a + 2] - cz;
-    const double c = q[a];
-    if (m == 0) {
-      acc += c;
-    } else if (m <= 3) {
-      const double d = (m == 1) ? xr : (m == 2) ? yr : zr;
-      acc += d * c;
-    } else {
-      double tr[9];
-      tr[0] = xr * xr * c; tr[1] = xr * yr * c; tr[2] = xr * zr * c;
-      tr[3] = yr * xr * c; tr[4] = yr * yr * c; tr[5] = yr * zr * c;
-      tr[6] = zr * xr * c; tr[7] = zr * yr * c; tr[8] = zr * zr * c;
-      const double qave = (tr[0] + tr[4] + tr[8]) / 3.0;
-      const int e = m - 4;
-      const double v = (e == 0 || e == 4 || e == 8) ? (tr[e] - qave) : (tr[e]);
-      acc += 1.5 * v;
-    }
+// Per-atom moment terms in parallel, then one thread per moment sums them in
+// atom order (the reference's accumulation order, so the sums are bitwise
+// those of the reference).
+__global__ void k_sdh_terms(int natoms, const double* __restrict__ xyz,
+                            const double* __restrict__ q, double cx, double cy, double cz,
+                            double* terms) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const double xr = xyz[3 * a] - cx, yr = xyz[3 * a + 1] - cy, zr = xyz[3 * a + 2] - cz;
+  const double c = q[a];
+  double tr[9];
+  tr[0] = xr * xr * c; tr[1] = xr * yr * c; tr[2] = xr * zr * c;
+  tr[3] = yr * xr * c; tr[4] = yr * yr * c; tr[5] = yr * zr * c;
+  tr[6] = zr * xr * c; tr[7] = zr * yr * c; tr[8] = zr * zr * c;
+  const double qave = (tr[0] + tr[4] + tr[8]) / 3.0;
+  terms[0 * (size_t)natoms + a] = c;
+  terms[1 * (size_t)natoms + a] = xr * c;
+  terms[2 * (size_t)natoms + a] = yr * c;
+  terms[3 * (size_t)natoms + a] = zr * c;
+  for (int e = 0; e < 9; e++) {
+    const double v = (e == 0 || e == 4 || e == 8) ? (tr[e] - qave) : (tr[e]);
+    terms[(4 + e) * (size_t)natoms + a] = 1.5 * v;
   }
+}
+
+__global__ void k_sdh_moments(int natoms, const double* __restrict__ terms, double* mom) {
+  const int m = threadIdx.x;
+  if (m >= 13) return;
+  const double* t = terms + (size_t)m * natoms;
+  double acc = 0.0;
+  for (int a = 0; a < natoms; a++) acc += t[a];
   mom[m] = acc;
 }
 
@@ -478,9 +484,11 @@ void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
   k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, a1, a2, a3, epsx, epsy, epsz);
 }
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
-                const double* q, double* mom, const double* xf, const double* yf,
-                const double* zf, double* gx, double* gy, double* gz) {
-  k_sdh_moments<<<1, 32, 0, s>>>(natoms, xyz, q, A.center[0], A.center[1], A.center[2], mom);
+                const double* q, double* terms, double* mom, const double* xf,
+                const double* yf, const double* zf, double* gx, double* gy, double* gz) {
+  k_sdh_terms<<<(natoms + 127) / 128, 128, 0, s>>>(natoms, xyz, q, A.center[0], A.center[1],
+                                                   A.center[2], terms);
+  k_sdh_moments<<<1, 32, 0, s>>>(natoms, terms, mom);
   const size_t tot = 2 * ((size_t)A.g.ny * A.g.nz + (size_t)A.g.nx * A.g.nz +
                           (size_t)A.g.nx * A.g.ny);
   k_sdh_faces<<<blocks_for(tot), kThreads, 0, s>>>(A, mom, xf, yf, zf, gx, gy, gz);

@@ -44,7 +44,7 @@ void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
                    const double* a3, double* epsx, double* epsy, double* epsz);
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
-                const double* q, double* mom, const double* xf, const double* yf,
+                const double* q, double* terms, double* mom, const double* xf, const double* yf,
                 const double* zf, double* gx, double* gy, double* gz);
 void launch_ccf(cudaStream_t s, size_t n, const double* kappa, double zkappa2, double* ccf);
 

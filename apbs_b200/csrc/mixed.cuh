@@ -9,4 +9,10 @@ struct MixedState;
 // FP64 solution in s->lev[0].x (Dirichlet values not yet restored).
 int mixed_solve(pmgb_solver* s, double errtol);
 void mixed_destroy(MixedState* m);
+// Inner linear solve of one Newton step in mixed precision.
+int mixed_newton_inner(pmgb_solver* s, double errtol_s);
+// Damped inexact Newton driver (solver.cu); mixed selects the inner solver.
+int newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed);
+void set_error(const char* fmt, ...);
+int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
 }  // namespace pmgb

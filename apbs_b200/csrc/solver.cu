@@ -359,7 +359,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
   dfree(s->band);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
-  dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref);
+  dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref); dfree(s->atom_terms);
   if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
   cudaStreamDestroy(s->own_stream);
@@ -491,9 +491,15 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
     A.pre = (1.6021773e-19 * 1.6021773e-19) /
             (4 * pi * 8.8541878e-12 * 1.3806581e-23 * p.temp);
     A.pre = A.pre * (1.0e10);
-    launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
+    if (natoms > s->terms_alloc) {
+      dfree(s->atom_terms);
+      s->atom_terms = nullptr;
+      if (!dalloc(&s->atom_terms, 13 * (size_t)natoms)) return 0;
+      s->terms_alloc = natoms;
+    }
+    launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
                s->gz);
-    note_launches(2);
+    note_launches(3);
   } else if (p.bcfl != PMGB_BCFL_ZERO) {
     set_error("pmgb_fillco: bcfl %d not implemented (zero and sdh are)", p.bcfl);
     return 0;
@@ -779,8 +785,11 @@ static int nresid_norm(pmgb_solver* s, const double* x, double* r, double* out) 
   return read_scalar(s, S_NRM, out);
 }
 
-// Damped inexact Newton (Vnewton, src/pmgc/newtond.c:162-548)
-static int newton(pmgb_solver* s, double errtol, int itmax) {
+
+// Damped inexact Newton (Vnewton, src/pmgc/newtond.c:162-548).  The inner
+// linear solve of each step is the FP64 V-cycle iteration (Vmvcs with
+// istop = 0), or FP32 V-cycles with FP64 refinement when mixed != 0.
+int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
   cudaStream_t st = s->stream;
   Level& F = s->lev[0];
   const size_t n = s->n;
@@ -808,7 +817,11 @@ static int newton(pmgb_solver* s, double errtol, int itmax) {
         (0.9 * xnorm_old <= 1.0 * pow(xnorm_old, 2.0)) ? 0.9 * xnorm_old : 1.0 * pow(xnorm_old, 2.0);
     CK(cudaMemsetAsync(F.xt, 0, n * sizeof(double), st));
     int it_s = 0;
-    if (!vcycles(s, 1, errtol_s, 1000, 1, &it_s)) return 0;
+    if (mixed) {
+      if (!mixed_newton_inner(s, errtol_s)) return 0;
+    } else {
+      if (!vcycles(s, 1, errtol_s, 1000, 1, &it_s)) return 0;
+    }
     if (idamp == 1) {
       double damp = 1.0;
       int iter_d = 0, mode = 0;
@@ -880,7 +893,7 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
       int iters = 0;
       ok = vcycles(s, 0, errtol, 200, 0, &iters);
     } else {
-      ok = newton(s, errtol, 200);
+      ok = newton_driver(s, errtol, 200, 0);
     }
   }
   if (!ok) return 0;
@@ -1016,6 +1029,66 @@ extern "C" int pmgb_solve_molecule(const pmgb_params* params, int precision, int
   if (ok && stats) pmgb_get_stats(s, stats);
   pmgb_destroy(s);
   return ok;
+}
+
+extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
+                                double* bytes) {
+  if (!s || !s->built || reps < 1) {
+    set_error("pmgb_time_kernel: solve first");
+    return 0;
+  }
+  cudaStream_t st = s->stream;
+  Level& F = s->lev[0];
+  const double fint = (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+  double b = 0.0;
+  CK(cudaStreamSynchronize(st));
+  CK(cudaEventRecord(s->ev[6], st));
+  for (int r = 0; r < reps; r++) {
+    switch (which) {
+      case PMGB_K_GS7_FP64:
+        // reads oE oN uC oC cc fc and x, writes x: 56 B per point per sweep
+        launch_gs7_colour(st, F.g, F.ops(), F.cc, F.fc, F.x, r & 1);
+        b = 28.0 * fint;
+        break;
+      case PMGB_K_GS27_WAVE: {
+        if (s->nlev < 3) { set_error("pmgb_time_kernel: needs >= 3 levels"); return 0; }
+        Level& C = s->lev[1];
+        const double cint = (double)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
+        if (!launch_gs27_wave(st, C.g, C.ops(), C.cc, C.w0, C.x, s->w1, 2, 1, s->plan[1]))
+          return 0;
+        // 14 coefficients + cc + f read, x read and written: 144 B per point
+        // per sweep; the residual pass reads the same and writes r
+        b = (2.0 * 144.0 + 144.0) * cint;
+        break;
+      }
+      case PMGB_K_RESID_FP64:
+        launch_resid(st, F.g, F.ops(), F.cc, F.fc, F.x, s->w1);
+        b = 56.0 * fint;
+        break;
+      case PMGB_K_CG_COARSE: {
+        Level& C = s->lev[s->nlev - 1];
+        const double cint = (double)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
+        if (!launch_cg_coarse(st, C.g, C.ops(), C.cc, C.w0, C.x, s->w1, s->w2, s->w3, 100,
+                              2.220446049250313e-16, s->d_iters))
+          return 0;
+        b = 100.0 * (16.0 + 2.0 + 6.0) * 8.0 * cint;
+        break;
+      }
+      case PMGB_K_GS7_FP32:
+        if (!mixed_time_gs7(s, r & 1, &b)) return 0;
+        break;
+      default:
+        set_error("pmgb_time_kernel: unknown kernel %d", which);
+        return 0;
+    }
+  }
+  CK(cudaEventRecord(s->ev[7], st));
+  CK(cudaEventSynchronize(s->ev[7]));
+  CK(cudaGetLastError());
+  *ms = elapsed_ms(s->ev[6], s->ev[7]) / reps;
+  *bytes = b;
+  note_launches(reps);
+  return 1;
 }
 
 extern "C" const char* pmgb_last_error(void) { return g_err; }

@@ -84,6 +84,8 @@ struct pmgb_solver {
   double* d_ref;
   int nref;
   int* d_npts;
+  double* atom_terms;  // 13 x natoms sdh moment terms
+  int terms_alloc;
   // state
   int filled, solved, built;
   std::vector<double> reslog;

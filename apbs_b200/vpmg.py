@@ -25,6 +25,8 @@ from .synth import PmgbParams
 FP64 = 0
 MIXED = 1
 
+K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")
 _lib = None
@@ -76,6 +78,8 @@ def lib():
         L.pmgb_destroy.restype = None
         L.pmgb_solve_molecule.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp,
                                           ctypes.POINTER(PmgbStats)]
+        L.pmgb_time_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp]
+        L.pmgb_time_kernel.restype = ctypes.c_int
         L.pmgb_last_error.restype = ctypes.c_char_p
         L.pmgb_launch_count.argtypes = [ctypes.c_int]
         L.pmgb_launch_count.restype = ctypes.c_longlong
@@ -182,6 +186,12 @@ class Vpmg:
         buf = np.zeros(8192)
         n = lib().pmgb_get_residual_history(self._h, _dp(buf), buf.size)
         return buf[:min(n, buf.size)].copy()
+
+    def time_kernel(self, which: int, reps: int = 20):
+        """Mean device ms per launch and algorithmic bytes per launch."""
+        ms, b = np.zeros(1), np.zeros(1)
+        _check(lib().pmgb_time_kernel(self._h, which, reps, _dp(ms), _dp(b)), "pmgb_time_kernel")
+        return float(ms[0]), float(b[0])
 
     def close(self):
         if self._h:

@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 PMG solve path: PB solves/s and p50/p99 latency,
+mixed precision (FP32 V-cycles + FP64 refinement) against plain FP64.
+
+Workload (default): mg-manual NPBE, 161^3 grid, 0.4 A spacing, 5000-atom
+seeded globular cluster (25 A radius, net charge +12), 0.1 M 1:1 salt,
+spl2 / smol / sdh, pdie 2, sdie 78.54 -- the synthetic stand-in for the
+benchmark's config of the same shape.  One step = one full calculation:
+coefficient fill from device-resident atoms, operator build, solve, energy.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank solves independent calculations (replicas;
+the path has no data-path collective) and the job throughput is the sum.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PB solves/s & p50/p99 latency, mixed vs FP64 GPU PMG at 1e-6 rel energy"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(name: str):
+    from apbs_b200 import synth
+    if name == "c1":
+        mol, params = synth.config1()
+        desc = ("mg-manual NPBE 161^3 h=0.4A, 5000-atom cluster r=25A net +12 (seed 1), "
+                "0.1M 1:1 salt, spl2/smol/sdh, pdie 2 sdie 78.54")
+    elif name == "c0":
+        mol, params = synth.config0()
+        desc = ("mg-manual LPBE 65^3 h=0.5A, 500-atom cluster r=12A net 0 (seed 0), "
+                "0.15M 1:1 salt, spl2/smol/sdh, pdie 2 sdie 78.54")
+    else:
+        raise SystemExit("unknown workload " + name)
+    return mol, params, desc
+
+
+def peak_hbm():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return None
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for name, v in zip(names, s[3:7]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        mx = float(self.samples[0][1]) if self.samples[0][1].replace(".", "").isdigit() else None
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def run_reference(args, rank):
+    """The reference's own CPU PMG (compiled unchanged in oracle/_ref) on the
+    same workload, every host thread, one full calculation per step."""
+    if rank != 0:
+        return
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    from oracle import ref
+    mol, params, desc = workload(args.workload)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return
+    for _ in range(args.warmup):
+        ref.run(params, mol)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.run(params, mol)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = args.steps / total
+    cores = int(os.environ.get("OMP_NUM_THREADS", ncores))
+    line = {
+        "metric": METRIC, "impl": "reference", "value": v, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "implementation": "reference APBS CPU PMG, OpenMP"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "reference",
+                         "sample": "%d full calculations (ctor+fillco+solve+energy)" % args.steps},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(args):
+    """Reference CPU PMG timed on a bounded sample (one calculation)."""
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    try:
+        from oracle import ref
+        if not ref.available():
+            return None
+        mol, params, _ = workload(args.workload)
+        n = 2 if args.workload == "c1" else 10
+        t0 = time.perf_counter()
+        for _ in range(n):
+            ref.run(params, mol)
+        dt = time.perf_counter() - t0
+        return {"value": n / dt, "unit": "solves/s",
+                "cores": int(os.environ.get("OMP_NUM_THREADS", ncores)), "kind": "reference",
+                "sample": "%d full calculations of the same workload" % n}
+    except Exception as e:  # the baseline must not break the GPU line
+        return {"value": None, "unit": "solves/s", "cores": ncores, "kind": "reference",
+                "sample": "failed: %s" % e}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c1", "c0"])
+    ap.add_argument("--headline", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from apbs_b200 import vpmg
+
+    mol, params, desc = workload(args.workload)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.Stream(device=dev)
+    d_xyz = torch.tensor(mol.xyz.reshape(-1), dtype=torch.float64, device=dev)
+    d_q = torch.tensor(mol.charge, dtype=torch.float64, device=dev)
+    d_r = torch.tensor(mol.radius, dtype=torch.float64, device=dev)
+    # pinned host copies for the end-to-end leg
+    h_xyz = torch.tensor(mol.xyz.reshape(-1), dtype=torch.float64).pin_memory()
+    h_q = torch.tensor(mol.charge, dtype=torch.float64).pin_memory()
+    h_r = torch.tensor(mol.radius, dtype=torch.float64).pin_memory()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    results = {}
+    precisions = [("fp64", vpmg.FP64), ("mixed", vpmg.MIXED)]
+    solvers = {}
+    for name, prec in precisions:
+        s = vpmg.Vpmg(params, prec)
+        s.set_stream(stream.cuda_stream)
+        solvers[name] = s
+
+    def step(s):
+        s.fillco_device(mol.natoms, d_xyz.data_ptr(), d_q.data_ptr(), d_r.data_ptr())
+        s.solve()
+        return s.energy()
+
+    clocks = None
+    for name, prec in precisions:
+        s = solvers[name]
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                e = step(s)
+        barrier()
+        sampler = ClockSampler(local_rank) if name == args.headline else None
+        if sampler:
+            sampler.start()
+        vpmg.lib().pmgb_launch_count(1)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for i in range(args.steps):
+                e = step(s)
+                ev[i + 1].record(stream)
+        barrier()
+        launches = vpmg.lib().pmgb_launch_count(1)
+        if sampler:
+            clocks = sampler.stop()
+        lat = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+        total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+        st = s.stats()
+        results[name] = {
+            "solves_per_s": sum_over_ranks(args.steps) / (total_ms / 1e3),
+            "ms_per_step": total_ms / args.steps,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "energy_kT": e, "vcycles": st["vcycles"], "newton_iters": st["newton_iters"],
+            "rel_residual": st["rel_residual"], "t_fill_ms": st["t_fill_ms"],
+            "t_setup_ms": st["t_setup_ms"], "t_solve_ms": st["t_solve_ms"],
+            "gpu_launches": int(launches),
+        }
+
+    head = results[args.headline]
+    e64 = results["fp64"]["energy_kT"]
+    emix = results["mixed"]["energy_kT"]
+
+    # end to end through the C ABI from pinned host buffers (H2D of the atoms,
+    # D2H of the energy), headline precision
+    s = solvers[args.headline]
+    class _HostMol:
+        natoms = mol.natoms
+        xyz = h_xyz.numpy()      # pinned memory, shared with the torch tensors
+        charge = h_q.numpy()
+        radius = h_r.numpy()
+    hm = _HostMol()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(args.steps):
+            s.fillco(hm)
+            s.solve()
+            s.energy()
+        ev1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    e2e = {"value": sum_over_ranks(args.steps) / (e2e_ms / 1e3), "unit": "solves/s",
+           "h2d_bytes_per_step": int(8 * (h_xyz.numel() + h_q.numel() + h_r.numel())),
+           "d2h_bytes_per_step": 8}
+
+    # roofline of the dominant kernel of the headline path, timed live
+    peak, peak_kind = peak_hbm()
+    kern = vpmg.K_GS7_FP32 if args.headline == "mixed" else vpmg.K_GS27_WAVE
+    kname = {vpmg.K_GS7_FP32: "k_gs7_f32", vpmg.K_GS27_WAVE: "k_gs27_wave",
+             vpmg.K_GS7_FP64: "k_gs7_colour"}[kern]
+    ms, nbytes = s.time_kernel(kern, 20) if args.headline == "mixed" else \
+        solvers["fp64"].time_kernel(kern, 5)
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(TRAFFIC_FILE) as f:
+            traffic = json.load(f).get(kname)
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "bytes_per_launch": nbytes, "ms_per_launch": ms,
+                "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
+    # the FP64 fine smoother for reference
+    ms64, b64 = solvers["fp64"].time_kernel(vpmg.K_GS7_FP64, 20)
+    smoother64 = {"kernel": "k_gs7_colour", "achieved": b64 / (ms64 * 1e-3) / 1e9,
+                  "frac": b64 / (ms64 * 1e-3) / 1e9 / peak, "ms_per_launch": ms64}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": head["solves_per_s"], "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if args.headline == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": desc, "headline": args.headline,
+                       "step": "fillco (device atoms) + build + solve + energy",
+                       "l2": "working set ~1 GB per calculation, larger than L2",
+                       "parallelism": "replicas x%d" % world},
+            "latency_ms": head["latency_ms"],
+            "fp64": results["fp64"], "mixed": results["mixed"],
+            "mixed_vs_fp64": {"speedup": results["mixed"]["solves_per_s"] /
+                              results["fp64"]["solves_per_s"],
+                              "energy_rel_err": abs(emix - e64) / abs(e64)},
+            "e2e": e2e, "gpu_launches": head["gpu_launches"],
+            "roofline": roofline, "smoother_fp64": smoother64,
+            "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+    for s in solvers.values():
+        s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

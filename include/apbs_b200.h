@@ -113,6 +113,19 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
                         const double *xyz, const double *charge, const double *radius,
                         double *energy_kT, double *u_or_null, pmgb_stats *stats_or_null);
 
+/* Kernels that pmgb_time_kernel can time in isolation. */
+#define PMGB_K_GS7_FP64 0    /* fine-level 7-point GS, one colour (half-sweep) */
+#define PMGB_K_GS27_WAVE 1   /* level-2 ordered 27-point GS, 2 sweeps + residual */
+#define PMGB_K_RESID_FP64 2  /* fine-level 7-point residual */
+#define PMGB_K_GS7_FP32 3    /* fine-level FP32 7-point GS half-sweep (mixed) */
+#define PMGB_K_CG_COARSE 4   /* coarsest-level CG (NPBE), up to 100 iterations */
+
+/* Launch one kernel `reps` times back to back on the solver's stream (after
+ * a solve, on its state) and report the mean device time per launch (CUDA
+ * events) and the algorithmic bytes one launch must move. */
+int pmgb_time_kernel(pmgb_solver *s, int which, int reps, double *ms_per_launch,
+                     double *bytes_per_launch);
+
 const char *pmgb_last_error(void);
 
 /* Number of kernel launches issued by the calling thread since the last

@@ -1,0 +1,45 @@
+"""Mixed precision (FP32 V-cycles, FP64 refinement) against the FP64 path:
+energy within 1e-6 relative, potential within 1e-5 of max |u|, and the same
+stopping rule satisfied."""
+import numpy as np
+import pytest
+
+from apbs_b200 import synth
+from apbs_b200.vpmg import FP64, MIXED, Vpmg
+
+pytestmark = pytest.mark.gpu
+
+TOL_E = 1e-6
+TOL_U = 1e-5
+
+
+def _cases():
+    m0, p0 = synth.config0()
+    m1 = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
+    p1 = synth.mg_manual(65, 0.5, m1.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    m2 = synth.cluster(400, 12.0, seed=7)
+    p2 = synth.mg_manual(97, 0.4, m2.center())
+    m4 = synth.cluster(120, 6.0, seed=11, net_charge=-2.0)
+    p4 = synth.mg_manual(33, 0.6, m4.center(), npbe=True, ions=((2, 0.05, 2.0), (-1, 0.1, 1.8)))
+    p5 = synth.mg_manual(49, 0.8, m2.center(), npbe=True)
+    return [("lpbe65", m0, p0), ("npbe65", m1, p1), ("lpbe97", m2, p2),
+            ("npbe33_2to1", m4, p4), ("npbe49", m2, p5)]
+
+
+CASES = _cases()
+
+
+def _solve(params, mol, prec):
+    with Vpmg(params, prec) as pmg:
+        pmg.fillco(mol)
+        pmg.solve()
+        return pmg.energy(), pmg.u, pmg.stats()
+
+
+@pytest.mark.parametrize("name,mol,params", CASES, ids=[c[0] for c in CASES])
+def test_mixed_matches_fp64(name, mol, params):
+    e64, u64, _ = _solve(params, mol, FP64)
+    emx, umx, st = _solve(params, mol, MIXED)
+    assert abs(emx - e64) <= TOL_E * abs(e64)
+    assert np.abs(umx - u64).max() <= TOL_U * np.abs(u64).max()
+    assert st["rel_residual"] <= 1e-6
