@@ -76,18 +76,22 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
   const int jmax = min(g.ny - 1, (int)floor((posy + yr) / hy));
   const int kmax = min(g.nz - 1, (int)floor((posz + zr) / hz));
   if (imax < imin || jmax < jmin || kmax < kmin) return;
-  const int ni = imax - imin + 1, nj = jmax - jmin + 1, nk = kmax - kmin + 1;
-  const int tot = ni * nj * nk;
-  for (int t = lane; t < tot; t += nlanes) {
-    const int kk = kmin + t % nk;
-    const int jj = jmin + (t / nk) % nj;
-    const int ii = imin + t / (nk * nj);
-    const double fi = (double)ii, fj = (double)jj, fk = (double)kk;
+  const int ni = imax - imin + 1, nj = jmax - jmin + 1;
+  // lanes take (i, j) columns; the column test of the reference prunes
+  // whole columns before the k loop
+  for (int t = lane; t < ni * nj; t += nlanes) {
+    const int ii = imin + t / nj, jj = jmin + t % nj;
+    const double fi = (double)ii, fj = (double)jj;
     const double dx2 = (posx - hx * fi) * (posx - hx * fi);
     const double dy2 = (posy - hy * fj) * (posy - hy * fj);
     if ((dx2 + dy2) > rtot2) continue;
-    const double dz2 = (posz - hz * fk) * (posz - hz * fk);
-    if ((dz2 + dy2 + dx2) <= rtot2) array[g.idx(ii, jj, kk)] = markVal;
+    double* col = array + g.idx(ii, jj, 0);
+    const size_t sz = (size_t)g.nx * g.ny;
+    for (int kk = kmin; kk <= kmax; kk++) {
+      const double fk = (double)kk;
+      const double dz2 = (posz - hz * fk) * (posz - hz * fk);
+      if ((dz2 + dy2 + dx2) <= rtot2) col[kk * sz] = markVal;
+    }
   }
 }
 
@@ -347,12 +351,24 @@ __global__ void k_sdh_terms(int natoms, const double* __restrict__ xyz,
 }
 
 __global__ void k_sdh_moments(int natoms, const double* __restrict__ terms, double* mom) {
-  const int m = threadIdx.x;
-  if (m >= 13) return;
-  const double* t = terms + (size_t)m * natoms;
+  // chunks of the 13 term rows are staged in shared memory by the whole
+  // block; thread m then adds its row in atom order
+  constexpr int CH = 384;
+  __shared__ double buf[13][CH];
   double acc = 0.0;
-  for (int a = 0; a < natoms; a++) acc += t[a];
-  mom[m] = acc;
+  const int m = threadIdx.x;
+  for (int a0 = 0; a0 < natoms; a0 += CH) {
+    const int len = min(CH, natoms - a0);
+    for (int t = threadIdx.x; t < 13 * CH; t += blockDim.x) {
+      const int r = t / CH, c = t % CH;
+      if (c < len) buf[r][c] = terms[(size_t)r * natoms + a0 + c];
+    }
+    __syncthreads();
+    if (m < 13)
+      for (int c = 0; c < len; c++) acc += buf[m][c];
+    __syncthreads();
+  }
+  if (m < 13) mom[m] = acc;
 }
 
 __device__ void multipolebc(double r, double kappa, double eps_p, double eps_w, double rad,
@@ -488,7 +504,7 @@ void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* yf, const double* zf, double* gx, double* gy, double* gz) {
   k_sdh_terms<<<(natoms + 127) / 128, 128, 0, s>>>(natoms, xyz, q, A.center[0], A.center[1],
                                                    A.center[2], terms);
-  k_sdh_moments<<<1, 32, 0, s>>>(natoms, terms, mom);
+  k_sdh_moments<<<1, 256, 0, s>>>(natoms, terms, mom);
   const size_t tot = 2 * ((size_t)A.g.ny * A.g.nz + (size_t)A.g.nx * A.g.nz +
                           (size_t)A.g.nx * A.g.ny);
   k_sdh_faces<<<blocks_for(tot), kThreads, 0, s>>>(A, mom, xf, yf, zf, gx, gy, gz);

@@ -7,6 +7,7 @@
 // global sums (norms, dot products) are reassociated (tree reductions).
 #include <cooperative_groups.h>
 
+#include "gs7_pipe.cuh"
 #include "mg_kernels.cuh"
 
 namespace cg = cooperative_groups;
@@ -106,50 +107,93 @@ __device__ inline double op_entry(const Op& op, Grid g, int i, int j, int k, int
   return -op.c[code][g.idx(si, sj, sk)];
 }
 
-__global__ void k_galerkin(Grid gf, Op fine, Grid gc, double* const* __restrict__ coarse_ptrs) {
+// Register-only form: with alpha = a - 2I (the fine point's offset in the
+// support of coarse point I) and d the stencil offset of A, the product
+// wa(alpha) A(a, a+d) reaches coarse target I + e with the trilinear weight
+// W(v, e) = prod_axis w(v - 2e), v = alpha + d in [-2, 2]^3 (w(0) = 1,
+// w(+-1) = 1/2, else 0).  Products are first summed per v (125 bins), then
+// each bin is spread to its <= 8 targets.  Every index is a compile-time
+// constant after unrolling, so the 27 accumulators stay in registers.
+__device__ __forceinline__ double wtl(int v) { return v == 0 ? 1.0 : ((v == 1 || v == -1) ? 0.5 : 0.0); }
+
+template <int NOP>
+__device__ __forceinline__ double op_entry_static(const Op& op, Grid g, int i, int j, int k,
+                                                  int dx, int dy, int dz) {
+  // same lookup as op_entry with (dx, dy, dz) known at compile time
+  if (dx == 0 && dy == 0 && dz == 0) return op.c[OC][g.idx(i, j, k)];
+  int si = i, sj = j, sk = k;
+  if (dz < 0 || (dz == 0 && dy < 0) || (dz == 0 && dy == 0 && dx < 0)) {
+    si = i + dx; sj = j + dy; sk = k + dz;
+    dx = -dx; dy = -dy; dz = -dz;
+  }
+  int code;
+  if (dz == 0) {
+    if (dy == 0) code = OE;
+    else if (dx == 0) code = ON;
+    else code = (dx > 0) ? ONE : ONW;
+  } else {
+    if (dx == 0 && dy == 0) code = UC;
+    else if (dy == 0) code = (dx > 0) ? UE : UW;
+    else if (dx == 0) code = (dy > 0) ? UN : US;
+    else if (dy > 0) code = (dx > 0) ? UNE : UNW;
+    else code = (dx > 0) ? USE : USW;
+  }
+  if (code >= NOP) return 0.0;
+  return -op.c[code][g.idx(si, sj, sk)];
+}
+
+template <int NOP>
+__global__ void __launch_bounds__(128) k_galerkin(Grid gf, Op fine, Grid gc,
+                                                  double* const* __restrict__ coarse_ptrs) {
   const int nx = gc.nx, ny = gc.ny, nz = gc.nz;
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
-  double* coarse[14];
-  for (int c = 0; c < 14; c++) coarse[c] = coarse_ptrs[c];
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
     const int I = 1 + (int)(q % (nx - 2));
     const int J = 1 + (int)((q / (nx - 2)) % (ny - 2));
     const int K = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    // couplings to coarse boundary points are zero (P vanishes there)
+    const bool okx[3] = {I - 1 >= 1, true, I + 1 <= nx - 2};
+    const bool oky[3] = {J - 1 >= 1, true, J + 1 <= ny - 2};
+    const bool okz[3] = {K - 1 >= 1, true, K + 1 <= nz - 2};
     double acc[27];
 #pragma unroll
     for (int t = 0; t < 27; t++) acc[t] = 0.0;
-    for (int a2 = -1; a2 <= 1; a2++)
-      for (int a1 = -1; a1 <= 1; a1++)
-        for (int a0 = -1; a0 <= 1; a0++) {
-          const int fi = 2 * I + a0, fj = 2 * J + a1, fk = 2 * K + a2;
-          const double wa = 1.0 / (double)(1 << (abs(a0) + abs(a1) + abs(a2)));
-          if (fi < 1 || fj < 1 || fk < 1 || fi > gf.nx - 2 || fj > gf.ny - 2 || fk > gf.nz - 2)
-            continue;
-          for (int b2 = -1; b2 <= 1; b2++)
-            for (int b1 = -1; b1 <= 1; b1++)
-              for (int b0 = -1; b0 <= 1; b0++) {
-                const int gi = fi + b0, gj = fj + b1, gk = fk + b2;
-                if (gi < 1 || gj < 1 || gk < 1 || gi > gf.nx - 2 || gj > gf.ny - 2 ||
-                    gk > gf.nz - 2)
-                  continue;
-                const double aab = op_entry(fine, gf, fi, fj, fk, b0, b1, b2);
-                if (aab == 0.0) continue;
-                for (int c2 = (gk - 1) / 2; c2 <= (gk + 1) / 2; c2++)
-                  for (int c1 = (gj - 1) / 2; c1 <= (gj + 1) / 2; c1++)
-                    for (int c0 = (gi - 1) / 2; c0 <= (gi + 1) / 2; c0++) {
-                      const int e0 = gi - 2 * c0, e1 = gj - 2 * c1, e2 = gk - 2 * c2;
-                      if (abs(e0) > 1 || abs(e1) > 1 || abs(e2) > 1) continue;
-                      if (c0 < 1 || c1 < 1 || c2 < 1 || c0 > nx - 2 || c1 > ny - 2 ||
-                          c2 > nz - 2)
-                        continue;
-                      if (abs(c0 - I) > 1 || abs(c1 - J) > 1 || abs(c2 - K) > 1) continue;
-                      const double wb = 1.0 / (double)(1 << (abs(e0) + abs(e1) + abs(e2)));
-                      acc[((c2 - K + 1) * 3 + (c1 - J + 1)) * 3 + (c0 - I + 1)] +=
-                          wa * aab * wb;
-                    }
+#pragma unroll
+    for (int vz = -2; vz <= 2; vz++)
+#pragma unroll
+      for (int vy = -2; vy <= 2; vy++)
+#pragma unroll
+        for (int vx = -2; vx <= 2; vx++) {
+          double bin = 0.0;
+#pragma unroll
+          for (int az = -1; az <= 1; az++)
+#pragma unroll
+            for (int ay = -1; ay <= 1; ay++)
+#pragma unroll
+              for (int ax = -1; ax <= 1; ax++) {
+                const int dx = vx - ax, dy = vy - ay, dz = vz - az;
+                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                if (NOP == 4 && (abs(dx) + abs(dy) + abs(dz)) > 1) continue;
+                const int fi = 2 * I + ax, fj = 2 * J + ay, fk = 2 * K + az;
+                const double wa = wtl(ax) * wtl(ay) * wtl(az);
+                bin += wa * op_entry_static<NOP>(fine, gf, fi, fj, fk, dx, dy, dz);
+              }
+#pragma unroll
+          for (int ez = -1; ez <= 1; ez++)
+#pragma unroll
+            for (int ey = -1; ey <= 1; ey++)
+#pragma unroll
+              for (int ex = -1; ex <= 1; ex++) {
+                const double w = wtl(vx - 2 * ex) * wtl(vy - 2 * ey) * wtl(vz - 2 * ez);
+                if (w == 0.0) continue;
+                if (okx[ex + 1] && oky[ey + 1] && okz[ez + 1])
+                  acc[((ez + 1) * 3 + (ey + 1)) * 3 + (ex + 1)] += w * bin;
               }
         }
+    double* coarse[14];
+#pragma unroll
+    for (int c = 0; c < 14; c++) coarse[c] = coarse_ptrs[c];
     const size_t id = gc.idx(I, J, K);
 #define ACC(dx, dy, dz) acc[(((dz) + 1) * 3 + ((dy) + 1)) * 3 + ((dx) + 1)]
     coarse[OC][id] = ACC(0, 0, 0);
@@ -172,7 +216,10 @@ __global__ void k_galerkin(Grid gf, Op fine, Grid gc, double* const* __restrict_
 
 void launch_galerkin(cudaStream_t s, Grid gf, Op fine, Grid gc, double* const* coarse_dev) {
   size_t nint = (size_t)(gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2);
-  k_galerkin<<<blocks_for(nint, 128), 128, 0, s>>>(gf, fine, gc, coarse_dev);
+  if (fine.nop == 4)
+    k_galerkin<4><<<blocks_for(nint, 128), 128, 0, s>>>(gf, fine, gc, coarse_dev);
+  else
+    k_galerkin<14><<<blocks_for(nint, 128), 128, 0, s>>>(gf, fine, gc, coarse_dev);
 }
 
 // ===========================================================================
@@ -326,6 +373,23 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
     const size_t id = g.idx(i, j, k);
     x[id] = sum7(op, g, x, id, fc[id]) / (op.c[OC][id] + cc[id]);
   }
+}
+
+int g_tune[8] = {8, 0, 0, 0, 0, 0, 0, 0};
+
+int gs7_chunk() { return g_tune[0] > 0 ? g_tune[0] : 8; }
+int gs7_blocks_per_sm() { return g_tune[1]; }
+
+int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                      double* x, double* r, int nsweep, int first_parity) {
+  Gs7Args<double> a;
+  a.g = g;
+  a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
+  a.cc = cc; a.fc = fc; a.x = x; a.r = r;
+  a.nhalf = 2 * nsweep;
+  a.first_parity = first_parity;
+  a.chunk = gs7_chunk();
+  return launch_gs7_pipe<double>(s, a) == cudaSuccess;
 }
 
 void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
@@ -930,6 +994,8 @@ __global__ void k_cg_coarse(Grid g, Op op, const double* __restrict__ cc,
     }
   }
   if (gtid == 0 && iters_out) iters_out[0] = iters;
+  // no CTA may exit while another can still read its shared memory
+  csync();
 }
 
 int launch_cg_coarse(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,

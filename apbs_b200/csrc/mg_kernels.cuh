@@ -22,6 +22,14 @@ void launch_interp_axpy(cudaStream_t s, Grid gc, const double* xc, Grid gf, doub
 // ---- stencils ----------------------------------------------------------------
 void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, int parity);
+// nsweep red-black sweeps (+ residual into r unless r is null) as one
+// temporally blocked cooperative kernel; planes per chunk from
+// PMGB_GS7_CHUNK (default 8).
+int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                      double* x, double* r, int nsweep, int first_parity);
+int gs7_chunk();
+int gs7_blocks_per_sm();
+extern int g_tune[8];
 void launch_resid(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                   const double* x, double* r);
 void launch_matvec(cudaStream_t s, Grid g, Op op, const double* cc, const double* x, double* y);

@@ -11,8 +11,8 @@
 //     instead of the lexicographic red-black order the FP64 path reproduces;
 //   * the hierarchy is coarsened (Galerkin, trilinear P) below the
 //     reference's coarsest level until at most 512 unknowns remain, and that
-//     level is solved exactly with a dense FP64 Cholesky factorisation of
-//     (A_c + diag cc_c).
+//     level is solved exactly with the dense FP64 inverse of (A_c + diag cc_c)
+//     (Gauss-Jordan, recomputed whenever cc changes).
 // For NPBE the Newton iteration (newtond.c:162-548) is unchanged and in FP64;
 // only its inner linear solves use FP32 V-cycles.
 #include <cooperative_groups.h>
@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "gs7_pipe.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
 
@@ -55,6 +56,15 @@ struct OpF {
 
 }  // namespace
 
+// one level of the FP32 hierarchy as seen by the tail kernel
+struct TLev {
+  Grid g;
+  const float* op[14];
+  const float* cc;
+  float* w0;
+  float* x;
+};
+
 struct MixedState {
   int nlev;
   MLevel lev[16];
@@ -67,6 +77,9 @@ struct MixedState {
   cudaGraphExec_t exec[2];
   long long kernels[2];
   int cc_ready;
+  int tail_first;     // first level run by the cluster tail kernel (0: none)
+  int tail_cluster;
+  TLev* d_tlev;       // device copies of the level descriptors
 };
 
 namespace {
@@ -388,68 +401,284 @@ __global__ void k_dense_build(Grid g, Op op, const double* __restrict__ cc, doub
   }
 }
 
-// In-place Cholesky (lower) by one CTA, right-looking.
-__global__ void k_dense_chol(double* M, int n, int* info) {
-  __shared__ double piv;
+// Inverse of the SPD coarsest matrix by Gauss-Jordan elimination (no
+// pivoting needed for SPD) in one CTA; the matrix lives in shared memory
+// when it fits.  M is replaced by its inverse.
+__global__ void k_dense_inverse(double* M, int n, int use_smem, int* info) {
+  extern __shared__ double sm[];
+  double* A = use_smem ? sm : M;
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
+  if (use_smem)
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = M[t];
   __syncthreads();
-  for (int j = 0; j < n; j++) {
-    if (threadIdx.x == 0) {
-      const double d = M[j * n + j];
-      if (!(d > 0.0)) bad = j + 1;
-      else {
-        piv = sqrt(d);
-        M[j * n + j] = piv;
-      }
+  for (int p = 0; p < n; p++) {
+    const double piv = A[p * n + p];
+    if (!(piv > 0.0)) {
+      if (threadIdx.x == 0) bad = p + 1;
     }
     __syncthreads();
     if (bad) break;
-    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) M[i * n + j] /= piv;
-    __syncthreads();
-    const int w = n - j - 1;
-    for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-      const int a = t / w, b = t % w;
-      if (b > a) continue;
-      const int i = j + 1 + a, l = j + 1 + b;
-      M[i * n + l] -= M[i * n + j] * M[l * n + j];
+    const double ipiv = 1.0 / piv;
+    // rows r != p: A[r][c] -= A[r][p] * A[p][c] / piv (c != p); column p and
+    // row p finished below
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int r = t / n, c = t % n;
+      if (r == p || c == p) continue;
+      A[t] -= A[r * n + p] * A[p * n + c] * ipiv;
     }
     __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      if (t == p) continue;
+      A[t * n + p] = -A[t * n + p] * ipiv;
+      A[p * n + t] = A[p * n + t] * ipiv;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) A[p * n + p] = ipiv;
+    __syncthreads();
   }
+  if (use_smem)
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) M[t] = A[t];
   if (threadIdx.x == 0) info[0] = bad;
 }
 
-// x = M^{-1} b on the coarsest level: gather FP32 rhs, two triangular
-// solves in FP64 (one warp), scatter to FP32 x (boundary zero).
-__global__ void k_dense_solve(Grid g, const double* __restrict__ L, int n,
-                              const float* __restrict__ rhs, float* x, double* v) {
+// x = M^{-1} b on the coarsest level (FP32 in/out, FP64 product).
+__global__ void k_dense_apply(Grid g, const double* __restrict__ Minv, int n,
+                              const float* __restrict__ rhs, float* x) {
+  extern __shared__ double b[];
   const int nx = g.nx, ny = g.ny;
   const int ex = nx - 2, ey = ny - 2;
   for (int q = threadIdx.x; q < n; q += blockDim.x)
-    v[q] = (double)rhs[g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey))];
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (int i = 0; i < n; i++) {  // L y = b
-      double t = 0.0;
-      for (int c = lane; c < i; c += 32) t += L[i * n + c] * v[c];
-      t = warp_sum(t);
-      if (lane == 0) v[i] = (v[i] - t) / L[i * n + i];
-      __syncwarp();
-    }
-    for (int i = n - 1; i >= 0; i--) {  // L^T x = y
-      double t = 0.0;
-      for (int c = i + 1 + lane; c < n; c += 32) t += L[c * n + i] * v[c];
-      t = warp_sum(t);
-      if (lane == 0) v[i] = (v[i] - t) / L[i * n + i];
-      __syncwarp();
-    }
-  }
-  __syncthreads();
+    b[q] = (double)rhs[g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey))];
   for (size_t q = threadIdx.x; q < g.n(); q += blockDim.x) x[q] = 0.f;
   __syncthreads();
-  for (int q = threadIdx.x; q < n; q += blockDim.x)
-    x[g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey))] = (float)v[q];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = wid; r < n; r += nw) {
+    double t = 0.0;
+    for (int c = lane; c < n; c += 32) t += Minv[(size_t)r * n + c] * b[c];
+    t = warp_sum(t);
+    if (lane == 0) x[g.idx(1 + r % ex, 1 + (r / ex) % ey, 1 + r / (ex * ey))] = (float)t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-level tail of the FP32 V-cycle in one cluster kernel: from level
+// `first` (restricting the residual of level first-1) down to the coarsest
+// level, the dense coarsest solve, and back up to level `first` (8-colour
+// smoothing, operator-weighted interpolation with the Hackbusch-Reusken
+// damping of Vmvcs, src/pmgc/mgcsd.c:450-500).  A cluster barrier separates
+// dependent steps; sums use distributed shared memory in rank order, so all
+// CTAs agree on every damping factor.  It ends by writing the damping sums
+// of the first -> first-1 correction for the caller.
+// ---------------------------------------------------------------------------
+
+struct TailArgs {
+  const TLev* lev;      // device array indexed by level
+  int first, last;      // tail levels; last is the coarsest
+  Grid gprev;           // grid of level first-1
+  const float* rprev;   // residual of level first-1
+  float* r;             // residual scratch (>= level first size)
+  const double* minv;   // dense inverse on the coarsest level
+  int nd;
+  double* xnum;         // damping sums of the first -> first-1 correction
+  double* xden;
+};
+
+__device__ __forceinline__ float nb27t(const TLev& L, const float* x, size_t id) {
+  OpF o;
+#pragma unroll
+  for (int c = 0; c < 14; c++) o.c[c] = L.op[c];
+  o.nop = 14;
+  return nb27(o, L.g, x, id);
+}
+
+template <int CLUSTER>
+__device__ __forceinline__ void tail_sync() {
+  if (CLUSTER > 1) cg::this_cluster().sync();
+  else __syncthreads();
+}
+
+// sum of two values over the cluster, same result in every thread
+template <int CLUSTER>
+__device__ void tail_sum2(double& a, double& b, double* sh, double* slots, int& phase) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[2 * wid] = a;
+    sh[2 * wid + 1] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      sa += sh[2 * w];
+      sb += sh[2 * w + 1];
+    }
+    slots[2 * phase] = sa;
+    slots[2 * phase + 1] = sb;
+  }
+  if (CLUSTER > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    double ta = 0.0, tb = 0.0;
+    for (int rk = 0; rk < CLUSTER; rk++) {
+      double* rs = cl.map_shared_rank(slots, rk);
+      ta += rs[2 * phase];
+      tb += rs[2 * phase + 1];
+    }
+    a = ta;
+    b = tb;
+  } else {
+    __syncthreads();
+    a = slots[2 * phase];
+    b = slots[2 * phase + 1];
+  }
+  phase ^= 1;
+}
+
+template <int CLUSTER>
+__device__ void tail_smooth(const TLev& L, int reverse, int gtid, int nthr) {
+  const Grid g = L.g;
+  const int hx = (g.nx - 1) / 2, hy = (g.ny - 1) / 2, hz = (g.nz - 1) / 2;
+  const int tot = hx * hy * hz;
+  for (int sw = 0; sw < 2; sw++)
+    for (int c8 = 0; c8 < 8; c8++) {
+      const int c = reverse ? 7 - c8 : c8;
+      const int pi = c & 1, pj = (c >> 1) & 1, pk = (c >> 2) & 1;
+      for (int t = gtid; t < tot; t += nthr) {
+        const int mi = t % hx, mj = (t / hx) % hy, mk = t / (hx * hy);
+        const int i = (pi ? 1 : 2) + 2 * mi, j = (pj ? 1 : 2) + 2 * mj, k = (pk ? 1 : 2) + 2 * mk;
+        if (i > g.nx - 2 || j > g.ny - 2 || k > g.nz - 2) continue;
+        const size_t id = g.idx(i, j, k);
+        L.x[id] = (L.w0[id] + nb27t(L, L.x, id)) / (L.op[OC][id] + L.cc[id]);
+      }
+      tail_sync<CLUSTER>();
+    }
+}
+
+// restriction src (grid gs) -> level L's w0 (all points, boundary 0)
+__device__ void tail_restrict(Grid gs, const float* src, const TLev& L, bool zero_x, int gtid,
+                              int nthr) {
+  const Grid gc = L.g;
+  const int n = (int)gc.n();
+  for (int q = gtid; q < n; q += nthr) {
+    const int i = q % gc.nx, j = (q / gc.nx) % gc.ny, k = q / (gc.nx * gc.ny);
+    if (zero_x) L.x[q] = 0.f;
+    if (i == 0 || j == 0 || k == 0 || i == gc.nx - 1 || j == gc.ny - 1 || k == gc.nz - 1) {
+      L.w0[q] = 0.f;
+      continue;
+    }
+    const int ii = 2 * i, jj = 2 * j, kk = 2 * k;
+    float acc = 0.f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+      for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+          const float w = 1.f / (float)(1 << (abs(dx) + abs(dy) + abs(dz)));
+          acc += w * src[gs.idx(ii + dx, jj + dy, kk + dz)];
+        }
+    L.w0[q] = acc;
+  }
+}
+
+// damping sums <x, w0> and <x, (A + cc) x> on level L
+template <int CLUSTER>
+__device__ void tail_damp(const TLev& L, int gtid, int nthr, double* sh, double* slots,
+                          int& phase, double& num, double& den) {
+  const Grid g = L.g;
+  const int ex = g.nx - 2, ey = g.ny - 2;
+  const int nint = ex * ey * (g.nz - 2);
+  double a = 0.0, b = 0.0;
+  for (int q = gtid; q < nint; q += nthr) {
+    const size_t id = g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey));
+    const float xv = L.x[id];
+    const float ax = (L.op[OC][id] + L.cc[id]) * xv - nb27t(L, L.x, id);
+    a += (double)xv * (double)L.w0[id];
+    b += (double)xv * (double)ax;
+  }
+  tail_sum2<CLUSTER>(a, b, sh, slots, phase);
+  num = a;
+  den = b;
+}
+
+template <int CLUSTER>
+__global__ void __launch_bounds__(512) k_vcycle_tail(TailArgs A) {
+  __shared__ double sh[64];
+  __shared__ double slots[4];
+  unsigned rank = 0;
+  if (CLUSTER > 1) rank = cg::this_cluster().block_rank();
+  const int gtid = rank * blockDim.x + threadIdx.x;
+  const int nthr = CLUSTER * blockDim.x;
+  int phase = 0;
+  // down
+  for (int l = A.first; l <= A.last; l++) {
+    const TLev& L = A.lev[l];
+    if (l == A.first) tail_restrict(A.gprev, A.rprev, L, true, gtid, nthr);
+    else tail_restrict(A.lev[l - 1].g, A.r, L, true, gtid, nthr);
+    tail_sync<CLUSTER>();
+    if (l != A.last) {
+      tail_smooth<CLUSTER>(L, 0, gtid, nthr);
+      const Grid g = L.g;
+      const int ex = g.nx - 2, ey = g.ny - 2, nint = ex * ey * (g.nz - 2);
+      for (int q = gtid; q < nint; q += nthr) {
+        const size_t id = g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey));
+        A.r[id] = L.w0[id] + nb27t(L, L.x, id) - (L.op[OC][id] + L.cc[id]) * L.x[id];
+      }
+      tail_sync<CLUSTER>();
+    }
+  }
+  // coarsest: x = Minv * w0 (one warp per row)
+  {
+    const TLev& L = A.lev[A.last];
+    const Grid g = L.g;
+    const int ex = g.nx - 2, ey = g.ny - 2;
+    const int lane = threadIdx.x & 31;
+    const int gw = gtid >> 5, nw = nthr >> 5;
+    for (int row = gw; row < A.nd; row += nw) {
+      double t = 0.0;
+      for (int c = lane; c < A.nd; c += 32)
+        t += A.minv[(size_t)row * A.nd + c] *
+             (double)L.w0[g.idx(1 + c % ex, 1 + (c / ex) % ey, 1 + c / (ex * ey))];
+      t = warp_sum(t);
+      if (lane == 0) L.x[g.idx(1 + row % ex, 1 + (row / ex) % ey, 1 + row / (ex * ey))] = (float)t;
+    }
+    tail_sync<CLUSTER>();
+  }
+  // up
+  for (int l = A.last - 1; l >= A.first; l--) {
+    const TLev& C = A.lev[l + 1];
+    const TLev& P = A.lev[l];
+    double num, den;
+    tail_damp<CLUSTER>(C, gtid, nthr, sh, slots, phase, num, den);
+    const float xdamp = (float)(num / den);
+    const Grid gf = P.g;
+    const int ex = gf.nx - 2, ey = gf.ny - 2, nint = ex * ey * (gf.nz - 2);
+    for (int q = gtid; q < nint; q += nthr) {
+      const int i = 1 + q % ex, j = 1 + (q / ex) % ey, k = 1 + q / (ex * ey);
+      const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
+      const int oi = i & 1, oj = j & 1, ok = k & 1;
+      float w = 0.f;
+      for (int c = 0; c <= ok; c++)
+        for (int b = 0; b <= oj; b++)
+          for (int a = 0; a <= oi; a++) w += C.x[C.g.idx(ii + a, jj + b, kk + c)];
+      w *= 1.f / (float)(1 << (oi + oj + ok));
+      P.x[gf.idx(i, j, k)] += xdamp * w;
+    }
+    tail_sync<CLUSTER>();
+    tail_smooth<CLUSTER>(P, 1, gtid, nthr);
+  }
+  // damping sums for the first -> first-1 correction (done by the caller)
+  double num, den;
+  tail_damp<CLUSTER>(A.lev[A.first], gtid, nthr, sh, slots, phase, num, den);
+  if (gtid == 0) {
+    A.xnum[0] = num;
+    A.xden[0] = den;
+  }
+  // no CTA may exit while another can still read its shared memory
+  tail_sync<CLUSTER>();
 }
 
 // ---------------------------------------------------------------------------
@@ -506,6 +735,32 @@ int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, 
   return 1;
 }
 
+cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity) {
+  if (!g_tune[3]) {
+    // colour passes: 2 sweeps, then the residual
+    const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
+    const OpF fo = opf(F);
+    for (int sw = 0; sw < 2; sw++) {
+      k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, first_parity);
+      k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x,
+                                                         1 - first_parity);
+    }
+    if (r) {
+      const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+      k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, r);
+    }
+    return cudaGetLastError();
+  }
+  Gs7Args<float> a;
+  a.g = F.g;
+  a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
+  a.cc = F.cc; a.fc = F.w0; a.x = x; a.r = r;
+  a.nhalf = 4;
+  a.first_parity = first_parity;
+  a.chunk = gs7_chunk();
+  return launch_gs7_pipe<float>(st, a);
+}
+
 int falloc(float** p, size_t n) {
   if (n == 0) n = 1;
   if (cudaMalloc((void**)p, n * sizeof(float)) != cudaSuccess) {
@@ -550,6 +805,7 @@ void mixed_destroy(MixedState* m) {
   if (m->dense) cudaFree(m->dense);
   if (m->dvec) cudaFree(m->dvec);
   if (m->dinfo) cudaFree(m->dinfo);
+  if (m->d_tlev) cudaFree(m->d_tlev);
   delete m;
 }
 
@@ -622,6 +878,49 @@ int mixed_setup(pmgb_solver* s) {
   }
   if (!dalloc64(&m->dense, (size_t)m->nd * m->nd) || !dalloc64(&m->dvec, m->nd)) return 0;
   CKM(cudaMalloc(&m->dinfo, sizeof(int) * 4));
+  // levels small enough for one cluster run in the tail kernel
+  m->tail_first = 0;
+  for (int l = 1; l < nl; l++) {
+    const Grid g = m->lev[l].g;
+    if ((size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2) <= 70000) {
+      m->tail_first = l;
+      break;
+    }
+  }
+  if (m->tail_first > 0) {
+    std::vector<TLev> tl(nl);
+    for (int l = 0; l < nl; l++) {
+      tl[l].g = m->lev[l].g;
+      for (int c = 0; c < 14; c++) tl[l].op[c] = m->lev[l].op[c];
+      tl[l].cc = m->lev[l].cc;
+      tl[l].w0 = m->lev[l].w0;
+      tl[l].x = m->lev[l].x;
+    }
+    CKM(cudaMalloc(&m->d_tlev, sizeof(TLev) * nl));
+    CKM(cudaMemcpy(m->d_tlev, tl.data(), sizeof(TLev) * nl, cudaMemcpyHostToDevice));
+    m->tail_cluster = 16;
+    if (cudaFuncSetAttribute(k_vcycle_tail<16>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1) != cudaSuccess) {
+      cudaGetLastError();
+      m->tail_cluster = 8;
+    } else {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(16, 1, 1);
+      cfg.blockDim = dim3(512, 1, 1);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 16;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_tail<16>, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        m->tail_cluster = 8;
+      }
+    }
+  }
   CKM(cudaStreamSynchronize(st));
   return 1;
 }
@@ -650,7 +949,12 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       const int nd = m->nd;
       k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, st>>>(L.g, L.ops64(), src,
                                                                        m->dense, nd);
-      k_dense_chol<<<1, 1024, 0, st>>>(m->dense, nd, m->dinfo);
+      const size_t smem = (size_t)nd * nd * sizeof(double);
+      const int use_smem = smem <= 200 * 1024;
+      if (use_smem)
+        cudaFuncSetAttribute(k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+      k_dense_inverse<<<1, 1024, use_smem ? smem : 0, st>>>(m->dense, nd, use_smem, m->dinfo);
       note_launches(2);
     }
   }
@@ -675,17 +979,15 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const int nl = m->nlev;
   MLevel& F = m->lev[0];
   const OpF fo = opf(F);
-  const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  for (int sw = 0; sw < 2; sw++) {
-    k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, F.x, 1);
-    k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, F.x, 0);
-    k += 2;
+  if (gs7_f32(st, F, F.x, m->r, 1) != cudaSuccess) {
+    set_error("FP32 gs7 pipeline launch failed");
+    return 0;
   }
-  k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, F.x, m->r);
-  k++;
-  for (int l = 1; l < nl; l++) {
+  k += g_tune[3] ? 1 : 5;
+  const int tf = m->tail_first > 0 ? m->tail_first : nl;
+  for (int l = 1; l < tf; l++) {
     MLevel& C = m->lev[l];
     k_restrict_f32<<<blocks_for(C.g.n()), kThreads, 0, st>>>(m->lev[l - 1].g, m->r, C.g,
                                                              C.w0);
@@ -698,28 +1000,62 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
       k++;
     }
   }
-  {
+  if (m->tail_first > 0) {
+    TailArgs A;
+    A.lev = m->d_tlev;
+    A.first = tf;
+    A.last = nl - 1;
+    A.gprev = m->lev[tf - 1].g;
+    A.rprev = m->r;
+    A.r = m->w2;
+    A.minv = m->dense;
+    A.nd = m->nd;
+    A.xnum = s->scal + S_XNUM_L + ((tf - 1) & 15);
+    A.xden = s->scal + S_XDEN_L + ((tf - 1) & 15);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m->tail_cluster, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = m->tail_cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = (m->tail_cluster == 16) ? cudaLaunchKernelEx(&cfg, k_vcycle_tail<16>, A)
+                                            : cudaLaunchKernelEx(&cfg, k_vcycle_tail<8>, A);
+    if (e != cudaSuccess) {
+      set_error("tail kernel launch: %s", cudaGetErrorString(e));
+      return 0;
+    }
+    k++;
+  } else {
     MLevel& C = m->lev[nl - 1];
-    k_dense_solve<<<1, 256, 0, st>>>(C.g, m->dense, m->nd, C.w0, C.x, m->dvec);
+    k_dense_apply<<<1, 512, m->nd * sizeof(double), st>>>(C.g, m->dense, m->nd, C.w0, C.x);
     k++;
   }
-  for (int l = nl - 2; l >= 0; l--) {
+  const int upstart = (m->tail_first > 0) ? tf - 1 : nl - 2;
+  for (int l = upstart; l >= 0; l--) {
     MLevel& C = m->lev[l + 1];
     MLevel& P = m->lev[l];
-    const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
-    k_matvec_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.x, m->w2);
-    dot_f32(st, C.g, C.x, C.w0, s->part, s->scal + S_XNUM_L + (l & 15));
-    dot_f32(st, C.g, C.x, m->w2, s->part + 2368, s->scal + S_XDEN_L + (l & 15));
+    if (l + 1 != tf || m->tail_first == 0) {
+      const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
+      k_matvec_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.x, m->w2);
+      dot_f32(st, C.g, C.x, C.w0, s->part, s->scal + S_XNUM_L + (l & 15));
+      dot_f32(st, C.g, C.x, m->w2, s->part + 2368, s->scal + S_XDEN_L + (l & 15));
+      k += 5;
+    }
     const size_t pint = (size_t)(P.g.nx - 2) * (P.g.ny - 2) * (P.g.nz - 2);
     k_interp_axpy_f32<<<blocks_for(pint), kThreads, 0, st>>>(
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
-    k += 6;
+    k += 1;
     if (l == 0) {
-      for (int sw = 0; sw < 2; sw++) {
-        k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, F.x, 0);
-        k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, F.x, 1);
-        k += 2;
+      if (gs7_f32(st, F, F.x, nullptr, 0) != cudaSuccess) {
+        set_error("FP32 gs7 pipeline launch failed");
+        return 0;
       }
+      k += g_tune[3] ? 1 : 4;
     } else {
       if (!gs27_mc(st, P, P.x, 2, 1, k)) return 0;
     }
@@ -821,6 +1157,20 @@ int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
   k_gs7_f32<<<blocks_for(nslots), kThreads, 0, s->stream>>>(F.g, opf(F), F.cc, F.w0, F.x,
                                                             parity);
   *bytes = 14.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+  return 1;
+}
+
+// One FP32 fine smoothing call (2 sweeps + residual) for kernel timing:
+// (2 x 28 + 28) B per point.
+int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
+  if (!mixed_setup(s)) return 0;
+  MixedState* m = s->mixed;
+  MLevel& F = m->lev[0];
+  if (gs7_f32(s->stream, F, F.x, m->r, 1) != cudaSuccess) {
+    set_error("FP32 gs7 pipeline launch failed");
+    return 0;
+  }
+  *bytes = 3.0 * 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   return 1;
 }
 

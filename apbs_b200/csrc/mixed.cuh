@@ -15,4 +15,5 @@ int mixed_newton_inner(pmgb_solver* s, double errtol_s);
 int newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed);
 void set_error(const char* fmt, ...);
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
+int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes);
 }  // namespace pmgb

@@ -183,6 +183,11 @@ Gs27Plan plan_for(Grid g) {
   const int ni = std::max(g.nx, std::max(g.ny, g.nz)) - 2;
   Gs27Plan p;
   if (g_max_cluster == 0) g_max_cluster = mg_init();
+  if (g_tune[2] > 0) {
+    p.cluster = std::min(g_tune[2], g_max_cluster);
+    p.threads = (p.cluster >= 8) ? 512 : 256;
+    return p;
+  }
   if (ni >= 60) { p.cluster = g_max_cluster; p.threads = 512; }
   else if (ni >= 28) { p.cluster = 8; p.threads = 256; }
   else if (ni >= 12) { p.cluster = 2; p.threads = 256; }
@@ -656,14 +661,23 @@ static int vcycle_body(pmgb_solver* s, int newton) {
   double* FC0 = newton ? F.rhs : F.fc;
   long long k = 0;
   // nu1 = 2 pre-smoothings on the fine level, then the residual
-  for (int sw = 0; sw < 2; sw++) {
-    launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
-    launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
-    k += 2;
+  if (g_tune[3]) {
+    if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1, 2, 1)) {
+      set_error("gs7 pipeline launch failed");
+      return 0;
+    }
+    k += 1;
+  } else {
+    for (int sw = 0; sw < 2; sw++) {
+      launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
+      launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
+      k += 2;
+    }
+    launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
+    k += 1;
   }
-  launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
   launch_copy_interior(st, F.g, s->w1, F.w0);
-  k += 2;
+  k += 1;
   // down
   for (int l = 1; l < nlev; l++) {
     Level& C = s->lev[l];
@@ -706,10 +720,18 @@ static int vcycle_body(pmgb_solver* s, int newton) {
                        s->scal + S_XDEN_L + l);
     k += 6;
     if (l == 0) {
-      for (int sw = 0; sw < 2; sw++) {
-        launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
-        launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
-        k += 2;
+      if (g_tune[3]) {
+        if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), nullptr, 2, 0)) {
+          set_error("gs7 pipeline launch failed");
+          return 0;
+        }
+        k += 1;
+      } else {
+        for (int sw = 0; sw < 2; sw++) {
+          launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
+          launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
+          k += 2;
+        }
       }
     } else {
       if (!launch_gs27_wave(st, P.g, P.ops(), CC(l), P.w0, X(l), nullptr, 2, 0, s->plan[l])) {
@@ -1077,6 +1099,17 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_FP32:
         if (!mixed_time_gs7(s, r & 1, &b)) return 0;
         break;
+      case PMGB_K_GS7_PIPE_FP64:
+        if (!launch_gs7_smooth(st, F.g, F.ops(), F.cc, F.fc, F.x, s->w1, 2, 1)) {
+          set_error("gs7 pipeline launch failed");
+          return 0;
+        }
+        // two sweeps (56 B per point each) + residual (56 B per point)
+        b = 3.0 * 56.0 * fint;
+        break;
+      case PMGB_K_GS7_PIPE_FP32:
+        if (!mixed_time_gs7_pipe(s, &b)) return 0;
+        break;
       default:
         set_error("pmgb_time_kernel: unknown kernel %d", which);
         return 0;
@@ -1089,6 +1122,20 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
   *bytes = b;
   note_launches(reps);
   return 1;
+}
+
+extern "C" int pmgb_set_tuning(int key, int value) {
+  if (key < 0 || key >= 8) {
+    set_error("pmgb_set_tuning: bad key %d", key);
+    return 0;
+  }
+  g_tune[key] = value;
+  return 1;
+}
+
+extern "C" int pmgb_get_tuning(int key) {
+  if (key < 0 || key >= 8) return -1;
+  return g_tune[key];
 }
 
 extern "C" const char* pmgb_last_error(void) { return g_err; }

@@ -26,6 +26,8 @@ FP64 = 0
 MIXED = 1
 
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
+K_GS7_PIPE_FP64, K_GS7_PIPE_FP32 = 5, 6
+TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")
@@ -80,6 +82,10 @@ def lib():
                                           ctypes.POINTER(PmgbStats)]
         L.pmgb_time_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.pmgb_time_kernel.restype = ctypes.c_int
+        L.pmgb_set_tuning.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.pmgb_set_tuning.restype = ctypes.c_int
+        L.pmgb_get_tuning.argtypes = [ctypes.c_int]
+        L.pmgb_get_tuning.restype = ctypes.c_int
         L.pmgb_last_error.restype = ctypes.c_char_p
         L.pmgb_launch_count.argtypes = [ctypes.c_int]
         L.pmgb_launch_count.restype = ctypes.c_longlong
@@ -90,6 +96,14 @@ def lib():
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
+
+
+def set_tuning(key: int, value: int) -> None:
+    _check(lib().pmgb_set_tuning(key, value), "pmgb_set_tuning")
+
+
+def get_tuning(key: int) -> int:
+    return int(lib().pmgb_get_tuning(key))
 
 
 def last_error() -> str:

@@ -119,6 +119,18 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_RESID_FP64 2  /* fine-level 7-point residual */
 #define PMGB_K_GS7_FP32 3    /* fine-level FP32 7-point GS half-sweep (mixed) */
 #define PMGB_K_CG_COARSE 4   /* coarsest-level CG (NPBE), up to 100 iterations */
+#define PMGB_K_GS7_PIPE_FP64 5  /* fine smoothing call: 2 sweeps + residual, FP64 */
+#define PMGB_K_GS7_PIPE_FP32 6  /* fine smoothing call: 2 sweeps + residual, FP32 */
+
+/* Launch-shape tunables (process-wide; read when a solver captures its
+ * V-cycle graph, so set them before the first solve).  The autotuner in
+ * apbs_b200/autotune.py picks them per grid size. */
+#define PMGB_TUNE_GS7_CHUNK 0          /* planes per pipeline chunk (default 8) */
+#define PMGB_TUNE_GS7_BLOCKS_PER_SM 1  /* CTAs per SM of the pipelined smoother (0 = max) */
+#define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 (0 = auto) */
+#define PMGB_TUNE_GS7_PIPELINED 3      /* 1: temporally blocked fine smoother, 0: colour passes */
+int pmgb_set_tuning(int key, int value);
+int pmgb_get_tuning(int key);
 
 /* Launch one kernel `reps` times back to back on the solver's stream (after
  * a solve, on its state) and report the mean device time per launch (CUDA
