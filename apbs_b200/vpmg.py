@@ -86,6 +86,8 @@ def lib():
         L.pmgb_set_tuning.restype = ctypes.c_int
         L.pmgb_get_tuning.argtypes = [ctypes.c_int]
         L.pmgb_get_tuning.restype = ctypes.c_int
+        L.pmgb_energy_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, dp]
+        L.pmgb_energy_noalloc.restype = ctypes.c_int
         L.pmgb_last_error.restype = ctypes.c_char_p
         L.pmgb_launch_count.argtypes = [ctypes.c_int]
         L.pmgb_launch_count.restype = ctypes.c_longlong
@@ -223,6 +225,20 @@ class Vpmg:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def energy_noalloc(params, d_u, d_charge, d_epsx=0, d_epsy=0, d_epsz=0, d_kappa=0,
+                   stream=0) -> float:
+    """Energy (kT) from device arrays the caller owns, with no device
+    allocation (pmgb_energy_noalloc).  Pointers are raw device addresses
+    (e.g. torch tensor.data_ptr()); stream is a cudaStream_t handle or 0."""
+    e = np.zeros(1)
+    _check(lib().pmgb_energy_noalloc(ctypes.byref(params), ctypes.c_void_p(d_u),
+                                     ctypes.c_void_p(d_charge), ctypes.c_void_p(d_epsx or None),
+                                     ctypes.c_void_p(d_epsy or None), ctypes.c_void_p(d_epsz or None),
+                                     ctypes.c_void_p(d_kappa or None), ctypes.c_void_p(stream or None),
+                                     _dp(e)), "pmgb_energy_noalloc")
+    return float(e[0])
 
 
 def solve_molecule(params, mol, precision=FP64, want_u=False):

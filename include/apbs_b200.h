@@ -138,6 +138,26 @@ int pmgb_get_tuning(int key);
 int pmgb_time_kernel(pmgb_solver *s, int which, int reps, double *ms_per_launch,
                      double *bytes_per_launch);
 
+/* Largest grid dimension pmgb_energy_noalloc accepts (points per axis). */
+#define PMGB_NOALLOC_MAX_DIM 1025
+
+/* Energy of a solved potential (as pmgb_energy) computed from device arrays
+ * the caller already holds, without allocating any device memory.  It has
+ * no counterpart in the reference; it serves callers that cannot allocate
+ * at this point -- code inside another framework's memory pool or a
+ * captured stream, where cudaMalloc would synchronise or is not allowed,
+ * and fixed-footprint embedded callers.  d_u is the potential with its
+ * boundary values, the maps are those of the fill (N = nx*ny*nz doubles;
+ * the dielectric and kappa maps may be NULL for LPBE).  Grids up to
+ * PMGB_NOALLOC_MAX_DIM points per axis; larger grids are rejected.  The
+ * scratch is one fixed 64 KiB device array per device, shared by every
+ * call: the first call on a device looks its address up (make that call
+ * before any stream capture), and calls that overlap on the GPU race on it.
+ * cuda_stream may be NULL (default stream); the call waits for its result. */
+int pmgb_energy_noalloc(const pmgb_params *params, const double *d_u, const double *d_charge,
+                        const double *d_epsx, const double *d_epsy, const double *d_epsz,
+                        const double *d_kappa, void *cuda_stream, double *energy_kT);
+
 const char *pmgb_last_error(void);
 
 /* Number of kernel launches issued by the calling thread since the last
