@@ -969,6 +969,40 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
   return 1;
 }
 
+int launch_tail(pmgb_solver* s, cudaStream_t st) {
+  MixedState* m = s->mixed;
+  const int nl = m->nlev, tf = m->tail_first;
+  TailArgs A;
+  A.lev = m->d_tlev;
+  A.first = tf;
+  A.last = nl - 1;
+  A.gprev = m->lev[tf - 1].g;
+  A.rprev = m->r;
+  A.r = m->w2;
+  A.minv = m->dense;
+  A.nd = m->nd;
+  A.xnum = s->scal + S_XNUM_L + ((tf - 1) & 15);
+  A.xden = s->scal + S_XDEN_L + ((tf - 1) & 15);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(m->tail_cluster, 1, 1);
+  cfg.blockDim = dim3(512, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = m->tail_cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = (m->tail_cluster == 16) ? cudaLaunchKernelEx(&cfg, k_vcycle_tail<16>, A)
+                                          : cudaLaunchKernelEx(&cfg, k_vcycle_tail<8>, A);
+  if (e != cudaSuccess) {
+    set_error("tail kernel launch: %s", cudaGetErrorString(e));
+    return 0;
+  }
+  return 1;
+}
+
 // One FP32 V-cycle on A e = w0 (fine rhs already in lev[0].w0), e -> lev[0].x,
 // then x64 += e, the FP64 residual of (fc64, cc64, x64) into lev[0].w0 and its
 // 1-norm into scal[S_RSNRM].
@@ -1001,34 +1035,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     }
   }
   if (m->tail_first > 0) {
-    TailArgs A;
-    A.lev = m->d_tlev;
-    A.first = tf;
-    A.last = nl - 1;
-    A.gprev = m->lev[tf - 1].g;
-    A.rprev = m->r;
-    A.r = m->w2;
-    A.minv = m->dense;
-    A.nd = m->nd;
-    A.xnum = s->scal + S_XNUM_L + ((tf - 1) & 15);
-    A.xden = s->scal + S_XDEN_L + ((tf - 1) & 15);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(m->tail_cluster, 1, 1);
-    cfg.blockDim = dim3(512, 1, 1);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = m->tail_cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaError_t e = (m->tail_cluster == 16) ? cudaLaunchKernelEx(&cfg, k_vcycle_tail<16>, A)
-                                            : cudaLaunchKernelEx(&cfg, k_vcycle_tail<8>, A);
-    if (e != cudaSuccess) {
-      set_error("tail kernel launch: %s", cudaGetErrorString(e));
-      return 0;
-    }
+    if (!launch_tail(s, st)) return 0;
     k++;
   } else {
     MLevel& C = m->lev[nl - 1];
@@ -1171,6 +1178,28 @@ int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
     return 0;
   }
   *bytes = 3.0 * 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+  return 1;
+}
+
+// The coarse tail alone, for kernel timing.  Algorithmic bytes per tail
+// level above the coarsest: 2+2 FP32 27-point sweeps, the residual and the
+// damping pass read 14 coefficients + cc + f + x (72 B per point each) and
+// the interpolation writes x: 6 x 72 + 8 = 440 B per interior point.
+int mixed_time_tail(pmgb_solver* s, double* bytes) {
+  if (!mixed_setup(s)) return 0;
+  MixedState* m = s->mixed;
+  if (m->tail_first <= 0) {
+    set_error("pmgb_time_kernel: this grid has no tail levels");
+    return 0;
+  }
+  if (!launch_tail(s, s->stream)) return 0;
+  double b = 0.0;
+  for (int l = m->tail_first; l < m->nlev - 1; l++) {
+    const Grid g = m->lev[l].g;
+    b += 440.0 * (double)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  }
+  b += 8.0 * (double)m->nd * m->nd;
+  *bytes = b;
   return 1;
 }
 

@@ -16,4 +16,5 @@ int newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed);
 void set_error(const char* fmt, ...);
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
 int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes);
+int mixed_time_tail(pmgb_solver* s, double* bytes);
 }  // namespace pmgb

@@ -1110,6 +1110,9 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_PIPE_FP32:
         if (!mixed_time_gs7_pipe(s, &b)) return 0;
         break;
+      case PMGB_K_VCYCLE_TAIL:
+        if (!mixed_time_tail(s, &b)) return 0;
+        break;
       default:
         set_error("pmgb_time_kernel: unknown kernel %d", which);
         return 0;

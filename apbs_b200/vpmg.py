@@ -26,7 +26,7 @@ FP64 = 0
 MIXED = 1
 
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
-K_GS7_PIPE_FP64, K_GS7_PIPE_FP32 = 5, 6
+K_GS7_PIPE_FP64, K_GS7_PIPE_FP32, K_VCYCLE_TAIL = 5, 6, 7
 TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

@@ -121,6 +121,7 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_CG_COARSE 4   /* coarsest-level CG (NPBE), up to 100 iterations */
 #define PMGB_K_GS7_PIPE_FP64 5  /* fine smoothing call: 2 sweeps + residual, FP64 */
 #define PMGB_K_GS7_PIPE_FP32 6  /* fine smoothing call: 2 sweeps + residual, FP32 */
+#define PMGB_K_VCYCLE_TAIL 7    /* mixed: coarse-level V-cycle tail (one cluster kernel) */
 
 /* Launch-shape tunables (process-wide; read when a solver captures its
  * V-cycle graph, so set them before the first solve).  The autotuner in
