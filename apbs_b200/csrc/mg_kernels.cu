@@ -1117,9 +1117,16 @@ void launch_fbound(cudaStream_t s, Grid g, double* x, const double* gx, const do
 // clamped exponential of Vcap_exp (src/generic/vcap.c:59-73).
 // pvec(i,j,k) = wx[i] wy[j] wz[k] (Vpmg_setPart, vpmg.c:627-870).
 // ===========================================================================
+// With complement, the weight extEnergy gives the coarse grid of a focusing
+// chain (vpmg.c:2508-2509): 1 - pvec where pvec <= VSMALL, else 0.
 __device__ __forceinline__ double pvec_at(const EnergyArgs& a, int i, int j, int k) {
-  const double v = a.wx[i] * a.wy[j] * a.wz[k];
-  return (fabs(v) < 1.0e-12) ? 0.0 : v;
+  double v = a.wx[i] * a.wy[j] * a.wz[k];
+  v = (fabs(v) < 1.0e-12) ? 0.0 : v;
+  if (a.complement) {
+    if (v > 1.0e-9) v = 1.0;
+    v = (1 - v) * 1.0;
+  }
+  return v;
 }
 
 __global__ void k_energy_partial(EnergyArgs a, double* part) {
@@ -1147,7 +1154,10 @@ __global__ void k_energy_partial(EnergyArgs a, double* part) {
         const double ez = a.epsz[q] * pz * (gzv * gzv);
         diel += (ex + ey + ez);
       }
-      if (pv * a.kappa[q] > 1.0e-9) {
+      if (pv * a.kappa[q] > 1.0e-9 && a.linear_qm) {
+        // Vpmg_qmEnergyNONLIN, LPBE branch (vpmg.c:1474-1479)
+        qm += (pv * a.zkappa2 * a.kappa[q] * (u * u));
+      } else if (pv * a.kappa[q] > 1.0e-9) {
         for (int s = 0; s < a.ions.nion; s++) {
           const double arg = -a.ions.q[s] * u;
           double e;

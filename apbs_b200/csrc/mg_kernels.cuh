@@ -97,9 +97,12 @@ struct EnergyArgs {
   const double* wy;
   const double* wz;
   double hx, hy, hz;
-  int nonlin;
+  int nonlin;          // also sum the dielectric and mobile-ion terms
   IonTable ions;       // raw concentrations in sconc for the qm term
   double zks2;
+  int linear_qm = 0;   // mobile-ion term in the LPBE form pvec zkappa2 kappa u^2
+  double zkappa2 = 0.0;
+  int complement = 0;  // weights flipped as extEnergy flips the coarse pvec
 };
 // out_dev[0] = sum pvec u charge, [1] = dielectric sum, [2] = mobile-ion sum,
 // [3] = number of clamped exponentials

@@ -35,6 +35,28 @@ void set_error(const char* fmt, ...) {
 }
 void note_launches(long long n) { g_launches += n; }
 
+// Per-axis partition weights of Vpmg_setPart (src/mg/vpmg.c:763-863) for the
+// partition [lo, hi] with no neighbouring processors (bflags all 0).
+void part_weights(int n, double h, double cent, double lo, double hi, double* w) {
+  const double small = 1.0e-12;
+  double xmin = cent - 0.5 * h * (n - 1);
+  for (int i = 0; i < n; i++) {
+    double x = i * h + xmin, ok;
+    if ((x < (hi - h / 2)) && (x > (lo + h / 2))) ok = 1.0;
+    else if (fabs(x - lo) < small) ok = 1.0;
+    else if (fabs(x - hi) < small) ok = 1.0;
+    else if ((x > (hi + h / 2)) || (x < (lo - h / 2))) ok = 0.0;
+    else if ((x < (hi + h / 2)) || (x > (lo - h / 2))) {
+      double x0 = (x - h / 2 >= lo) ? x - h / 2 : lo;
+      double x1 = (x + h / 2 <= hi) ? x + h / 2 : hi;
+      ok = fabs(x1 - x0) / h;
+      if (ok < 0.0 && fabs(ok) < small) ok = 0.0;
+      if (ok > 1.0 && fabs(ok - 1.0) < small) ok = 1.0;
+    } else ok = 0.0;
+    w[i] = ok;
+  }
+}
+
 }  // namespace pmgb
 
 using namespace pmgb;
@@ -113,28 +135,6 @@ void phys_setup(pmgb_solver* s, int natoms, const double* xyz, const double* r) 
     s->ions.sconc[i] = zks2 * p.ion_conc[i];
     s->ions_e.q[i] = p.ion_q[i];
     s->ions_e.sconc[i] = p.ion_conc[i];
-  }
-}
-
-// Per-axis partition weights of Vpmg_setPart (src/mg/vpmg.c:627-870) for a
-// partition equal to the mg-manual domain (no neighbouring processors).
-void part_weights(int n, double h, double cent, double lo, double hi, double* w) {
-  const double small = 1.0e-12;
-  double xmin = cent - 0.5 * h * (n - 1);
-  for (int i = 0; i < n; i++) {
-    double x = i * h + xmin, ok;
-    if ((x < (hi - h / 2)) && (x > (lo + h / 2))) ok = 1.0;
-    else if (fabs(x - lo) < small) ok = 1.0;
-    else if (fabs(x - hi) < small) ok = 1.0;
-    else if ((x > (hi + h / 2)) || (x < (lo - h / 2))) ok = 0.0;
-    else if ((x < (hi + h / 2)) || (x > (lo - h / 2))) {
-      double x0 = (x - h / 2 >= lo) ? x - h / 2 : lo;
-      double x1 = (x + h / 2 <= hi) ? x + h / 2 : hi;
-      ok = fabs(x1 - x0) / h;
-      if (ok < 0.0 && fabs(ok) < small) ok = 0.0;
-      if (ok > 1.0 && fabs(ok - 1.0) < small) ok = 1.0;
-    } else ok = 0.0;
-    w[i] = ok;
   }
 }
 
@@ -363,6 +363,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
   dfree(s->band);
+  dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
   dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref); dfree(s->atom_terms);
   if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
@@ -480,10 +481,18 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
     launch_fill_value(st, s->epsz, n, p.pdie);
     note_launches(4);
   }
-  // boundary values (bcCalc)
-  CK(cudaMemsetAsync(s->gx, 0, sizeof(double) * 2 * p.ny * p.nz, st));
-  CK(cudaMemsetAsync(s->gy, 0, sizeof(double) * 2 * p.nx * p.nz, st));
-  CK(cudaMemsetAsync(s->gz, 0, sizeof(double) * 2 * p.nx * p.ny, st));
+  // boundary values (bcCalc), except when focusing (vpmg.c:5404-5409): the
+  // faces were set from the coarse solution by pmgb_focus
+  if (p.bcfl == PMGB_BCFL_FOCUS) {
+    if (!s->focused) {
+      set_error("pmgb_fillco: bcfl focus needs pmgb_focus with a solved coarse calculation first");
+      return 0;
+    }
+  } else {
+    CK(cudaMemsetAsync(s->gx, 0, sizeof(double) * 2 * p.ny * p.nz, st));
+    CK(cudaMemsetAsync(s->gy, 0, sizeof(double) * 2 * p.nx * p.nz, st));
+    CK(cudaMemsetAsync(s->gz, 0, sizeof(double) * 2 * p.nx * p.ny, st));
+  }
   if (p.bcfl == PMGB_BCFL_SDH) {
     SdhArgs A;
     A.g = s->g;
@@ -505,8 +514,8 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
     launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
                s->gz);
     note_launches(3);
-  } else if (p.bcfl != PMGB_BCFL_ZERO) {
-    set_error("pmgb_fillco: bcfl %d not implemented (zero and sdh are)", p.bcfl);
+  } else if (p.bcfl != PMGB_BCFL_ZERO && p.bcfl != PMGB_BCFL_FOCUS) {
+    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh and focus are)", p.bcfl);
     return 0;
   }
   CK(cudaEventRecord(s->ev[1], st));
@@ -931,8 +940,8 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
   return 1;
 }
 
-// Vpmg_energy (src/mg/vpmg.c:1248-1277) with extFlag = 1 and no external
-// contributions (non-focused calculation)
+// Vpmg_energy (src/mg/vpmg.c:1248-1277) with extFlag = 1: the external
+// terms are those pmgb_focus left (zero for a non-focused calculation)
 extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
   if (!s || !s->solved) {
     set_error("pmgb_energy: no solution");
@@ -965,10 +974,12 @@ extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
   CK(cudaStreamSynchronize(st));
   const pmgb_params& p = s->p;
   double qf = sums[0] * p.hx * p.hy * p.hz / s->zmagic;
+  qf += s->ext_qf;
   double diel = 0.0, qm = 0.0, e;
   if (a.nonlin) {
     diel = 0.5 * sums[1] * p.hx * p.hy * p.hz;
     diel = diel / s->zmagic;
+    diel += s->ext_di;
     if (!(s->zkappa2 < 1.0e-9)) {
       if (sums[3] > 0.0) {
         set_error("pmgb_energy: clamped exponentials in the mobile-ion energy");
@@ -976,6 +987,7 @@ extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
       }
       qm = sums[2] * p.hx * p.hy * p.hz;
       qm = qm / s->zmagic;
+      qm += s->ext_qm;
     }
     e = qf - diel - qm;
   } else {

@@ -86,6 +86,11 @@ struct pmgb_solver {
   int* d_npts;
   double* atom_terms;  // 13 x natoms sdh moment terms
   int terms_alloc;
+  // focusing: faces set from a coarse solution, energies outside the domain
+  int focused;
+  double ext_qf, ext_di, ext_qm;
+  double* focus_w;  // coarse-grid partition weights for the external energy
+  int focus_w_alloc;
   // state
   int filled, solved, built;
   std::vector<double> reslog;

@@ -160,3 +160,36 @@ def config1(seed: int = 1):
     mol = cluster(5000, 25.0, seed, net_charge=12.0)
     return mol, mg_manual(161, 0.4, mol.center(), npbe=True,
                           ions=((1.0, 0.1, 2.0), (-1.0, 0.1, 2.0)))
+
+
+def subregion_center(mol: Molecule, nsub: int, seed: int) -> np.ndarray:
+    """Bounding-box midpoint of a seeded sub-region: one atom drawn from the
+    seed and its ``nsub - 1`` nearest neighbours."""
+    rng = np.random.default_rng(seed)
+    a = int(rng.integers(mol.natoms))
+    d = np.einsum("ij,ij->i", mol.xyz - mol.xyz[a], mol.xyz - mol.xyz[a])
+    sel = mol.xyz[np.argsort(d, kind="stable")[:nsub]]
+    return 0.5 * (sel.max(axis=0) + sel.min(axis=0))
+
+
+def focus_pair(mol: Molecule, coarse_dime, coarse_h, fine_dime, fine_h, fine_center,
+               **kw):
+    """Coarse (bcfl sdh) and fine (bcfl focus) mg-manual blocks of one focusing
+    chain.  The fine centre is moved inside the coarse box where needed, as
+    the mg-auto setup keeps the fine domain inside the coarse one."""
+    pc = mg_manual(coarse_dime, coarse_h, mol.center(), bcfl=BCFL_SDH, **kw)
+    half_c = 0.5 * (coarse_dime - 1) * coarse_h
+    half_f = 0.5 * (fine_dime - 1) * fine_h
+    c0 = mol.center()
+    fc = np.clip(np.asarray(fine_center, dtype=float), c0 - half_c + half_f, c0 + half_c - half_f)
+    pf = mg_manual(fine_dime, fine_h, fc, bcfl=BCFL_FOCUS, **kw)
+    return pc, pf
+
+
+def config2(seed: int = 1):
+    """Focusing on the 161^3 molecule: coarse 97^3 at 1.0 A, then fine 129^3 at
+    0.35 A centred on a 30-atom sub-region; LPBE, 0.1 M 1:1 salt."""
+    mol = cluster(5000, 25.0, seed, net_charge=12.0)
+    pc, pf = focus_pair(mol, 97, 1.0, 129, 0.35, subregion_center(mol, 30, seed + 100),
+                        ions=((1.0, 0.1, 2.0), (-1.0, 0.1, 2.0)))
+    return mol, pc, pf

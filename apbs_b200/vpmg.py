@@ -46,6 +46,8 @@ class PmgbStats(ctypes.Structure):
         ("energy_kT", ctypes.c_double), ("qf", ctypes.c_double),
         ("diel", ctypes.c_double), ("qm", ctypes.c_double),
         ("sas_points", ctypes.c_int), ("status", ctypes.c_int),
+        ("ext_qf", ctypes.c_double), ("ext_diel", ctypes.c_double),
+        ("ext_qm", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -70,6 +72,7 @@ def lib():
         L.pmgb_set_stream.argtypes = [vp, vp]
         L.pmgb_fillco_device.argtypes = [vp, ctypes.c_int, vp, vp, vp]
         L.pmgb_set_coefficients.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.pmgb_focus.argtypes = [vp, vp, ctypes.c_int]
         L.pmgb_solve.argtypes = [vp]
         L.pmgb_energy.argtypes = [vp, dp]
         L.pmgb_get_potential.argtypes = [vp, dp]
@@ -157,6 +160,12 @@ class Vpmg:
         xyz, q, r = _atoms(mol)
         self._keep = (xyz, q, r)
         _check(lib().pmgb_fillco(self._h, mol.natoms, _dp(xyz), _dp(q), _dp(r)), "pmgb_fillco")
+
+    def focus(self, coarse: "Vpmg", calc_energy: bool = True):
+        """Boundary values (and, with calc_energy, the external energy) from
+        a solved coarse calculation: Vpmg_ctor with focusFlag = 1.  Call
+        before fillco; this calculation must use bcfl focus."""
+        _check(lib().pmgb_focus(self._h, coarse._h, 1 if calc_energy else 0), "pmgb_focus")
 
     def set_coefficients(self, charge, epsx, epsy, epsz, kappa, faces):
         p = self.params

@@ -56,6 +56,7 @@ typedef struct pmgb_stats {
     double qf, diel, qm;  /* energy components (kT) */
     int sas_points;       /* accessible surface points used by the fill */
     int status;           /* 0 ok, nonzero: last device-side status code */
+    double ext_qf, ext_diel, ext_qm; /* energies outside the domain (focusing) */
 } pmgb_stats;
 
 /* Vpmg_ctor: allocate device state for one calculation on the current CUDA
@@ -77,6 +78,21 @@ int pmgb_fillco(pmgb_solver *s, int natoms, const double *xyz, const double *cha
 /* Same, with the atom arrays already in device memory. */
 int pmgb_fillco_device(pmgb_solver *s, int natoms, const double *d_xyz,
                        const double *d_charge, const double *d_radius);
+
+/* Focusing: Vpmg_ctor with focusFlag = 1 and pmgOLD = coarse (vpmg.h:226;
+ * vpmg.c:225-262).  Fills the Dirichlet faces of `fine` by trilinear
+ * interpolation of the solved coarse potential (focusFillBound,
+ * vpmg.c:1914-2414) and, when calc_energy is nonzero (energyFlag != PCE_NO),
+ * the energy of the coarse solution outside the fine domain, kept for the
+ * fine pmgb_energy (extEnergy, vpmg.c:2416-2545).  `fine` must have been
+ * created with bcfl PMGB_BCFL_FOCUS and be filled afterwards with
+ * pmgb_fillco (which then leaves the faces alone, vpmg.c:5404-5409); the
+ * fine domain must lie inside the coarse one (the reference asserts).  Both
+ * solvers must be on the current device.  The coarse solver is not
+ * destroyed (the reference's Vpmg_ctor2 destroys pmgOLD; call
+ * pmgb_destroy when done).  Work is ordered after the coarse solver's
+ * stream and issued on the fine solver's stream. */
+int pmgb_focus(pmgb_solver *fine, pmgb_solver *coarse, int calc_energy);
 
 /* Load coefficient maps produced elsewhere (host arrays of N = nx*ny*nz
  * doubles; faces as in the header comment).  The atom list is needed only

@@ -560,7 +560,10 @@ static void do_fill(const pmgb_params *p, const Phys *ph, int natoms,
             f->epsx[t] = f->epsy[t] = f->epsz[t] = p->pdie;
         }
     }
-    if (p->bcfl == PMGB_BCFL_SDH) {
+    if (p->bcfl == PMGB_BCFL_FOCUS) {
+        /* Vpmg_fillco leaves the faces alone when focusing (vpmg.c:5404-5409):
+         * they were set from the coarse solution by focus_fill_bound. */
+    } else if (p->bcfl == PMGB_BCFL_SDH) {
         bc_sdh(p, ph, natoms, xyz, q, f->xf, f->yf, f->zf, f->gx, f->gy, f->gz);
     } else {
         memset(f->gx, 0, sizeof(double) * 2 * ny * nz);
@@ -1290,8 +1293,8 @@ static int newton(Solver *s, const pmgb_params *p, const Phys *ph,
 /* ===================================================================== */
 static void part_weights(int n, double h, double cent, double lo, double hi,
                          double *w) {
-    /* Vpmg_setPart per-axis weight for a partition equal to the domain
-     * (mg-manual: no neighbouring processors, bflags all 0) */
+    /* Vpmg_setPart per-axis weight (vpmg.c:763-863) for the partition
+     * [lo, hi] with no neighbouring processors (bflags all 0) */
     int i;
     double xmin = cent - 0.5 * h * (n - 1);
     for (i = 0; i < n; i++) {
@@ -1311,30 +1314,41 @@ static void part_weights(int n, double h, double cent, double lo, double hi,
     }
 }
 
-static void energies(const pmgb_params *p, const Phys *ph, const Fill *f,
-                     const double *u, double *out) {
+/* Energy sums of one solved calculation with partition weights pvec:
+ *   pvec = setPart(lo, hi) weights (vpmg.c:863-866), or, with complement,
+ *   the flipped weights extEnergy gives the coarse grid (vpmg.c:2508-2509):
+ *   1 - pvec where pvec <= VSMALL, else 0.
+ * comps: 0 qf only; 1 qf, diel and qm in the form the calculation's own
+ * nonlinearity selects (Vpmg_qmEnergyNONLIN linear/nonlinear branches).
+ * sums[0] qf, [1] diel, [2] qm, all in kT (vpmg.c:1279-1488, 1861-1891). */
+static void energy_terms(const pmgb_params *p, const Phys *ph, const Fill *f,
+                         const double *u, const double lo[3],
+                         const double hi[3], int complement, int comps,
+                         double sums[3]) {
     int nx = p->nx, ny = p->ny, nz = p->nz, i, j, k, s;
     size_t n = (size_t)nx * ny * nz, t;
     double *wx = (double *)malloc(sizeof(double) * (nx + ny + nz));
     double *wy = wx + nx, *wz = wy + ny, *pvec;
-    double qf = 0.0, diel = 0.0, qm = 0.0, h3 = p->hx * p->hy * p->hz;
-    part_weights(nx, p->hx, p->center[0], p->center[0] - 0.5 * ((nx - 1) * p->hx),
-                 p->center[0] + 0.5 * ((nx - 1) * p->hx), wx);
-    part_weights(ny, p->hy, p->center[1], p->center[1] - 0.5 * ((ny - 1) * p->hy),
-                 p->center[1] + 0.5 * ((ny - 1) * p->hy), wy);
-    part_weights(nz, p->hz, p->center[2], p->center[2] - 0.5 * ((nz - 1) * p->hz),
-                 p->center[2] + 0.5 * ((nz - 1) * p->hz), wz);
+    double qf = 0.0, diel = 0.0, qm = 0.0;
+    part_weights(nx, p->hx, p->center[0], lo[0], hi[0], wx);
+    part_weights(ny, p->hy, p->center[1], lo[1], hi[1], wy);
+    part_weights(nz, p->hz, p->center[2], lo[2], hi[2], wz);
     pvec = (double *)malloc(sizeof(double) * n);
     for (k = 0; k < nz; k++)
         for (j = 0; j < ny; j++)
             for (i = 0; i < nx; i++) {
                 double v = wx[i] * wy[j] * wz[k];
-                pvec[IJK(i, j, k)] = (fabs(v) < VPMGSMALL) ? 0.0 : v;
+                v = (fabs(v) < VPMGSMALL) ? 0.0 : v;
+                if (complement) {
+                    if (v > VSMALL) v = 1.0;
+                    v = (1 - v) * 1.0;
+                }
+                pvec[IJK(i, j, k)] = v;
             }
     /* Vpmg_qfEnergyVolume (vpmg.c:1861-1891) */
     for (t = 0; t < n; t++) qf += (pvec[t] * u[t] * f->charge[t]);
     qf = qf * p->hx * p->hy * p->hz / ph->zmagic;
-    if (p->nonlin && ph->ionstr > 0.) {
+    if (comps) {
         /* Vpmg_dielEnergy (vpmg.c:1279-1340) */
         for (k = 0; k < nz - 1; k++)
             for (j = 0; j < ny - 1; j++)
@@ -1355,30 +1369,160 @@ static void energies(const pmgb_params *p, const Phys *ph, const Fill *f,
         /* Vpmg_qmEnergyNONLIN (vpmg.c:1401-1488) with Vcap_exp (vcap.c:59) */
         if (!(ph->zkappa2 < VSMALL)) {
             double zks2 = 0.5 * ph->zkappa2 / ph->ionstr;
-            for (t = 0; t < n; t++) {
-                if (pvec[t] * f->kappa[t] > VSMALL) {
-                    for (s = 0; s < p->nion; s++) {
-                        double a = -p->ion_q[s] * u[t], e;
-                        if (a > EXPCLAMP) e = exp(EXPCLAMP);
-                        else if (a < -EXPCLAMP) e = exp(-EXPCLAMP);
-                        else e = exp(a);
-                        qm += (pvec[t] * f->kappa[t] * zks2 * p->ion_conc[s] * (e - 1.0));
+            if (p->nonlin) {
+                for (t = 0; t < n; t++) {
+                    if (pvec[t] * f->kappa[t] > VSMALL) {
+                        for (s = 0; s < p->nion; s++) {
+                            double a = -p->ion_q[s] * u[t], e;
+                            if (a > EXPCLAMP) e = exp(EXPCLAMP);
+                            else if (a < -EXPCLAMP) e = exp(-EXPCLAMP);
+                            else e = exp(a);
+                            qm += (pvec[t] * f->kappa[t] * zks2 * p->ion_conc[s] * (e - 1.0));
+                        }
                     }
                 }
+            } else {
+                for (t = 0; t < n; t++)
+                    if (pvec[t] * f->kappa[t] > VSMALL)
+                        qm += (pvec[t] * ph->zkappa2 * f->kappa[t] * (u[t] * u[t]));
+                qm = 0.5 * qm;
             }
             qm = qm * p->hx * p->hy * p->hz;
             qm = qm / ph->zmagic;
         }
-        out[0] = qf - diel - qm;
-    } else {
-        out[0] = 0.5 * qf;
     }
-    out[7] = qf;
-    out[8] = diel;
-    out[9] = qm;
-    (void)h3;
+    sums[0] = qf;
+    sums[1] = diel;
+    sums[2] = qm;
     free(pvec);
     free(wx);
+}
+
+static void domain_box(const pmgb_params *p, double lo[3], double hi[3]) {
+    /* setPartMG partition for mg-manual: center -/+ glen/2 (routines.c:1712-1718) */
+    lo[0] = p->center[0] - 0.5 * ((p->nx - 1) * p->hx);
+    hi[0] = p->center[0] + 0.5 * ((p->nx - 1) * p->hx);
+    lo[1] = p->center[1] - 0.5 * ((p->ny - 1) * p->hy);
+    hi[1] = p->center[1] + 0.5 * ((p->ny - 1) * p->hy);
+    lo[2] = p->center[2] - 0.5 * ((p->nz - 1) * p->hz);
+    hi[2] = p->center[2] + 0.5 * ((p->nz - 1) * p->hz);
+}
+
+/* Vpmg_energy (vpmg.c:1248-1277) with extFlag = 1: ext[] holds the
+ * energies a focusing parent left outside this domain (zero otherwise). */
+static void energies(const pmgb_params *p, const Phys *ph, const Fill *f,
+                     const double *u, const double ext[3], double *out) {
+    double lo[3], hi[3], t[3];
+    int full = (p->nonlin && ph->ionstr > 0.);
+    domain_box(p, lo, hi);
+    energy_terms(p, ph, f, u, lo, hi, 0, full, t);
+    t[0] += ext[0];
+    if (full) {
+        t[1] += ext[1];
+        /* Vpmg_qmEnergyNONLIN returns before adding extQmEnergy when the
+         * ionic strength term vanishes (vpmg.c:1438-1445) */
+        if (!(ph->zkappa2 < VSMALL)) t[2] += ext[2];
+        out[0] = t[0] - t[1] - t[2];
+    } else {
+        out[0] = 0.5 * t[0];
+        t[1] = t[2] = 0.0;
+    }
+    out[7] = t[0];
+    out[8] = t[1];
+    out[9] = t[2];
+}
+
+/* ===================================================================== */
+/* Focusing (src/mg/vpmg.c:1914-2545)                                     */
+/* ===================================================================== */
+
+/* Trilinear value of the coarse potential at (x,y,z), focusFillBound's
+ * per-point body (vpmg.c:2100-2129).  Returns 0 off the coarse mesh. */
+static int focus_value(const pmgb_params *pc, const double *data,
+                       const double mnO[3], const double mxO[3], double x,
+                       double y, double z, double *uval) {
+    int nx = pc->nx, ny = pc->ny, nz = pc->nz;
+    double ifl, jfl, kfl, dx, dy, dz;
+    int ihi, ilo, jhi, jlo, khi, klo;
+    if (!((x >= (mnO[0] - VSMALL)) && (y >= (mnO[1] - VSMALL)) &&
+          (z >= (mnO[2] - VSMALL)) && (x <= (mxO[0] + VSMALL)) &&
+          (y <= (mxO[1] + VSMALL)) && (z <= (mxO[2] + VSMALL))))
+        return 0;
+    ifl = (x - mnO[0]) / pc->hx;
+    jfl = (y - mnO[1]) / pc->hy;
+    kfl = (z - mnO[2]) / pc->hz;
+    ihi = (int)ceil(ifl);
+    if (ihi > (nx - 1)) ihi = nx - 1;
+    ilo = (int)floor(ifl);
+    if (ilo < 0) ilo = 0;
+    jhi = (int)ceil(jfl);
+    if (jhi > (ny - 1)) jhi = ny - 1;
+    jlo = (int)floor(jfl);
+    if (jlo < 0) jlo = 0;
+    khi = (int)ceil(kfl);
+    if (khi > (nz - 1)) khi = nz - 1;
+    klo = (int)floor(kfl);
+    if (klo < 0) klo = 0;
+    dx = ifl - (double)ilo;
+    dy = jfl - (double)jlo;
+    dz = kfl - (double)klo;
+    *uval = dx * dy * dz * data[IJK(ihi, jhi, khi)] +
+            dx * (1.0 - dy) * dz * data[IJK(ihi, jlo, khi)] +
+            dx * dy * (1.0 - dz) * data[IJK(ihi, jhi, klo)] +
+            dx * (1.0 - dy) * (1.0 - dz) * data[IJK(ihi, jlo, klo)] +
+            (1.0 - dx) * dy * dz * data[IJK(ilo, jhi, khi)] +
+            (1.0 - dx) * (1.0 - dy) * dz * data[IJK(ilo, jlo, khi)] +
+            (1.0 - dx) * dy * (1.0 - dz) * data[IJK(ilo, jhi, klo)] +
+            (1.0 - dx) * (1.0 - dy) * (1.0 - dz) * data[IJK(ilo, jlo, klo)];
+    return 1;
+}
+
+/* focusFillBound (vpmg.c:1914-2414): Dirichlet slots 0/1 of the six fine
+ * faces from the coarse solution; the Neumann slots are not stored. */
+static int focus_fill_bound(const pmgb_params *pc, const double *uc,
+                            const pmgb_params *pf, double *gx, double *gy,
+                            double *gz) {
+    double mnO[3], mxO[3], mnN[3], mxN[3];
+    const double hO[3] = {pc->hx, pc->hy, pc->hz}, hN[3] = {pf->hx, pf->hy, pf->hz};
+    const int nO[3] = {pc->nx, pc->ny, pc->nz}, nN[3] = {pf->nx, pf->ny, pf->nz};
+    int d, i, j, k, nx = pf->nx, ny = pf->ny, nz = pf->nz;
+    for (d = 0; d < 3; d++) {
+        mnN[d] = pf->center[d] - ((double)(nN[d] - 1) * hN[d]) / 2.0;
+        mxN[d] = pf->center[d] + ((double)(nN[d] - 1) * hN[d]) / 2.0;
+        mnO[d] = pc->center[d] - ((double)(nO[d] - 1) * hO[d]) / 2.0;
+        mxO[d] = pc->center[d] + ((double)(nO[d] - 1) * hO[d]) / 2.0;
+    }
+    for (d = 0; d < 3; d++) {
+        if (fabs(mnO[d] - mnN[d]) < VSMALL) mnN[d] = mnO[d];
+        if (fabs(mxO[d] - mxN[d]) < VSMALL) mxN[d] = mxO[d];
+    }
+    for (d = 0; d < 3; d++)
+        if (mxN[d] > mxO[d] || mnO[d] > mnN[d]) return 0;
+    for (k = 0; k < nz; k++)
+        for (j = 0; j < ny; j++) {
+            double y = mnN[1] + j * hN[1], z = mnN[2] + k * hN[2];
+            if (!focus_value(pc, uc, mnO, mxO, mnN[0], y, z, &gx[((size_t)0 * nz + k) * ny + j]))
+                return 0;
+            if (!focus_value(pc, uc, mnO, mxO, mxN[0], y, z, &gx[((size_t)1 * nz + k) * ny + j]))
+                return 0;
+        }
+    for (k = 0; k < nz; k++)
+        for (i = 0; i < nx; i++) {
+            double x = mnN[0] + i * hN[0], z = mnN[2] + k * hN[2];
+            if (!focus_value(pc, uc, mnO, mxO, x, mnN[1], z, &gy[((size_t)0 * nz + k) * nx + i]))
+                return 0;
+            if (!focus_value(pc, uc, mnO, mxO, x, mxN[1], z, &gy[((size_t)1 * nz + k) * nx + i]))
+                return 0;
+        }
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            double x = mnN[0] + i * hN[0], y = mnN[1] + j * hN[1];
+            if (!focus_value(pc, uc, mnO, mxO, x, y, mnN[2], &gz[((size_t)0 * ny + j) * nx + i]))
+                return 0;
+            if (!focus_value(pc, uc, mnO, mxO, x, y, mxN[2], &gz[((size_t)1 * ny + j) * nx + i]))
+                return 0;
+        }
+    return 1;
 }
 
 /* ===================================================================== */
@@ -1424,10 +1568,19 @@ int oracle_pmg_fill(const pmgb_params *p, int natoms, const double *xyz,
     return 1;
 }
 
-int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
-                   const double *q, const double *r, double *u, double *maps,
-                   double *faces, double *out, double *reslog, int reslog_cap,
-                   int verbose) {
+/* What a solved calculation hands to a focused child: its maps, potential
+ * and physical scalars (the reference keeps them in pmgOLD). */
+typedef struct {
+    Phys ph;
+    Fill f;
+    double *u;
+    double ext[3];
+} Kept;
+
+static int run_calc(const pmgb_params *p, int natoms, const double *xyz,
+                    const double *q, const double *r, const double *faces_in,
+                    const double ext[3], double *u, double *maps, double *faces,
+                    double *out, double *reslog, int reslog_cap, Kept *keep) {
     Phys ph;
     Fill f;
     Solver s;
@@ -1435,7 +1588,6 @@ int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
     size_t n = (size_t)nx * ny * nz, t;
     double t0, t1, t2, t3, t4, errtol = (p->etol > 0.0) ? p->etol : 1.0e-6;
     double *ccf;
-    (void)verbose;
     memset(&s, 0, sizeof(s));
     s.reslog = reslog;
     s.reslog_cap = reslog_cap;
@@ -1443,6 +1595,11 @@ int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
     phys_setup(p, natoms, xyz, r, &ph);
     fill_alloc(p, &f);
     t1 = now_s();
+    if (p->bcfl == PMGB_BCFL_FOCUS) {
+        if (!faces_in) return 0;
+        memcpy(f.gx, faces_in, sizeof(double) * 2 * ((size_t)ny * nz + (size_t)nx * nz +
+                                                     (size_t)nx * ny));
+    }
     do_fill(p, &ph, natoms, xyz, q, r, &f);
     t2 = now_s();
     if (maps) memcpy(maps, f.charge, sizeof(double) * 5 * n);
@@ -1509,7 +1666,16 @@ int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
                 x[IJK(i, j, nz - 1)] = f.gz[((size_t)1 * ny + j) * nx + i];
             }
         if (u) memcpy(u, x, sizeof(double) * n);
-        energies(p, &ph, &f, x, out);
+        energies(p, &ph, &f, x, ext, out);
+        if (keep) {
+            keep->ph = ph;
+            keep->f = f;
+            keep->u = (double *)malloc(sizeof(double) * n);
+            memcpy(keep->u, x, sizeof(double) * n);
+            keep->ext[0] = ext[0];
+            keep->ext[1] = ext[1];
+            keep->ext[2] = ext[2];
+        }
     }
     t4 = now_s();
     out[1] = (double)s.progress;
@@ -1528,6 +1694,68 @@ int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
         free(L->cp); free(L->rhs); free(L->xt);
     }
     free(s.w1); free(s.w2); free(s.w3); free(s.band); free(ccf);
-    fill_free(&f);
+    if (!keep) fill_free(&f);
     return 1;
+}
+
+int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
+                   const double *q, const double *r, double *u, double *maps,
+                   double *faces, double *out, double *reslog, int reslog_cap,
+                   int verbose) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    (void)verbose;
+    if (p->bcfl == PMGB_BCFL_FOCUS) return 0; /* needs a parent: oracle_pmg_focus */
+    return run_calc(p, natoms, xyz, q, r, NULL, zero, u, maps, faces, out, reslog,
+                    reslog_cap, NULL);
+}
+
+/* extEnergy (vpmg.c:2416-2545) for a non-parallel chain: the coarse
+ * calculation's qf/diel/qm over the complement of the fine domain, each with
+ * the coarse calculation's own external terms added (extFlag = 1). */
+static void ext_energy(const pmgb_params *pc, const Kept *kc,
+                       const pmgb_params *pf, double ext[3]) {
+    double lo[3], hi[3], t[3];
+    domain_box(pf, lo, hi);
+    energy_terms(pc, &kc->ph, &kc->f, kc->u, lo, hi, 1, 1, t);
+    ext[0] = t[0] + kc->ext[0];
+    ext[1] = t[1] + kc->ext[1];
+    ext[2] = (kc->ph.zkappa2 < VSMALL) ? 0.0 : t[2] + kc->ext[2];
+}
+
+int oracle_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
+                     const double *xyz, const double *q, const double *r,
+                     double *u, double *faces, double *out, double *reslog,
+                     int reslog_cap, int verbose) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    double outc[16], ext[3], *fin;
+    size_t nfaces = 2 * ((size_t)pf->ny * pf->nz + (size_t)pf->nx * pf->nz +
+                         (size_t)pf->nx * pf->ny);
+    Kept kc;
+    int rc, nlog;
+    (void)verbose;
+    if (pc->bcfl == PMGB_BCFL_FOCUS || pf->bcfl != PMGB_BCFL_FOCUS) return 0;
+    memset(outc, 0, sizeof(outc));
+    if (!run_calc(pc, natoms, xyz, q, r, NULL, zero, NULL, NULL, NULL, outc, reslog,
+                  reslog_cap, &kc))
+        return 0;
+    fin = (double *)calloc(nfaces, sizeof(double));
+    rc = focus_fill_bound(pc, kc.u, pf, fin, fin + 2 * (size_t)pf->ny * pf->nz,
+                          fin + 2 * ((size_t)pf->ny * pf->nz + (size_t)pf->nx * pf->nz));
+    if (rc) {
+        ext_energy(pc, &kc, pf, ext);
+        nlog = (int)outc[2];
+        rc = run_calc(pf, natoms, xyz, q, r, fin, ext, u, NULL, faces, out,
+                      reslog ? reslog + (nlog < reslog_cap ? nlog : reslog_cap) : NULL,
+                      reslog_cap - (nlog < reslog_cap ? nlog : reslog_cap), NULL);
+        out[1] += outc[1];
+        out[2] += outc[2];
+        out[12] = ext[0];
+        out[13] = ext[1];
+        out[14] = ext[2];
+        out[15] = outc[0];
+    }
+    free(fin);
+    free(kc.u);
+    fill_free(&kc.f);
+    return rc;
 }

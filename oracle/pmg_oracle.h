@@ -29,6 +29,19 @@ int oracle_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
                    double *faces, double *out, double *reslog, int reslog_cap,
                    int verbose);
 
+/* Two-level focusing chain, as initMG builds it for an ELEC block with
+ * bcfl focus after a solved one (routines.c:1458-1475): the coarse
+ * calculation pc (bcfl zero/sdh) is solved, the fine one pf (bcfl focus)
+ * takes its faces from the coarse potential (focusFillBound) and the energy
+ * outside its domain from the coarse solution (extEnergy), then is solved.
+ * u, faces: the fine calculation's; out as above for the fine calculation
+ * (energies include the external terms) plus [12..14] extQf, extDiel,
+ * extQm and [15] the coarse energy; [1], [2] and reslog cover both solves. */
+int oracle_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
+                     const double *xyz, const double *q, const double *r,
+                     double *u, double *faces, double *out, double *reslog,
+                     int reslog_cap, int verbose);
+
 /* Coefficient fill only (Vpmg_fillco): maps and faces as above. */
 int oracle_pmg_fill(const pmgb_params *p, int natoms, const double *xyz,
                     const double *q, const double *r, double *maps,

@@ -26,6 +26,9 @@ def lib():
                                         dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
         _lib.oracle_pmg_fill.restype = ctypes.c_int
         _lib.oracle_pmg_fill.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, dp, dp]
+        _lib.oracle_pmg_focus.restype = ctypes.c_int
+        _lib.oracle_pmg_focus.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
+                                        dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
     return _lib
 
 
@@ -85,3 +88,34 @@ def fill(params, mol):
     shape = (params.nz, params.ny, params.nx)
     m = maps.reshape(5, *shape)
     return dict(charge=m[0], epsx=m[1], epsy=m[2], epsz=m[3], kappa=m[4], faces=faces)
+
+
+def focus(coarse, fine, mol, want_faces=False, reslog_cap=8192):
+    """Two-block focusing chain (coarse solve, then the bcfl-focus block whose
+    faces and external energy come from it), computed by the oracle.
+
+    Returns the fine block's u, energy (with the external terms), faces on
+    request, the external energies and the coarse energy."""
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(mol.charge, dtype=np.float64)
+    r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    n = fine.nx * fine.ny * fine.nz
+    u = np.zeros(n)
+    nfaces = 2 * (fine.ny * fine.nz + fine.nx * fine.nz + fine.nx * fine.ny)
+    faces = np.zeros(nfaces) if want_faces else None
+    out = np.zeros(16)
+    reslog = np.zeros(reslog_cap)
+    rc = lib().oracle_pmg_focus(ctypes.byref(coarse), ctypes.byref(fine), mol.natoms, _ptr(xyz), _ptr(q),
+                  _ptr(r), _ptr(u), _ptr(faces), _ptr(out), _ptr(reslog), reslog_cap, 0)
+    if rc != 1:
+        raise RuntimeError("oracle focusing run failed")
+    res = {
+        "u": u.reshape(fine.nz, fine.ny, fine.nx), "energy_kT": out[0],
+        "progress_msgs": int(out[1]), "reslog": reslog[: min(int(out[2]), reslog_cap)].copy(),
+        "t_ctor": out[3], "t_fillco": out[4], "t_solve": out[5], "t_energy": out[6],
+        "qf": out[7], "diel": out[8], "qm": out[9],
+        "ext_qf": out[12], "ext_diel": out[13], "ext_qm": out[14], "coarse_energy_kT": out[15],
+    }
+    if faces is not None:
+        res["faces"] = faces
+    return res

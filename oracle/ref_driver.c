@@ -7,7 +7,8 @@
  *
  * The call sequence mirrors initMG / solveMG / setPartMG / energyMG of the
  * reference (src/routines.c:1314-1606, 1635-1674, 1676-1724, 1726-1801) for
- * a single non-focused mg-manual ELEC block, starting from an in-memory atom
+ * a single non-focused mg-manual ELEC block (ref_pmg_run) or a coarse block
+ * followed by a bcfl-focus block (ref_pmg_focus), starting from an in-memory atom
  * list instead of a PQR file (Valist_readPQR, src/generic/valist.c:606, is
  * replaced by filling the Valist directly and calling Valist_getStatistics).
  */
@@ -181,6 +182,124 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
     Vpmgp_dtor(&pmgp);
     Vpbe_dtor(&pbe);
     MGparm_dtor(&mg);
+    Valist_dtor(&alist);
+    return 1;
+}
+
+/* Focusing chain of two mg-manual ELEC blocks on one molecule, as main.c
+ * runs them (src/main.c:529-620 via initMG/solveMG/setPartMG/energyMG): the
+ * coarse block pc is built, filled, solved and its energy taken; the fine
+ * block pf (bcfl focus) is constructed with focusFlag=1 and pmgOLD = the
+ * coarse Vpmg (routines.c:1458-1469), which fills its faces from the coarse
+ * potential, computes the external energies and destroys the coarse Vpmg
+ * (vpmg.c:225-262, 396).  Outputs as ref_pmg_run for the fine block, plus
+ * out[12..14] = extQf, extDiel, extQm and out[15] = the coarse energy; the
+ * residual log and message count cover both solves. */
+int ref_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
+                  const double *xyz, const double *q, const double *r,
+                  double *u, double *faces, double *out, double *reslog,
+                  int reslog_cap, int verbose) {
+    int i, n, rc;
+    double t0, t1, t2, t3, t4;
+    double ionc[PMGB_MAXION], ionr[PMGB_MAXION], ionq[PMGB_MAXION];
+    double partMin[3], partMax[3];
+    Valist *alist;
+    MGparm *mgc, *mgf;
+    Vpbe *pbec, *pbef;
+    Vpmgp *pmgpc, *pmgpf;
+    Vpmg *pmgc, *pmgf;
+
+    if (pf->bcfl != PMGB_BCFL_FOCUS || pc->bcfl == PMGB_BCFL_FOCUS) return 0;
+    oracle_shim_set_verbose(verbose);
+    oracle_shim_set_log(reslog, reslog_cap);
+    for (i = 0; i < pc->nion && i < PMGB_MAXION; i++) {
+        ionc[i] = pc->ion_conc[i];
+        ionr[i] = pc->ion_radius[i];
+        ionq[i] = pc->ion_q[i];
+    }
+    alist = make_alist(natoms, xyz, q, r);
+
+    /* coarse block */
+    mgc = make_mgparm(pc);
+    pbec = Vpbe_ctor(alist, pc->nion, ionc, ionr, ionq, pc->temp, pc->pdie,
+                     pc->sdie, pc->srad, 0, pc->sdens, 0.0, 0.0, 0.0, 0.0);
+    if (pbec == VNULL) return 0;
+    pmgpc = Vpmgp_ctor(mgc);
+    pmgpc->bcfl = (Vbcfl)pc->bcfl;
+    pmgpc->xcent = pc->center[0];
+    pmgpc->ycent = pc->center[1];
+    pmgpc->zcent = pc->center[2];
+    pmgc = Vpmg_ctor(pmgpc, pbec, 0, VNULL, mgc, PCE_NO);
+    rc = Vpmg_fillco(pmgc, (Vsurf_Meth)pc->srfm, 0.3, (Vchrg_Meth)pc->chgm,
+                     0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
+                     VNULL);
+    if (rc != 1) return 0;
+    if (Vpmg_solve(pmgc) != 1) return 0;
+    for (i = 0; i < 3; i++) {
+        partMin[i] = mgc->center[i] - 0.5 * mgc->glen[i];
+        partMax[i] = mgc->center[i] + 0.5 * mgc->glen[i];
+    }
+    Vpmg_setPart(pmgc, partMin, partMax, mgc->partDisjOwnSide);
+    out[15] = Vpmg_energy(pmgc, 1);
+
+    /* fine block: Vpmg_ctor with focusing destroys the coarse Vpmg */
+    t0 = now_s();
+    mgf = make_mgparm(pf);
+    pbef = Vpbe_ctor(alist, pf->nion, ionc, ionr, ionq, pf->temp, pf->pdie,
+                     pf->sdie, pf->srad, 1, pf->sdens, 0.0, 0.0, 0.0, 0.0);
+    if (pbef == VNULL) return 0;
+    pmgpf = Vpmgp_ctor(mgf);
+    pmgpf->bcfl = (Vbcfl)pf->bcfl;
+    pmgpf->xcent = pf->center[0];
+    pmgpf->ycent = pf->center[1];
+    pmgpf->zcent = pf->center[2];
+    pmgf = Vpmg_ctor(pmgpf, pbef, 1, pmgc, mgf, PCE_TOTAL);
+    out[12] = pmgf->extQfEnergy;
+    out[13] = pmgf->extDiEnergy;
+    out[14] = pmgf->extQmEnergy;
+    Vpmgp_dtor(&pmgpc);
+    Vpbe_dtor(&pbec);
+    MGparm_dtor(&mgc);
+    t1 = now_s();
+    rc = Vpmg_fillco(pmgf, (Vsurf_Meth)pf->srfm, 0.3, (Vchrg_Meth)pf->chgm,
+                     0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
+                     VNULL);
+    t2 = now_s();
+    if (rc != 1) return 0;
+    n = pf->nx * pf->ny * pf->nz;
+    if (faces) {
+        size_t fx = (size_t)pf->ny * pf->nz, fy = (size_t)pf->nx * pf->nz,
+               fz = (size_t)pf->nx * pf->ny;
+        memcpy(faces, pmgf->gxcf, sizeof(double) * 2 * fx);
+        memcpy(faces + 2 * fx, pmgf->gycf, sizeof(double) * 2 * fy);
+        memcpy(faces + 2 * fx + 2 * fy, pmgf->gzcf, sizeof(double) * 2 * fz);
+    }
+    rc = Vpmg_solve(pmgf);
+    t3 = now_s();
+    if (rc != 1) return 0;
+    if (u) memcpy(u, pmgf->u, sizeof(double) * n);
+    for (i = 0; i < 3; i++) {
+        partMin[i] = mgf->center[i] - 0.5 * mgf->glen[i];
+        partMax[i] = mgf->center[i] + 0.5 * mgf->glen[i];
+    }
+    Vpmg_setPart(pmgf, partMin, partMax, mgf->partDisjOwnSide);
+    out[0] = Vpmg_energy(pmgf, 1);
+    t4 = now_s();
+    out[1] = (double)oracle_shim_iter_count();
+    out[2] = (double)oracle_shim_log_count();
+    out[3] = t1 - t0;
+    out[4] = t2 - t1;
+    out[5] = t3 - t2;
+    out[6] = t4 - t3;
+    out[7] = Vpmg_qfEnergy(pmgf, 1);
+    out[8] = (pf->nonlin) ? Vpmg_dielEnergy(pmgf, 1) : 0.0;
+    out[9] = (pf->nonlin) ? Vpmg_qmEnergy(pmgf, 1) : 0.0;
+    oracle_shim_set_log(VNULL, 0);
+
+    Vpmg_dtor(&pmgf);
+    Vpmgp_dtor(&pmgpf);
+    Vpbe_dtor(&pbef);
+    MGparm_dtor(&mgf);
     Valist_dtor(&alist);
     return 1;
 }

@@ -38,3 +38,33 @@ def test_restatement_matches_reference(name, mol, params):
     scale = np.abs(a["u"]).max()
     assert np.abs(a["u"] - b["u"]).max() <= 1e-12 * scale
     assert abs(a["energy_kT"] - b["energy_kT"]) <= 1e-12 * abs(a["energy_kT"])
+
+
+def _focus_cases():
+    m = synth.cluster(200, 9.0, seed=5, net_charge=2.0)
+    c = synth.subregion_center(m, 30, 7)
+    lp = synth.focus_pair(m, 33, 1.0, 33, 0.45, c)
+    np_ = synth.focus_pair(m, 33, 1.0, 33, 0.45, c, npbe=True,
+                           ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    m2 = synth.cluster(150, 8.0, seed=9, net_charge=-1.0)
+    lp2 = synth.focus_pair(m2, 49, 0.9, 33, 0.5, synth.subregion_center(m2, 30, 3),
+                           srfm=synth.SRFM_MOL, ions=((2, 0.05, 2.0), (-1, 0.1, 1.8)))
+    return [("lpbe33_focus", m, *lp), ("npbe33_focus", m, *np_), ("lpbe49to33_mol_2to1", m2, *lp2)]
+
+
+@pytest.mark.parametrize("name,mol,pc,pf", _focus_cases(), ids=lambda c: c if isinstance(c, str) else "")
+def test_focusing_restatement_matches_reference(name, mol, pc, pf):
+    a = ref.focus(pc, pf, mol, want_faces=True)
+    b = port.focus(pc, pf, mol, want_faces=True)
+    # the faces interpolate coarse potentials that agree to round-off
+    fscale = np.abs(a["faces"]).max()
+    assert np.abs(a["faces"] - b["faces"]).max() <= 1e-13 * fscale
+    for k in ("ext_qf", "ext_diel", "ext_qm", "coarse_energy_kT"):
+        assert abs(a[k] - b[k]) <= 1e-12 * max(abs(a[k]), 1e-30), k
+    assert len(a["reslog"]) == len(b["reslog"])
+    np.testing.assert_allclose(b["reslog"], a["reslog"], rtol=2e-6)
+    scale = np.abs(a["u"]).max()
+    assert np.abs(a["u"] - b["u"]).max() <= 1e-12 * scale
+    assert abs(a["energy_kT"] - b["energy_kT"]) <= 1e-12 * abs(a["energy_kT"])
+    # the focused energy differs from the plain one by the external term
+    assert a["ext_qf"] != 0.0
