@@ -77,6 +77,10 @@ struct MixedState {
   cudaGraphExec_t exec[2];
   long long kernels[2];
   int cc_ready;
+  int lo;             // lowest level with FP32 storage (0, or the FP64 coarsest)
+  int zero_cc;        // levels >= lo carry no Helmholtz term (band operator)
+  int* d_flag;        // device flag of the band restencil check
+  int stale;          // FP64 operators rebuilt since the FP32 copies were made
   int tail_first;     // first level run by the cluster tail kernel (0: none)
   int tail_cluster;
   TLev* d_tlev;       // device copies of the level descriptors
@@ -116,10 +120,10 @@ void to_f32(cudaStream_t s, const double* a, float* b, size_t n) {
 // ---------------------------------------------------------------------------
 // FP32 stencils
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float nb27(const OpF& o, Grid g, const float* x, size_t id) {
+template <typename T>
+__device__ __forceinline__ T nb27g(const T* const* c, Grid g, const T* x, size_t id) {
   const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
-  const float* const* c = o.c;
-  float t = c[ON][id] * x[id + sy] + c[ON][id - sy] * x[id - sy] + c[OE][id] * x[id + 1] +
+  T t = c[ON][id] * x[id + sy] + c[ON][id - sy] * x[id - sy] + c[OE][id] * x[id + 1] +
             c[OE][id - 1] * x[id - 1];
   t += c[ONE][id] * x[id + sy + 1] + c[ONW][id] * x[id + sy - 1] +
        c[ONW][id - sy + 1] * x[id - sy + 1] + c[ONE][id - sy - 1] * x[id - sy - 1];
@@ -135,6 +139,10 @@ __device__ __forceinline__ float nb27(const OpF& o, Grid g, const float* x, size
        c[UNW][id - sz - sy + 1] * x[id - sz - sy + 1] +
        c[UNE][id - sz - sy - 1] * x[id - sz - sy - 1];
   return t;
+}
+
+__device__ __forceinline__ float nb27(const OpF& o, Grid g, const float* x, size_t id) {
+  return nb27g<float>(o.c, g, x, id);
 }
 
 __device__ __forceinline__ float nb7(const OpF& o, Grid g, const float* x, size_t id) {
@@ -604,20 +612,23 @@ __device__ void tail_damp(const TLev& L, int gtid, int nthr, double* sh, double*
   den = b;
 }
 
+// One V-cycle from level A.first down to the dense level and back.  With
+// rhs_given the right-hand side of level first is already in its w0;
+// otherwise it is restricted from the residual of level first-1.
 template <int CLUSTER>
-__global__ void __launch_bounds__(512) k_vcycle_tail(TailArgs A) {
-  __shared__ double sh[64];
-  __shared__ double slots[4];
-  unsigned rank = 0;
-  if (CLUSTER > 1) rank = cg::this_cluster().block_rank();
-  const int gtid = rank * blockDim.x + threadIdx.x;
-  const int nthr = CLUSTER * blockDim.x;
-  int phase = 0;
+__device__ void tail_cycle(const TailArgs& A, bool rhs_given, int gtid, int nthr, double* sh,
+                           double* slots, int& phase) {
   // down
   for (int l = A.first; l <= A.last; l++) {
     const TLev& L = A.lev[l];
-    if (l == A.first) tail_restrict(A.gprev, A.rprev, L, true, gtid, nthr);
-    else tail_restrict(A.lev[l - 1].g, A.r, L, true, gtid, nthr);
+    if (l == A.first && rhs_given) {
+      const int n = (int)L.g.n();
+      for (int q = gtid; q < n; q += nthr) L.x[q] = 0.f;
+    } else if (l == A.first) {
+      tail_restrict(A.gprev, A.rprev, L, true, gtid, nthr);
+    } else {
+      tail_restrict(A.lev[l - 1].g, A.r, L, true, gtid, nthr);
+    }
     tail_sync<CLUSTER>();
     if (l != A.last) {
       tail_smooth<CLUSTER>(L, 0, gtid, nthr);
@@ -670,6 +681,18 @@ __global__ void __launch_bounds__(512) k_vcycle_tail(TailArgs A) {
     tail_sync<CLUSTER>();
     tail_smooth<CLUSTER>(P, 1, gtid, nthr);
   }
+}
+
+template <int CLUSTER>
+__global__ void __launch_bounds__(512) k_vcycle_tail(TailArgs A) {
+  __shared__ double sh[64];
+  __shared__ double slots[4];
+  unsigned rank = 0;
+  if (CLUSTER > 1) rank = cg::this_cluster().block_rank();
+  const int gtid = rank * blockDim.x + threadIdx.x;
+  const int nthr = CLUSTER * blockDim.x;
+  int phase = 0;
+  tail_cycle<CLUSTER>(A, false, gtid, nthr, sh, slots, phase);
   // damping sums for the first -> first-1 correction (done by the caller)
   double num, den;
   tail_damp<CLUSTER>(A.lev[A.first], gtid, nthr, sh, slots, phase, num, den);
@@ -677,6 +700,126 @@ __global__ void __launch_bounds__(512) k_vcycle_tail(TailArgs A) {
     A.xnum[0] = num;
     A.xden[0] = den;
   }
+  // no CTA may exit while another can still read its shared memory
+  tail_sync<CLUSTER>();
+}
+
+// The reference's coarsest band matrix (Vbuildband1_27,
+// src/pmgc/buildBd.c:183-306) written back as a symmetric 27-point operator
+// B: diagonal oC without the Helmholtz term, and each of the 13 couplings a
+// band column q = (i,j,k) stores with the row q + off becomes the coupling
+// of (i,j,k) with its geometric neighbour at that offset.  Several of those
+// values come from the coefficient of a different pair (the band's
+// diagonal couplings), so B is not A_c; it is what the reference factors and
+// solves.  A nonzero value whose band row is not the geometric neighbour (an
+// offset that wraps across the grid edge) cannot be expressed this way and
+// raises *wrap.
+struct OpW {
+  double* c[14];
+};
+
+__global__ void k_band_restencil(Grid g, Op a, OpW b, int* wrap) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int ex = nx - 2, exy = (nx - 2) * (ny - 2);
+  const int nint = exy * (nz - 2);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nint; q += gridDim.x * blockDim.x) {
+    const int i = 1 + q % ex, j = 1 + (q / ex) % (ny - 2), k = 1 + q / exy;
+    const double* const* c = a.c;
+    b.c[OC][g.idx(i, j, k)] = c[OC][g.idx(i, j, k)];
+    // (band offset, value, geometric displacement, target array, target point)
+    auto put = [&](int off, double v, int di, int dj, int dk, int arr, int ti, int tj, int tk) {
+      const int pi = i + di, pj = j + dj, pk = k + dk;
+      if (pi >= 1 && pi <= nx - 2 && pj >= 1 && pj <= ny - 2 && pk >= 1 && pk <= nz - 2) {
+        b.c[arr][g.idx(ti, tj, tk)] = v;
+      } else if (v != 0.0 && q + off >= 0) {
+        atomicOr(wrap, 1);
+      }
+    };
+    put(-1, c[OE][g.idx(i - 1, j, k)], -1, 0, 0, OE, i - 1, j, k);
+    put(-ex, c[ON][g.idx(i, j - 1, k)], 0, -1, 0, ON, i, j - 1, k);
+    put(-ex + 1, c[ONE][g.idx(i, j - 1, k)], 1, -1, 0, ONW, i + 1, j - 1, k);
+    put(-ex - 1, c[ONW][g.idx(i, j - 1, k)], -1, -1, 0, ONE, i - 1, j - 1, k);
+    put(-exy, c[UC][g.idx(i, j, k - 1)], 0, 0, -1, UC, i, j, k - 1);
+    put(-exy + 1, c[UE][g.idx(i, j, k - 1)], 1, 0, -1, UW, i + 1, j, k - 1);
+    put(-exy - 1, c[UW][g.idx(i, j, k - 1)], -1, 0, -1, UE, i - 1, j, k - 1);
+    put(-exy + ex, c[UN][g.idx(i, j, k - 1)], 0, 1, -1, US, i, j + 1, k - 1);
+    put(-exy - ex, c[US][g.idx(i, j, k - 1)], 0, -1, -1, UN, i, j - 1, k - 1);
+    put(-exy + ex + 1, c[UNE][g.idx(i, j, k - 1)], 1, 1, -1, USW, i + 1, j + 1, k - 1);
+    put(-exy + ex - 1, c[UNW][g.idx(i, j, k - 1)], -1, 1, -1, USE, i - 1, j + 1, k - 1);
+    put(-exy - ex + 1, c[USE][g.idx(i, j, k - 1)], 1, -1, -1, UNW, i + 1, j - 1, k - 1);
+    put(-exy - ex - 1, c[USW][g.idx(i, j, k - 1)], -1, -1, -1, UNE, i - 1, j - 1, k - 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exact-to-round-off solve of the FP64 coarsest level (FP64 path, LPBE):
+// B x = b, B the reference's band matrix as a 27-point operator
+// (k_band_restencil), by FP64 iterative refinement, each correction one FP32
+// V-cycle over Galerkin levels of B below (tail_cycle with the residual as
+// its right-hand side), until ||b - B x||_2 <= rtol ||b||_2.  It stands in
+// for the reference's banded Cholesky (Vdpbfa/Vdpbsl, src/pmgc/mlinpckd.c),
+// whose factorisation and substitution are sequential in the number of
+// unknowns; any solve of B exact to round-off gives the V-cycle the same
+// coarse-grid correction.
+// ---------------------------------------------------------------------------
+struct ExactArgs {
+  TailArgs T;        // FP32 hierarchy; T.first is the FP64 coarsest level
+  Grid g;            // grid of the FP64 coarsest level
+  const double* op[14];
+  const double* cc;
+  const double* b;
+  double* x;
+  double* r;         // FP64 residual scratch of the level's size
+  int maxit;
+  double rtol;
+  int* iters;        // refinement steps taken
+};
+
+template <int CLUSTER>
+__global__ void __launch_bounds__(512) k_coarse_exact(ExactArgs E) {
+  __shared__ double sh[64];
+  __shared__ double slots[4];
+  unsigned rank = 0;
+  if (CLUSTER > 1) rank = cg::this_cluster().block_rank();
+  const int gtid = rank * blockDim.x + threadIdx.x;
+  const int nthr = CLUSTER * blockDim.x;
+  int phase = 0;
+  const Grid g = E.g;
+  const int ex = g.nx - 2, ey = g.ny - 2, nint = ex * ey * (g.nz - 2);
+  const int n = (int)g.n();
+  const TLev& L = E.T.lev[E.T.first];
+  for (int q = gtid; q < n; q += nthr) E.x[q] = 0.0;
+  tail_sync<CLUSTER>();
+  double bn = 0.0;
+  int it = 0;
+  for (;; it++) {
+    double rr = 0.0, unused = 0.0;
+    for (int q = gtid; q < nint; q += nthr) {
+      const size_t id = g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey));
+      const double v = E.b[id] + nb27g<double>(E.op, g, E.x, id) -
+                       (E.op[OC][id] + E.cc[id]) * E.x[id];
+      E.r[id] = v;
+      rr += v * v;
+    }
+    tail_sum2<CLUSTER>(rr, unused, sh, slots, phase);  // every CTA sees the same sum
+    const double rn = sqrt(rr);
+    if (it == 0) bn = rn;
+    if (bn == 0.0 || rn <= E.rtol * bn || it >= E.maxit) break;
+    for (int q = gtid; q < n; q += nthr) {
+      const int i = q % g.nx, j = (q / g.nx) % g.ny, k = q / (g.nx * g.ny);
+      const bool bd = (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 ||
+                       k == g.nz - 1);
+      L.w0[q] = bd ? 0.f : (float)E.r[q];
+    }
+    tail_sync<CLUSTER>();
+    tail_cycle<CLUSTER>(E.T, true, gtid, nthr, sh, slots, phase);
+    for (int q = gtid; q < nint; q += nthr) {
+      const size_t id = g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey));
+      E.x[id] += (double)L.x[id];
+    }
+    tail_sync<CLUSTER>();
+  }
+  if (gtid == 0) E.iters[0] = it;
   // no CTA may exit while another can still read its shared memory
   tail_sync<CLUSTER>();
 }
@@ -785,6 +928,10 @@ int dalloc64(double** p, size_t n) {
 
 }  // namespace
 
+void mixed_mark_stale(MixedState* m) {
+  if (m) m->stale = 1;
+}
+
 void mixed_destroy(MixedState* m) {
   if (!m) return;
   for (int e = 0; e < 2; e++)
@@ -806,28 +953,41 @@ void mixed_destroy(MixedState* m) {
   if (m->dvec) cudaFree(m->dvec);
   if (m->dinfo) cudaFree(m->dinfo);
   if (m->d_tlev) cudaFree(m->d_tlev);
+  if (m->d_flag) cudaFree(m->d_flag);
   delete m;
 }
 
 namespace {
 
 // Build the FP32 hierarchy from the FP64 one (plus extra Galerkin levels).
-int mixed_setup(pmgb_solver* s) {
+int mixed_setup_from(pmgb_solver* s, int lo) {
   if (s->mixed) return 1;
   MixedState* m = new MixedState();
   memset(m, 0, sizeof(*m));
   s->mixed = m;
+  m->lo = lo;
   cudaStream_t st = s->stream;
   // levels shared with the FP64 hierarchy
   int nl = 0;
+  m->zero_cc = (lo > 0);
   for (int l = 0; l < s->nlev; l++, nl++) {
     MLevel& L = m->lev[l];
     L.g = s->lev[l].g;
     L.nop = s->lev[l].nop;
-    for (int c = 0; c < L.nop; c++) L.op64[c] = s->lev[l].op[c];
-    L.own64 = 0;
-    L.cc64 = nullptr;
+    if (lo > 0 && l == lo) {
+      // exact coarse solve of the FP64 path: the reference's band matrix
+      // written as a 27-point operator (k_band_restencil), without cc
+      L.own64 = 1;
+      for (int c = 0; c < L.nop; c++)
+        if (!dalloc64(&L.op64[c], L.g.n())) return 0;
+      if (!dalloc64(&L.cc64, L.g.n())) return 0;
+    } else {
+      for (int c = 0; c < L.nop; c++) L.op64[c] = s->lev[l].op[c];
+      L.own64 = 0;
+      L.cc64 = nullptr;
+    }
   }
+  if (lo > 0) CKM(cudaMalloc(&m->d_flag, sizeof(int)));
   // extra coarse levels until <= 512 interior unknowns or the grid cannot
   // be coarsened exactly
   while (nl < 16) {
@@ -847,29 +1007,21 @@ int mixed_setup(pmgb_solver* s) {
     nl++;
   }
   m->nlev = nl;
-  // Galerkin operators of the extra levels
-  double** dptrs = nullptr;
-  CKM(cudaMalloc(&dptrs, sizeof(double*) * 14 * 16));
-  for (int l = s->nlev; l < nl; l++) {
-    CKM(cudaMemcpyAsync(dptrs + 14 * l, m->lev[l].op64, sizeof(double*) * 14,
-                        cudaMemcpyHostToDevice, st));
-    launch_galerkin(st, m->lev[l - 1].g, m->lev[l - 1].ops64(), m->lev[l].g, dptrs + 14 * l);
-    note_launches(1);
-  }
-  CKM(cudaStreamSynchronize(st));
-  cudaFree(dptrs);
-  // FP32 storage and conversion
-  for (int l = 0; l < nl; l++) {
+  // operator pointers of the extra levels join the solver's device table
+  for (int l = s->nlev; l < nl; l++)
+    CKM(cudaMemcpy(s->d_opptrs + 14 * l, m->lev[l].op64, sizeof(double*) * 14,
+                   cudaMemcpyHostToDevice));
+  // FP32 storage (filled by mixed_refresh)
+  for (int l = lo; l < nl; l++) {
     MLevel& L = m->lev[l];
     const size_t n = L.g.n();
-    for (int c = 0; c < L.nop; c++) {
+    for (int c = 0; c < L.nop; c++)
       if (!falloc(&L.op[c], n)) return 0;
-      to_f32(st, L.op64[c], L.op[c], n);
-      note_launches(1);
-    }
     if (!falloc(&L.cc, n) || !falloc(&L.w0, n) || !falloc(&L.x, n)) return 0;
   }
-  if (!falloc(&m->r, s->n) || !falloc(&m->w2, s->n)) return 0;
+  m->stale = 1;
+  const size_t nscr = m->lev[lo].g.n();
+  if (!falloc(&m->r, nscr) || !falloc(&m->w2, nscr)) return 0;
   const Grid gc = m->lev[nl - 1].g;
   m->nd = (gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2);
   if (m->nd > 4096) {
@@ -880,7 +1032,7 @@ int mixed_setup(pmgb_solver* s) {
   CKM(cudaMalloc(&m->dinfo, sizeof(int) * 4));
   // levels small enough for one cluster run in the tail kernel
   m->tail_first = 0;
-  for (int l = 1; l < nl; l++) {
+  for (int l = (lo > 0 ? lo : 1); l < nl; l++) {
     const Grid g = m->lev[l].g;
     if ((size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2) <= 70000) {
       m->tail_first = l;
@@ -900,6 +1052,8 @@ int mixed_setup(pmgb_solver* s) {
     CKM(cudaMemcpy(m->d_tlev, tl.data(), sizeof(TLev) * nl, cudaMemcpyHostToDevice));
     m->tail_cluster = 16;
     if (cudaFuncSetAttribute(k_vcycle_tail<16>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1) != cudaSuccess ||
+        cudaFuncSetAttribute(k_coarse_exact<16>, cudaFuncAttributeNonPortableClusterSizeAllowed,
                              1) != cudaSuccess) {
       cudaGetLastError();
       m->tail_cluster = 8;
@@ -914,14 +1068,42 @@ int mixed_setup(pmgb_solver* s) {
       attr[0].val.clusterDim.z = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
-      int ncl = 0;
-      if (cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_tail<16>, &cfg) != cudaSuccess || ncl < 1) {
+      int ncl = 0, ncl2 = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, k_vcycle_tail<16>, &cfg) != cudaSuccess || ncl < 1 ||
+          cudaOccupancyMaxActiveClusters(&ncl2, k_coarse_exact<16>, &cfg) != cudaSuccess ||
+          ncl2 < 1) {
         cudaGetLastError();
         m->tail_cluster = 8;
       }
     }
   }
   CKM(cudaStreamSynchronize(st));
+  return 1;
+}
+
+int mixed_setup(pmgb_solver* s) { return mixed_setup_from(s, 0); }
+
+// Galerkin operators of the extra levels and the FP32 copies of every
+// level's operator, after each rebuild of the FP64 hierarchy.
+int mixed_refresh(pmgb_solver* s) {
+  MixedState* m = s->mixed;
+  if (!m->stale) return 1;
+  cudaStream_t st = s->stream;
+  for (int l = s->nlev; l < m->nlev; l++) {
+    launch_galerkin(st, m->lev[l - 1].g, m->lev[l - 1].ops64(), m->lev[l].g,
+                    s->d_opptrs + 14 * l);
+    note_launches(1);
+  }
+  for (int l = m->lo; l < m->nlev; l++) {
+    MLevel& L = m->lev[l];
+    for (int c = 0; c < L.nop; c++) {
+      to_f32(st, L.op64[c], L.op[c], L.g.n());
+      note_launches(1);
+    }
+  }
+  CKM(cudaGetLastError());
+  m->stale = 0;
+  m->cc_ready = 0;
   return 1;
 }
 
@@ -933,7 +1115,12 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
   for (int l = 0; l < m->nlev; l++) {
     MLevel& L = m->lev[l];
     const double* src;
-    if (l < s->nlev) {
+    if (m->zero_cc) {
+      // band operator below the FP64 hierarchy: no Helmholtz term anywhere
+      if (l < m->lo) continue;
+      CKM(cudaMemsetAsync(L.cc, 0, L.g.n() * sizeof(float), st));
+      src = L.cc64;  // allocated zero and never written
+    } else if (l < s->nlev) {
       src = newton ? s->lev[l].cp : s->lev[l].cc;
     } else {
       const double* prev = (l - 1 < s->nlev) ? (newton ? s->lev[l - 1].cp : s->lev[l - 1].cc)
@@ -942,8 +1129,10 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       note_launches(1);
       src = L.cc64;
     }
-    to_f32(st, src, L.cc, L.g.n());
-    note_launches(1);
+    if (l >= m->lo && !m->zero_cc) {
+      to_f32(st, src, L.cc, L.g.n());
+      note_launches(1);
+    }
     if (l == m->nlev - 1) {
       // dense factor of (A_c + cc) on the coarsest level
       const int nd = m->nd;
@@ -1146,7 +1335,7 @@ int refine(pmgb_solver* s, int newton, const double* cc64, const double* fc64, d
 // with s->lev[*].cp and .rhs in place): xt = 0 and refine until
 // ||rhs - J xt||_1 <= errtol_s.
 int mixed_newton_inner(pmgb_solver* s, double errtol_s) {
-  if (!mixed_setup(s)) return 0;
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   if (!mixed_set_cc(s, 1)) return 0;
   Level& F = s->lev[0];
   CKM(cudaMemsetAsync(F.xt, 0, s->n * sizeof(double), s->stream));
@@ -1157,7 +1346,7 @@ int mixed_newton_inner(pmgb_solver* s, double errtol_s) {
 // One FP32 fine-level half-sweep for kernel timing; 6 FP32 arrays read and
 // x read/written: 14 B per point per half-sweep.
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
-  if (!mixed_setup(s)) return 0;
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
   const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
@@ -1170,7 +1359,7 @@ int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
 // One FP32 fine smoothing call (2 sweeps + residual) for kernel timing:
 // (2 x 28 + 28) B per point.
 int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
-  if (!mixed_setup(s)) return 0;
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
   if (gs7_f32(s->stream, F, F.x, m->r, 1) != cudaSuccess) {
@@ -1186,10 +1375,10 @@ int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
 // damping pass read 14 coefficients + cc + f + x (72 B per point each) and
 // the interpolation writes x: 6 x 72 + 8 = 440 B per interior point.
 int mixed_time_tail(pmgb_solver* s, double* bytes) {
-  if (!mixed_setup(s)) return 0;
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
-  if (m->tail_first <= 0) {
-    set_error("pmgb_time_kernel: this grid has no tail levels");
+  if (m->lo != 0 || m->tail_first <= 0) {
+    set_error("pmgb_time_kernel: no mixed-precision tail levels in this calculation");
     return 0;
   }
   if (!launch_tail(s, s->stream)) return 0;
@@ -1203,8 +1392,94 @@ int mixed_time_tail(pmgb_solver* s, double* bytes) {
   return 1;
 }
 
+// FP64 path, LPBE: prepare the exact coarse solve of the FP64 coarsest level
+// (FP32 Galerkin levels below it and the dense inverse at the bottom).
+// Returns 1 when it is available, 0 when the band solve must be used.
+int coarse_exact_prepare(pmgb_solver* s) {
+  const int lo = s->nlev - 1;
+  if (!s->mixed) {
+    if (!mixed_setup_from(s, lo)) {
+      // e.g. a coarsest level that cannot be coarsened further: fall back
+      if (s->mixed) {
+        mixed_destroy(s->mixed);
+        s->mixed = nullptr;
+      }
+      cudaGetLastError();
+      return 0;
+    }
+  }
+  MixedState* m = s->mixed;
+  if (m->lo != lo || m->nlev <= lo + 1) return 0;
+  // B, the operator the reference's band solve inverts
+  cudaStream_t st = s->stream;
+  MLevel& L = m->lev[lo];
+  const Grid g = L.g;
+  const int nint = (g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  OpW b;
+  for (int c = 0; c < 14; c++) {
+    b.c[c] = L.op64[c];
+    CKM(cudaMemsetAsync(b.c[c], 0, g.n() * sizeof(double), st));
+  }
+  CKM(cudaMemsetAsync(m->d_flag, 0, sizeof(int), st));
+  k_band_restencil<<<blocks_for(nint), kThreads, 0, st>>>(g, s->lev[lo].ops(), b, m->d_flag);
+  note_launches(1);
+  int wrap = 0;
+  CKM(cudaMemcpyAsync(&wrap, m->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKM(cudaStreamSynchronize(st));
+  if (wrap) return 0;  // keep the band factorisation
+  m->stale = 1;
+  if (!mixed_refresh(s)) return 0;
+  if (!mixed_set_cc(s, 0)) return 0;
+  return 1;
+}
+
+int launch_coarse_exact(pmgb_solver* s, cudaStream_t st, const double* cc, const double* b,
+                        double* x) {
+  MixedState* m = s->mixed;
+  const int lo = m->lo;
+  ExactArgs E;
+  E.T.lev = m->d_tlev;
+  E.T.first = lo;
+  E.T.last = m->nlev - 1;
+  E.T.gprev = m->lev[lo].g;
+  E.T.rprev = nullptr;
+  E.T.r = m->w2;
+  E.T.minv = m->dense;
+  E.T.nd = m->nd;
+  E.T.xnum = s->scal + S_TMP;
+  E.T.xden = s->scal + S_TMP;
+  E.g = s->lev[lo].g;
+  for (int c = 0; c < 14; c++) E.op[c] = m->lev[lo].op64[c];
+  E.cc = m->lev[lo].cc64;  // the band matrix has no Helmholtz term
+  (void)cc;
+  E.b = b;
+  E.x = x;
+  E.r = s->w3;
+  E.maxit = 40;
+  E.rtol = 1.0e-12;
+  E.iters = s->d_iters + 8;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(m->tail_cluster, 1, 1);
+  cfg.blockDim = dim3(512, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = m->tail_cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = (m->tail_cluster == 16) ? cudaLaunchKernelEx(&cfg, k_coarse_exact<16>, E)
+                                          : cudaLaunchKernelEx(&cfg, k_coarse_exact<8>, E);
+  if (e != cudaSuccess) {
+    set_error("exact coarse solve launch: %s", cudaGetErrorString(e));
+    return 0;
+  }
+  return 1;
+}
+
 int mixed_solve(pmgb_solver* s, double errtol) {
-  if (!mixed_setup(s)) return 0;
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   CKM(cudaMemsetAsync(s->lev[0].x, 0, s->n * sizeof(double), s->stream));
   if (!s->p.nonlin) {
     if (!s->mixed->cc_ready && !mixed_set_cc(s, 0)) return 0;

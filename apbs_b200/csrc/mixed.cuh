@@ -9,6 +9,7 @@ struct MixedState;
 // FP64 solution in s->lev[0].x (Dirichlet values not yet restored).
 int mixed_solve(pmgb_solver* s, double errtol);
 void mixed_destroy(MixedState* m);
+void mixed_mark_stale(MixedState* m);
 // Inner linear solve of one Newton step in mixed precision.
 int mixed_newton_inner(pmgb_solver* s, double errtol_s);
 // Damped inexact Newton driver (solver.cu); mixed selects the inner solver.
@@ -17,4 +18,9 @@ void set_error(const char* fmt, ...);
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
 int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes);
 int mixed_time_tail(pmgb_solver* s, double* bytes);
+// FP64 path, LPBE: exact-to-round-off solve of the FP64 coarsest level
+// (FP64 refinement over FP32 V-cycles of extra Galerkin levels).
+int coarse_exact_prepare(pmgb_solver* s);
+int launch_coarse_exact(pmgb_solver* s, cudaStream_t st, const double* cc, const double* b,
+                        double* x);
 }  // namespace pmgb

@@ -290,6 +290,14 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
   if (ok) ok &= (cudaMalloc(&s->d_iters, 16 * sizeof(int)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_info, 16 * sizeof(int)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_npts, sizeof(int)) == cudaSuccess);
+  if (ok) ok &= (cudaMalloc(&s->d_opptrs, sizeof(double*) * 14 * 16) == cudaSuccess);
+  if (ok) {
+    // the operator arrays never move, so the pointer table is written once
+    double* tab[14 * 16] = {nullptr};
+    for (int l = 0; l < s->nlev; l++)
+      for (int c = 0; c < 14; c++) tab[14 * l + c] = s->lev[l].op[c];
+    ok &= (cudaMemcpy(s->d_opptrs, tab, sizeof(tab), cudaMemcpyHostToDevice) == cudaSuccess);
+  }
   if (!ok) {
     pmgb_destroy(s);
     return 0;
@@ -362,6 +370,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->w1); dfree(s->w2); dfree(s->w3);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
+  dfree(s->d_opptrs);
   dfree(s->band);
   dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
@@ -617,21 +626,27 @@ static int build_ops(pmgb_solver* s) {
                     s->charge, s->gx, s->gy, s->gz, F.op[OC], F.op[OE], F.op[ON], F.op[UC],
                     F.cc, F.fc);
   note_launches(2);
-  double** dptrs = nullptr;
-  CK(cudaMalloc(&dptrs, sizeof(double*) * 14 * s->nlev));
   for (int l = 1; l < s->nlev; l++) {
     Level& C = s->lev[l];
     Level& P = s->lev[l - 1];
-    CK(cudaMemcpyAsync(dptrs + 14 * l, C.op, sizeof(double*) * 14, cudaMemcpyHostToDevice, st));
-    launch_galerkin(st, P.g, P.ops(), C.g, dptrs + 14 * l);
+    launch_galerkin(st, P.g, P.ops(), C.g, s->d_opptrs + 14 * l);
     launch_restrict(st, P.g, P.cc, C.g, C.cc);
     launch_restrict(st, P.g, P.fc, C.g, C.fc);
     note_launches(3);
   }
-  CK(cudaStreamSynchronize(st));
-  cudaFree(dptrs);
-  // coarsest direct solve for the linear problem (Vbuildband, buildBd.c:57-117)
-  s->mgsolv = s->p.nonlin ? 0 : 1;
+  // the mixed-precision path re-derives its FP32 hierarchy from these
+  if (s->mixed) mixed_mark_stale(s->mixed);
+  // coarsest direct solve for the linear problem (Vbuildband, buildBd.c:57-117);
+  // the mixed-precision path solves its own, coarser, level densely instead
+  s->mgsolv = (s->p.nonlin || s->precision == PMGB_MIXED) ? 0 : 1;
+  if (s->mgsolv == 1) {
+    // a coarsest level above 512 unknowns is solved by exact refinement
+    // instead: the banded factor and its substitutions are sequential
+    const Grid gc = s->lev[s->nlev - 1].g;
+    if ((size_t)(gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2) > 512 && g_tune[4] == 0 &&
+        coarse_exact_prepare(s))
+      s->mgsolv = 2;
+  }
   if (s->mgsolv == 1) {
     Level& C = s->lev[s->nlev - 1];
     const int ex = C.g.nx - 2, exy = (C.g.nx - 2) * (C.g.ny - 2);
@@ -707,6 +722,9 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     Level& C = s->lev[nlev - 1];
     if (s->mgsolv == 1) {
       launch_band_solve(st, C.g, s->band, s->bn, s->bm, s->blda, C.w0, X(nlev - 1));
+      k++;
+    } else if (s->mgsolv == 2) {
+      if (!launch_coarse_exact(s, st, CC(nlev - 1), C.w0, X(nlev - 1))) return 0;
       k++;
     } else {
       launch_zero(st, X(nlev - 1), C.g.n());
@@ -912,7 +930,7 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
   CK(cudaEventRecord(s->ev[2], st));
   if (!s->built && !build_ops(s)) return 0;
   CK(cudaEventRecord(s->ev[3], st));
-  s->st.coarse_method = s->mgsolv;
+  s->st.coarse_method = (s->precision == PMGB_MIXED) ? 2 : (s->mgsolv == 2 ? 3 : s->mgsolv);
   const double errtol = (s->p.etol > 0.0) ? s->p.etol : 1.0e-6;
   int ok;
   if (s->precision == PMGB_MIXED) {
@@ -1069,6 +1087,11 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
                                 double* bytes) {
   if (!s || !s->built || reps < 1) {
     set_error("pmgb_time_kernel: solve first");
+    return 0;
+  }
+  if ((which == PMGB_K_GS7_FP32 || which == PMGB_K_GS7_PIPE_FP32 ||
+       which == PMGB_K_VCYCLE_TAIL) && s->precision != PMGB_MIXED) {
+    set_error("pmgb_time_kernel: kernel %d belongs to the mixed-precision path", which);
     return 0;
   }
   cudaStream_t st = s->stream;

@@ -70,6 +70,7 @@ struct pmgb_solver {
   double *nw_r0, *nw_ws, *nw_keepx, *nw_keepr;  // Newton work vectors
   double* part;
   double* scal;
+  double** d_opptrs;  // device table of operator pointers, 14 per level (16 levels)
   int* d_iters;
   int* d_info;
   // coarsest direct solve

@@ -46,7 +46,8 @@ typedef struct pmgb_stats {
     int vcycles;          /* V-cycles executed (all Newton steps included) */
     int newton_iters;     /* Newton iterations (NPBE), 0 for LPBE */
     int refinements;      /* outer refinement steps (PMGB_MIXED) */
-    int coarse_method;    /* 1 band Cholesky, 0 conjugate gradients */
+    int coarse_method;    /* coarsest solve: 0 conjugate gradients, 1 band Cholesky,
+                             2 dense inverse (mixed), 3 exact refinement (FP64, large) */
     double rel_residual;  /* final relative residual of the stopping test */
     double t_fill_ms;     /* coefficient fill, device time */
     double t_setup_ms;    /* operator build + Galerkin + coarse factor */
@@ -146,6 +147,9 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_GS7_BLOCKS_PER_SM 1  /* CTAs per SM of the pipelined smoother (0 = max) */
 #define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 (0 = auto) */
 #define PMGB_TUNE_GS7_PIPELINED 3      /* 1: temporally blocked fine smoother, 0: colour passes */
+#define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded
+                                          Cholesky of the reference, 0: exact refinement
+                                          above 512 unknowns */
 int pmgb_set_tuning(int key, int value);
 int pmgb_get_tuning(int key);
 

@@ -43,3 +43,26 @@ def test_mixed_matches_fp64(name, mol, params):
     assert abs(emx - e64) <= TOL_E * abs(e64)
     assert np.abs(umx - u64).max() <= TOL_U * np.abs(u64).max()
     assert st["rel_residual"] <= 1e-6
+
+
+@pytest.mark.parametrize("npbe", [False, True], ids=["lpbe", "npbe"])
+def test_solver_reuse_across_molecules(npbe):
+    """A calculation refilled with another molecule gives the answer of a
+    fresh one (the FP32 hierarchy follows every operator rebuild)."""
+    ions = ((1, 0.1, 2.0), (-1, 0.1, 2.0))
+    ma = synth.cluster(150, 8.0, seed=21)
+    mb = synth.cluster(150, 8.0, seed=22, net_charge=2.0)
+    p = synth.mg_manual(33, 0.6, ma.center(), npbe=npbe, ions=ions)
+    for prec in (FP64, MIXED):
+        fresh = {}
+        for name, m in (("a", ma), ("b", mb)):
+            with Vpmg(p, prec) as pmg:
+                pmg.fillco(m)
+                pmg.solve()
+                fresh[name] = pmg.energy()
+        with Vpmg(p, prec) as pmg:
+            for name, m in (("a", ma), ("b", mb), ("a", ma)):
+                pmg.fillco(m)
+                pmg.solve()
+                e = pmg.energy()
+                assert abs(e - fresh[name]) <= 1e-10 * abs(fresh[name]), (prec, name)

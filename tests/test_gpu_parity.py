@@ -90,3 +90,29 @@ def test_repeat_solve_is_deterministic():
         e2, u2 = pmg.energy(), pmg.u
     assert abs(e1 - e2) <= 1e-13 * abs(e1)
     assert np.abs(u1 - u2).max() <= 1e-13 * np.abs(u1).max()
+
+
+def test_exact_coarse_solve_matches_band():
+    """Above 512 coarsest unknowns the FP64 LPBE path solves the coarsest level
+    by exact refinement instead of the reference's banded Cholesky; both are
+    exact to round-off, so the two runs agree far inside the parity bar."""
+    from apbs_b200.vpmg import TUNE_BAND_ALWAYS, get_tuning, set_tuning
+    m = synth.cluster(400, 12.0, seed=7)
+    p = synth.mg_manual(49, 0.8, m.center())
+    out = {}
+    old = get_tuning(TUNE_BAND_ALWAYS)
+    try:
+        for band in (1, 0):
+            set_tuning(TUNE_BAND_ALWAYS, band)
+            with Vpmg(p, FP64) as pmg:
+                pmg.fillco(m)
+                pmg.solve()
+                out[band] = (pmg.energy(), pmg.u, pmg.residual_history(), pmg.stats())
+    finally:
+        set_tuning(TUNE_BAND_ALWAYS, old)
+    assert out[1][3]["coarse_method"] == 1 and out[0][3]["coarse_method"] == 3
+    assert len(out[1][2]) == len(out[0][2])
+    np.testing.assert_allclose(out[0][2], out[1][2], rtol=1e-9)
+    scale = np.abs(out[1][1]).max()
+    assert np.abs(out[0][1] - out[1][1]).max() <= 1e-12 * scale
+    assert abs(out[0][0] - out[1][0]) <= 1e-12 * abs(out[1][0])
