@@ -115,14 +115,15 @@ int gs7_blocks_per_sm();
 // requested CTAs per SM).
 template <typename T>
 inline int gs7_pipe_grid() {
-  static int nsm = 0, per = 0;
-  if (nsm == 0) {
-    int dev = 0;
+  // initialised once, thread-safely (function-local static)
+  static const int2 sm_per = [] {
+    int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gs7_pipe<T>, 256, 0);
-    if (per < 1) per = 1;
-  }
+    return make_int2(nsm, per < 1 ? 1 : per);
+  }();
+  const int nsm = sm_per.x, per = sm_per.y;
   int want = gs7_blocks_per_sm();
   int use = (want > 0 && want < per) ? want : per;
   return nsm * use;

@@ -1109,6 +1109,8 @@ int mixed_refresh(pmgb_solver* s) {
 
 // Helmholtz term on every mixed level from the fine FP64 term cc0:
 // restrict through the FP64 levels (where not already present) and convert.
+constexpr size_t kDenseSmemMax = 200 * 1024;
+
 int mixed_set_cc(pmgb_solver* s, int newton) {
   MixedState* m = s->mixed;
   cudaStream_t st = s->stream;
@@ -1139,10 +1141,12 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, st>>>(L.g, L.ops64(), src,
                                                                        m->dense, nd);
       const size_t smem = (size_t)nd * nd * sizeof(double);
-      const int use_smem = smem <= 200 * 1024;
-      if (use_smem)
-        cudaFuncSetAttribute(k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+      const int use_smem = smem <= kDenseSmemMax;
+      // the attribute is set once, to the largest size any call uses: calls
+      // from concurrent host threads would otherwise race on it
+      static const cudaError_t attr = cudaFuncSetAttribute(
+          k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmemMax);
+      (void)attr;
       k_dense_inverse<<<1, 1024, use_smem ? smem : 0, st>>>(m->dense, nd, use_smem, m->dinfo);
       note_launches(2);
     }

@@ -88,6 +88,26 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+// Stream-ordered (re)allocation with geometric growth: a calculation reused
+// for a larger molecule neither synchronises the device (as cudaFree does)
+// nor reallocates for every small increase.
+template <typename T>
+int grow(T** p, size_t* cap, size_t need, cudaStream_t st) {
+  if (*p && need <= *cap) return 1;
+  const size_t n = std::max(need, *cap + *cap / 2);
+  if (*p) cudaFreeAsync(*p, st);
+  *p = nullptr;
+  *cap = 0;
+  const cudaError_t e = cudaMallocAsync((void**)p, std::max<size_t>(n, 1) * sizeof(T), st);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    set_error("cudaMallocAsync(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    return 0;
+  }
+  *cap = n;
+  return 1;
+}
+
 // Vpbe_ctor2 scalars (src/generic/vpbe.c:264-411) and the ion tables of
 // Vpmg_ctor2 (src/mg/vpmg.c:340-377).
 void phys_setup(pmgb_solver* s, int natoms, const double* xyz, const double* r) {
@@ -177,12 +197,15 @@ int read_scalar(pmgb_solver* s, int slot, double* v) {
 }
 
 // GS27 launch shape per level (cluster of CTAs for the wavefront).
-int g_max_cluster = 0;
+int max_cluster() {
+  static const int mc = mg_init();  // probed once, thread-safely
+  return mc;
+}
 
 Gs27Plan plan_for(Grid g) {
   const int ni = std::max(g.nx, std::max(g.ny, g.nz)) - 2;
   Gs27Plan p;
-  if (g_max_cluster == 0) g_max_cluster = mg_init();
+  const int g_max_cluster = max_cluster();
   if (g_tune[2] > 0) {
     p.cluster = std::min(g_tune[2], g_max_cluster);
     p.threads = (p.cluster >= 8) ? 512 : 256;
@@ -200,6 +223,8 @@ Gs27Plan plan_for(Grid g) {
 // ===========================================================================
 // construction
 // ===========================================================================
+static int set_geometry(pmgb_solver* s);
+
 extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver** out) {
   *out = nullptr;
   if (!params) {
@@ -302,7 +327,26 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     pmgb_destroy(s);
     return 0;
   }
-  // Geometry (Vpmg_fillco, vpmg.c:5332-5366) and the coordinate arrays.
+  if (!set_geometry(s)) {
+    pmgb_destroy(s);
+    return 0;
+  }
+  s->vc_exec[0] = s->vc_exec[1] = nullptr;
+  s->vc_kernels[0] = s->vc_kernels[1] = 0;
+  // the allocations above zero-fill on the legacy stream
+  if (cudaStreamSynchronize(0) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    set_error("pmgb_create: device error during setup");
+    pmgb_destroy(s);
+    return 0;
+  }
+  *out = s;
+  return 1;
+}
+
+// Geometry (Vpmg_fillco, vpmg.c:5332-5366), the coordinate arrays and the
+// partition weights of the calculation's domain, from s->p.
+static int set_geometry(pmgb_solver* s) {
+  const pmgb_params& p = s->p;
   {
     const double xlen = (p.nx - 1) * p.hx, ylen = (p.ny - 1) * p.hy, zlen = (p.nz - 1) * p.hz;
     s->G.g = s->g;
@@ -328,29 +372,109 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     cudaMemcpy(s->zf, zf.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice);
     cudaMemcpy(s->wx, wx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice);
     cudaMemcpy(s->wy, wy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->wz, wz.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice);
+    cudaStream_t st = s->stream;
+    CK(cudaMemcpyAsync(s->xf, xf.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->yf, yf.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->zf, zf.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->wx, wx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->wy, wy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->wz, wz.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
   }
-  s->vc_exec[0] = s->vc_exec[1] = nullptr;
-  s->vc_kernels[0] = s->vc_kernels[1] = 0;
-  if (cudaDeviceSynchronize() != cudaSuccess) {
-    set_error("pmgb_create: device error during setup");
-    pmgb_destroy(s);
+  return 1;
+}
+
+extern "C" int pmgb_reconfigure(pmgb_solver* s, const pmgb_params* params) {
+  if (!s || !params) {
+    set_error("pmgb_reconfigure: null argument");
     return 0;
   }
-  *out = s;
+  const pmgb_params& p = *params;
+  if (p.nx != s->p.nx || p.ny != s->p.ny || p.nz != s->p.nz || p.nlev != s->p.nlev) {
+    set_error("pmgb_reconfigure: grid %dx%dx%d/%d differs from the calculation's %dx%dx%d/%d",
+              p.nx, p.ny, p.nz, p.nlev, s->p.nx, s->p.ny, s->p.nz, s->p.nlev);
+    return 0;
+  }
+  if (p.nion < 0 || p.nion > PMGB_MAXION) {
+    set_error("pmgb_reconfigure: nion %d outside 0..%d", p.nion, PMGB_MAXION);
+    return 0;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->p = p;
+  if (!set_geometry(s)) return 0;
+  s->filled = s->solved = s->built = 0;
+  s->focused = 0;
+  s->ext_qf = s->ext_di = s->ext_qm = 0.0;
+  memset(&s->st, 0, sizeof(s->st));
   return 1;
 }
 
 extern "C" int pmgb_set_stream(pmgb_solver* s, void* stream) {
   if (!s) return 0;
-  CK(cudaStreamSynchronize(s->stream));
-  for (int m = 0; m < 2; m++)
-    if (s->vc_exec[m]) {
-      cudaGraphExecDestroy(s->vc_exec[m]);
-      s->vc_exec[m] = nullptr;
-    }
+  const cudaError_t e = cudaStreamSynchronize(s->stream);
+  // switch even after an error, so no stale stream handle is kept; captured
+  // V-cycle graphs hold no stream and stay valid
   s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+  if (e != cudaSuccess) {
+    set_error("pmgb_set_stream: %s", cudaGetErrorString(e));
+    return 0;
+  }
   return 1;
+}
+
+// Device bytes one calculation holds once filled and solved: the maps,
+// the level hierarchy with its work vectors, the FP32 hierarchy (mixed
+// precision, or the FP64 path's exact coarsest solve), the banded factor
+// of a small FP64 coarsest level, and per-atom fill work (accessible-
+// surface flags dominate: ~4 pi (r_max + srad)^2 sdens reference points per
+// atom, with r_max taken as 3 A).
+extern "C" size_t pmgb_footprint(const pmgb_params* params, int precision, int natoms) {
+  if (!params) return 0;
+  const pmgb_params& p = *params;
+  size_t nl[16];
+  int gx[16], gy[16], gz[16];
+  int nlev = p.nlev < 1 ? 1 : (p.nlev > 12 ? 12 : p.nlev);
+  gx[0] = p.nx; gy[0] = p.ny; gz[0] = p.nz;
+  for (int l = 1; l < nlev; l++) {
+    gx[l] = (gx[l - 1] - 1) / 2 + 1;
+    gy[l] = (gy[l - 1] - 1) / 2 + 1;
+    gz[l] = (gz[l - 1] - 1) / 2 + 1;
+  }
+  for (int l = 0; l < nlev; l++) nl[l] = (size_t)gx[l] * gy[l] * gz[l];
+  const size_t n = nl[0];
+  size_t d = 0;  // doubles
+  d += 6 * n + 3 * n + 3 * n + 4 * n;  // maps, smoothing scratch, w1-3, Newton vectors
+  d += 2 * ((size_t)p.ny * p.nz + (size_t)p.nx * p.nz + (size_t)p.nx * p.ny);
+  d += 2 * (size_t)(p.nx + p.ny + p.nz) + 16 + 4 * 1184 + 64 + S_COUNT;
+  for (int l = 0; l < nlev; l++) d += (size_t)((l == 0 ? 4 : 14) + 7) * nl[l];
+  size_t bytes = d * sizeof(double);
+  // FP32 hierarchy from level lo, plus Galerkin levels down to <= 512 unknowns
+  const int lo = (precision == PMGB_MIXED) ? 0 : nlev - 1;
+  const size_t nc_int = (size_t)(gx[nlev - 1] - 2) * (gy[nlev - 1] - 2) * (gz[nlev - 1] - 2);
+  const bool fp32 = (precision == PMGB_MIXED) || (!p.nonlin && nc_int > 512);
+  if (fp32) {
+    for (int l = lo; l < nlev; l++)
+      bytes += (size_t)((l == 0 ? 4 : 14) + 3) * nl[l] * sizeof(float);
+    if (precision != PMGB_MIXED) bytes += 15 * nl[lo] * sizeof(double);
+    int cx = gx[nlev - 1], cy = gy[nlev - 1], cz = gz[nlev - 1];
+    size_t nint = nc_int;
+    while (nint > 512 && (cx - 1) % 2 == 0 && (cy - 1) % 2 == 0 && (cz - 1) % 2 == 0 && cx > 3) {
+      cx = (cx - 1) / 2 + 1;
+      cy = (cy - 1) / 2 + 1;
+      cz = (cz - 1) / 2 + 1;
+      const size_t nc = (size_t)cx * cy * cz;
+      bytes += 15 * nc * sizeof(double) + 17 * nc * sizeof(float);
+      nint = (size_t)(cx - 2) * (cy - 2) * (cz - 2);
+    }
+    bytes += 2 * nl[lo] * sizeof(float) + nint * nint * sizeof(double);
+  } else if (!p.nonlin) {
+    const size_t ex = gx[nlev - 1] - 2, exy = ex * (gy[nlev - 1] - 2);
+    bytes += ((exy + ex + 2) * nc_int + nc_int) * sizeof(double);
+  }
+  const double pi = 3.14159265358979323846;
+  const double nref = 4.0 * pi * (3.0 + p.srad) * (3.0 + p.srad) * (p.sdens > 0 ? p.sdens : 10.0);
+  bytes += (size_t)natoms * ((size_t)nref + 64 + 18 * sizeof(double) + 2 * sizeof(int));
+  return bytes;
 }
 
 extern "C" void pmgb_destroy(pmgb_solver* s) {
@@ -375,7 +499,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
   dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref); dfree(s->atom_terms);
-  if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
+  dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
   cudaStreamDestroy(s->own_stream);
   delete s;
@@ -416,12 +540,8 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
       const int nsphere = (int)ceil(maxarea * p.sdens);
       std::vector<double> ref;
       const int nref = ref_sphere(nsphere, ref);
-      if (nref != s->nref) {
-        dfree(s->d_ref);
-        s->d_ref = nullptr;
-        if (!dalloc(&s->d_ref, 3 * (size_t)nref)) return 0;
-        s->nref = nref;
-      }
+      if (!grow(&s->d_ref, &s->ref_alloc, 3 * (size_t)nref, st)) return 0;
+      s->nref = nref;
       CK(cudaMemcpyAsync(s->d_ref, ref.data(), sizeof(double) * 3 * nref,
                          cudaMemcpyHostToDevice, st));
       // atom cell grid
@@ -439,26 +559,24 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
         C.n[d] = (int)ceil((hi[d] - C.lo[d]) / C.cs) + 2;
         ncell *= C.n[d];
       }
-      if (ncell + 1 > s->ncell_alloc) {
-        dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos);
-        CK(cudaMalloc(&s->cell_count, sizeof(int) * (ncell + 1)));
-        CK(cudaMalloc(&s->cell_start, sizeof(int) * (ncell + 1)));
-        CK(cudaMalloc(&s->cell_fillpos, sizeof(int) * (ncell + 1)));
-        s->ncell_alloc = ncell + 1;
-      }
-      if (!s->cell_of) {
-        CK(cudaMalloc(&s->cell_of, sizeof(int) * std::max(natoms, 1)));
-        CK(cudaMalloc(&s->cell_sorted, sizeof(int) * std::max(natoms, 1)));
+      {
+        size_t c1 = s->ncell_alloc, c2 = s->ncell_alloc, c3 = s->ncell_alloc;
+        if (!grow(&s->cell_count, &c1, (size_t)ncell + 1, st) ||
+            !grow(&s->cell_start, &c2, (size_t)ncell + 1, st) ||
+            !grow(&s->cell_fillpos, &c3, (size_t)ncell + 1, st))
+          return 0;
+        s->ncell_alloc = std::min(c1, std::min(c2, c3));
+        size_t a1 = s->cellof_alloc, a2 = s->cellof_alloc;
+        if (!grow(&s->cell_of, &a1, (size_t)natoms, st) ||
+            !grow(&s->cell_sorted, &a2, (size_t)natoms, st))
+          return 0;
+        s->cellof_alloc = std::min(a1, a2);
       }
       launch_cell_build(st, C, natoms, s->d_xyz, s->cell_count, s->cell_start,
                         s->cell_fillpos, s->cell_of, s->cell_sorted);
       note_launches(3);
       const size_t nflags = (size_t)natoms * nref;
-      if (nflags > s->sas_flags_alloc) {
-        dfree(s->sas_flags);
-        CK(cudaMalloc(&s->sas_flags, nflags));
-        s->sas_flags_alloc = nflags;
-      }
+      if (!grow(&s->sas_flags, &s->sas_flags_alloc, nflags, st)) return 0;
       launch_sas(st, s->G, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
                  s->cell_start, s->cell_sorted, s->sas_flags, s->d_npts, s->epsx, s->epsy,
                  s->epsz);
@@ -514,12 +632,7 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
     A.pre = (1.6021773e-19 * 1.6021773e-19) /
             (4 * pi * 8.8541878e-12 * 1.3806581e-23 * p.temp);
     A.pre = A.pre * (1.0e10);
-    if (natoms > s->terms_alloc) {
-      dfree(s->atom_terms);
-      s->atom_terms = nullptr;
-      if (!dalloc(&s->atom_terms, 13 * (size_t)natoms)) return 0;
-      s->terms_alloc = natoms;
-    }
+    if (!grow(&s->atom_terms, &s->terms_alloc, 13 * (size_t)natoms, st)) return 0;
     launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
                s->gz);
     note_launches(3);
@@ -544,16 +657,17 @@ extern "C" int pmgb_fillco(pmgb_solver* s, int natoms, const double* xyz, const 
     set_error("pmgb_fillco: bad arguments");
     return 0;
   }
-  if (natoms > s->natoms || !s->own_atoms) {
-    if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
-    s->d_xyz = s->d_q = s->d_r = nullptr;
-    if (!dalloc(&s->d_xyz, 3 * (size_t)natoms) || !dalloc(&s->d_q, natoms) ||
-        !dalloc(&s->d_r, natoms))
+  {
+    size_t c1 = 3 * s->atoms_cap, c2 = s->atoms_cap, c3 = s->atoms_cap;
+    if (!grow(&s->a_xyz, &c1, 3 * (size_t)natoms, s->stream) ||
+        !grow(&s->a_q, &c2, (size_t)natoms, s->stream) ||
+        !grow(&s->a_r, &c3, (size_t)natoms, s->stream))
       return 0;
-    s->own_atoms = 1;
-    dfree(s->cell_of); dfree(s->cell_sorted);
-    s->cell_of = s->cell_sorted = nullptr;
+    s->atoms_cap = std::min(c1 / 3, std::min(c2, c3));
   }
+  s->d_xyz = s->a_xyz;
+  s->d_q = s->a_q;
+  s->d_r = s->a_r;
   s->natoms = natoms;
   CK(cudaMemcpyAsync(s->d_xyz, xyz, sizeof(double) * 3 * natoms, cudaMemcpyHostToDevice,
                      s->stream));
@@ -575,15 +689,9 @@ extern "C" int pmgb_fillco_device(pmgb_solver* s, int natoms, const double* d_xy
   std::vector<double> xyz(3 * (size_t)natoms), r(natoms);
   CK(cudaMemcpy(xyz.data(), d_xyz, sizeof(double) * 3 * natoms, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(r.data(), d_radius, sizeof(double) * natoms, cudaMemcpyDeviceToHost));
-  if (s->own_atoms) { dfree(s->d_xyz); dfree(s->d_q); dfree(s->d_r); }
-  s->own_atoms = 0;
   s->d_xyz = const_cast<double*>(d_xyz);
   s->d_q = const_cast<double*>(d_charge);
   s->d_r = const_cast<double*>(d_radius);
-  if (natoms != s->natoms) {
-    dfree(s->cell_of); dfree(s->cell_sorted);
-    s->cell_of = s->cell_sorted = nullptr;
-  }
   s->natoms = natoms;
   return do_fill(s, xyz.data(), r.data());
 }
@@ -777,7 +885,12 @@ static int vcycle_body(pmgb_solver* s, int newton) {
 }
 
 static int ensure_graph(pmgb_solver* s, int newton) {
+  if (s->vc_exec[newton] && s->vc_mgsolv[newton] != s->mgsolv) {
+    cudaGraphExecDestroy(s->vc_exec[newton]);
+    s->vc_exec[newton] = nullptr;
+  }
   if (s->vc_exec[newton]) return 1;
+  s->vc_mgsolv[newton] = s->mgsolv;
   cudaGraph_t graph;
   CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int ok = vcycle_body(s, newton);

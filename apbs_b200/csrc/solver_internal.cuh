@@ -59,10 +59,11 @@ struct pmgb_solver {
   double *charge, *epsx, *epsy, *epsz, *kappa, *ccf;
   double *gx, *gy, *gz, *xf, *yf, *zf, *wx, *wy, *wz, *mom;
   double* tmp3;  // 3N scratch for smoothing
-  // atoms
+  // atoms (d_* point at the owned buffers a_* or at the caller's arrays)
   int natoms;
   double *d_xyz, *d_q, *d_r;
-  int own_atoms;
+  double *a_xyz, *a_q, *a_r;
+  size_t atoms_cap;
   // hierarchy
   int nlev;
   Level lev[12];
@@ -78,15 +79,17 @@ struct pmgb_solver {
   double* band;
   int bn, bm, blda;
   // fill work
+  // fill work, grown stream-ordered and geometrically (never shrinks)
   int *cell_count, *cell_start, *cell_fillpos, *cell_of, *cell_sorted;
-  int ncell_alloc;
+  size_t ncell_alloc, cellof_alloc;
   unsigned char* sas_flags;
   size_t sas_flags_alloc;
   double* d_ref;
   int nref;
+  size_t ref_alloc;
   int* d_npts;
   double* atom_terms;  // 13 x natoms sdh moment terms
-  int terms_alloc;
+  size_t terms_alloc;
   // focusing: faces set from a coarse solution, energies outside the domain
   int focused;
   double ext_qf, ext_di, ext_qm;
@@ -101,6 +104,7 @@ struct pmgb_solver {
   // graphs of one V-cycle (linear / Newton system)
   cudaGraphExec_t vc_exec[2];
   long long vc_kernels[2];
+  int vc_mgsolv[2];  // coarsest-solve kind each graph was captured with
   pmgb::MixedState* mixed;
 };
 

@@ -193,3 +193,50 @@ def config2(seed: int = 1):
     pc, pf = focus_pair(mol, 97, 1.0, 129, 0.35, subregion_center(mol, 30, seed + 100),
                         ions=((1.0, 0.1, 2.0), (-1.0, 0.1, 2.0)))
     return mol, pc, pf
+
+
+def _rotation(rng) -> np.ndarray:
+    """Uniform random rotation (QR of a Gaussian matrix, sign-fixed)."""
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q = q * np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q
+
+
+def binding_sweep(npose: int = 64, seed: int = 3, rec_atoms: int = 3000, rec_radius: float = 20.0,
+                  lig_atoms: int = 40, lig_radius: float = 5.0, rec_dime: int = 129,
+                  lig_dimes=(33, 49, 65), h: float = 0.55,
+                  ions=((1.0, 0.15, 2.0), (-1.0, 0.15, 2.0)), etol: float = 0.0):
+    """Binding-energy sweep: a receptor cluster and `npose` seeded rigid poses
+    of a ligand cluster (net charge -1) placed on the receptor surface.
+
+    Returns (receptor job, [(complex job, ligand job)] * npose), each job a
+    (params, molecule) pair, all LPBE.  The receptor and every complex use
+    the same grid (rec_dime^3 at spacing h centred on the receptor); each
+    ligand grid has the same spacing, a dimension drawn from `lig_dimes`, and
+    a centre on the same lattice, so the three energies of a pose share the
+    grid placement and dG = E_complex - E_receptor - E_ligand.  etol is the
+    solver tolerance of every job (0: the default 1e-6)."""
+    rng = np.random.default_rng(seed)
+    rec = cluster(rec_atoms, rec_radius, seed)
+    lig0 = cluster(lig_atoms, lig_radius, seed + 1, net_charge=-1.0)
+    lig0 = Molecule(lig0.xyz - lig0.xyz.mean(axis=0), lig0.charge, lig0.radius)
+    c = rec.center()
+    rec_job = (mg_manual(rec_dime, h, c, ions=ions, etol=etol), rec)
+    half = 0.5 * (rec_dime - 1) * h
+    pairs = []
+    for _ in range(npose):
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        pos = c + d * (rec_radius + lig_radius + 1.5)
+        lig = Molecule(lig0.xyz @ _rotation(rng).T + pos, lig0.charge, lig0.radius)
+        cplx = Molecule(np.vstack([rec.xyz, lig.xyz]), np.concatenate([rec.charge, lig.charge]),
+                        np.concatenate([rec.radius, lig.radius]))
+        assert np.all(np.abs(cplx.xyz - c) < half - 2.0), "complex leaves the grid"
+        dime = int(rng.choice(lig_dimes))
+        # ligand grid centre on the receptor lattice nearest the ligand centre
+        lc = c + np.round((lig.center() - c) / h) * h
+        pairs.append(((mg_manual(rec_dime, h, c, ions=ions, etol=etol), cplx),
+                      (mg_manual(dime, h, lc, ions=ions, etol=etol), lig)))
+    return rec_job, pairs

@@ -158,6 +158,76 @@ def cpu_baseline_sample(args):
                 "sample": "failed: %s" % e}
 
 
+def serving_measurements(args):
+    """The batched and served workloads through the native serving loop:
+    the Poisson request stream (LPBE/NPBE 80/20, grids 33^3-225^3) and the
+    binding-energy sweep (1 receptor + 64 complexes at 129^3, 64 ligands at
+    33^3-65^3), each in mixed precision and in FP64."""
+    import numpy as np
+
+    from apbs_b200 import serve, synth
+    from apbs_b200.vpmg import FP64, MIXED
+    out = {}
+    if args.serve_n > 0:
+        stream = serve.serving_stream(args.serve_n, seed=4, rate=200.0)
+        rec = {"workload": "Poisson arrivals 200/s, %d requests, LPBE/NPBE 80/20, dime "
+                           "{33,65,97,129,161,225}^3, 200-8000 atoms, I ~ U[0,0.3] M (seed 4)"
+                           % args.serve_n,
+               "server": "8 worker streams, budget 80%% of free HBM, warm pools (the stream "
+                         "replayed once untimed so every grid shape is resident)"}
+        for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+            with serve.Server(prec, max_inflight=8) as srv:
+                serve.replay(srv, stream, time_scale=0.0)     # resident calculations
+                r = serve.replay(srv, stream)
+                st = srv.stats()
+            pts = sum(q.params.nx * q.params.ny * q.params.nz for q in stream)
+            errors = sorted({x["error"] for x in r["results"] if x["status"] != 1})
+            rec[name] = {"solves_per_s": r["solves_per_s"], "p50_ms": r["p50_ms"],
+                         "p99_ms": r["p99_ms"], "failed": r["failed"], "errors": errors,
+                         "wall_s": r["wall_s"],
+                         "grid_points_per_s": pts / r["wall_s"],
+                         "mean_service_ms": st["mean_service_ms"],
+                         "inflight_peak": st["inflight_peak"], "bytes_peak": st["bytes_peak"],
+                         "reused": st["reused"], "created": st["created"]}
+            rec[name + "_energies"] = [x["energy_kT"] for x in r["results"]]
+        e_mx = np.array(rec.pop("mixed_energies"))
+        e_64 = np.array(rec.pop("fp64_energies"))
+        both = (e_mx != 0.0) & (e_64 != 0.0)
+        rec["energy_rel_err_max"] = float(np.max(np.abs(e_mx[both] - e_64[both]) /
+                                                 np.abs(e_64[both])))
+        rec["mixed_vs_fp64"] = rec["mixed"]["solves_per_s"] / rec["fp64"]["solves_per_s"]
+        out["serving"] = rec
+    if args.sweep_poses > 0:
+        rec_job, pairs = synth.binding_sweep(args.sweep_poses, etol=1e-9)
+        jobs = [rec_job] + [j for pr in pairs for j in pr]
+        rec = {"workload": "binding sweep: 3000-atom receptor + %d poses of a 40-atom ligand, "
+                           "complexes 129^3 at 0.55 A, ligands 33-65^3 on the same lattice, "
+                           "%d LPBE solves to a 1e-9 relative residual"
+                           % (args.sweep_poses, len(jobs))}
+        energies = {}
+        for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+            with serve.Server(prec, max_inflight=8) as srv:
+                serve.replay(srv, [serve.StreamRequest(0.0, p, m) for p, m in jobs[:16]], 0.0)
+                t0 = time.perf_counter()
+                ids = [srv.submit(p, m) for p, m in jobs]
+                res = [srv.wait(i) for i in ids]
+                wall = time.perf_counter() - t0
+            energies[name] = np.array([x["energy_kT"] for x in res])
+            pts = sum(p.nx * p.ny * p.nz for p, _ in jobs)
+            rec[name] = {"solves_per_s": len(jobs) / wall, "wall_s": wall,
+                         "grid_points_per_s": pts / wall,
+                         "failed": sum(1 for x in res if x["status"] != 1)}
+        kcal = 1.380662e-23 * 298.15 * 6.022045e23 / 4184.0
+        dg = {}
+        for name, e in energies.items():
+            dg[name] = np.array([e[1 + 2 * k] - e[0] - e[2 + 2 * k] for k in range(len(pairs))])
+        rec["dG_max_abs_diff_kcal"] = float(np.max(np.abs(dg["mixed"] - dg["fp64"])) * kcal)
+        rec["dG_range_kcal"] = [float(dg["fp64"].min() * kcal), float(dg["fp64"].max() * kcal)]
+        rec["mixed_vs_fp64"] = rec["mixed"]["solves_per_s"] / rec["fp64"]["solves_per_s"]
+        out["batch"] = rec
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -167,6 +237,10 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c1", "c0"])
     ap.add_argument("--headline", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-n", type=int, default=100,
+                    help="requests in the serving-stream measurement (0 skips it)")
+    ap.add_argument("--sweep-poses", type=int, default=64,
+                    help="poses of the binding-energy sweep measurement (0 skips it)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="profiling mode: run the steps of one precision and nothing else")
     args = ap.parse_args()
@@ -333,6 +407,12 @@ def main():
         smoothers[nm] = {"achieved": ach, "frac": ach / peak, "ms_per_launch": ms_k,
                          "bytes_per_launch": b_k}
 
+    extra = {}
+    if world == 1:
+        for sv in solvers.values():
+            sv.close()
+        extra = serving_measurements(args)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args)
@@ -355,7 +435,7 @@ def main():
                               "energy_rel_err": abs(emix - e64) / abs(e64)},
             "e2e": e2e, "gpu_launches": head["gpu_launches"],
             "roofline": roofline, "smoothers": smoothers,
-            "cpu_baseline": cpu, "clocks": clocks,
+            "cpu_baseline": cpu, "clocks": clocks, **extra,
         }
         print(json.dumps(line), flush=True)
 

@@ -179,6 +179,96 @@ int pmgb_energy_noalloc(const pmgb_params *params, const double *d_u, const doub
                         const double *d_epsx, const double *d_epsy, const double *d_epsz,
                         const double *d_kappa, void *cuda_stream, double *energy_kT);
 
+/* Reuse a calculation for another one on the same grid (nx, ny, nz, nlev):
+ * new centre, spacing, physics and boundary kind; the device arrays stay
+ * allocated.  It has no counterpart in the reference (which builds a new
+ * Vpmg per ELEC block); it lets a serving loop keep grids resident. */
+int pmgb_reconfigure(pmgb_solver *s, const pmgb_params *params);
+
+/* Device bytes a calculation of this shape holds once filled and solved
+ * with natoms atoms (used for admission by HBM footprint). */
+size_t pmgb_footprint(const pmgb_params *params, int precision, int natoms);
+
+/* ------------------------------------------------------------------------
+ * Serving loop: many independent calculations on one GPU.
+ *
+ * A native request loop with no counterpart in the reference (whose main
+ * loop runs ELEC blocks one after another, src/main.c:529).  Requests are
+ * queued in arrival order; `max_inflight` worker threads, each with its own
+ * CUDA stream, take the head of the queue as soon as a worker is free and
+ * the request's device footprint fits the budget next to the calculations
+ * already resident, so requests that arrive while others run are admitted
+ * as slots and memory free up and their work overlaps on the device.
+ * Finished calculations stay resident in a pool keyed by grid shape and are
+ * reused (pmgb_reconfigure) by later requests of that shape; idle ones are
+ * released, oldest first, when a new request needs their memory.
+ * ------------------------------------------------------------------------ */
+typedef struct pmgb_server pmgb_server;
+
+typedef struct pmgb_server_config {
+    int precision;            /* PMGB_FP64 or PMGB_MIXED */
+    int max_inflight;         /* worker slots (concurrent calculations), >= 1 */
+    size_t hbm_budget_bytes;  /* admission limit; 0 = 80% of the device's free memory */
+    int pool_per_shape;       /* idle calculations kept per grid shape:
+                                 0 = max(2, max_inflight), < 0 = none */
+} pmgb_server_config;
+
+typedef struct pmgb_result {
+    int status;               /* 1 done, 0 queued or running, -1 failed */
+    double energy_kT;         /* Vpmg_energy of the calculation */
+    double latency_ms;        /* submit -> done */
+    double queue_ms;          /* submit -> start */
+    double service_ms;        /* start -> done */
+    long long admit_order;    /* 1-based position in the order of admission */
+    pmgb_stats stats;
+    char error[256];
+} pmgb_result;
+
+typedef struct pmgb_server_stats {
+    long long submitted, done, failed;
+    double p50_ms, p99_ms, mean_ms;   /* latency (submit -> done) of finished requests */
+    double mean_service_ms;
+    size_t bytes_in_use, bytes_peak, budget;
+    long long created, reused, evicted; /* calculations built, pooled ones reused, released */
+    int inflight_peak;
+} pmgb_server_stats;
+
+int pmgb_server_create(const pmgb_server_config *config, pmgb_server **out);
+
+/* The device side of the loop as plain callbacks.  pmgb_server_create uses
+ * the CUDA calculation (pmgb_create, pmgb_fillco, pmgb_solve, pmgb_energy);
+ * pmgb_server_create_ex takes a replacement, so the queueing, admission
+ * and pooling logic can be exercised without a GPU. */
+typedef struct pmgb_server_backend {
+    void *ctx;
+    size_t (*footprint)(void *ctx, const pmgb_params *params, int precision, int natoms);
+    void *(*create)(void *ctx, const pmgb_params *params, int precision);
+    int (*reconfigure)(void *ctx, void *calc, const pmgb_params *params);
+    /* fill + solve + energy; returns 1 on success */
+    int (*run)(void *ctx, void *calc, int natoms, const double *xyz, const double *charge,
+               const double *radius, double *energy_kT);
+    void (*destroy)(void *ctx, void *calc);
+} pmgb_server_backend;
+
+int pmgb_server_create_ex(const pmgb_server_config *config, const pmgb_server_backend *backend,
+                          pmgb_server **out);
+/* Queue one calculation (fill from the host atom arrays, solve, energy).
+ * The arrays are copied; u_out, when not NULL, receives the potential
+ * (nx*ny*nz doubles) and must stay valid until the request is done.
+ * Returns the request id (> 0), or 0 when the request can never fit. */
+long long pmgb_server_submit(pmgb_server *srv, const pmgb_params *params, int natoms,
+                             const double *xyz, const double *charge, const double *radius,
+                             double *u_out);
+/* Status of a request without waiting (the return value is result->status). */
+int pmgb_server_poll(pmgb_server *srv, long long id, pmgb_result *result);
+/* Wait for a request to finish. */
+int pmgb_server_wait(pmgb_server *srv, long long id, pmgb_result *result);
+/* Wait until every submitted request has finished. */
+int pmgb_server_drain(pmgb_server *srv);
+int pmgb_server_get_stats(pmgb_server *srv, pmgb_server_stats *stats);
+/* Drain, stop the workers and release every calculation. */
+void pmgb_server_destroy(pmgb_server *srv);
+
 const char *pmgb_last_error(void);
 
 /* Number of kernel launches issued by the calling thread since the last
