@@ -8,6 +8,7 @@
 #include <cooperative_groups.h>
 
 #include "gs7_pipe.cuh"
+#include "gs7_sweep.cuh"
 #include "mg_kernels.cuh"
 
 namespace cg = cooperative_groups;
@@ -376,6 +377,17 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
 }
 
 int g_tune[8] = {8, 0, 0, 0, 0, 0, 0, 0};
+
+int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                       const double* xin, double* xout, int first_parity) {
+  Gs7Sweep<double> a;
+  a.g = g;
+  a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
+  a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
+  a.c1 = first_parity;
+  a.kchunk = 16;
+  return launch_gs7_sweep<double, 32, 8>(s, a) == cudaSuccess;
+}
 
 int gs7_chunk() { return g_tune[0] > 0 ? g_tune[0] : 8; }
 int gs7_blocks_per_sm() { return g_tune[1]; }

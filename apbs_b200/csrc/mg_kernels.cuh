@@ -25,6 +25,9 @@ void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const do
 // nsweep red-black sweeps (+ residual into r unless r is null) as one
 // temporally blocked cooperative kernel; planes per chunk from
 // PMGB_GS7_CHUNK (default 8).
+// one full red-black sweep in one pass, xin -> xout (boundaries of both zero)
+int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                       const double* xin, double* xout, int first_parity);
 int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                       double* x, double* r, int nsweep, int first_parity);
 int gs7_chunk();

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gs7_pipe.cuh"
+#include "gs7_sweep.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
 
@@ -70,6 +71,7 @@ struct MixedState {
   MLevel lev[16];
   float* r;      // fine-sized FP32 scratch
   float* w2;     // fine-sized FP32 scratch
+  float* xs;     // second fine FP32 iterate of the single-pass sweep (zero boundary)
   double* dense;  // coarsest dense factor (n x n)
   double* dvec;   // coarsest rhs / solution in FP64
   int nd;
@@ -878,7 +880,27 @@ int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, 
   return 1;
 }
 
-cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity) {
+cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
+                    float* xs) {
+  if (!g_tune[3] && g_tune[5] == 2 && xs) {
+    // two single-pass sweeps x -> xs -> x, then the residual
+    Gs7Sweep<float> a;
+    a.g = F.g;
+    a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
+    a.cc = F.cc; a.fc = F.w0;
+    a.c1 = first_parity;
+    a.kchunk = 16;
+    a.xin = x; a.xout = xs;
+    cudaError_t e = launch_gs7_sweep<float, 32, 8>(st, a);
+    a.xin = xs; a.xout = x;
+    if (e == cudaSuccess) e = launch_gs7_sweep<float, 32, 8>(st, a);
+    if (r && e == cudaSuccess) {
+      const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+      k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, opf(F), F.cc, F.w0, x, r);
+      e = cudaGetLastError();
+    }
+    return e;
+  }
   if (!g_tune[3]) {
     // colour passes: 2 sweeps, then the residual
     const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
@@ -949,6 +971,7 @@ void mixed_destroy(MixedState* m) {
   }
   if (m->r) cudaFree(m->r);
   if (m->w2) cudaFree(m->w2);
+  if (m->xs) cudaFree(m->xs);
   if (m->dense) cudaFree(m->dense);
   if (m->dvec) cudaFree(m->dvec);
   if (m->dinfo) cudaFree(m->dinfo);
@@ -1022,6 +1045,7 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
   m->stale = 1;
   const size_t nscr = m->lev[lo].g.n();
   if (!falloc(&m->r, nscr) || !falloc(&m->w2, nscr)) return 0;
+  if (lo == 0 && !falloc(&m->xs, nscr)) return 0;
   const Grid gc = m->lev[nl - 1].g;
   m->nd = (gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2);
   if (m->nd > 4096) {
@@ -1208,7 +1232,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const OpF fo = opf(F);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  if (gs7_f32(st, F, F.x, m->r, 1) != cudaSuccess) {
+  if (gs7_f32(st, F, F.x, m->r, 1, m->xs) != cudaSuccess) {
     set_error("FP32 gs7 pipeline launch failed");
     return 0;
   }
@@ -1251,7 +1275,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
-      if (gs7_f32(st, F, F.x, nullptr, 0) != cudaSuccess) {
+      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs) != cudaSuccess) {
         set_error("FP32 gs7 pipeline launch failed");
         return 0;
       }
@@ -1360,13 +1384,33 @@ int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
   return 1;
 }
 
+// One FP32 single-pass sweep for kernel timing: 28 B per point per sweep
+// (6 FP32 arrays read, x read and written once).
+int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
+  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
+  MixedState* m = s->mixed;
+  MLevel& F = m->lev[0];
+  Gs7Sweep<float> a;
+  a.g = F.g;
+  a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
+  a.cc = F.cc; a.fc = F.w0; a.xin = F.x; a.xout = m->xs;
+  a.c1 = 1;
+  a.kchunk = 16;
+  if (launch_gs7_sweep<float, 32, 8>(s->stream, a) != cudaSuccess) {
+    set_error("FP32 sweep launch failed");
+    return 0;
+  }
+  *bytes = 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+  return 1;
+}
+
 // One FP32 fine smoothing call (2 sweeps + residual) for kernel timing:
 // (2 x 28 + 28) B per point.
 int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
-  if (gs7_f32(s->stream, F, F.x, m->r, 1) != cudaSuccess) {
+  if (gs7_f32(s->stream, F, F.x, m->r, 1, m->xs) != cudaSuccess) {
     set_error("FP32 gs7 pipeline launch failed");
     return 0;
   }

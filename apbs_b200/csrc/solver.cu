@@ -308,7 +308,7 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     ok &= dalloc(&L.cp, nl) && dalloc(&L.rhs, nl) && dalloc(&L.xt, nl);
     s->plan[l] = plan_for(L.g);
   }
-  ok &= dalloc(&s->w1, n) && dalloc(&s->w2, n) && dalloc(&s->w3, n);
+  ok &= dalloc(&s->w1, n) && dalloc(&s->w2, n) && dalloc(&s->w3, n) && dalloc(&s->xs, n);
   ok &= dalloc(&s->nw_r0, n) && dalloc(&s->nw_ws, n) && dalloc(&s->nw_keepx, n) &&
         dalloc(&s->nw_keepr, n);
   ok &= dalloc(&s->part, 4 * 1184 + 64) && dalloc(&s->scal, S_COUNT);
@@ -491,7 +491,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
     for (int c = 0; c < 14; c++) dfree(L.op[c]);
     dfree(L.cc); dfree(L.fc); dfree(L.x); dfree(L.w0); dfree(L.cp); dfree(L.rhs); dfree(L.xt);
   }
-  dfree(s->w1); dfree(s->w2); dfree(s->w3);
+  dfree(s->w1); dfree(s->w2); dfree(s->w3); dfree(s->xs);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
   dfree(s->d_opptrs);
@@ -799,7 +799,7 @@ static int vcycle_body(pmgb_solver* s, int newton) {
       return 0;
     }
     k += 1;
-  } else {
+  } else if (g_tune[5] == 1) {
     for (int sw = 0; sw < 2; sw++) {
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
@@ -807,6 +807,15 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     }
     launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
     k += 1;
+  } else {
+    // two single-pass sweeps, x -> xs -> x
+    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1) ||
+        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1)) {
+      set_error("gs7 sweep launch failed");
+      return 0;
+    }
+    launch_resid(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1);
+    k += 3;
   }
   launch_copy_interior(st, F.g, s->w1, F.w0);
   k += 1;
@@ -861,12 +870,19 @@ static int vcycle_body(pmgb_solver* s, int newton) {
           return 0;
         }
         k += 1;
-      } else {
+      } else if (g_tune[5] == 1) {
         for (int sw = 0; sw < 2; sw++) {
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
           k += 2;
         }
+      } else {
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0) ||
+            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0)) {
+          set_error("gs7 sweep launch failed");
+          return 0;
+        }
+        k += 2;
       }
     } else {
       if (!launch_gs27_wave(st, P.g, P.ops(), CC(l), P.w0, X(l), nullptr, 2, 0, s->plan[l])) {
@@ -1203,7 +1219,8 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
     return 0;
   }
   if ((which == PMGB_K_GS7_FP32 || which == PMGB_K_GS7_PIPE_FP32 ||
-       which == PMGB_K_VCYCLE_TAIL) && s->precision != PMGB_MIXED) {
+       which == PMGB_K_VCYCLE_TAIL || which == PMGB_K_GS7_SWEEP_FP32) &&
+      s->precision != PMGB_MIXED) {
     set_error("pmgb_time_kernel: kernel %d belongs to the mixed-precision path", which);
     return 0;
   }
@@ -1260,6 +1277,18 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         break;
       case PMGB_K_VCYCLE_TAIL:
         if (!mixed_time_tail(s, &b)) return 0;
+        break;
+      case PMGB_K_GS7_SWEEP_FP64:
+        // one full sweep: oE oN uC oC cc fc and x read, x written: 56 B per point
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), F.cc, F.fc, (r & 1) ? s->xs : F.x,
+                                (r & 1) ? F.x : s->xs, 1)) {
+          set_error("gs7 sweep launch failed");
+          return 0;
+        }
+        b = 56.0 * fint;
+        break;
+      case PMGB_K_GS7_SWEEP_FP32:
+        if (!mixed_time_gs7_sweep(s, &b)) return 0;
         break;
       default:
         set_error("pmgb_time_kernel: unknown kernel %d", which);

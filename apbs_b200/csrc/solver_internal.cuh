@@ -68,6 +68,7 @@ struct pmgb_solver {
   int nlev;
   Level lev[12];
   double *w1, *w2, *w3;
+  double* xs;  // second fine iterate for the out-of-place sweep kernel (zero boundary)
   double *nw_r0, *nw_ws, *nw_keepx, *nw_keepr;  // Newton work vectors
   double* part;
   double* scal;

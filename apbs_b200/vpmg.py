@@ -27,8 +27,10 @@ MIXED = 1
 
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
 K_GS7_PIPE_FP64, K_GS7_PIPE_FP32, K_VCYCLE_TAIL = 5, 6, 7
+K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
 TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 TUNE_BAND_ALWAYS = 4
+TUNE_GS7_COLOUR_PASSES = 5
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")

@@ -400,7 +400,9 @@ def main():
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
     # the fine-level smoothers (HBM-bound), FP64 and FP32
     smoothers = {}
-    for nm, sv, k in (("k_gs7_colour", solvers["fp64"], vpmg.K_GS7_FP64),
+    for nm, sv, k in (("k_gs7_sweep<double>", solvers["fp64"], vpmg.K_GS7_SWEEP_FP64),
+                      ("k_gs7_sweep<float>", solvers["mixed"], vpmg.K_GS7_SWEEP_FP32),
+                      ("k_gs7_colour", solvers["fp64"], vpmg.K_GS7_FP64),
                       ("k_gs7_f32", solvers["mixed"], vpmg.K_GS7_FP32)):
         ms_k, b_k = sv.time_kernel(k, 20)
         ach = b_k / (ms_k * 1e-3) / 1e9

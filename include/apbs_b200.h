@@ -139,6 +139,8 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_GS7_PIPE_FP64 5  /* fine smoothing call: 2 sweeps + residual, FP64 */
 #define PMGB_K_GS7_PIPE_FP32 6  /* fine smoothing call: 2 sweeps + residual, FP32 */
 #define PMGB_K_VCYCLE_TAIL 7    /* mixed: coarse-level V-cycle tail (one cluster kernel) */
+#define PMGB_K_GS7_SWEEP_FP64 8 /* fine-level 7-point GS, one full sweep in one pass, FP64 */
+#define PMGB_K_GS7_SWEEP_FP32 9 /* the same, FP32 (mixed) */
 
 /* Launch-shape tunables (process-wide; read when a solver captures its
  * V-cycle graph, so set them before the first solve).  The autotuner in
@@ -147,6 +149,9 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_GS7_BLOCKS_PER_SM 1  /* CTAs per SM of the pipelined smoother (0 = max) */
 #define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 (0 = auto) */
 #define PMGB_TUNE_GS7_PIPELINED 3      /* 1: temporally blocked fine smoother, 0: colour passes */
+#define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
+                                          kernel, FP32 one launch per colour), 1 = one launch
+                                          per colour, 2 = single-pass sweeps in FP32 too */
 #define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded
                                           Cholesky of the reference, 0: exact refinement
                                           above 512 unknowns */
