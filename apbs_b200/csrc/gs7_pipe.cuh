@@ -109,12 +109,11 @@ __global__ void __launch_bounds__(256) k_gs7_pipe(Gs7Args<T> a) {
   }
 }
 
-int gs7_blocks_per_sm();
 
 // Co-resident grid for the cooperative launch: SMs x min(occupancy limit,
 // requested CTAs per SM).
 template <typename T>
-inline int gs7_pipe_grid() {
+inline int gs7_pipe_grid(int want) {
   // initialised once, thread-safely (function-local static)
   static const int2 sm_per = [] {
     int dev = 0, nsm = 0, per = 0;
@@ -124,16 +123,15 @@ inline int gs7_pipe_grid() {
     return make_int2(nsm, per < 1 ? 1 : per);
   }();
   const int nsm = sm_per.x, per = sm_per.y;
-  int want = gs7_blocks_per_sm();
   int use = (want > 0 && want < per) ? want : per;
   return nsm * use;
 }
 
 template <typename T>
-inline cudaError_t launch_gs7_pipe(cudaStream_t s, const Gs7Args<T>& a) {
+inline cudaError_t launch_gs7_pipe(cudaStream_t s, const Gs7Args<T>& a, int blocks_per_sm) {
   Gs7Args<T> arg = a;
   void* params[] = {&arg};
-  return cudaLaunchCooperativeKernel((void*)k_gs7_pipe<T>, dim3(gs7_pipe_grid<T>()), dim3(256),
+  return cudaLaunchCooperativeKernel((void*)k_gs7_pipe<T>, dim3(gs7_pipe_grid<T>(blocks_per_sm)), dim3(256),
                                      params, 0, s);
 }
 

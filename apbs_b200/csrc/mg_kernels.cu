@@ -376,32 +376,30 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[8] = {8, 0, 0, 0, 0, 0, 0, 0};
+int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 0, 0, 0, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                       const double* xin, double* xout, int first_parity) {
+                       const double* xin, double* xout, int first_parity, int kchunk) {
   Gs7Sweep<double> a;
   a.g = g;
   a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
   a.c1 = first_parity;
-  a.kchunk = 16;
+  a.kchunk = kchunk;
   return launch_gs7_sweep<double, 32, 8>(s, a) == cudaSuccess;
 }
 
-int gs7_chunk() { return g_tune[0] > 0 ? g_tune[0] : 8; }
-int gs7_blocks_per_sm() { return g_tune[1]; }
 
 int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                      double* x, double* r, int nsweep, int first_parity) {
+                      double* x, double* r, int nsweep, int first_parity, const int* tune) {
   Gs7Args<double> a;
   a.g = g;
   a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.cc = cc; a.fc = fc; a.x = x; a.r = r;
   a.nhalf = 2 * nsweep;
   a.first_parity = first_parity;
-  a.chunk = gs7_chunk();
-  return launch_gs7_pipe<double>(s, a) == cudaSuccess;
+  a.chunk = tune[0] > 0 ? tune[0] : 8;
+  return launch_gs7_pipe<double>(s, a, tune[1]) == cudaSuccess;
 }
 
 void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,

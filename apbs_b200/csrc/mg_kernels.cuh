@@ -27,12 +27,10 @@ void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const do
 // PMGB_GS7_CHUNK (default 8).
 // one full red-black sweep in one pass, xin -> xout (boundaries of both zero)
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                       const double* xin, double* xout, int first_parity);
+                       const double* xin, double* xout, int first_parity, int kchunk);
 int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                      double* x, double* r, int nsweep, int first_parity);
-int gs7_chunk();
-int gs7_blocks_per_sm();
-extern int g_tune[8];
+                      double* x, double* r, int nsweep, int first_parity, const int* tune);
+extern int g_tune[16];
 void launch_resid(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                   const double* x, double* r);
 void launch_matvec(cudaStream_t s, Grid g, Op op, const double* cc, const double* x, double* y);

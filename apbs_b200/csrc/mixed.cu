@@ -881,15 +881,15 @@ int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, 
 }
 
 cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
-                    float* xs) {
-  if (!g_tune[3] && g_tune[5] == 2 && xs) {
+                    float* xs, const int* tune) {
+  if (!tune[3] && tune[5] == 2 && xs) {
     // two single-pass sweeps x -> xs -> x, then the residual
     Gs7Sweep<float> a;
     a.g = F.g;
     a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
     a.cc = F.cc; a.fc = F.w0;
     a.c1 = first_parity;
-    a.kchunk = 16;
+    a.kchunk = tune[6];
     a.xin = x; a.xout = xs;
     cudaError_t e = launch_gs7_sweep<float, 32, 8>(st, a);
     a.xin = xs; a.xout = x;
@@ -901,7 +901,7 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
     }
     return e;
   }
-  if (!g_tune[3]) {
+  if (!tune[3]) {
     // colour passes: 2 sweeps, then the residual
     const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
     const OpF fo = opf(F);
@@ -922,8 +922,8 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
   a.cc = F.cc; a.fc = F.w0; a.x = x; a.r = r;
   a.nhalf = 4;
   a.first_parity = first_parity;
-  a.chunk = gs7_chunk();
-  return launch_gs7_pipe<float>(st, a);
+  a.chunk = tune[0] > 0 ? tune[0] : 8;
+  return launch_gs7_pipe<float>(st, a, tune[1]);
 }
 
 int falloc(float** p, size_t n) {
@@ -1055,10 +1055,12 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
   if (!dalloc64(&m->dense, (size_t)m->nd * m->nd) || !dalloc64(&m->dvec, m->nd)) return 0;
   CKM(cudaMalloc(&m->dinfo, sizeof(int) * 4));
   // levels small enough for one cluster run in the tail kernel
-  m->tail_first = 0;
-  for (int l = (lo > 0 ? lo : 1); l < nl; l++) {
+  // the exact coarse solve of the FP64 path always runs its levels in one
+  // cluster; the mixed V-cycle does from the first level under the limit
+  m->tail_first = (lo > 0) ? lo : 0;
+  for (int l = 1; lo == 0 && l < nl; l++) {
     const Grid g = m->lev[l].g;
-    if ((size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2) <= 70000) {
+    if ((size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2) <= (size_t)s->tune[8]) {
       m->tail_first = l;
       break;
     }
@@ -1232,11 +1234,11 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const OpF fo = opf(F);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  if (gs7_f32(st, F, F.x, m->r, 1, m->xs) != cudaSuccess) {
+  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, s->tune) != cudaSuccess) {
     set_error("FP32 gs7 pipeline launch failed");
     return 0;
   }
-  k += g_tune[3] ? 1 : 5;
+  k += s->tune[3] ? 1 : 5;
   const int tf = m->tail_first > 0 ? m->tail_first : nl;
   for (int l = 1; l < tf; l++) {
     MLevel& C = m->lev[l];
@@ -1275,11 +1277,11 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
-      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs) != cudaSuccess) {
+      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, s->tune) != cudaSuccess) {
         set_error("FP32 gs7 pipeline launch failed");
         return 0;
       }
-      k += g_tune[3] ? 1 : 4;
+      k += s->tune[3] ? 1 : 4;
     } else {
       if (!gs27_mc(st, P, P.x, 2, 1, k)) return 0;
     }
@@ -1395,7 +1397,7 @@ int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
   a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
   a.cc = F.cc; a.fc = F.w0; a.xin = F.x; a.xout = m->xs;
   a.c1 = 1;
-  a.kchunk = 16;
+  a.kchunk = s->tune[6];
   if (launch_gs7_sweep<float, 32, 8>(s->stream, a) != cudaSuccess) {
     set_error("FP32 sweep launch failed");
     return 0;
@@ -1410,7 +1412,7 @@ int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
-  if (gs7_f32(s->stream, F, F.x, m->r, 1, m->xs) != cudaSuccess) {
+  if (gs7_f32(s->stream, F, F.x, m->r, 1, m->xs, s->tune) != cudaSuccess) {
     set_error("FP32 gs7 pipeline launch failed");
     return 0;
   }

@@ -91,6 +91,7 @@ struct pmgb_server {
   long long created = 0, reused = 0, evicted = 0, admitted = 0;
   int inflight = 0, inflight_peak = 0;
   std::vector<double> lat, service;
+  std::map<Shape, std::vector<std::pair<int, int>>> shape_tune;
 
   Shape shape_of(const pmgb_params& p) const { return Shape(p.nx, p.ny, p.nz, p.nlev); }
 
@@ -191,8 +192,15 @@ void pmgb_server::worker_main() {
     if (!calc) {
       calc = be.create(be.ctx, &rq->p, cfg.precision);
       if (calc) {
-        std::lock_guard<std::mutex> lk(mu);
-        created++;
+        std::vector<std::pair<int, int>> tv;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          created++;
+          auto it = shape_tune.find(shape_of(rq->p));
+          if (it != shape_tune.end()) tv = it->second;
+        }
+        if (cuda)
+          for (const auto& kv : tv) pmgb_solver_set_tuning((pmgb_solver*)calc, kv.first, kv.second);
       }
     } else if (!be.reconfigure(be.ctx, calc, &rq->p)) {
       be.destroy(be.ctx, calc);
@@ -345,6 +353,20 @@ extern "C" long long pmgb_server_submit(pmgb_server* srv, const pmgb_params* par
   srv->submitted++;
   srv->cv_work.notify_one();
   return rq->id;
+}
+
+extern "C" int pmgb_server_set_shape_tuning(pmgb_server* srv, const pmgb_params* shape, int key,
+                                            int value) {
+  if (!srv || !shape || key < 0 || key >= PMGB_TUNE_NKEYS) return 0;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto& v = srv->shape_tune[srv->shape_of(*shape)];
+  for (auto& kv : v)
+    if (kv.first == key) {
+      kv.second = value;
+      return 1;
+    }
+  v.emplace_back(key, value);
+  return 1;
 }
 
 extern "C" int pmgb_server_poll(pmgb_server* srv, long long id, pmgb_result* result) {

@@ -202,19 +202,22 @@ int max_cluster() {
   return mc;
 }
 
-Gs27Plan plan_for(Grid g) {
+Gs27Plan plan_for(Grid g, const int* tune) {
   const int ni = std::max(g.nx, std::max(g.ny, g.nz)) - 2;
   Gs27Plan p;
-  const int g_max_cluster = max_cluster();
-  if (g_tune[2] > 0) {
-    p.cluster = std::min(g_tune[2], g_max_cluster);
-    p.threads = (p.cluster >= 8) ? 512 : 256;
-    return p;
-  }
-  if (ni >= 60) { p.cluster = g_max_cluster; p.threads = 512; }
-  else if (ni >= 28) { p.cluster = 8; p.threads = 256; }
-  else if (ni >= 12) { p.cluster = 2; p.threads = 256; }
-  else { p.cluster = 1; p.threads = 256; }
+  const int mc = max_cluster();
+  auto pick = [&](int want, int dflt) {
+    int c = want > 0 ? want : dflt;
+    c = std::min(c, mc);
+    int p2 = 1;  // a power of two
+    while (p2 * 2 <= c) p2 *= 2;
+    return p2;
+  };
+  if (ni >= 60) p.cluster = pick(tune[2], mc);
+  else if (ni >= 28) p.cluster = pick(tune[7], 8);
+  else if (ni >= 12) p.cluster = 2;
+  else p.cluster = 1;
+  p.threads = (p.cluster >= 8) ? 512 : 256;
   return p;
 }
 
@@ -281,6 +284,7 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     return 0;
   }
   s->stream = s->own_stream;
+  for (int i = 0; i < 16; i++) s->tune[i] = g_tune[i];
   for (int i = 0; i < 8; i++) cudaEventCreate(&s->ev[i]);
   const size_t n = s->n;
   int ok = 1;
@@ -306,7 +310,7 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     for (int c = 0; c < L.nop; c++) ok &= dalloc(&L.op[c], nl);
     ok &= dalloc(&L.cc, nl) && dalloc(&L.fc, nl) && dalloc(&L.x, nl) && dalloc(&L.w0, nl);
     ok &= dalloc(&L.cp, nl) && dalloc(&L.rhs, nl) && dalloc(&L.xt, nl);
-    s->plan[l] = plan_for(L.g);
+    s->plan[l] = plan_for(L.g, s->tune);
   }
   ok &= dalloc(&s->w1, n) && dalloc(&s->w2, n) && dalloc(&s->w3, n) && dalloc(&s->xs, n);
   ok &= dalloc(&s->nw_r0, n) && dalloc(&s->nw_ws, n) && dalloc(&s->nw_keepx, n) &&
@@ -751,7 +755,7 @@ static int build_ops(pmgb_solver* s) {
     // a coarsest level above 512 unknowns is solved by exact refinement
     // instead: the banded factor and its substitutions are sequential
     const Grid gc = s->lev[s->nlev - 1].g;
-    if ((size_t)(gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2) > 512 && g_tune[4] == 0 &&
+    if ((size_t)(gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2) > 512 && s->tune[4] == 0 &&
         coarse_exact_prepare(s))
       s->mgsolv = 2;
   }
@@ -793,13 +797,13 @@ static int vcycle_body(pmgb_solver* s, int newton) {
   double* FC0 = newton ? F.rhs : F.fc;
   long long k = 0;
   // nu1 = 2 pre-smoothings on the fine level, then the residual
-  if (g_tune[3]) {
-    if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1, 2, 1)) {
+  if (s->tune[3]) {
+    if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1, 2, 1, s->tune)) {
       set_error("gs7 pipeline launch failed");
       return 0;
     }
     k += 1;
-  } else if (g_tune[5] == 1) {
+  } else if (s->tune[5] == 1) {
     for (int sw = 0; sw < 2; sw++) {
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
@@ -809,8 +813,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     k += 1;
   } else {
     // two single-pass sweeps, x -> xs -> x
-    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1) ||
-        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1)) {
+    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6]) ||
+        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6])) {
       set_error("gs7 sweep launch failed");
       return 0;
     }
@@ -864,21 +868,21 @@ static int vcycle_body(pmgb_solver* s, int newton) {
                        s->scal + S_XDEN_L + l);
     k += 6;
     if (l == 0) {
-      if (g_tune[3]) {
-        if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), nullptr, 2, 0)) {
+      if (s->tune[3]) {
+        if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), nullptr, 2, 0, s->tune)) {
           set_error("gs7 pipeline launch failed");
           return 0;
         }
         k += 1;
-      } else if (g_tune[5] == 1) {
+      } else if (s->tune[5] == 1) {
         for (int sw = 0; sw < 2; sw++) {
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
           k += 2;
         }
       } else {
-        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0) ||
-            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0)) {
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6]) ||
+            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1265,7 +1269,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         if (!mixed_time_gs7(s, r & 1, &b)) return 0;
         break;
       case PMGB_K_GS7_PIPE_FP64:
-        if (!launch_gs7_smooth(st, F.g, F.ops(), F.cc, F.fc, F.x, s->w1, 2, 1)) {
+        if (!launch_gs7_smooth(st, F.g, F.ops(), F.cc, F.fc, F.x, s->w1, 2, 1, s->tune)) {
           set_error("gs7 pipeline launch failed");
           return 0;
         }
@@ -1281,7 +1285,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_SWEEP_FP64:
         // one full sweep: oE oN uC oC cc fc and x read, x written: 56 B per point
         if (!launch_gs7_sweep64(st, F.g, F.ops(), F.cc, F.fc, (r & 1) ? s->xs : F.x,
-                                (r & 1) ? F.x : s->xs, 1)) {
+                                (r & 1) ? F.x : s->xs, 1, s->tune[6])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1305,7 +1309,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
 }
 
 extern "C" int pmgb_set_tuning(int key, int value) {
-  if (key < 0 || key >= 8) {
+  if (key < 0 || key >= PMGB_TUNE_NKEYS) {
     set_error("pmgb_set_tuning: bad key %d", key);
     return 0;
   }
@@ -1314,8 +1318,38 @@ extern "C" int pmgb_set_tuning(int key, int value) {
 }
 
 extern "C" int pmgb_get_tuning(int key) {
-  if (key < 0 || key >= 8) return -1;
+  if (key < 0 || key >= PMGB_TUNE_NKEYS) return -1;
   return g_tune[key];
+}
+
+extern "C" int pmgb_solver_set_tuning(pmgb_solver* s, int key, int value) {
+  if (!s || key < 0 || key >= PMGB_TUNE_NKEYS) {
+    set_error("pmgb_solver_set_tuning: bad solver or key %d", key);
+    return 0;
+  }
+  if (s->tune[key] == value) return 1;
+  CK(cudaStreamSynchronize(s->stream));
+  s->tune[key] = value;
+  // launch shapes are baked into the captured V-cycle graphs
+  for (int m = 0; m < 2; m++)
+    if (s->vc_exec[m]) {
+      cudaGraphExecDestroy(s->vc_exec[m]);
+      s->vc_exec[m] = nullptr;
+    }
+  for (int l = 0; l < s->nlev; l++) s->plan[l] = plan_for(s->lev[l].g, s->tune);
+  if (s->mixed) {
+    // the FP32 hierarchy and its graphs are rebuilt with the new shapes
+    mixed_destroy(s->mixed);
+    s->mixed = nullptr;
+    s->built = 0;
+    s->solved = 0;
+  }
+  return 1;
+}
+
+extern "C" int pmgb_solver_get_tuning(pmgb_solver* s, int key) {
+  if (!s || key < 0 || key >= PMGB_TUNE_NKEYS) return -1;
+  return s->tune[key];
 }
 
 extern "C" const char* pmgb_last_error(void) { return g_err; }

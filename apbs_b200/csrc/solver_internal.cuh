@@ -96,6 +96,7 @@ struct pmgb_solver {
   double ext_qf, ext_di, ext_qm;
   double* focus_w;  // coarse-grid partition weights for the external energy
   int focus_w_alloc;
+  int tune[16];  // launch-shape tunables (PMGB_TUNE_*), copied from the defaults at creation
   // state
   int filled, solved, built;
   std::vector<double> reslog;

@@ -91,6 +91,8 @@ def lib():
         L.pmgb_server_get_stats.restype = ctypes.c_int
         L.pmgb_server_destroy.argtypes = [vp]
         L.pmgb_server_destroy.restype = None
+        L.pmgb_server_set_shape_tuning.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int]
+        L.pmgb_server_set_shape_tuning.restype = ctypes.c_int
         L.pmgb_footprint.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.pmgb_footprint.restype = ctypes.c_size_t
         _bound = True
@@ -135,6 +137,31 @@ class Server:
         if u_out is not None:
             self._keep[rid] = u_out
         return int(rid)
+
+    def set_shape_tuning(self, params, key: int, value: int):
+        """Tunable for every calculation of this grid shape built from now on."""
+        if lib().pmgb_server_set_shape_tuning(self._h, ctypes.byref(params), key, value) != 1:
+            raise RuntimeError("pmgb_server_set_shape_tuning failed")
+
+    def apply_table(self, table: dict, precision: int) -> int:
+        """Apply an autotuner table (apbs_b200.autotune) per grid shape; where
+        LPBE and NPBE entries of a shape differ, the LPBE one wins.  Returns
+        the number of shapes tuned."""
+        shapes = {}
+        for key, e in table.items():
+            dims, nlev, prec, eq = key.split("/")
+            if prec != ("mixed" if precision == MIXED else "fp64"):
+                continue
+            if dims + nlev in shapes and eq == "npbe":
+                continue
+            shapes[dims + nlev] = (dims, int(nlev), e["tune"])
+        for dims, nlev, tune in shapes.values():
+            p = synth.PmgbParams()
+            p.nx, p.ny, p.nz = (int(d) for d in dims.split("x"))
+            p.nlev = nlev
+            for k, v in tune.items():
+                self.set_shape_tuning(p, int(k), int(v))
+        return len(shapes)
 
     def poll(self, rid: int) -> dict:
         res = Result()

@@ -31,6 +31,8 @@ K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
 TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5
+TUNE_GS7_SWEEP_KCHUNK, TUNE_GS27_CLUSTER_MID, TUNE_TAIL_MAX_POINTS = 6, 7, 8
+TUNE_NKEYS = 16
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")
@@ -88,6 +90,10 @@ def lib():
                                           ctypes.POINTER(PmgbStats)]
         L.pmgb_time_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.pmgb_time_kernel.restype = ctypes.c_int
+        L.pmgb_solver_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.pmgb_solver_set_tuning.restype = ctypes.c_int
+        L.pmgb_solver_get_tuning.argtypes = [vp, ctypes.c_int]
+        L.pmgb_solver_get_tuning.restype = ctypes.c_int
         L.pmgb_set_tuning.argtypes = [ctypes.c_int, ctypes.c_int]
         L.pmgb_set_tuning.restype = ctypes.c_int
         L.pmgb_get_tuning.argtypes = [ctypes.c_int]
@@ -214,6 +220,13 @@ class Vpmg:
         buf = np.zeros(8192)
         n = lib().pmgb_get_residual_history(self._h, _dp(buf), buf.size)
         return buf[:min(n, buf.size)].copy()
+
+    def set_tuning(self, key: int, value: int):
+        """Launch-shape tunable of this calculation only (PMGB_TUNE_*)."""
+        _check(lib().pmgb_solver_set_tuning(self._h, key, value), "pmgb_solver_set_tuning")
+
+    def get_tuning(self, key: int) -> int:
+        return int(lib().pmgb_solver_get_tuning(self._h, key))
 
     def time_kernel(self, which: int, reps: int = 20):
         """Mean device ms per launch and algorithmic bytes per launch."""

@@ -165,7 +165,7 @@ def serving_measurements(args):
     33^3-65^3), each in mixed precision and in FP64."""
     import numpy as np
 
-    from apbs_b200 import serve, synth
+    from apbs_b200 import autotune, serve, synth
     from apbs_b200.vpmg import FP64, MIXED
     out = {}
     if args.serve_n > 0:
@@ -177,6 +177,7 @@ def serving_measurements(args):
                          "replayed once untimed so every grid shape is resident)"}
         for name, prec in (("mixed", MIXED), ("fp64", FP64)):
             with serve.Server(prec, max_inflight=8) as srv:
+                srv.apply_table(autotune.load_table(), prec)
                 serve.replay(srv, stream, time_scale=0.0)     # resident calculations
                 r = serve.replay(srv, stream)
                 st = srv.stats()
@@ -207,6 +208,7 @@ def serving_measurements(args):
         energies = {}
         for name, prec in (("mixed", MIXED), ("fp64", FP64)):
             with serve.Server(prec, max_inflight=8) as srv:
+                srv.apply_table(autotune.load_table(), prec)
                 serve.replay(srv, [serve.StreamRequest(0.0, p, m) for p, m in jobs[:16]], 0.0)
                 t0 = time.perf_counter()
                 ids = [srv.submit(p, m) for p, m in jobs]
@@ -299,9 +301,13 @@ def main():
     precisions = [("fp64", vpmg.FP64), ("mixed", vpmg.MIXED)]
     if args.only:
         precisions = [p for p in precisions if p[0] == args.only]
+    from apbs_b200 import autotune
+    table = autotune.load_table()
     solvers = {}
+    tuned = {}
     for name, prec in precisions:
         s = vpmg.Vpmg(params, prec)
+        tuned[name] = autotune.apply(s, table)   # launch shapes from the autotuner's table
         s.set_stream(stream.cuda_stream)
         solvers[name] = s
 
@@ -429,7 +435,12 @@ def main():
             "config": {"workload": desc, "headline": args.headline,
                        "step": "fillco (device atoms) + build + solve + energy",
                        "l2": "working set ~1 GB per calculation, larger than L2",
-                       "parallelism": "replicas x%d" % world},
+                       "parallelism": "replicas x%d" % world,
+                       "tuning": {"table": "apbs_b200/tuning/b200.json",
+                                  "mixed": {autotune.KEY_NAMES.get(k, str(k)): v
+                                            for k, v in tuned.get("mixed", {}).items()},
+                                  "fp64": {autotune.KEY_NAMES.get(k, str(k)): v
+                                           for k, v in tuned.get("fp64", {}).items()}}},
             "latency_ms": head["latency_ms"],
             "fp64": results["fp64"], "mixed": results["mixed"],
             "mixed_vs_fp64": {"speedup": results["mixed"]["solves_per_s"] /

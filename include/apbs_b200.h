@@ -142,21 +142,33 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_GS7_SWEEP_FP64 8 /* fine-level 7-point GS, one full sweep in one pass, FP64 */
 #define PMGB_K_GS7_SWEEP_FP32 9 /* the same, FP32 (mixed) */
 
-/* Launch-shape tunables (process-wide; read when a solver captures its
- * V-cycle graph, so set them before the first solve).  The autotuner in
- * apbs_b200/autotune.py picks them per grid size. */
+/* Launch-shape tunables.  pmgb_set_tuning sets the process-wide defaults a
+ * calculation copies when it is created; pmgb_solver_set_tuning changes one
+ * calculation (its captured V-cycle graphs are rebuilt on the next solve).
+ * The autotuner (apbs_b200/autotune.py) times whole solves per grid shape
+ * and keeps the best values in a table.  No key changes a result beyond
+ * round-off; the FP64 smoother and wavefront keys change none at all. */
 #define PMGB_TUNE_GS7_CHUNK 0          /* planes per pipeline chunk (default 8) */
 #define PMGB_TUNE_GS7_BLOCKS_PER_SM 1  /* CTAs per SM of the pipelined smoother (0 = max) */
-#define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 (0 = auto) */
+#define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 on levels with
+                                          >= 60 interior points per axis (0 = device max) */
 #define PMGB_TUNE_GS7_PIPELINED 3      /* 1: temporally blocked fine smoother, 0: colour passes */
-#define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
-                                          kernel, FP32 one launch per colour), 1 = one launch
-                                          per colour, 2 = single-pass sweeps in FP32 too */
 #define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded
                                           Cholesky of the reference, 0: exact refinement
                                           above 512 unknowns */
+#define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
+                                          kernel, FP32 one launch per colour), 1 = one launch
+                                          per colour, 2 = single-pass sweeps in FP32 too */
+#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 16) */
+#define PMGB_TUNE_GS27_CLUSTER_MID 7   /* the same as key 2 for levels with 28-59 interior
+                                          points per axis (0 = 8) */
+#define PMGB_TUNE_TAIL_MAX_POINTS 8    /* mixed: largest level (interior points) run inside
+                                          the one-cluster V-cycle tail (default 70000) */
+#define PMGB_TUNE_NKEYS 16
 int pmgb_set_tuning(int key, int value);
 int pmgb_get_tuning(int key);
+int pmgb_solver_set_tuning(pmgb_solver *s, int key, int value);
+int pmgb_solver_get_tuning(pmgb_solver *s, int key);
 
 /* Launch one kernel `reps` times back to back on the solver's stream (after
  * a solve, on its state) and report the mean device time per launch (CUDA
@@ -266,6 +278,9 @@ long long pmgb_server_submit(pmgb_server *srv, const pmgb_params *params, int na
                              double *u_out);
 /* Status of a request without waiting (the return value is result->status). */
 int pmgb_server_poll(pmgb_server *srv, long long id, pmgb_result *result);
+/* Launch-shape tunable (PMGB_TUNE_*) for every calculation of this grid
+ * shape (nx, ny, nz, nlev of params) the loop builds from now on. */
+int pmgb_server_set_shape_tuning(pmgb_server *srv, const pmgb_params *shape, int key, int value);
 /* Wait for a request to finish. */
 int pmgb_server_wait(pmgb_server *srv, long long id, pmgb_result *result);
 /* Wait until every submitted request has finished. */

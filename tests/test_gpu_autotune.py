@@ -1,0 +1,64 @@
+"""Per-calculation launch-shape tuning on the device: the FP64 variants give
+bitwise the same solve, the mixed ones agree to round-off, two calculations
+in one process keep their own settings, and the tuner returns a setting from
+its candidates."""
+import numpy as np
+import pytest
+
+from apbs_b200 import autotune, synth
+from apbs_b200.vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
+                            TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_TAIL_MAX_POINTS,
+                            Vpmg)
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(p, m, prec, tune):
+    with Vpmg(p, prec) as pmg:
+        for k, v in tune.items():
+            pmg.set_tuning(k, v)
+        pmg.fillco(m)
+        pmg.solve()
+        return pmg.energy(), pmg.u, pmg.residual_history()
+
+
+def test_fp64_launch_shapes_do_not_change_the_solve():
+    m = synth.cluster(400, 11.0, seed=12, net_charge=2.0)
+    p = synth.mg_manual(129, 0.4, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    e0, u0, h0 = _solve(p, m, FP64, {})
+    for tune in ({TUNE_GS27_CLUSTER: 4}, {TUNE_GS27_CLUSTER_MID: 16},
+                 {TUNE_GS7_SWEEP_KCHUNK: 8}, {TUNE_GS7_COLOUR_PASSES: 1}):
+        e, u, h = _solve(p, m, FP64, tune)
+        assert e == e0 and np.array_equal(u, u0) and np.array_equal(h, h0), tune
+
+
+def test_mixed_tail_limit_changes_only_round_off():
+    m = synth.cluster(400, 11.0, seed=12)
+    p = synth.mg_manual(129, 0.4, m.center())
+    e0, u0, _ = _solve(p, m, MIXED, {})
+    for lim in (20000, 200000):
+        e, u, _ = _solve(p, m, MIXED, {TUNE_TAIL_MAX_POINTS: lim})
+        assert abs(e - e0) <= 1e-9 * abs(e0)
+
+
+def test_tuning_is_per_calculation():
+    m = synth.cluster(200, 9.0, seed=3)
+    p = synth.mg_manual(65, 0.5, m.center())
+    with Vpmg(p, FP64) as a, Vpmg(p, FP64) as b:
+        a.set_tuning(TUNE_GS7_SWEEP_KCHUNK, 8)
+        assert a.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == 8
+        assert b.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == 16
+        for s in (a, b):
+            s.fillco(m)
+            s.solve()
+        assert a.energy() == b.energy()
+
+
+def test_tuner_returns_a_candidate():
+    m = synth.cluster(200, 9.0, seed=3)
+    p = synth.mg_manual(65, 0.5, m.center())
+    cands = {TUNE_GS7_SWEEP_KCHUNK: [16, 8], TUNE_GS7_COLOUR_PASSES: [0, 1]}
+    e = autotune.tune(p, m, FP64, reps=2, candidates=cands)
+    assert int(e["tune"][str(TUNE_GS7_SWEEP_KCHUNK)]) in (16, 8)
+    assert 0.0 < e["ms"] <= e["default_ms"]
+    assert len(e["trials"]) == 3
