@@ -827,6 +827,161 @@ __global__ void __launch_bounds__(512) k_coarse_exact(ExactArgs E) {
 }
 
 // ---------------------------------------------------------------------------
+// Batched solves: one persistent kernel for many mixed-precision LPBE
+// calculations.  The descriptors of all calculations (their FP64 fine-level
+// arrays and their FP32 level tables) are packed in one device array; each
+// thread-block cluster takes one calculation and runs its whole refinement
+// loop without returning to the host: the FP64 residual of Vmvcs's stopping
+// test (src/pmgc/mgcsd.c:312-330, 1-norms), then per correction one FP32
+// V-cycle -- 7-point red-black GS on the fine level, the one-cluster tail of
+// levels 1 .. coarsest (tail_cycle), the Hackbusch-Reusken damping of the
+// level-1 correction, interpolation and post-smoothing -- and the FP64
+// accumulation.  It is the sequence of the per-launch mixed V-cycle graph, so
+// calculations of uneven grid sizes share one launch and overlap on the SMs.
+// ---------------------------------------------------------------------------
+struct BatchItem {
+  TailArgs T;             // FP32 levels 1 .. coarsest (T.first = 1)
+  Grid g;                 // fine grid
+  const double* op[4];    // FP64 fine operator: oC oE oN uC
+  const double* cc;
+  const double* fc;
+  double* x;              // FP64 potential (interior; boundary zero)
+  const float* op32[4];   // FP32 fine operator
+  const float* cc32;
+  float* w0;              // FP32 fine right-hand side (the FP64 residual)
+  float* e;               // FP32 fine correction
+  float* r;               // FP32 fine residual (T.rprev)
+  double errtol;
+  int itmax;
+  int nlog;
+  double* out;            // [0] corrections, [1] final relative residual, [2..] log
+};
+
+// one colour of the FP32 fine-level red-black GS (the update of k_gs7_f32)
+template <int CLUSTER>
+__device__ void batch_gs7(const BatchItem& B, int parity, int gtid, int nthr) {
+  const Grid g = B.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const int hr = (nx - 1) / 2;
+  const int nslots = hr * (ny - 2) * (nz - 2);
+  for (int q = gtid; q < nslots; q += nthr) {
+    const int m = q % hr;
+    const int j = 1 + (q / hr) % (ny - 2);
+    const int k = 1 + q / (hr * (ny - 2));
+    const int i = 1 + (((1 + j + k) & 1) != parity) + 2 * m;
+    if (i > nx - 2) continue;
+    const size_t id = g.idx(i, j, k);
+    const float* const* o = B.op32;
+    const float* x = B.e;
+    const float nb = o[ON][id] * x[id + sy] + o[ON][id - sy] * x[id - sy] + o[OE][id] * x[id + 1] +
+                     o[OE][id - 1] * x[id - 1] + o[UC][id - sz] * x[id - sz] +
+                     o[UC][id] * x[id + sz];
+    B.e[id] = (B.w0[id] + nb) / (o[OC][id] + B.cc32[id]);
+  }
+  tail_sync<CLUSTER>();
+}
+
+template <int CLUSTER>
+__global__ void __launch_bounds__(512) k_batch_solve(const BatchItem* __restrict__ items) {
+  __shared__ double sh[64];
+  __shared__ double slots[4];
+  const BatchItem& B = items[blockIdx.x / CLUSTER];
+  const unsigned rank = cg::this_cluster().block_rank();
+  const int gtid = rank * blockDim.x + threadIdx.x;
+  const int nthr = CLUSTER * blockDim.x;
+  int phase = 0;
+  const Grid g = B.g;
+  const int nx = g.nx, ny = g.ny;
+  const int ex = nx - 2, ey = ny - 2, nint = ex * ey * (g.nz - 2);
+  const int n = (int)g.n();
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  auto interior = [&](int q) { return g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey)); };
+
+  // x = 0; ||f||_1 (Vxnrm1 on the interior)
+  double fs = 0.0, u2 = 0.0;
+  for (int q = gtid; q < n; q += nthr) B.x[q] = 0.0;
+  for (int q = gtid; q < nint; q += nthr) fs += fabs(B.fc[interior(q)]);
+  tail_sum2<CLUSTER>(fs, u2, sh, slots, phase);
+  const double rsden = (fs == 0.0) ? 1.0 : fs;
+  // FP64 residual r = f - (A + cc) x -> FP32 right-hand side, and ||r||_1
+  auto residual = [&]() {
+    double acc = 0.0, unused = 0.0;
+    for (int q = gtid; q < nint; q += nthr) {
+      const size_t id = interior(q);
+      const double* const* o = B.op;
+      const double* x = B.x;
+      const double r = B.fc[id] + o[ON][id] * x[id + sy] + o[ON][id - sy] * x[id - sy] +
+                       o[OE][id] * x[id + 1] + o[OE][id - 1] * x[id - 1] +
+                       o[UC][id - sz] * x[id - sz] + o[UC][id] * x[id + sz] -
+                       (o[OC][id] + B.cc[id]) * x[id];
+      B.w0[id] = (float)r;
+      acc += fabs(r);
+    }
+    tail_sum2<CLUSTER>(acc, unused, sh, slots, phase);
+    return acc;
+  };
+  double rs = residual();
+  if (gtid == 0 && B.nlog > 0) B.out[2] = rs / rsden;
+  int it = 0;
+  while (it < B.itmax && rs / rsden > B.errtol) {
+    // FP32 V-cycle on A e = w0
+    for (int q = gtid; q < n; q += nthr) B.e[q] = 0.f;
+    tail_sync<CLUSTER>();
+    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    for (int q = gtid; q < nint; q += nthr) {
+      const size_t id = interior(q);
+      const float* const* o = B.op32;
+      const float* x = B.e;
+      const float nb = o[ON][id] * x[id + sy] + o[ON][id - sy] * x[id - sy] +
+                       o[OE][id] * x[id + 1] + o[OE][id - 1] * x[id - 1] +
+                       o[UC][id - sz] * x[id - sz] + o[UC][id] * x[id + sz];
+      B.r[id] = B.w0[id] + nb - (o[OC][id] + B.cc32[id]) * x[id];
+    }
+    tail_sync<CLUSTER>();
+    tail_cycle<CLUSTER>(B.T, false, gtid, nthr, sh, slots, phase);
+    const TLev& C = B.T.lev[1];
+    double num, den;
+    tail_damp<CLUSTER>(C, gtid, nthr, sh, slots, phase, num, den);
+    const float xdamp = (float)(num / den);
+    for (int q = gtid; q < nint; q += nthr) {
+      const int i = 1 + q % ex, j = 1 + (q / ex) % ey, k = 1 + q / (ex * ey);
+      const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
+      const int oi = i & 1, oj = j & 1, ok = k & 1;
+      float w = 0.f;
+      for (int c = 0; c <= ok; c++)
+        for (int b = 0; b <= oj; b++)
+          for (int a = 0; a <= oi; a++) w += C.x[C.g.idx(ii + a, jj + b, kk + c)];
+      w *= 1.f / (float)(1 << (oi + oj + ok));
+      B.e[g.idx(i, j, k)] += xdamp * w;
+    }
+    tail_sync<CLUSTER>();
+    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    for (int q = gtid; q < nint; q += nthr) {
+      const size_t id = interior(q);
+      B.x[id] += (double)B.e[id];
+    }
+    tail_sync<CLUSTER>();
+    rs = residual();
+    it++;
+    if (gtid == 0 && it < B.nlog) B.out[2 + it] = rs / rsden;
+    if (!(rs == rs)) break;  // non-finite: reported by the host
+  }
+  if (gtid == 0) {
+    B.out[0] = (double)it;
+    B.out[1] = rs / rsden;
+  }
+  // no CTA may exit while another can still read its shared memory
+  tail_sync<CLUSTER>();
+}
+
+// ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
 int mc_cluster_size(Grid g) {
@@ -1541,3 +1696,157 @@ int mixed_solve(pmgb_solver* s, double errtol) {
 }
 
 }  // namespace pmgb
+
+// ---------------------------------------------------------------------------
+// Batched solve entry point
+// ---------------------------------------------------------------------------
+extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_stream) {
+  using namespace pmgb;
+  if (!solvers || n < 1) {
+    set_error("pmgb_batch_solve: no calculations");
+    return 0;
+  }
+  int dev = -1;
+  CKM(cudaGetDevice(&dev));
+  for (int b = 0; b < n; b++) {
+    pmgb_solver* s = solvers[b];
+    if (!s || !s->filled || s->precision != PMGB_MIXED || s->p.nonlin || s->device != dev) {
+      set_error("pmgb_batch_solve: calculation %d is not a filled mixed-precision LPBE "
+                "calculation on the current device", b);
+      return 0;
+    }
+  }
+  // operators, FP32 hierarchies and coarsest inverses, per calculation
+  int cl = 16;
+  for (int b = 0; b < n; b++) {
+    pmgb_solver* s = solvers[b];
+    if (!s->built && !solver_build(s)) return 0;
+    if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
+    if (!s->mixed->cc_ready && !mixed_set_cc(s, 0)) return 0;
+    if (s->mixed->tail_first != 1) {
+      set_error("pmgb_batch_solve: calculation %d (%dx%dx%d) is too large for one cluster "
+                "(its level 1 exceeds the tail limit)", b, s->p.nx, s->p.ny, s->p.nz);
+      return 0;
+    }
+    cl = std::min(cl, s->mixed->tail_cluster);
+  }
+  static const int cl16_ok = [] {
+    if (cudaFuncSetAttribute(k_batch_solve<16>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(16, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 16;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, k_batch_solve<16>, &cfg) != cudaSuccess || ncl < 1) {
+      cudaGetLastError();
+      return 0;
+    }
+    return 1;
+  }();
+  if (!cl16_ok) cl = 8;
+  cudaStream_t st = cuda_stream ? (cudaStream_t)cuda_stream : solvers[0]->stream;
+  for (int b = 0; b < n; b++) CKM(cudaStreamSynchronize(solvers[b]->stream));
+  // the packed descriptor table
+  const int nlog = 64;
+  std::vector<BatchItem> items(n);
+  BatchItem* d_items = nullptr;
+  double* d_out = nullptr;
+  CKM(cudaMallocAsync((void**)&d_items, sizeof(BatchItem) * n, st));
+  CKM(cudaMallocAsync((void**)&d_out, sizeof(double) * (2 + nlog) * n, st));
+  for (int b = 0; b < n; b++) {
+    pmgb_solver* s = solvers[b];
+    MixedState* m = s->mixed;
+    BatchItem& B = items[b];
+    B.T.lev = m->d_tlev;
+    B.T.first = 1;
+    B.T.last = m->nlev - 1;
+    B.T.gprev = m->lev[0].g;
+    B.T.rprev = m->r;
+    B.T.r = m->w2;
+    B.T.minv = m->dense;
+    B.T.nd = m->nd;
+    B.T.xnum = s->scal + S_TMP;
+    B.T.xden = s->scal + S_TMP;
+    B.g = s->g;
+    for (int c = 0; c < 4; c++) {
+      B.op[c] = s->lev[0].op[c];
+      B.op32[c] = m->lev[0].op[c];
+    }
+    B.cc = s->lev[0].cc;
+    B.fc = s->lev[0].fc;
+    B.x = s->lev[0].x;
+    B.cc32 = m->lev[0].cc;
+    B.w0 = m->lev[0].w0;
+    B.e = m->lev[0].x;
+    B.r = m->r;
+    B.errtol = (s->p.etol > 0.0) ? s->p.etol : 1.0e-6;
+    B.itmax = 200;
+    B.nlog = nlog;
+    B.out = d_out + (size_t)(2 + nlog) * b;
+  }
+  CKM(cudaMemcpyAsync(d_items, items.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice, st));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl * n, 1, 1);
+  cfg.blockDim = dim3(512, 1, 1);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = (cl == 16) ? cudaLaunchKernelEx(&cfg, k_batch_solve<16>, (const BatchItem*)d_items)
+                             : cudaLaunchKernelEx(&cfg, k_batch_solve<8>, (const BatchItem*)d_items);
+  if (e != cudaSuccess) {
+    set_error("pmgb_batch_solve: launch: %s", cudaGetErrorString(e));
+    cudaFreeAsync(d_items, st);
+    cudaFreeAsync(d_out, st);
+    return 0;
+  }
+  note_launches(1);
+  std::vector<double> out((size_t)(2 + nlog) * n);
+  CKM(cudaMemcpyAsync(out.data(), d_out, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, st));
+  // Dirichlet values back on the boundary (VfboundPMG, mgdrvd.c:557)
+  for (int b = 0; b < n; b++) {
+    pmgb_solver* s = solvers[b];
+    launch_fbound(st, s->g, s->lev[0].x, s->gx, s->gy, s->gz);
+  }
+  note_launches(n);
+  cudaFreeAsync(d_items, st);
+  cudaFreeAsync(d_out, st);
+  CKM(cudaStreamSynchronize(st));
+  CKM(cudaGetLastError());
+  int ok = 1;
+  for (int b = 0; b < n; b++) {
+    pmgb_solver* s = solvers[b];
+    const double* o = out.data() + (size_t)(2 + nlog) * b;
+    const int iters = (int)o[0];
+    s->reslog.clear();
+    for (int i = 0; i <= iters && i < nlog; i++) s->reslog.push_back(o[2 + i]);
+    s->st.vcycles = iters;
+    s->st.refinements = iters;
+    s->st.newton_iters = 0;
+    s->st.rel_residual = o[1];
+    s->st.coarse_method = 2;
+    s->st.t_setup_ms = 0.0;
+    s->st.t_solve_ms = 0.0;
+    if (!(o[1] == o[1])) {
+      set_error("pmgb_batch_solve: non-finite residual in calculation %d", b);
+      ok = 0;
+      continue;
+    }
+    s->solved = 1;
+  }
+  return ok;
+}

@@ -22,6 +22,8 @@ int mixed_time_tail(pmgb_solver* s, double* bytes);
 // FP64 path, LPBE: exact-to-round-off solve of the FP64 coarsest level
 // (FP64 refinement over FP32 V-cycles of extra Galerkin levels).
 int coarse_exact_prepare(pmgb_solver* s);
+// operator build of solver.cu (Galerkin hierarchy, coarsest factor)
+int solver_build(pmgb_solver* s);
 int launch_coarse_exact(pmgb_solver* s, cudaStream_t st, const double* cc, const double* b,
                         double* x);
 }  // namespace pmgb

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "apbs_b200.h"
+#include "solver_internal.cuh"
 
 namespace {
 
@@ -106,16 +107,27 @@ struct pmgb_server {
       if (q.shape == sh) return true;
     return false;
   }
-  // the head request can start now
-  bool head_admissible() const {
-    if (queue.empty()) return false;
-    const Request* h = queue.front();
+  // a request can start now
+  bool admissible(const Request* h) const {
     if (has_idle(shape_of(h->p))) return true;
     return in_use - idle_bytes() + h->bytes <= budget;
   }
+  bool head_admissible() const { return !queue.empty() && admissible(queue.front()); }
+
+  struct Slot {
+    Request* rq = nullptr;
+    void* calc = nullptr;
+    size_t held = 0;
+  };
+  long long batches = 0, batched = 0;
+  int batch_peak = 0;
 
   void worker_main();
   int run_request(Request* rq, void* calc, void* stream);
+  Slot admit_at(size_t pos, std::vector<void*>& release);
+  bool batchable(const Request* rq) const;
+  void* prepare(Slot& sl);
+  void* finish(Slot& sl, int status);
 };
 
 // Runs one request on its calculation; the status is published by the
@@ -141,6 +153,103 @@ int pmgb_server::run_request(Request* rq, void* calc, void* stream) {
   return ok ? 1 : -1;
 }
 
+// Takes request `pos` of the queue (the caller holds the lock and has
+// checked it is admissible): a pooled calculation of its shape or reserved
+// memory.
+pmgb_server::Slot pmgb_server::admit_at(size_t pos, std::vector<void*>& release) {
+  Slot sl;
+  sl.rq = queue[pos];
+  queue.erase(queue.begin() + pos);
+  const Shape sh = shape_of(sl.rq->p);
+  // a resident calculation of this shape, most recently used first
+  int pick = -1;
+  for (int i = 0; i < (int)idle.size(); i++)
+    if (idle[i].shape == sh && (pick < 0 || idle[i].last_used > idle[pick].last_used)) pick = i;
+  if (pick >= 0) {
+    sl.calc = idle[pick].calc;
+    sl.held = idle[pick].bytes;
+    idle.erase(idle.begin() + pick);
+    reused++;
+  } else {
+    // release idle calculations, least recently used first, until it fits
+    std::sort(idle.begin(), idle.end(),
+              [](const Pooled& a, const Pooled& b) { return a.last_used < b.last_used; });
+    while (in_use + sl.rq->bytes > budget && !idle.empty()) {
+      in_use -= idle.front().bytes;
+      release.push_back(idle.front().calc);
+      idle.erase(idle.begin());
+      evicted++;
+    }
+    in_use += sl.rq->bytes;
+    sl.held = sl.rq->bytes;
+  }
+  peak = std::max(peak, in_use);
+  inflight++;
+  inflight_peak = std::max(inflight_peak, inflight);
+  sl.rq->t_start = now_ms();
+  sl.rq->admit_order = ++admitted;
+  return sl;
+}
+
+// Mixed-precision LPBE on a grid whose level 1 fits the one-cluster tail:
+// these share one persistent kernel (pmgb_batch_solve).
+bool pmgb_server::batchable(const Request* rq) const {
+  return cuda && cfg.max_batch > 1 && cfg.precision == PMGB_MIXED && !rq->p.nonlin &&
+         rq->p.nx <= 65 && rq->p.ny <= 65 && rq->p.nz <= 65;
+}
+
+// A calculation for the slot (pooled one reconfigured, or a new one).
+void* pmgb_server::prepare(Slot& sl) {
+  void* calc = sl.calc;
+  if (!calc) {
+    calc = be.create(be.ctx, &sl.rq->p, cfg.precision);
+    if (calc) {
+      std::vector<std::pair<int, int>> tv;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        created++;
+        auto it = shape_tune.find(shape_of(sl.rq->p));
+        if (it != shape_tune.end()) tv = it->second;
+      }
+      if (cuda)
+        for (const auto& kv : tv) pmgb_solver_set_tuning((pmgb_solver*)calc, kv.first, kv.second);
+    }
+  } else if (!be.reconfigure(be.ctx, calc, &sl.rq->p)) {
+    be.destroy(be.ctx, calc);
+    calc = be.create(be.ctx, &sl.rq->p, cfg.precision);
+  }
+  sl.calc = calc;
+  if (!calc) sl.rq->err = cuda ? pmgb_last_error() : "backend create failed";
+  return calc;
+}
+
+// Publishes a finished slot and keeps its calculation resident (or drops it).
+void* pmgb_server::finish(Slot& sl, int status) {
+  Request* rq = sl.rq;
+  void* drop = nullptr;
+  rq->status = status;
+  rq->t_end = now_ms();
+  inflight--;
+  if (rq->status == 1) {
+    done++;
+    lat.push_back(rq->t_end - rq->t_submit);
+    service.push_back(rq->t_end - rq->t_start);
+  } else {
+    failed++;
+  }
+  // keep the calculation resident unless its shape's pool is full
+  const Shape sh = shape_of(rq->p);
+  int same = 0;
+  for (const Pooled& q : idle) same += (q.shape == sh);
+  if (sl.calc && rq->status == 1 && same < cfg.pool_per_shape) {
+    idle.push_back(Pooled{sl.calc, sh, sl.held, rq->t_end});
+  } else {
+    drop = sl.calc;
+    in_use -= sl.held;
+  }
+  return drop;
+}
+
 void pmgb_server::worker_main() {
   cudaStream_t stream = nullptr;
   if (cuda) {
@@ -148,96 +257,72 @@ void pmgb_server::worker_main() {
     cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
   }
   for (;;) {
-    Request* rq = nullptr;
-    void* calc = nullptr;
-    size_t held = 0;
+    std::vector<Slot> slots;
     std::vector<void*> release;
     {
       std::unique_lock<std::mutex> lk(mu);
       cv_work.wait(lk, [&] { return (stop && queue.empty()) || head_admissible(); });
       if (queue.empty()) break;  // stopping
-      rq = queue.front();
-      queue.pop_front();
-      const Shape sh = shape_of(rq->p);
-      // a resident calculation of this shape, most recently used first
-      int pick = -1;
-      for (int i = 0; i < (int)idle.size(); i++)
-        if (idle[i].shape == sh && (pick < 0 || idle[i].last_used > idle[pick].last_used))
-          pick = i;
-      if (pick >= 0) {
-        calc = idle[pick].calc;
-        held = idle[pick].bytes;
-        idle.erase(idle.begin() + pick);
-        reused++;
-      } else {
-        // release idle calculations, least recently used first, until it fits
-        std::sort(idle.begin(), idle.end(),
-                  [](const Pooled& a, const Pooled& b) { return a.last_used < b.last_used; });
-        while (in_use + rq->bytes > budget && !idle.empty()) {
-          in_use -= idle.front().bytes;
-          release.push_back(idle.front().calc);
-          idle.erase(idle.begin());
-          evicted++;
+      slots.push_back(admit_at(0, release));
+      // continuous batching: small mixed LPBE requests waiting anywhere in
+      // the queue join a small head in one persistent kernel (they need
+      // little memory; larger requests keep their order among themselves)
+      if (batchable(slots[0].rq))
+        for (size_t q = 0; q < queue.size() && (int)slots.size() < cfg.max_batch;) {
+          if (batchable(queue[q]) && admissible(queue[q]))
+            slots.push_back(admit_at(q, release));
+          else
+            q++;
         }
-        in_use += rq->bytes;
-        held = rq->bytes;
-      }
-      peak = std::max(peak, in_use);
-      inflight++;
-      inflight_peak = std::max(inflight_peak, inflight);
-      rq->t_start = now_ms();
-      rq->admit_order = ++admitted;
+      batch_peak = std::max(batch_peak, (int)slots.size());
     }
     for (void* c : release) be.destroy(be.ctx, c);
-    if (!calc) {
-      calc = be.create(be.ctx, &rq->p, cfg.precision);
-      if (calc) {
-        std::vector<std::pair<int, int>> tv;
-        {
-          std::lock_guard<std::mutex> lk(mu);
-          created++;
-          auto it = shape_tune.find(shape_of(rq->p));
-          if (it != shape_tune.end()) tv = it->second;
-        }
-        if (cuda)
-          for (const auto& kv : tv) pmgb_solver_set_tuning((pmgb_solver*)calc, kv.first, kv.second);
-      }
-    } else if (!be.reconfigure(be.ctx, calc, &rq->p)) {
-      be.destroy(be.ctx, calc);
-      calc = be.create(be.ctx, &rq->p, cfg.precision);
-    }
-    int status;
-    if (calc) {
-      status = run_request(rq, calc, stream);
+    std::vector<int> status(slots.size(), -1);
+    if (slots.size() == 1) {
+      if (prepare(slots[0])) status[0] = run_request(slots[0].rq, slots[0].calc, stream);
     } else {
-      status = -1;
-      rq->err = cuda ? pmgb_last_error() : "backend create failed";
+      // fill each on its own stream (the fills overlap on the device), solve
+      // all in one launch, then the energies
+      std::vector<pmgb_solver*> calcs;
+      std::vector<int> member;
+      for (size_t b = 0; b < slots.size(); b++) {
+        Request* rq = slots[b].rq;
+        if (!prepare(slots[b])) continue;
+        pmgb_solver* s = (pmgb_solver*)slots[b].calc;
+        if (pmgb_set_stream(s, nullptr) &&
+            pmgb::fillco_issue(s, (int)rq->q.size(), rq->xyz.data(), rq->q.data(),
+                               rq->r.data())) {
+          calcs.push_back(s);
+          member.push_back((int)b);
+        } else {
+          rq->err = pmgb_last_error();
+        }
+      }
+      const int ok = calcs.empty() ? 0 : pmgb_batch_solve(calcs.data(), (int)calcs.size(), stream);
+      const std::string berr = ok ? "" : pmgb_last_error();
+      for (size_t c = 0; c < calcs.size(); c++) {
+        Request* rq = slots[member[c]].rq;
+        double e = 0.0;
+        int good = ok && pmgb_energy(calcs[c], &e) && pmgb_get_stats(calcs[c], &rq->st);
+        if (good && rq->u_out) good = pmgb_get_potential(calcs[c], rq->u_out);
+        if (!good) rq->err = ok ? pmgb_last_error() : berr;
+        rq->energy = e;
+        status[member[c]] = good ? 1 : -1;
+        pmgb_set_stream(calcs[c], nullptr);
+      }
+      std::lock_guard<std::mutex> lk(mu);
+      batches++;
+      batched += (long long)calcs.size();
     }
-    void* drop = nullptr;
+    std::vector<void*> drops;
     {
       std::lock_guard<std::mutex> lk(mu);
-      rq->status = status;
-      rq->t_end = now_ms();
-      inflight--;
-      if (rq->status == 1) {
-        done++;
-        lat.push_back(rq->t_end - rq->t_submit);
-        service.push_back(rq->t_end - rq->t_start);
-      } else {
-        failed++;
-      }
-      // keep the calculation resident unless its shape's pool is full
-      const Shape sh = shape_of(rq->p);
-      int same = 0;
-      for (const Pooled& q : idle) same += (q.shape == sh);
-      if (calc && rq->status == 1 && same < cfg.pool_per_shape) {
-        idle.push_back(Pooled{calc, sh, held, rq->t_end});
-      } else {
-        drop = calc;
-        in_use -= held;
+      for (size_t b = 0; b < slots.size(); b++) {
+        void* d = finish(slots[b], status[b]);
+        if (d) drops.push_back(d);
       }
     }
-    if (drop) be.destroy(be.ctx, drop);
+    for (void* d : drops) be.destroy(be.ctx, d);
     cv_done.notify_all();
     cv_work.notify_all();
   }
@@ -251,7 +336,9 @@ int server_start(pmgb_server* srv, const pmgb_server_config* cfg) {
   if (srv->cfg.max_inflight < 1) srv->cfg.max_inflight = 1;
   // by default a shape keeps as many calculations as can run at once, so a
   // burst of one shape never has to release (cudaFree synchronises the device)
-  if (cfg->pool_per_shape == 0) srv->cfg.pool_per_shape = std::max(2, srv->cfg.max_inflight);
+  if (cfg->max_batch == 0) srv->cfg.max_batch = 16;
+  if (cfg->pool_per_shape == 0)
+    srv->cfg.pool_per_shape = std::max(2, srv->cfg.max_inflight) * std::max(1, srv->cfg.max_batch);
   else if (cfg->pool_per_shape < 0) srv->cfg.pool_per_shape = 0;
   srv->budget = cfg->hbm_budget_bytes;
   for (int i = 0; i < srv->cfg.max_inflight; i++)
@@ -427,6 +514,9 @@ extern "C" int pmgb_server_get_stats(pmgb_server* srv, pmgb_server_stats* st) {
   st->reused = srv->reused;
   st->evicted = srv->evicted;
   st->inflight_peak = srv->inflight_peak;
+  st->batches = srv->batches;
+  st->batched = srv->batched;
+  st->batch_peak = srv->batch_peak;
   return 1;
 }
 

@@ -512,19 +512,31 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
 // ===========================================================================
 // fill (Vpmg_fillco)
 // ===========================================================================
-static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
+// Statistics of a fill issued without waiting (time, surface points).
+static int settle_fill(pmgb_solver* s) {
+  if (!s->fill_pending) return 1;
+  CK(cudaEventSynchronize(s->ev[1]));
+  s->st.t_fill_ms = elapsed_ms(s->ev[0], s->ev[1]);
+  int npts = 0;
+  CK(cudaMemcpy(&npts, s->d_npts, sizeof(int), cudaMemcpyDeviceToHost));
+  s->st.sas_points = npts;
+  s->fill_pending = 0;
+  return 1;
+}
+
+static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int wait) {
   const pmgb_params& p = s->p;
   cudaStream_t st = s->stream;
   const size_t n = s->n;
   const int natoms = s->natoms;
   phys_setup(s, natoms, h_xyz, h_r);
   CK(cudaEventRecord(s->ev[0], st));
+  CK(cudaMemsetAsync(s->d_npts, 0, sizeof(int), st));
   // charge (fillcoChargeSpline2)
   CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
   launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
   note_launches(1);
   const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
-  int sas_pts = 0;
   if (!islap) {
     // dielectric (fillcoCoefMolDielNoSmooth)
     launch_fill_value(st, s->epsx, n, p.sdie);
@@ -585,7 +597,6 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
                  s->cell_start, s->cell_sorted, s->sas_flags, s->d_npts, s->epsx, s->epsy,
                  s->epsz);
       note_launches(2);
-      CK(cudaMemcpyAsync(&sas_pts, s->d_npts, sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     if (p.srfm == PMGB_SRFM_SMOL) {
       CK(cudaMemcpyAsync(s->tmp3, s->epsx, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -645,18 +656,20 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r) {
     return 0;
   }
   CK(cudaEventRecord(s->ev[1], st));
-  CK(cudaStreamSynchronize(st));
   CK(cudaGetLastError());
-  s->st.t_fill_ms = elapsed_ms(s->ev[0], s->ev[1]);
-  s->st.sas_points = sas_pts;
   s->filled = 1;
   s->built = 0;
   s->solved = 0;
+  s->fill_pending = 1;
+  if (wait) {
+    CK(cudaStreamSynchronize(st));
+    return settle_fill(s);
+  }
   return 1;
 }
 
-extern "C" int pmgb_fillco(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
-                           const double* radius) {
+static int fillco_host(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
+                       const double* radius, int wait) {
   if (!s || natoms <= 0 || !xyz || !charge || !radius) {
     set_error("pmgb_fillco: bad arguments");
     return 0;
@@ -679,7 +692,17 @@ extern "C" int pmgb_fillco(pmgb_solver* s, int natoms, const double* xyz, const 
                      s->stream));
   CK(cudaMemcpyAsync(s->d_r, radius, sizeof(double) * natoms, cudaMemcpyHostToDevice,
                      s->stream));
-  return do_fill(s, xyz, radius);
+  return do_fill(s, xyz, radius, wait);
+}
+
+extern "C" int pmgb_fillco(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
+                           const double* radius) {
+  return fillco_host(s, natoms, xyz, charge, radius, 1);
+}
+
+int pmgb::fillco_issue(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
+                       const double* radius) {
+  return fillco_host(s, natoms, xyz, charge, radius, 0);
 }
 
 extern "C" int pmgb_fillco_device(pmgb_solver* s, int natoms, const double* d_xyz,
@@ -697,7 +720,7 @@ extern "C" int pmgb_fillco_device(pmgb_solver* s, int natoms, const double* d_xy
   s->d_q = const_cast<double*>(d_charge);
   s->d_r = const_cast<double*>(d_radius);
   s->natoms = natoms;
-  return do_fill(s, xyz.data(), r.data());
+  return do_fill(s, xyz.data(), r.data(), 1);
 }
 
 extern "C" int pmgb_set_coefficients(pmgb_solver* s, const double* charge, const double* epsx,
@@ -784,6 +807,8 @@ static int build_ops(pmgb_solver* s) {
   s->built = 1;
   return 1;
 }
+
+int pmgb::solver_build(pmgb_solver* s) { return build_ops(s); }
 
 // ===========================================================================
 // one V-cycle (body of the do-loop of Vmvcs, src/pmgc/mgcsd.c:312-562)
@@ -1191,6 +1216,7 @@ extern "C" int pmgb_get_maps(pmgb_solver* s, double* maps, double* faces) {
 
 extern "C" int pmgb_get_stats(pmgb_solver* s, pmgb_stats* out) {
   if (!s || !out) return 0;
+  if (!settle_fill(s)) return 0;
   *out = s->st;
   return 1;
 }

@@ -11,6 +11,14 @@ struct MixedState;
 void note_launches(long long n);
 }  // namespace pmgb
 
+struct pmgb_solver;
+namespace pmgb {
+// pmgb_fillco without waiting for the device: the fill is queued on the
+// calculation's stream and its statistics are read when first asked for.
+int fillco_issue(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
+                 const double* radius);
+}  // namespace pmgb
+
 namespace pmgb {
 
 struct Level {
@@ -99,6 +107,7 @@ struct pmgb_solver {
   int tune[16];  // launch-shape tunables (PMGB_TUNE_*), copied from the defaults at creation
   // state
   int filled, solved, built;
+  int fill_pending;  // fill issued without waiting; its statistics not yet read
   std::vector<double> reslog;
   pmgb_stats st;
   Gs27Plan plan[12];

@@ -22,7 +22,8 @@ _bound = False
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_inflight", ctypes.c_int),
-                ("hbm_budget_bytes", ctypes.c_size_t), ("pool_per_shape", ctypes.c_int)]
+                ("hbm_budget_bytes", ctypes.c_size_t), ("pool_per_shape", ctypes.c_int),
+                ("max_batch", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -47,7 +48,9 @@ class ServerStats(ctypes.Structure):
                 ("mean_service_ms", ctypes.c_double), ("bytes_in_use", ctypes.c_size_t),
                 ("bytes_peak", ctypes.c_size_t), ("budget", ctypes.c_size_t),
                 ("created", ctypes.c_longlong), ("reused", ctypes.c_longlong),
-                ("evicted", ctypes.c_longlong), ("inflight_peak", ctypes.c_int)]
+                ("evicted", ctypes.c_longlong), ("inflight_peak", ctypes.c_int),
+                ("batches", ctypes.c_longlong), ("batched", ctypes.c_longlong),
+                ("batch_peak", ctypes.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -113,9 +116,9 @@ class Server:
     calls are replaced by callbacks, which runs the loop without a GPU."""
 
     def __init__(self, precision=MIXED, max_inflight=4, hbm_budget_bytes=0, pool_per_shape=0,
-                 backend: Backend | None = None):
+                 backend: Backend | None = None, max_batch=0):
         self._h = ctypes.c_void_p()
-        cfg = ServerConfig(precision, max_inflight, hbm_budget_bytes, pool_per_shape)
+        cfg = ServerConfig(precision, max_inflight, hbm_budget_bytes, pool_per_shape, max_batch)
         self._keep = {}
         if backend is None:
             ok = lib().pmgb_server_create(ctypes.byref(cfg), ctypes.byref(self._h))

@@ -90,6 +90,8 @@ def lib():
                                           ctypes.POINTER(PmgbStats)]
         L.pmgb_time_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp]
         L.pmgb_time_kernel.restype = ctypes.c_int
+        L.pmgb_batch_solve.argtypes = [ctypes.POINTER(vp), ctypes.c_int, vp]
+        L.pmgb_batch_solve.restype = ctypes.c_int
         L.pmgb_solver_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.pmgb_solver_set_tuning.restype = ctypes.c_int
         L.pmgb_solver_get_tuning.argtypes = [vp, ctypes.c_int]
@@ -264,6 +266,14 @@ def energy_noalloc(params, d_u, d_charge, d_epsx=0, d_epsy=0, d_epsz=0, d_kappa=
                                      ctypes.c_void_p(d_kappa or None), ctypes.c_void_p(stream or None),
                                      _dp(e)), "pmgb_energy_noalloc")
     return float(e[0])
+
+
+def batch_solve(calcs, stream_handle: int = 0) -> None:
+    """Solve filled mixed-precision LPBE calculations in one persistent
+    kernel launch (pmgb_batch_solve); each is then solved as by Vpmg.solve."""
+    arr = (ctypes.c_void_p * len(calcs))(*[c._h.value for c in calcs])
+    _check(lib().pmgb_batch_solve(arr, len(calcs), ctypes.c_void_p(stream_handle or None)),
+           "pmgb_batch_solve")
 
 
 def solve_molecule(params, mol, precision=FP64, want_u=False):

@@ -196,6 +196,17 @@ int pmgb_energy_noalloc(const pmgb_params *params, const double *d_u, const doub
                         const double *d_epsx, const double *d_epsy, const double *d_epsz,
                         const double *d_kappa, void *cuda_stream, double *energy_kT);
 
+/* Solve many filled mixed-precision LPBE calculations (each from
+ * pmgb_create(..., PMGB_MIXED) + pmgb_fillco) in one persistent kernel:
+ * one thread-block cluster per calculation runs its whole refinement loop on
+ * the device, so calculations of uneven grid sizes share one launch.  Each
+ * calculation's level 1 must fit the one-cluster tail (fine grids up to 65^3
+ * with the default tail limit).  Afterwards each calculation is solved as by
+ * pmgb_solve (pmgb_energy, pmgb_get_potential, pmgb_get_stats).  Work runs on
+ * cuda_stream (NULL: the first calculation's stream).  No counterpart in the
+ * reference, which solves its calculations one after another. */
+int pmgb_batch_solve(pmgb_solver *const *solvers, int n, void *cuda_stream);
+
 /* Reuse a calculation for another one on the same grid (nx, ny, nz, nlev):
  * new centre, spacing, physics and boundary kind; the device arrays stay
  * allocated.  It has no counterpart in the reference (which builds a new
@@ -227,7 +238,10 @@ typedef struct pmgb_server_config {
     int max_inflight;         /* worker slots (concurrent calculations), >= 1 */
     size_t hbm_budget_bytes;  /* admission limit; 0 = 80% of the device's free memory */
     int pool_per_shape;       /* idle calculations kept per grid shape:
-                                 0 = max(2, max_inflight), < 0 = none */
+                                 0 = max(2, max_inflight) * max_batch, < 0 = none */
+    int max_batch;            /* mixed LPBE requests up to 65^3 admitted together and
+                                 solved in one persistent kernel (pmgb_batch_solve):
+                                 0 = 16, 1 = no batching */
 } pmgb_server_config;
 
 typedef struct pmgb_result {
@@ -248,6 +262,8 @@ typedef struct pmgb_server_stats {
     size_t bytes_in_use, bytes_peak, budget;
     long long created, reused, evicted; /* calculations built, pooled ones reused, released */
     int inflight_peak;
+    long long batches, batched;       /* persistent-kernel launches and the requests in them */
+    int batch_peak;
 } pmgb_server_stats;
 
 int pmgb_server_create(const pmgb_server_config *config, pmgb_server **out);

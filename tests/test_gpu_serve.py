@@ -51,6 +51,8 @@ def test_results_same_alone_and_in_mix(precision):
     assert st["done"] == len(jobs)
     assert st["bytes_peak"] <= budget
     assert st["inflight_peak"] > 1           # requests overlapped on the device
+    if precision == MIXED:                   # small LPBE requests shared persistent kernels
+        assert st["batched"] >= 2 and st["batch_peak"] >= 2
 
 
 def test_mixed_in_mix_matches_fp64_alone():
