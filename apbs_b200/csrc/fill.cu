@@ -5,6 +5,8 @@
 // trees: the integer index bounds (ceil/floor of FP64 expressions) and the
 // FP64 comparisons that decide which grid points a sphere marks are then
 // identical to the reference's, so the maps are bitwise equal.
+#include <algorithm>
+
 #include "fill_kernels.cuh"
 
 namespace pmgb {
@@ -458,6 +460,181 @@ __global__ void k_ccf(size_t n, const double* __restrict__ kappa, double zkappa2
 void launch_fill_value(cudaStream_t s, double* a, size_t n, double v) {
   k_fill_value<<<blocks_for(n), kThreads, 0, s>>>(a, n, v);
 }
+// ---------------------------------------------------------------------------
+// chgm spl0: fillcoChargeSpline1 (src/mg/vpmg.c:4986-5089), the charge of each
+// on-mesh atom split trilinearly over its 8 nearest points (FP64 atomics:
+// grid points shared by several atoms sum in a different order than the
+// reference's atom loop).
+// ---------------------------------------------------------------------------
+__global__ void k_charge_tril(FillGeom G, int natoms, const double* __restrict__ xyz,
+                              const double* __restrict__ q, double zmagic, double* charge) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const int nx = G.g.nx, ny = G.g.ny;
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2];
+  if ((ax <= G.xmin[0]) || (ax >= G.xmax[0]) || (ay <= G.xmin[1]) || (ay >= G.xmax[1]) ||
+      (az <= G.xmin[2]) || (az >= G.xmax[2]))
+    return;
+  const double px = ax - G.xmin[0], py = ay - G.xmin[1], pz = az - G.xmin[2];
+  const double c = q[a] * zmagic / (hx * hy * hz);
+  const double fi = px / hx, fj = py / hy, fk = pz / hz;
+  const int ihi = (int)ceil(fi), ilo = (int)floor(fi);
+  const int jhi = (int)ceil(fj), jlo = (int)floor(fj);
+  const int khi = (int)ceil(fk), klo = (int)floor(fk);
+  const double dx = fi - (double)(ilo), dy = fj - (double)(jlo), dz = fk - (double)(klo);
+  auto at = [&](int i, int j, int k) { return ((size_t)k * ny + j) * nx + i; };
+  atomicAdd(&charge[at(ihi, jhi, khi)], (dx * dy * dz * c));
+  atomicAdd(&charge[at(ihi, jlo, khi)], (dx * (1.0 - dy) * dz * c));
+  atomicAdd(&charge[at(ihi, jhi, klo)], (dx * dy * (1.0 - dz) * c));
+  atomicAdd(&charge[at(ihi, jlo, klo)], (dx * (1.0 - dy) * (1.0 - dz) * c));
+  atomicAdd(&charge[at(ilo, jhi, khi)], ((1.0 - dx) * dy * dz * c));
+  atomicAdd(&charge[at(ilo, jlo, khi)], ((1.0 - dx) * (1.0 - dy) * dz * c));
+  atomicAdd(&charge[at(ilo, jhi, klo)], ((1.0 - dx) * dy * (1.0 - dz) * c));
+  atomicAdd(&charge[at(ilo, jlo, klo)], ((1.0 - dx) * (1.0 - dy) * (1.0 - dz) * c));
+}
+
+void launch_charge_tril(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                        const double* q, double zmagic, double* charge) {
+  if (natoms <= 0) return;
+  k_charge_tril<<<(natoms + 127) / 128, 128, 0, s>>>(G, natoms, xyz, q, zmagic, charge);
+}
+
+// ---------------------------------------------------------------------------
+// bcfl mdh: bcflnew (src/mg/vpmg.c:3289-3367, packUnpack 3220-3287).  One
+// thread per stored face value sums, over all atoms in atom order, the
+// Debye-Hueckel potential of each charge at that boundary point (a point on
+// several faces gets the same value on each); atoms are staged through
+// shared memory in chunks.
+// ---------------------------------------------------------------------------
+constexpr int kMdhChunk = 256;
+
+__global__ void __launch_bounds__(256) k_mdh_faces(MdhArgs A, int natoms,
+                                                  const double* __restrict__ xyz,
+                                                  const double* __restrict__ q,
+                                                  const double* __restrict__ r) {
+  __shared__ double sx[kMdhChunk], sy_[kMdhChunk], sz_[kMdhChunk], sq[kMdhChunk], sr[kMdhChunk];
+  const int nx = A.g.nx, ny = A.g.ny, nz = A.g.nz;
+  const long long nfx = 2LL * ny * nz, nfy = 2LL * nx * nz, nfz = 2LL * nx * ny;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool valid = t < nfx + nfy + nfz;
+  double gxp = 0.0, gyp = 0.0, gzp = 0.0;
+  double* dst = nullptr;
+  if (valid) {
+    if (t < nfx) {
+      const int j = (int)(t % ny), k = (int)((t / ny) % nz), slot = (int)(t / ((long long)ny * nz));
+      gxp = A.xf[slot ? nx - 1 : 0]; gyp = A.yf[j]; gzp = A.zf[k];
+      dst = A.gx + t;
+    } else if (t < nfx + nfy) {
+      const long long u = t - nfx;
+      const int i = (int)(u % nx), k = (int)((u / nx) % nz), slot = (int)(u / ((long long)nx * nz));
+      gxp = A.xf[i]; gyp = A.yf[slot ? ny - 1 : 0]; gzp = A.zf[k];
+      dst = A.gy + u;
+    } else {
+      const long long u = t - nfx - nfy;
+      const int i = (int)(u % nx), j = (int)((u / nx) % ny), slot = (int)(u / ((long long)nx * ny));
+      gxp = A.xf[i]; gyp = A.yf[j]; gzp = A.zf[slot ? nz - 1 : 0];
+      dst = A.gz + u;
+    }
+  }
+  const double ec = 1.6021773e-19;
+  double val = 0.0;
+  for (int a0 = 0; a0 < natoms; a0 += kMdhChunk) {
+    const int na = min(kMdhChunk, natoms - a0);
+    __syncthreads();
+    for (int c = threadIdx.x; c < na; c += blockDim.x) {
+      sx[c] = xyz[3 * (a0 + c)];
+      sy_[c] = xyz[3 * (a0 + c) + 1];
+      sz_[c] = xyz[3 * (a0 + c) + 2];
+      sq[c] = ec * q[a0 + c];
+      sr[c] = r[a0 + c];
+    }
+    __syncthreads();
+    if (valid) {
+      for (int c = 0; c < na; c++) {
+        const double dx = gxp - sx[c], dy = gyp - sy_[c], dz = gzp - sz_[c];
+        const double dist = sqrt((dx * dx) + (dy * dy) + (dz * dz));
+        if (A.xkappa > 1.0e-9)
+          val += A.pre1 * (sq[c] / dist) * exp(-A.xkappa * (dist - sr[c])) /
+                 (1 + A.xkappa * sr[c]);
+        else
+          val += A.pre1 * (sq[c] / dist);
+      }
+    }
+  }
+  if (valid) *dst = 0.0 + val;
+}
+
+void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz, const double* q,
+                const double* r) {
+  const long long total = 2LL * ((long long)A.g.ny * A.g.nz + (long long)A.g.nx * A.g.nz +
+                                 (long long)A.g.nx * A.g.ny);
+  k_mdh_faces<<<(int)((total + 255) / 256), 256, 0, s>>>(A, natoms, xyz, q, r);
+}
+
+// ---------------------------------------------------------------------------
+// Vpmg_qfEnergyPoint (src/mg/vpmg.c:1704-1789) for chgm spl0: the potential
+// interpolated trilinearly at each atom times its charge and its partition
+// weight (Vpmg_setPart's atom rule for the domain box, vpmg.c:673-720);
+// per-block partial sums, then one block adds them.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_qf_point(FillGeom G, int natoms,
+                                                 const double* __restrict__ xyz,
+                                                 const double* __restrict__ q,
+                                                 const double* __restrict__ u, double* part) {
+  __shared__ double sh[32];
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  double acc = 0.0;
+  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < natoms; a += gridDim.x * blockDim.x) {
+    const double* pos = xyz + 3 * a;
+    double part_id = 1.0;
+    for (int d = 0; d < 3; d++) {
+      const double lo = G.xmin[d], hi = G.xmax[d];
+      double ok;
+      if ((pos[d] < hi) && (pos[d] > lo)) ok = 1;
+      else if (fabs(pos[d] - lo) < 1.0e-12) ok = 1;
+      else if (fabs(pos[d] - hi) < 1.0e-12) ok = 1;
+      else ok = 0;
+      part_id = (d == 0) ? ok : part_id * ok;
+    }
+    const double fi = (pos[0] - G.xmin[0]) / G.h[0];
+    const double fj = (pos[1] - G.xmin[1]) / G.h[1];
+    const double fk = (pos[2] - G.xmin[2]) / G.h[2];
+    const int ihi = (int)ceil(fi), ilo = (int)floor(fi);
+    const int jhi = (int)ceil(fj), jlo = (int)floor(fj);
+    const int khi = (int)ceil(fk), klo = (int)floor(fk);
+    if (!(part_id > 0)) continue;
+    if (!((ihi < nx) && (jhi < ny) && (khi < nz) && (ilo >= 0) && (jlo >= 0) && (klo >= 0)))
+      continue;
+    const double dx = fi - (double)(ilo), dy = fj - (double)(jlo), dz = fk - (double)(klo);
+    auto U = [&](int i, int j, int k) { return u[((size_t)k * ny + j) * nx + i]; };
+    const double uval =
+        dx * dy * dz * U(ihi, jhi, khi) + dx * (1.0 - dy) * dz * U(ihi, jlo, khi) +
+        dx * dy * (1.0 - dz) * U(ihi, jhi, klo) + dx * (1.0 - dy) * (1.0 - dz) * U(ihi, jlo, klo) +
+        (1.0 - dx) * dy * dz * U(ilo, jhi, khi) + (1.0 - dx) * (1.0 - dy) * dz * U(ilo, jlo, khi) +
+        (1.0 - dx) * dy * (1.0 - dz) * U(ilo, jhi, klo) +
+        (1.0 - dx) * (1.0 - dy) * (1.0 - dz) * U(ilo, jlo, klo);
+    acc += (uval * q[a] * part_id);
+  }
+  const double t = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_qf_point_final(const double* __restrict__ part, int nparts, double* out) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[i];
+  const double t = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) out[0] = t;
+}
+
+void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                     const double* q, const double* u, double* part, double* out) {
+  const int nb = std::max(1, std::min(1184, (natoms + 255) / 256));
+  k_qf_point<<<nb, 256, 0, s>>>(G, natoms, xyz, q, u, part);
+  k_qf_point_final<<<1, 256, 0, s>>>(part, nb, out);
+}
+
 void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                         const double* q, double zmagic, double* charge) {
   if (natoms <= 0) return;

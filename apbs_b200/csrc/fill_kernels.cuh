@@ -28,6 +28,25 @@ struct SdhArgs {
 };
 
 void launch_fill_value(cudaStream_t s, double* a, size_t n, double v);
+struct MdhArgs {
+  Grid g;
+  const double* xf;
+  const double* yf;
+  const double* zf;
+  double* gx;
+  double* gy;
+  double* gz;
+  double pre1;    // e_c / (4 pi eps0 eps_w k_B T) * 1e10
+  double xkappa;  // 1/A
+};
+void launch_charge_tril(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                        const double* q, double zmagic, double* charge);
+void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz, const double* q,
+                const double* r);
+// sum over atoms of the trilinearly interpolated potential x charge (part:
+// up to 1184 doubles of scratch; out: one double)
+void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                     const double* q, const double* u, double* part, double* out);
 void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                         const double* q, double zmagic, double* charge);
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,

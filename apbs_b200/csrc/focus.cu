@@ -142,6 +142,10 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
     set_error("pmgb_focus: the fine calculation must be created with bcfl focus");
     return 0;
   }
+  if (fine->p.chgm != PMGB_CHGM_SPL2 || coarse->p.chgm != PMGB_CHGM_SPL2) {
+    set_error("pmgb_focus: focusing is implemented for chgm spl2");
+    return 0;
+  }
   if (!coarse->solved) {
     set_error("pmgb_focus: the coarse calculation has not been solved");
     return 0;

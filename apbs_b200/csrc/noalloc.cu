@@ -83,6 +83,10 @@ extern "C" int pmgb_energy_noalloc(const pmgb_params* p, const double* d_u,
               p->nz, PMGB_NOALLOC_MAX_DIM);
     return 0;
   }
+  if (p->chgm != PMGB_CHGM_SPL2) {
+    set_error("pmgb_energy_noalloc: the charge-map energy needs chgm spl2");
+    return 0;
+  }
   if (p->nonlin && (!d_epsx || !d_epsy || !d_epsz || !d_kappa)) {
     set_error("pmgb_energy_noalloc: NPBE needs the dielectric and kappa maps");
     return 0;

@@ -239,8 +239,8 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     set_error("pmgb_create: unsupported grid %dx%dx%d nlev %d", p.nx, p.ny, p.nz, p.nlev);
     return 0;
   }
-  if (p.chgm != PMGB_CHGM_SPL2) {
-    set_error("pmgb_create: only chgm spl2 is implemented");
+  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL) {
+    set_error("pmgb_create: chgm %d not implemented (spl0 and spl2 are)", p.chgm);
     return 0;
   }
   if (p.nion > 8) {
@@ -534,7 +534,10 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   CK(cudaMemsetAsync(s->d_npts, 0, sizeof(int), st));
   // charge (fillcoChargeSpline2)
   CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
-  launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+  if (p.chgm == PMGB_CHGM_TRIL)
+    launch_charge_tril(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+  else
+    launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
   note_launches(1);
   const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
   if (!islap) {
@@ -651,8 +654,24 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
                s->gz);
     note_launches(3);
+  } else if (p.bcfl == PMGB_BCFL_MDH) {
+    // bcflnew (vpmg.c:3289-3367)
+    MdhArgs A;
+    A.g = s->g;
+    A.xf = s->xf;
+    A.yf = s->yf;
+    A.zf = s->zf;
+    A.gx = s->gx;
+    A.gy = s->gy;
+    A.gz = s->gz;
+    const double pi = 3.14159265358979323846;
+    A.pre1 = ((1.6021773e-19) / (4 * pi * 8.8541878e-12 * p.sdie * 1.3806581e-23 * p.temp)) *
+             (1.0e10);
+    A.xkappa = s->xkappa;
+    launch_mdh(st, A, natoms, s->d_xyz, s->d_q, s->d_r);
+    note_launches(1);
   } else if (p.bcfl != PMGB_BCFL_ZERO && p.bcfl != PMGB_BCFL_FOCUS) {
-    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh and focus are)", p.bcfl);
+    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh, mdh and focus are)", p.bcfl);
     return 0;
   }
   CK(cudaEventRecord(s->ev[1], st));
@@ -741,6 +760,7 @@ extern "C" int pmgb_set_coefficients(pmgb_solver* s, const double* charge, const
   // scalar physics without atoms: ionic strength and Debye parameters
   double dummy_xyz[3] = {p.center[0], p.center[1], p.center[2]}, dummy_r = 0.0;
   phys_setup(s, 1, dummy_xyz, &dummy_r);
+  s->natoms = 0;  // no atom list: the point-charge (spl0) energy is unavailable
   s->filled = 1;
   s->built = 0;
   s->solved = 0;
@@ -1150,6 +1170,18 @@ extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
   CK(cudaStreamSynchronize(st));
   const pmgb_params& p = s->p;
   double qf = sums[0] * p.hx * p.hy * p.hz / s->zmagic;
+  if (p.chgm == PMGB_CHGM_TRIL) {
+    // Vpmg_qfEnergyPoint (vpmg.c:1704-1789): charges at the atoms
+    if (s->natoms <= 0 || !s->d_xyz) {
+      set_error("pmgb_energy: chgm spl0 needs the atom list (pmgb_fillco)");
+      return 0;
+    }
+    launch_qf_point(st, s->G, s->natoms, s->d_xyz, s->d_q, s->lev[0].x, s->part,
+                    s->scal + S_TMP);
+    note_launches(2);
+    CK(cudaMemcpyAsync(&qf, s->scal + S_TMP, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
   qf += s->ext_qf;
   double diel = 0.0, qm = 0.0, e;
   if (a.nonlin) {

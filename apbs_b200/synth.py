@@ -21,7 +21,7 @@ import numpy as np
 
 PMGB_MAXION = 8
 SRFM_MOL, SRFM_SMOL = 0, 1
-CHGM_SPL2 = 1
+CHGM_TRIL, CHGM_SPL2 = 0, 1
 BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS = 0, 1, 2, 4
 
 

@@ -19,6 +19,7 @@
 #define PMGB_SRFM_MOL 0
 #define PMGB_SRFM_SMOL 1
 /* Charge method codes (Vchrg_Meth, src/generic/vhal.h:231-234). */
+#define PMGB_CHGM_TRIL 0   /* chgm spl0: trilinear to the 8 nearest points */
 #define PMGB_CHGM_SPL2 1
 /* Boundary condition codes (Vbcfl, src/generic/vhal.h:208-216). */
 #define PMGB_BCFL_ZERO 0
@@ -33,7 +34,7 @@ typedef struct pmgb_params {
     double center[3];       /* grid centre in Angstrom ("gcent") */
     int nonlin;             /* 0 = lpbe, 1 = npbe */
     int srfm;               /* PMGB_SRFM_* */
-    int chgm;               /* PMGB_CHGM_SPL2 */
+    int chgm;               /* PMGB_CHGM_TRIL (spl0) or PMGB_CHGM_SPL2 */
     int bcfl;               /* PMGB_BCFL_* */
     double pdie;            /* solute dielectric */
     double sdie;            /* solvent dielectric */

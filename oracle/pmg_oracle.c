@@ -188,6 +188,48 @@ static void fill_charge_spl2(const pmgb_params *p, const Phys *ph, int natoms,
     }
 }
 
+/* fillcoChargeSpline1 (chgm spl0), vpmg.c:4986-5089 */
+static void fill_charge_tril(const pmgb_params *p, const Phys *ph, int natoms,
+                             const double *xyz, const double *q,
+                             const double *xmn, const double *xmx,
+                             double *charge) {
+    int nx = p->nx, ny = p->ny, nz = p->nz, a;
+    double hx = p->hx, hy = p->hy, hz = p->hz;
+    memset(charge, 0, sizeof(double) * (size_t)nx * ny * nz);
+    for (a = 0; a < natoms; a++) {
+        const double *ap = xyz + 3 * a;
+        double px, py, pz, c, fi, fj, fk, dx, dy, dz;
+        int ihi, ilo, jhi, jlo, khi, klo;
+        if ((ap[0] <= xmn[0]) || (ap[0] >= xmx[0]) || (ap[1] <= xmn[1]) ||
+            (ap[1] >= xmx[1]) || (ap[2] <= xmn[2]) || (ap[2] >= xmx[2]))
+            continue;
+        px = ap[0] - xmn[0];
+        py = ap[1] - xmn[1];
+        pz = ap[2] - xmn[2];
+        c = q[a] * ph->zmagic / (hx * hy * hz);
+        fi = px / hx;
+        fj = py / hy;
+        fk = pz / hz;
+        ihi = (int)ceil(fi);
+        ilo = (int)floor(fi);
+        jhi = (int)ceil(fj);
+        jlo = (int)floor(fj);
+        khi = (int)ceil(fk);
+        klo = (int)floor(fk);
+        dx = fi - (double)ilo;
+        dy = fj - (double)jlo;
+        dz = fk - (double)klo;
+        charge[IJK(ihi, jhi, khi)] += (dx * dy * dz * c);
+        charge[IJK(ihi, jlo, khi)] += (dx * (1.0 - dy) * dz * c);
+        charge[IJK(ihi, jhi, klo)] += (dx * dy * (1.0 - dz) * c);
+        charge[IJK(ihi, jlo, klo)] += (dx * (1.0 - dy) * (1.0 - dz) * c);
+        charge[IJK(ilo, jhi, khi)] += ((1.0 - dx) * dy * dz * c);
+        charge[IJK(ilo, jlo, khi)] += ((1.0 - dx) * (1.0 - dy) * dz * c);
+        charge[IJK(ilo, jhi, klo)] += ((1.0 - dx) * dy * (1.0 - dz) * c);
+        charge[IJK(ilo, jlo, klo)] += ((1.0 - dx) * (1.0 - dy) * (1.0 - dz) * c);
+    }
+}
+
 /* markSphere, vpmg.c:6444-6491 */
 static void mark_sphere(double rtot, const double *tpos, int nx, int ny, int nz,
                         double hx, double hy, double hz, double xmin,
@@ -530,6 +572,58 @@ typedef struct {
     double xmn[3], xmx[3];
 } Fill;
 
+/* bcflnew (bcfl mdh), vpmg.c:3289-3367 with packAtoms/packUnpack
+ * (3195-3287): every boundary point gets the sum over all atoms, in atom
+ * order, of the Debye-Hueckel potential of each charge; a point on several
+ * faces gets the same value on each. */
+static double mdh_value(const Phys *ph, double pre1, int natoms, const double *xyz,
+                        const double *q, const double *r, double gx, double gy,
+                        double gz) {
+    const double ec = 1.6021773e-19;
+    double val = 0.0;
+    int a;
+    for (a = 0; a < natoms; a++) {
+        double dx = gx - xyz[3 * a], dy = gy - xyz[3 * a + 1], dz = gz - xyz[3 * a + 2];
+        double dist = sqrt((dx * dx) + (dy * dy) + (dz * dz));
+        double charge = ec * q[a];
+        if (ph->xkappa > VSMALL)
+            val += pre1 * (charge / dist) * exp(-ph->xkappa * (dist - r[a])) /
+                   (1 + ph->xkappa * r[a]);
+        else
+            val += pre1 * (charge / dist);
+    }
+    return val;
+}
+
+static void bc_mdh(const pmgb_params *p, const Phys *ph, int natoms, const double *xyz,
+                   const double *q, const double *r, const Fill *f) {
+    const double ec = 1.6021773e-19, eps0 = 8.8541878e-12, kb = 1.3806581e-23;
+    const double pi = 3.14159265358979323846;
+    const double pre1 = ((ec) / (4 * pi * eps0 * p->sdie * kb * p->temp)) * (1.0e10);
+    int nx = p->nx, ny = p->ny, nz = p->nz, i, j, k;
+    for (k = 0; k < nz; k++)
+        for (j = 0; j < ny; j++) {
+            f->gx[((size_t)0 * nz + k) * ny + j] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[0], f->yf[j], f->zf[k]);
+            f->gx[((size_t)1 * nz + k) * ny + j] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[nx - 1], f->yf[j], f->zf[k]);
+        }
+    for (k = 0; k < nz; k++)
+        for (i = 0; i < nx; i++) {
+            f->gy[((size_t)0 * nz + k) * nx + i] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[i], f->yf[0], f->zf[k]);
+            f->gy[((size_t)1 * nz + k) * nx + i] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[i], f->yf[ny - 1], f->zf[k]);
+        }
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            f->gz[((size_t)0 * ny + j) * nx + i] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[i], f->yf[j], f->zf[0]);
+            f->gz[((size_t)1 * ny + j) * nx + i] =
+                0.0 + mdh_value(ph, pre1, natoms, xyz, q, r, f->xf[i], f->yf[j], f->zf[nz - 1]);
+        }
+}
+
 static void do_fill(const pmgb_params *p, const Phys *ph, int natoms,
                     const double *xyz, const double *q, const double *r,
                     Fill *f) {
@@ -548,7 +642,10 @@ static void do_fill(const pmgb_params *p, const Phys *ph, int natoms,
     for (i = 0; i < ny; i++) f->yf[i] = f->xmn[1] + i * p->hy;
     for (i = 0; i < nz; i++) f->zf[i] = f->xmn[2] + i * p->hz;
     islap = (ph->ionstr < VPMGSMALL) && (fabs(p->pdie - p->sdie) < VPMGSMALL);
-    fill_charge_spl2(p, ph, natoms, xyz, q, f->xmn, f->xmx, f->charge);
+    if (p->chgm == PMGB_CHGM_TRIL)
+        fill_charge_tril(p, ph, natoms, xyz, q, f->xmn, f->xmx, f->charge);
+    else
+        fill_charge_spl2(p, ph, natoms, xyz, q, f->xmn, f->xmx, f->charge);
     if (!islap) {
         fill_diel(p, ph, natoms, xyz, r, f->xmn, f->xmx, f->epsx, f->epsy, f->epsz);
         if (p->srfm == PMGB_SRFM_SMOL) smooth_diel(p, f->epsx, f->epsy, f->epsz);
@@ -565,6 +662,8 @@ static void do_fill(const pmgb_params *p, const Phys *ph, int natoms,
          * they were set from the coarse solution by focus_fill_bound. */
     } else if (p->bcfl == PMGB_BCFL_SDH) {
         bc_sdh(p, ph, natoms, xyz, q, f->xf, f->yf, f->zf, f->gx, f->gy, f->gz);
+    } else if (p->bcfl == PMGB_BCFL_MDH) {
+        bc_mdh(p, ph, natoms, xyz, q, r, f);
     } else {
         memset(f->gx, 0, sizeof(double) * 2 * ny * nz);
         memset(f->gy, 0, sizeof(double) * 2 * nx * nz);
@@ -1410,12 +1509,60 @@ static void domain_box(const pmgb_params *p, double lo[3], double hi[3]) {
 
 /* Vpmg_energy (vpmg.c:1248-1277) with extFlag = 1: ext[] holds the
  * energies a focusing parent left outside this domain (zero otherwise). */
+/* Vpmg_qfEnergyPoint (chgm spl0), vpmg.c:1704-1789: the potential
+ * interpolated trilinearly at each atom, times its charge and its partition
+ * weight (Vpmg_setPart's atom rule, vpmg.c:673-720, for the domain box). */
+static double qf_point(const pmgb_params *p, const Fill *f, const double *u, int natoms,
+                       const double *xyz, const double *q) {
+    int nx = p->nx, ny = p->ny, nz = p->nz, a, d;
+    double lo[3], hi[3], energy = 0.0;
+    domain_box(p, lo, hi);
+    for (a = 0; a < natoms; a++) {
+        const double *pos = xyz + 3 * a;
+        double ok[3], part, fi, fj, fk, dx, dy, dz, uval;
+        int ihi, ilo, jhi, jlo, khi, klo;
+        for (d = 0; d < 3; d++) {
+            if ((pos[d] < hi[d]) && (pos[d] > lo[d])) ok[d] = 1;
+            else if (fabs(pos[d] - lo[d]) < VPMGSMALL) ok[d] = 1;
+            else if (fabs(pos[d] - hi[d]) < VPMGSMALL) ok[d] = 1;
+            else ok[d] = 0;
+        }
+        part = ok[0] * ok[1] * ok[2];
+        fi = (pos[0] - f->xmn[0]) / p->hx;
+        fj = (pos[1] - f->xmn[1]) / p->hy;
+        fk = (pos[2] - f->xmn[2]) / p->hz;
+        ihi = (int)ceil(fi);
+        ilo = (int)floor(fi);
+        jhi = (int)ceil(fj);
+        jlo = (int)floor(fj);
+        khi = (int)ceil(fk);
+        klo = (int)floor(fk);
+        if (!(part > 0)) continue;
+        if (!((ihi < nx) && (jhi < ny) && (khi < nz) && (ilo >= 0) && (jlo >= 0) && (klo >= 0)))
+            continue;
+        dx = fi - (double)ilo;
+        dy = fj - (double)jlo;
+        dz = fk - (double)klo;
+        uval = dx * dy * dz * u[IJK(ihi, jhi, khi)] + dx * (1.0 - dy) * dz * u[IJK(ihi, jlo, khi)] +
+               dx * dy * (1.0 - dz) * u[IJK(ihi, jhi, klo)] +
+               dx * (1.0 - dy) * (1.0 - dz) * u[IJK(ihi, jlo, klo)] +
+               (1.0 - dx) * dy * dz * u[IJK(ilo, jhi, khi)] +
+               (1.0 - dx) * (1.0 - dy) * dz * u[IJK(ilo, jlo, khi)] +
+               (1.0 - dx) * dy * (1.0 - dz) * u[IJK(ilo, jhi, klo)] +
+               (1.0 - dx) * (1.0 - dy) * (1.0 - dz) * u[IJK(ilo, jlo, klo)];
+        energy += (uval * q[a] * part);
+    }
+    return energy;
+}
+
 static void energies(const pmgb_params *p, const Phys *ph, const Fill *f,
-                     const double *u, const double ext[3], double *out) {
+                     const double *u, const double ext[3], int natoms, const double *xyz,
+                     const double *q, double *out) {
     double lo[3], hi[3], t[3];
     int full = (p->nonlin && ph->ionstr > 0.);
     domain_box(p, lo, hi);
     energy_terms(p, ph, f, u, lo, hi, 0, full, t);
+    if (p->chgm == PMGB_CHGM_TRIL) t[0] = qf_point(p, f, u, natoms, xyz, q);
     t[0] += ext[0];
     if (full) {
         t[1] += ext[1];
@@ -1666,7 +1813,7 @@ static int run_calc(const pmgb_params *p, int natoms, const double *xyz,
                 x[IJK(i, j, nz - 1)] = f.gz[((size_t)1 * ny + j) * nx + i];
             }
         if (u) memcpy(u, x, sizeof(double) * n);
-        energies(p, &ph, &f, x, ext, out);
+        energies(p, &ph, &f, x, ext, natoms, xyz, q, out);
         if (keep) {
             keep->ph = ph;
             keep->f = f;
@@ -1734,6 +1881,7 @@ int oracle_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
     int rc, nlog;
     (void)verbose;
     if (pc->bcfl == PMGB_BCFL_FOCUS || pf->bcfl != PMGB_BCFL_FOCUS) return 0;
+    if (pc->chgm != PMGB_CHGM_SPL2 || pf->chgm != PMGB_CHGM_SPL2) return 0;
     memset(outc, 0, sizeof(outc));
     if (!run_calc(pc, natoms, xyz, q, r, NULL, zero, NULL, NULL, NULL, outc, reslog,
                   reslog_cap, &kc))

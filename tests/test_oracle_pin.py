@@ -19,8 +19,15 @@ def _cases():
     p3 = synth.mg_manual(49, 0.8, m2.center(), srfm=synth.SRFM_MOL)
     m4 = synth.cluster(120, 6.0, seed=11, net_charge=-2.0)
     p4 = synth.mg_manual(33, 0.6, m4.center(), npbe=True, ions=((2, 0.05, 2.0), (-1, 0.1, 1.8)))
+    m5 = synth.cluster(150, 8.0, seed=11, net_charge=2.0)
+    p5 = synth.mg_manual(33, 0.6, m5.center(), bcfl=synth.BCFL_MDH)
+    p6 = synth.mg_manual(33, 0.6, m5.center(), bcfl=synth.BCFL_MDH, npbe=True)
+    p6.chgm = synth.CHGM_TRIL
+    p7 = synth.mg_manual(33, 0.6, m5.center(), ions=())
+    p7.chgm = synth.CHGM_TRIL
     return [("config0", m0, p0), ("npbe65", m1, p1), ("lpbe97_band", m2, p2),
-            ("lpbe49_mol", m2, p3), ("npbe33_2to1", m4, p4)]
+            ("lpbe49_mol", m2, p3), ("npbe33_2to1", m4, p4), ("lpbe33_mdh", m5, p5),
+            ("npbe33_mdh_spl0", m5, p6), ("lpbe33_spl0_noions", m5, p7)]
 
 
 @pytest.mark.parametrize("name,mol,params", _cases(), ids=lambda c: c if isinstance(c, str) else "")
