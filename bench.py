@@ -235,6 +235,33 @@ def serving_measurements(args):
     return out
 
 
+def profile_batch(args):
+    """Profiling mode: the binding sweep's 64 ligands (33-65^3 LPBE, mixed)
+    solved by the persistent batched kernel, `--warmup` untimed launches and
+    `--steps` timed ones."""
+    import torch
+
+    from apbs_b200 import synth
+    from apbs_b200.vpmg import MIXED, Vpmg, batch_solve
+    _, pairs = synth.binding_sweep(64)
+    ligs = [pr[1] for pr in pairs]
+    calcs = [Vpmg(p, MIXED) for p, _ in ligs]
+    for c, (_, m) in zip(calcs, ligs):
+        c.fillco(m)
+    for _ in range(max(args.warmup, 1)):
+        batch_solve(calcs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch_solve(calcs)
+    torch.cuda.synchronize()
+    ms = 1e3 * (time.perf_counter() - t0) / max(args.steps, 1)
+    print(json.dumps({"profile_run": "batch", "calculations": len(calcs), "ms_per_launch": ms,
+                      "solves_per_s": len(calcs) / (ms * 1e-3)}), flush=True)
+    for c in calcs:
+        c.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -248,8 +275,9 @@ def main():
                     help="requests in the serving-stream measurement (0 skips it)")
     ap.add_argument("--sweep-poses", type=int, default=64,
                     help="poses of the binding-energy sweep measurement (0 skips it)")
-    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
-                    help="profiling mode: run the steps of one precision and nothing else")
+    ap.add_argument("--only", choices=["mixed", "fp64", "batch"], default=None,
+                    help="profiling mode: run the steps of one precision (or the batched "
+                         "kernel on the binding sweep's ligands) and nothing else")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -258,6 +286,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.only == "batch":
+        profile_batch(args)
         return
 
     import numpy as np
