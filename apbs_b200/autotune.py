@@ -28,7 +28,8 @@ from typing import Callable
 
 from . import vpmg
 from .vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
-                   TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_TAIL_MAX_POINTS)
+                   TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_MC_COOPERATIVE,
+                   TUNE_TAIL_MAX_POINTS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
@@ -43,6 +44,7 @@ CANDIDATES = {
     },
     MIXED: {
         TUNE_TAIL_MAX_POINTS: [70000, 20000, 200000],
+        TUNE_MC_COOPERATIVE: [0, 1],
         TUNE_GS7_COLOUR_PASSES: [0, 2],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
     },
@@ -50,7 +52,7 @@ CANDIDATES = {
 
 KEY_NAMES = {TUNE_GS27_CLUSTER: "gs27_cluster", TUNE_GS27_CLUSTER_MID: "gs27_cluster_mid",
              TUNE_GS7_COLOUR_PASSES: "gs7_colour_passes", TUNE_GS7_SWEEP_KCHUNK: "gs7_sweep_kchunk",
-             TUNE_TAIL_MAX_POINTS: "tail_max_points"}
+             TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative"}
 
 
 def shape_key(params, precision: int) -> str:

@@ -255,6 +255,34 @@ __global__ void k_gs27_mc_colour(Grid g, OpF o, const float* __restrict__ cc,
   }
 }
 
+// all colours of nsweep sweeps on a large level in one cooperative launch,
+// a grid-wide barrier between colours (the updates of k_gs27_mc_colour)
+__global__ void __launch_bounds__(256) k_gs27_mc_coop(Grid g, OpF o, const float* __restrict__ cc,
+                                                     const float* __restrict__ fc, float* x,
+                                                     int nsweep, int reverse) {
+  cg::grid_group grid = cg::this_grid();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int hx = (nx - 1) / 2, hy = (ny - 1) / 2, hz = (nz - 1) / 2;
+  const size_t tot = (size_t)hx * hy * hz;
+  const size_t gtid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t nthr = (size_t)gridDim.x * blockDim.x;
+  for (int sw = 0; sw < nsweep; sw++)
+    for (int c8 = 0; c8 < 8; c8++) {
+      const int c = reverse ? 7 - c8 : c8;
+      const int pi = c & 1, pj = (c >> 1) & 1, pk = (c >> 2) & 1;
+      for (size_t t = gtid; t < tot; t += nthr) {
+        const int mi = (int)(t % hx), mj = (int)((t / hx) % hy), mk = (int)(t / ((size_t)hx * hy));
+        const int i = (pi ? 1 : 2) + 2 * mi;
+        const int j = (pj ? 1 : 2) + 2 * mj;
+        const int k = (pk ? 1 : 2) + 2 * mk;
+        if (i > nx - 2 || j > ny - 2 || k > nz - 2) continue;
+        const size_t id = g.idx(i, j, k);
+        x[id] = (fc[id] + nb27(o, g, x, id)) / (o.c[OC][id] + cc[id]);
+      }
+      grid.sync();
+    }
+}
+
 __global__ void k_restrict_f32(Grid gf, const float* __restrict__ xin, Grid gc, float* xout) {
   const int cx = gc.nx, cy = gc.ny, cz = gc.nz;
   const size_t n = gc.n();
@@ -415,36 +443,36 @@ __global__ void k_dense_build(Grid g, Op op, const double* __restrict__ cc, doub
 // pivoting needed for SPD) in one CTA; the matrix lives in shared memory
 // when it fits.  M is replaced by its inverse.
 __global__ void k_dense_inverse(double* M, int n, int use_smem, int* info) {
+  // dynamic shared memory: [matrix (use_smem) | pivot row (n) | pivot column (n)]
   extern __shared__ double sm[];
   double* A = use_smem ? sm : M;
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
+  double* rowp = use_smem ? sm + (size_t)n * n : sm;
+  double* colp = rowp + n;
   if (use_smem)
     for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = M[t];
   __syncthreads();
+  int bad = 0;
   for (int p = 0; p < n; p++) {
-    const double piv = A[p * n + p];
-    if (!(piv > 0.0)) {
-      if (threadIdx.x == 0) bad = p + 1;
-    }
-    __syncthreads();
-    if (bad) break;
-    const double ipiv = 1.0 / piv;
-    // rows r != p: A[r][c] -= A[r][p] * A[p][c] / piv (c != p); column p and
-    // row p finished below
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-      const int r = t / n, c = t % n;
-      if (r == p || c == p) continue;
-      A[t] -= A[r * n + p] * A[p * n + c] * ipiv;
-    }
-    __syncthreads();
+    // the pivot row and column before this step
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      if (t == p) continue;
-      A[t * n + p] = -A[t * n + p] * ipiv;
-      A[p * n + t] = A[p * n + t] * ipiv;
+      rowp[t] = A[p * n + t];
+      colp[t] = A[t * n + p];
     }
     __syncthreads();
-    if (threadIdx.x == 0) A[p * n + p] = ipiv;
+    const double piv = rowp[p];
+    if (!(piv > 0.0)) {  // every thread reads the same value
+      bad = p + 1;
+      break;
+    }
+    const double ipiv = 1.0 / piv;
+    // Gauss-Jordan step: A[r][c] -= A[r][p] A[p][c] / piv off row and column
+    // p; column p becomes -A[r][p] / piv, row p A[p][c] / piv, the pivot 1/piv
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int r = t / n, c = t - r * n;
+      if (r == p) A[t] = (c == p) ? ipiv : rowp[c] * ipiv;
+      else if (c == p) A[t] = -colp[r] * ipiv;
+      else A[t] -= colp[r] * rowp[c] * ipiv;
+    }
     __syncthreads();
   }
   if (use_smem)
@@ -992,9 +1020,31 @@ int mc_cluster_size(Grid g) {
   return 1;
 }
 
-int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, long long& k) {
+int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, long long& k,
+            int cooperative) {
   const int cl = mc_cluster_size(L.g);
   const OpF o = opf(L);
+  if (cl == 0 && cooperative) {
+    static const int coop_grid = [] {
+      int dev = 0, nsm = 0, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_gs27_mc_coop, 256, 0);
+      return nsm * (per < 1 ? 1 : per);
+    }();
+    Grid g = L.g;
+    const float* cc = L.cc;
+    const float* fc = L.w0;
+    void* args[] = {&g, (void*)&o, &cc, &fc, &x, &nsweep, &reverse};
+    const cudaError_t e = cudaLaunchCooperativeKernel((void*)k_gs27_mc_coop, dim3(coop_grid),
+                                                      dim3(256), args, 0, s);
+    k++;
+    if (e != cudaSuccess) {
+      set_error("gs27 multicolour cooperative launch: %s", cudaGetErrorString(e));
+      return 0;
+    }
+    return 1;
+  }
   if (cl == 0) {
     const size_t tot = (size_t)((L.g.nx - 1) / 2) * ((L.g.ny - 1) / 2) * ((L.g.nz - 1) / 2);
     for (int sw = 0; sw < nsweep; sw++)
@@ -1321,14 +1371,15 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       const int nd = m->nd;
       k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, st>>>(L.g, L.ops64(), src,
                                                                        m->dense, nd);
-      const size_t smem = (size_t)nd * nd * sizeof(double);
-      const int use_smem = smem <= kDenseSmemMax;
+      const size_t smem_all = ((size_t)nd * nd + 2 * (size_t)nd) * sizeof(double);
+      const int use_smem = smem_all <= kDenseSmemMax;
+      const size_t smem = use_smem ? smem_all : 2 * (size_t)nd * sizeof(double);
       // the attribute is set once, to the largest size any call uses: calls
       // from concurrent host threads would otherwise race on it
       static const cudaError_t attr = cudaFuncSetAttribute(
           k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmemMax);
       (void)attr;
-      k_dense_inverse<<<1, 1024, use_smem ? smem : 0, st>>>(m->dense, nd, use_smem, m->dinfo);
+      k_dense_inverse<<<1, 1024, smem, st>>>(m->dense, nd, use_smem, m->dinfo);
       note_launches(2);
     }
   }
@@ -1402,7 +1453,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     k++;
     if (l != nl - 1) {
       CKM(cudaMemsetAsync(C.x, 0, C.g.n() * sizeof(float), st));
-      if (!gs27_mc(st, C, C.x, 2, 0, k)) return 0;
+      if (!gs27_mc(st, C, C.x, 2, 0, k, s->tune[9])) return 0;
       const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
       k_resid_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.w0, C.x, m->r);
       k++;
@@ -1438,7 +1489,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
       }
       k += s->tune[3] ? 1 : 4;
     } else {
-      if (!gs27_mc(st, P, P.x, 2, 1, k)) return 0;
+      if (!gs27_mc(st, P, P.x, 2, 1, k, s->tune[9])) return 0;
     }
   }
   // x64 += e ; r = f - (A + cc) x64 (FP64) -> FP32 rhs ; ||r||_1

@@ -32,6 +32,7 @@ TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5
 TUNE_GS7_SWEEP_KCHUNK, TUNE_GS27_CLUSTER_MID, TUNE_TAIL_MAX_POINTS = 6, 7, 8
+TUNE_MC_COOPERATIVE = 9
 TUNE_NKEYS = 16
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

@@ -164,6 +164,9 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
                                           points per axis (0 = 8) */
 #define PMGB_TUNE_TAIL_MAX_POINTS 8    /* mixed: largest level (interior points) run inside
                                           the one-cluster V-cycle tail (default 70000) */
+#define PMGB_TUNE_MC_COOPERATIVE 9    /* mixed: 8-colour GS on levels above 200000 interior
+                                          points as one cooperative launch per smoothing call
+                                          (1) instead of one launch per colour (0) */
 #define PMGB_TUNE_NKEYS 16
 int pmgb_set_tuning(int key, int value);
 int pmgb_get_tuning(int key);

@@ -62,3 +62,14 @@ def test_tuner_returns_a_candidate():
     assert int(e["tune"][str(TUNE_GS7_SWEEP_KCHUNK)]) in (16, 8)
     assert 0.0 < e["ms"] <= e["default_ms"]
     assert len(e["trials"]) == 3
+
+
+def test_mixed_cooperative_smoother_matches_per_colour():
+    """The 8-colour GS of a large level as one launch per colour (default) or
+    one cooperative launch per call: the same updates in the same order."""
+    from apbs_b200.vpmg import TUNE_MC_COOPERATIVE
+    m = synth.cluster(300, 10.0, seed=4)
+    p = synth.mg_manual(161, 0.4, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    e0, u0, h0 = _solve(p, m, MIXED, {})
+    e1, u1, h1 = _solve(p, m, MIXED, {TUNE_MC_COOPERATIVE: 1})
+    assert e0 == e1 and np.array_equal(u0, u1) and np.array_equal(h0, h1)
