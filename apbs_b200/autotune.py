@@ -4,9 +4,10 @@ Each calculation carries its own launch-shape tunables (PMGB_TUNE_* in
 include/apbs_b200.h): the cluster size of the ordered 27-point wavefront on
 the large and middle levels, the fine smoother's kernel and its plane chunk,
 and the size limit of the one-cluster coarse V-cycle tail of the
-mixed-precision path.  None changes a result beyond round-off (the FP64
-smoother and wavefront keys change none at all), so the best values are a
-pure speed question that depends on the grid shape and on the device.
+mixed-precision path, and the smoothing counts of the mixed path's inner FP32
+V-cycle.  The FP64 keys change no result at all; the mixed keys change the
+path to the converged solution (the same stopping test holds), so the best
+values are a speed question that depends on the grid shape and the device.
 
 The tuner times whole solves of the actual problem (device time of
 pmgb_solve from CUDA events, best of a few after a warm-up solve that
@@ -29,7 +30,7 @@ from typing import Callable
 from . import vpmg
 from .vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
                    TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_MC_COOPERATIVE,
-                   TUNE_TAIL_MAX_POINTS)
+                   TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS, TUNE_TAIL_MAX_POINTS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
@@ -43,6 +44,8 @@ CANDIDATES = {
         TUNE_GS7_SWEEP_KCHUNK: [16, 8, 32],
     },
     MIXED: {
+        TUNE_MIXED_COARSE_SWEEPS: [2, 1, 3],
+        TUNE_MIXED_FINE_SWEEPS: [2, 1, 3],
         TUNE_TAIL_MAX_POINTS: [70000, 20000, 200000],
         TUNE_MC_COOPERATIVE: [0, 1],
         TUNE_GS7_COLOUR_PASSES: [0, 2],
@@ -52,7 +55,9 @@ CANDIDATES = {
 
 KEY_NAMES = {TUNE_GS27_CLUSTER: "gs27_cluster", TUNE_GS27_CLUSTER_MID: "gs27_cluster_mid",
              TUNE_GS7_COLOUR_PASSES: "gs7_colour_passes", TUNE_GS7_SWEEP_KCHUNK: "gs7_sweep_kchunk",
-             TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative"}
+             TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative",
+             TUNE_MIXED_COARSE_SWEEPS: "mixed_coarse_sweeps",
+             TUNE_MIXED_FINE_SWEEPS: "mixed_fine_sweeps"}
 
 
 def shape_key(params, precision: int) -> str:

@@ -376,7 +376,7 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 0, 0, 0, 0, 0, 0};
+int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk) {

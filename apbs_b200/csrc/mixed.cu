@@ -520,6 +520,7 @@ struct TailArgs {
   int nd;
   double* xnum;         // damping sums of the first -> first-1 correction
   double* xden;
+  int nsweep;           // 8-colour sweeps before and after each coarse correction
 };
 
 __device__ __forceinline__ float nb27t(const TLev& L, const float* x, size_t id) {
@@ -576,11 +577,11 @@ __device__ void tail_sum2(double& a, double& b, double* sh, double* slots, int& 
 }
 
 template <int CLUSTER>
-__device__ void tail_smooth(const TLev& L, int reverse, int gtid, int nthr) {
+__device__ void tail_smooth(const TLev& L, int reverse, int gtid, int nthr, int nsweep) {
   const Grid g = L.g;
   const int hx = (g.nx - 1) / 2, hy = (g.ny - 1) / 2, hz = (g.nz - 1) / 2;
   const int tot = hx * hy * hz;
-  for (int sw = 0; sw < 2; sw++)
+  for (int sw = 0; sw < nsweep; sw++)
     for (int c8 = 0; c8 < 8; c8++) {
       const int c = reverse ? 7 - c8 : c8;
       const int pi = c & 1, pj = (c >> 1) & 1, pk = (c >> 2) & 1;
@@ -661,7 +662,7 @@ __device__ void tail_cycle(const TailArgs& A, bool rhs_given, int gtid, int nthr
     }
     tail_sync<CLUSTER>();
     if (l != A.last) {
-      tail_smooth<CLUSTER>(L, 0, gtid, nthr);
+      tail_smooth<CLUSTER>(L, 0, gtid, nthr, A.nsweep);
       const Grid g = L.g;
       const int ex = g.nx - 2, ey = g.ny - 2, nint = ex * ey * (g.nz - 2);
       for (int q = gtid; q < nint; q += nthr) {
@@ -709,7 +710,7 @@ __device__ void tail_cycle(const TailArgs& A, bool rhs_given, int gtid, int nthr
       P.x[gf.idx(i, j, k)] += xdamp * w;
     }
     tail_sync<CLUSTER>();
-    tail_smooth<CLUSTER>(P, 1, gtid, nthr);
+    tail_smooth<CLUSTER>(P, 1, gtid, nthr, A.nsweep);
   }
 }
 
@@ -882,6 +883,7 @@ struct BatchItem {
   double errtol;
   int itmax;
   int nlog;
+  int fine_sweeps;        // red-black sweeps before and after the coarse correction
   double* out;            // [0] corrections, [1] final relative residual, [2..] log
 };
 
@@ -956,10 +958,10 @@ __global__ void __launch_bounds__(512) k_batch_solve(const BatchItem* __restrict
     // FP32 V-cycle on A e = w0
     for (int q = gtid; q < n; q += nthr) B.e[q] = 0.f;
     tail_sync<CLUSTER>();
-    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    for (int sw = 0; sw < B.fine_sweeps; sw++) {
+      batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+      batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+    }
     for (int q = gtid; q < nint; q += nthr) {
       const size_t id = interior(q);
       const float* const* o = B.op32;
@@ -987,10 +989,10 @@ __global__ void __launch_bounds__(512) k_batch_solve(const BatchItem* __restrict
       B.e[g.idx(i, j, k)] += xdamp * w;
     }
     tail_sync<CLUSTER>();
-    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 0, gtid, nthr);
-    batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    for (int sw = 0; sw < B.fine_sweeps; sw++) {
+      batch_gs7<CLUSTER>(B, 0, gtid, nthr);
+      batch_gs7<CLUSTER>(B, 1, gtid, nthr);
+    }
     for (int q = gtid; q < nint; q += nthr) {
       const size_t id = interior(q);
       B.x[id] += (double)B.e[id];
@@ -1087,7 +1089,7 @@ int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, 
 
 cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
                     float* xs, const int* tune) {
-  if (!tune[3] && tune[5] == 2 && xs) {
+  if (!tune[3] && tune[5] == 2 && tune[11] == 2 && xs) {
     // two single-pass sweeps x -> xs -> x, then the residual
     Gs7Sweep<float> a;
     a.g = F.g;
@@ -1106,11 +1108,11 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
     }
     return e;
   }
-  if (!tune[3]) {
-    // colour passes: 2 sweeps, then the residual
+  if (!tune[3] || tune[11] != 2) {
+    // colour passes: the sweeps, then the residual
     const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
     const OpF fo = opf(F);
-    for (int sw = 0; sw < 2; sw++) {
+    for (int sw = 0; sw < tune[11]; sw++) {
       k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, first_parity);
       k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x,
                                                          1 - first_parity);
@@ -1406,6 +1408,7 @@ int launch_tail(pmgb_solver* s, cudaStream_t st) {
   A.r = m->w2;
   A.minv = m->dense;
   A.nd = m->nd;
+  A.nsweep = s->tune[10];
   A.xnum = s->scal + S_XNUM_L + ((tf - 1) & 15);
   A.xden = s->scal + S_XDEN_L + ((tf - 1) & 15);
   cudaLaunchConfig_t cfg = {};
@@ -1444,7 +1447,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     set_error("FP32 gs7 pipeline launch failed");
     return 0;
   }
-  k += s->tune[3] ? 1 : 5;
+  k += (s->tune[3] && s->tune[11] == 2) ? 1 : 2 * s->tune[11] + 1;
   const int tf = m->tail_first > 0 ? m->tail_first : nl;
   for (int l = 1; l < tf; l++) {
     MLevel& C = m->lev[l];
@@ -1453,7 +1456,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     k++;
     if (l != nl - 1) {
       CKM(cudaMemsetAsync(C.x, 0, C.g.n() * sizeof(float), st));
-      if (!gs27_mc(st, C, C.x, 2, 0, k, s->tune[9])) return 0;
+      if (!gs27_mc(st, C, C.x, s->tune[10], 0, k, s->tune[9])) return 0;
       const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
       k_resid_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.w0, C.x, m->r);
       k++;
@@ -1487,9 +1490,9 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
         set_error("FP32 gs7 pipeline launch failed");
         return 0;
       }
-      k += s->tune[3] ? 1 : 4;
+      k += (s->tune[3] && s->tune[11] == 2) ? 1 : 2 * s->tune[11];
     } else {
-      if (!gs27_mc(st, P, P.x, 2, 1, k, s->tune[9])) return 0;
+      if (!gs27_mc(st, P, P.x, s->tune[10], 1, k, s->tune[9])) return 0;
     }
   }
   // x64 += e ; r = f - (A + cc) x64 (FP64) -> FP32 rhs ; ||r||_1
@@ -1702,6 +1705,7 @@ int launch_coarse_exact(pmgb_solver* s, cudaStream_t st, const double* cc, const
   E.T.r = m->w2;
   E.T.minv = m->dense;
   E.T.nd = m->nd;
+  E.T.nsweep = 2;
   E.T.xnum = s->scal + S_TMP;
   E.T.xden = s->scal + S_TMP;
   E.g = s->lev[lo].g;
@@ -1826,6 +1830,8 @@ extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_s
     B.T.r = m->w2;
     B.T.minv = m->dense;
     B.T.nd = m->nd;
+    B.T.nsweep = s->tune[10];
+    B.fine_sweeps = s->tune[11];
     B.T.xnum = s->scal + S_TMP;
     B.T.xden = s->scal + S_TMP;
     B.g = s->g;

@@ -1371,6 +1371,11 @@ extern "C" int pmgb_set_tuning(int key, int value) {
     set_error("pmgb_set_tuning: bad key %d", key);
     return 0;
   }
+  if ((key == PMGB_TUNE_MIXED_COARSE_SWEEPS || key == PMGB_TUNE_MIXED_FINE_SWEEPS) &&
+      (value < 1 || value > 4)) {
+    set_error("pmgb_set_tuning: sweeps must be 1..4");
+    return 0;
+  }
   g_tune[key] = value;
   return 1;
 }
@@ -1383,6 +1388,11 @@ extern "C" int pmgb_get_tuning(int key) {
 extern "C" int pmgb_solver_set_tuning(pmgb_solver* s, int key, int value) {
   if (!s || key < 0 || key >= PMGB_TUNE_NKEYS) {
     set_error("pmgb_solver_set_tuning: bad solver or key %d", key);
+    return 0;
+  }
+  if ((key == PMGB_TUNE_MIXED_COARSE_SWEEPS || key == PMGB_TUNE_MIXED_FINE_SWEEPS) &&
+      (value < 1 || value > 4)) {
+    set_error("pmgb_solver_set_tuning: sweeps must be 1..4");
     return 0;
   }
   if (s->tune[key] == value) return 1;

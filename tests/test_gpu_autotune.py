@@ -73,3 +73,18 @@ def test_mixed_cooperative_smoother_matches_per_colour():
     e0, u0, h0 = _solve(p, m, MIXED, {})
     e1, u1, h1 = _solve(p, m, MIXED, {TUNE_MC_COOPERATIVE: 1})
     assert e0 == e1 and np.array_equal(u0, u1) and np.array_equal(h0, h1)
+
+
+def test_mixed_smoothing_counts_reach_the_same_solution():
+    """The inner FP32 V-cycle's smoothing counts change the path, not the
+    converged answer: every setting meets the stopping test and the energy
+    agrees with FP64 to the mixed-precision tolerance."""
+    from apbs_b200.vpmg import TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS
+    m = synth.cluster(400, 11.0, seed=12, net_charge=2.0)
+    for npbe in (False, True):
+        p = synth.mg_manual(97, 0.4, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+        e64, _, _ = _solve(p, m, FP64, {})
+        for tune in ({TUNE_MIXED_COARSE_SWEEPS: 1}, {TUNE_MIXED_FINE_SWEEPS: 1},
+                     {TUNE_MIXED_COARSE_SWEEPS: 3, TUNE_MIXED_FINE_SWEEPS: 3}):
+            e, _, _ = _solve(p, m, MIXED, tune)
+            assert abs(e - e64) <= 1e-6 * abs(e64), (npbe, tune)
