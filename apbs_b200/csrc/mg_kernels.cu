@@ -376,16 +376,18 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
+int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};  // key 12: staged sweep
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                       const double* xin, double* xout, int first_parity, int kchunk) {
+                       const double* xin, double* xout, int first_parity, int kchunk,
+                       int staged) {
   Gs7Sweep<double> a;
   a.g = g;
   a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
   a.c1 = first_parity;
   a.kchunk = kchunk;
+  if (staged) return launch_gs7_sweep_async<double, 32, 8>(s, a) == cudaSuccess;
   return launch_gs7_sweep<double, 32, 8>(s, a) == cudaSuccess;
 }
 

@@ -858,8 +858,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     k += 1;
   } else {
     // two single-pass sweeps, x -> xs -> x
-    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6]) ||
-        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6])) {
+    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6], s->tune[12]) ||
+        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6], s->tune[12])) {
       set_error("gs7 sweep launch failed");
       return 0;
     }
@@ -926,8 +926,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
           k += 2;
         }
       } else {
-        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6]) ||
-            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6])) {
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6], s->tune[12]) ||
+            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6], s->tune[12])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1343,7 +1343,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_SWEEP_FP64:
         // one full sweep: oE oN uC oC cc fc and x read, x written: 56 B per point
         if (!launch_gs7_sweep64(st, F.g, F.ops(), F.cc, F.fc, (r & 1) ? s->xs : F.x,
-                                (r & 1) ? F.x : s->xs, 1, s->tune[6])) {
+                                (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }

@@ -170,6 +170,8 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_MIXED_COARSE_SWEEPS 10 /* mixed: 8-colour GS sweeps before and after each
                                             coarse correction on 27-point levels (default 2) */
 #define PMGB_TUNE_MIXED_FINE_SWEEPS 11 /* mixed: red-black sweeps on the fine level (default 2) */
+#define PMGB_TUNE_GS7_SWEEP_STAGED 12 /* single-pass sweep with plane tiles staged through
+                                          shared memory by asynchronous copies (1) */
 #define PMGB_TUNE_NKEYS 16
 int pmgb_set_tuning(int key, int value);
 int pmgb_get_tuning(int key);

@@ -126,23 +126,27 @@ def test_exact_coarse_solve_matches_band():
 
 
 def test_single_pass_sweep_matches_colour_passes():
-    """The fine smoother's single-pass sweep kernel (default) and the one-launch-
-    per-colour kernels compute the same red-black sweep: bitwise equal results."""
-    from apbs_b200.vpmg import TUNE_GS7_COLOUR_PASSES, get_tuning, set_tuning
+    """The fine smoother's single-pass sweep kernel (default), its variant with
+    shared-memory staged planes and the one-launch-per-colour kernels compute
+    the same red-black sweep: bitwise equal results."""
+    from apbs_b200.vpmg import (TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_STAGED, get_tuning,
+                                set_tuning)
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
     out = {}
     old = get_tuning(TUNE_GS7_COLOUR_PASSES)
     try:
         for npbe in (False, True):
             p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
-            for passes in (1, 0):
+            for passes, staged in ((1, 0), (0, 0), (0, 1)):
                 set_tuning(TUNE_GS7_COLOUR_PASSES, passes)
                 with Vpmg(p, FP64) as pmg:
+                    pmg.set_tuning(TUNE_GS7_SWEEP_STAGED, staged)
                     pmg.fillco(m)
                     pmg.solve()
-                    out[(npbe, passes)] = (pmg.u, pmg.residual_history())
+                    out[(npbe, passes, staged)] = (pmg.u, pmg.residual_history())
     finally:
         set_tuning(TUNE_GS7_COLOUR_PASSES, old)
     for npbe in (False, True):
-        assert np.array_equal(out[(npbe, 0)][0], out[(npbe, 1)][0])
-        assert np.array_equal(out[(npbe, 0)][1], out[(npbe, 1)][1])
+        for var in ((0, 0), (0, 1)):
+            assert np.array_equal(out[(npbe,) + var][0], out[(npbe, 1, 0)][0]), var
+            assert np.array_equal(out[(npbe,) + var][1], out[(npbe, 1, 0)][1]), var
