@@ -79,10 +79,12 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
   const int kmax = min(g.nz - 1, (int)floor((posz + zr) / hz));
   if (imax < imin || jmax < jmin || kmax < kmin) return;
   const int ni = imax - imin + 1, nj = jmax - jmin + 1;
-  // lanes take (i, j) columns; the column test of the reference prunes
-  // whole columns before the k loop
+  // lanes take (i, j) columns, consecutive lanes consecutive i so a warp's
+  // stores to one plane fall on a few contiguous runs; the column test of the
+  // reference prunes whole columns before the k loop.  Every store writes the
+  // same value, so the order of the stores does not matter.
   for (int t = lane; t < ni * nj; t += nlanes) {
-    const int ii = imin + t / nj, jj = jmin + t % nj;
+    const int ii = imin + t % ni, jj = jmin + t / ni;
     const double fi = (double)ii, fj = (double)jj;
     const double dx2 = (posx - hx * fi) * (posx - hx * fi);
     const double dy2 = (posy - hy * fj) * (posy - hy * fj);
@@ -195,73 +197,86 @@ __global__ void k_cell_fill(int natoms, const int* __restrict__ cell_of, int* fi
   atoms_sorted[p] = a;
 }
 
+// One thread per (atom, reference point); the accessible points are appended
+// to a list (warp-aggregated), so the marking pass runs over them only.
 __global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xyz,
                            const double* __restrict__ r, const double* __restrict__ ref,
                            int nref, double srad, const int* __restrict__ start,
-                           const int* __restrict__ atoms_sorted, unsigned char* flags,
-                           int* npts) {
+                           const int* __restrict__ atoms_sorted, unsigned* list, int* npts) {
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (tid >= (long long)natoms * nref) return;
-  const int a = (int)(tid / nref), t = (int)(tid % nref);
-  const double arad = r[a];
-  unsigned char acc = 0;
-  if (!(arad < 1.0e-9)) {
-    const double rad = arad + srad;
-    const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
-    const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
-    const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
-    int c[3];
-    const double pp[3] = {px, py, pz};
-    for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
-    acc = 1;
-    for (int dz = -1; dz <= 1 && acc; dz++)
-      for (int dy = -1; dy <= 1 && acc; dy++)
-        for (int dx = -1; dx <= 1 && acc; dx++) {
-          const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
-          if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
-            continue;
-          const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
-          for (int s = start[cell]; s < start[cell + 1]; s++) {
-            const int b = atoms_sorted[s];
-            if (b == a) continue;
-            const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1],
-                         d2 = pz - xyz[3 * b + 2];
-            const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
-            const double rr = r[b] + srad;
-            if (dist2 < rr * rr) {
-              acc = 0;
-              break;
+  bool acc = false;
+  if (tid < (long long)natoms * nref) {
+    const int a = (int)(tid / nref), t = (int)(tid % nref);
+    const double arad = r[a];
+    if (!(arad < 1.0e-9)) {
+      const double rad = arad + srad;
+      const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
+      const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
+      const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+      int c[3];
+      const double pp[3] = {px, py, pz};
+      for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
+      acc = true;
+      for (int dz = -1; dz <= 1 && acc; dz++)
+        for (int dy = -1; dy <= 1 && acc; dy++)
+          for (int dx = -1; dx <= 1 && acc; dx++) {
+            const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+            if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
+              continue;
+            const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
+            for (int s = start[cell]; s < start[cell + 1]; s++) {
+              const int b = atoms_sorted[s];
+              if (b == a) continue;
+              const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1],
+                           d2 = pz - xyz[3 * b + 2];
+              const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+              const double rr = r[b] + srad;
+              if (dist2 < rr * rr) {
+                acc = false;
+                break;
+              }
             }
           }
-        }
+    }
   }
-  flags[tid] = acc;
-  if (acc) atomicAdd(npts, 1);
+  const unsigned m = __ballot_sync(0xffffffffu, acc);
+  if (m) {
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(npts, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (acc) list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)tid;
+  }
 }
 
 // Probe spheres around accessible SAS points reset the three dielectric
-// grids to epsw (vpmg.c:4456-4496).  One warp per surface point.
-__global__ void k_sas_mark(FillGeom G, int natoms, const double* __restrict__ xyz,
+// grids to epsw (vpmg.c:4456-4496).  One warp per listed surface point; the
+// grid is sized for the device and strides over the list, whose length the
+// test pass left in *npts.
+__global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
                            const double* __restrict__ r, const double* __restrict__ ref,
-                           int nref, double srad, double epsw,
-                           const unsigned char* __restrict__ flags, double* epsx, double* epsy,
+                           int nref, double srad, double epsw, const unsigned* __restrict__ list,
+                           const int* __restrict__ npts, double* epsx, double* epsy,
                            double* epsz) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int n = *npts;
   const int lane = threadIdx.x & 31;
-  if (w >= (long long)natoms * nref) return;
-  if (!flags[w]) return;
-  const int a = (int)(w / nref), t = (int)(w % nref);
-  const double rad = r[a] + srad;
-  const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
-  const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
-  const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
-  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
-                    G.xmin[2], epsx, epsw, lane, 32);
-  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
-                    G.xmin[2], epsy, epsw, lane, 32);
-  mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
-                    (G.xmin[2] + 0.5 * hz), epsz, epsw, lane, 32);
+  for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < n;
+       w += nwarps) {
+    const unsigned tid = list[w];
+    const int a = (int)(tid / (unsigned)nref), t = (int)(tid % (unsigned)nref);
+    const double rad = r[a] + srad;
+    const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
+    const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
+    const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
+                      G.xmin[2], epsx, epsw, lane, 32);
+    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
+                      G.xmin[2], epsy, epsw, lane, 32);
+    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
+                      (G.xmin[2] + 0.5 * hz), epsz, epsw, lane, 32);
+  }
 }
 
 // 9-point harmonic-mean smoothing, fillcoCoefMolDielSmooth (vpmg.c:4500-4628).
@@ -662,15 +677,27 @@ void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const doub
 }
 void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
                 const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, unsigned char* flags,
+                double epsw, const int* start, const int* sorted, unsigned* list,
                 int* npts, double* epsx, double* epsy, double* epsz) {
   const long long tot = (long long)natoms * nref;
   if (tot <= 0) return;
   cudaMemsetAsync(npts, 0, sizeof(int), s);
   k_sas_test<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(C, natoms, xyz, r, ref, nref, srad,
-                                                           start, sorted, flags, npts);
-  k_sas_mark<<<(unsigned)((tot * 32 + 255) / 256), 256, 0, s>>>(
-      G, natoms, xyz, r, ref, nref, srad, epsw, flags, epsx, epsy, epsz);
+                                                           start, sorted, list, npts);
+  static const int nblocks = [] {
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sas_mark, 256, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    return sms * per_sm;
+  }();
+  const long long want = (tot + 7) / 8;  // 8 warps per block
+  const unsigned nb = (unsigned)std::min<long long>(nblocks, want);
+  k_sas_mark<<<nb, 256, 0, s>>>(G, xyz, r, ref, nref, srad, epsw, list, npts, epsx, epsy,
+                                epsz);
 }
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
                    const double* a3, double* epsx, double* epsy, double* epsz) {

@@ -58,7 +58,7 @@ void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const doub
                        int* count, int* start, int* fillpos, int* cell_of, int* sorted);
 void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
                 const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, unsigned char* flags,
+                double epsw, const int* start, const int* sorted, unsigned* list,
                 int* npts, double* epsx, double* epsy, double* epsz);
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
                    const double* a3, double* epsx, double* epsy, double* epsz);

@@ -376,7 +376,7 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};  // key 12: staged sweep
+int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
@@ -560,6 +560,210 @@ __global__ void k_gs27_wave(Grid g, Op op, const double* __restrict__ cc,
       __syncthreads();
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// The same wavefront schedule with one CTA per interior plane k, synchronised
+// point to point instead of by a barrier over all CTAs.
+//
+// A step's items on plane k read values of planes k-1, k and k+1 only, so a
+// CTA may start step s once its two neighbour planes have finished step s-1;
+// each CTA publishes the number of steps it has finished in a counter.  A CTA
+// then runs at most one step ahead of its neighbours and never starts step s+1
+// before they have finished step s, so every value a step reads was written
+// in an earlier step and no value is overwritten before the step that reads
+// it, exactly as with the barrier: the iterates are bitwise those of
+// k_gs27_wave.  Spreading the planes over up to all SMs (one CTA each, a
+// cooperative launch so that all are resident together) divides the
+// per-step work that bounds the one-cluster kernel by the number of planes.
+//
+// The counters of a level are never reset between launches: every CTA of a
+// launch finishes all steps (after a wait that ran out it records the
+// failure in *err and stops waiting), so at the start of a launch all
+// counters of the level are equal and each CTA takes its own as the base.
+// Differences are taken modulo 2^32.
+// ---------------------------------------------------------------------------
+constexpr long long kWaveWaitNs = 200LL * 1000 * 1000;  // 200 ms per wait
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Coefficients of one point's 27-point update in the order sum27 reads them.
+struct Coef27 {
+  double o[8], u[9], d[9], f, oc, cc;
+};
+__device__ __forceinline__ void load_coef27(const Op& op, const double* __restrict__ cc,
+                                            const double* __restrict__ fc, size_t id, size_t sy,
+                                            size_t sz, Coef27& C) {
+  const double* const* c = op.c;
+  C.o[0] = c[ON][id]; C.o[1] = c[ON][id - sy]; C.o[2] = c[OE][id]; C.o[3] = c[OE][id - 1];
+  C.o[4] = c[ONE][id]; C.o[5] = c[ONW][id]; C.o[6] = c[ONW][id - sy + 1];
+  C.o[7] = c[ONE][id - sy - 1];
+  C.u[0] = c[UC][id]; C.u[1] = c[UN][id]; C.u[2] = c[US][id]; C.u[3] = c[UE][id];
+  C.u[4] = c[UW][id]; C.u[5] = c[UNE][id]; C.u[6] = c[UNW][id]; C.u[7] = c[USE][id];
+  C.u[8] = c[USW][id];
+  C.d[0] = c[UC][id - sz]; C.d[1] = c[US][id - sz + sy]; C.d[2] = c[UN][id - sz - sy];
+  C.d[3] = c[UW][id - sz + 1]; C.d[4] = c[UE][id - sz - 1]; C.d[5] = c[USW][id - sz + sy + 1];
+  C.d[6] = c[USE][id - sz + sy - 1]; C.d[7] = c[UNW][id - sz - sy + 1];
+  C.d[8] = c[UNE][id - sz - sy - 1];
+  C.f = fc[id]; C.oc = c[OC][id]; C.cc = cc[id];
+}
+// tmpO, tmpU, tmpD of sum27<true> from prefetched coefficients: the same
+// products added in the same order.
+__device__ __forceinline__ void sum27_pre(const Coef27& C, const double* x, size_t id,
+                                          size_t sy, size_t sz, double& tO, double& tU,
+                                          double& tD) {
+  auto X = [&](size_t p) -> double { return __ldcg(x + p); };
+  tO = +C.o[0] * X(id + sy) + C.o[1] * X(id - sy) + C.o[2] * X(id + 1) +
+       C.o[3] * X(id - 1) + C.o[4] * X(id + sy + 1) + C.o[5] * X(id + sy - 1) +
+       C.o[6] * X(id - sy + 1) + C.o[7] * X(id - sy - 1);
+  tU = +C.u[0] * X(id + sz) + C.u[1] * X(id + sz + sy) + C.u[2] * X(id + sz - sy) +
+       C.u[3] * X(id + sz + 1) + C.u[4] * X(id + sz - 1) + C.u[5] * X(id + sz + sy + 1) +
+       C.u[6] * X(id + sz + sy - 1) + C.u[7] * X(id + sz - sy + 1) +
+       C.u[8] * X(id + sz - sy - 1);
+  tD = +C.d[0] * X(id - sz) + C.d[1] * X(id - sz + sy) + C.d[2] * X(id - sz - sy) +
+       C.d[3] * X(id - sz + 1) + C.d[4] * X(id - sz - 1) + C.d[5] * X(id - sz + sy + 1) +
+       C.d[6] * X(id - sz + sy - 1) + C.d[7] * X(id - sz - sy + 1) +
+       C.d[8] * X(id - sz - sy - 1);
+}
+
+constexpr int kPlanesThreads = 384;  // a step's items never exceed the CTA
+
+__global__ void __launch_bounds__(kPlanesThreads, 1)
+    k_gs27_planes(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ fc,
+                  double* x, double* r, int nhalf, int first_parity, int do_resid,
+                  unsigned* counters, int* err) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  const int tmin = 1 + 2 * 1, tmax = (ny - 2) + 2 * (nz - 2);
+  const int nphase = nhalf + (do_resid ? 1 : 0);
+  const int resid_lag = kWaveLag * (nhalf - 1) + 4;
+  const int last_start = do_resid ? resid_lag : kWaveLag * (nhalf - 1);
+  const int nsteps = (tmax - tmin + 1) + last_start;
+  const int hr = (nx - 1) / 2;
+  const int c = blockIdx.x, k = 1 + c;  // this CTA's plane
+  const int ncta = gridDim.x;
+  __shared__ unsigned base_sh;
+  __shared__ int failed_sh;
+  if (threadIdx.x == 0) {
+    base_sh = counters[c];
+    failed_sh = 0;
+  }
+  __syncthreads();
+  const unsigned base = base_sh;
+  // this thread's item of step s: the point id, 0 = none, 1 = GS update,
+  // 2 = residual (every item of a step is one thread's: blockDim covers them)
+  auto item_of = [&](int s, size_t& id) -> int {
+    int m = threadIdx.x;
+    for (int ph = 0; ph < nphase; ph++) {
+      const int lag = (ph < nhalf) ? kWaveLag * ph : resid_lag;
+      const int t = tmin + s - lag;
+      const int j = t - 2 * k;
+      if (t < tmin || t > tmax || j < 1 || j > ny - 2) continue;
+      const int cnt = (ph < nhalf) ? hr : (nx - 2);
+      if (m >= cnt) {
+        m -= cnt;
+        continue;
+      }
+      if (ph < nhalf) {
+        const int parity = (first_parity + ph) & 1;
+        const int i = 1 + (((1 + j + k) & 1) != parity) + 2 * m;
+        if (i > nx - 2) return 0;
+        id = g.idx(i, j, k);
+        return 1;
+      }
+      id = g.idx(1 + m, j, k);
+      return 2;
+    }
+    return 0;
+  };
+  size_t id = 0;
+  int kind = (nsteps > 0) ? item_of(0, id) : 0;
+  Coef27 C;
+  if (kind) load_coef27(op, cc, fc, id, sy, sz, C);
+  for (int s = 0; s < nsteps; s++) {
+    if (s > 0) {
+      if (threadIdx.x == 0 && !failed_sh) {
+        const unsigned need = base + (unsigned)s;
+        const unsigned long long t0 = global_ns();
+        for (int nb = -1; nb <= 1; nb += 2) {
+          if (c + nb < 0 || c + nb >= ncta) continue;
+          const unsigned* f = counters + c + nb;
+          while ((int)(ld_acquire(f) - need) < 0) {
+            if ((long long)(global_ns() - t0) > kWaveWaitNs) {
+              failed_sh = 1;
+              atomicAdd(err, 1);
+              break;
+            }
+          }
+          if (failed_sh) break;
+        }
+      }
+      __syncthreads();
+    }
+    if (kind) {
+      double tO, tU, tD;
+      sum27_pre(C, x, id, sy, sz, tO, tU, tD);
+      if (kind == 1) {
+        __stcg(x + id, (C.f + (tO + tU + tD)) / (C.oc + C.cc));
+      } else {
+        r[id] = C.f + tO + tU + tD - (C.oc + C.cc) * __ldcg(x + id);
+      }
+    }
+    // the next step's coefficients do not depend on this step: fetch them
+    // while the neighbour planes finish
+    size_t nid = 0;
+    const int nkind = (s + 1 < nsteps) ? item_of(s + 1, nid) : 0;
+    if (nkind) load_coef27(op, cc, fc, nid, sy, sz, C);
+    kind = nkind;
+    id = nid;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release(counters + c, base + (unsigned)(s + 1));
+    }
+  }
+}
+
+int wave_planes_fit(Grid g) {
+  static const int capacity = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs27_planes, kPlanesThreads,
+                                                      0) != cudaSuccess)
+      per_sm = 0;
+    return sms * per_sm;
+  }();
+  const int planes = g.nz - 2;
+  const int items = 4 * ((g.nx - 1) / 2) + (g.nx - 2);  // two sweeps + residual
+  return planes >= 2 && planes <= kWavePlanesMax && planes <= capacity &&
+         items <= kPlanesThreads;
+}
+
+int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                       double* x, double* r, int nsweep, int first_parity, unsigned* counters,
+                       int* err) {
+  int nhalf = 2 * nsweep;
+  int do_resid = (r != nullptr) ? 1 : 0;
+  const int hr = (g.nx - 1) / 2;
+  const int items = nhalf * hr + (do_resid ? g.nx - 2 : 0);
+  if (items > kPlanesThreads) return 0;
+  const int threads = std::max(64, (items + 31) / 32 * 32);
+  void* args[] = {&g, &op, &cc, &fc, &x, &r, &nhalf, &first_parity, &do_resid, &counters, &err};
+  return cudaLaunchCooperativeKernel((void*)k_gs27_planes, dim3(g.nz - 2), dim3(threads), args,
+                                     0, s) == cudaSuccess;
 }
 
 int mg_init() {
@@ -1010,14 +1214,353 @@ __global__ void k_cg_coarse(Grid g, Op op, const double* __restrict__ cc,
   csync();
 }
 
+// The same iteration for a coarsest level that one CTA holds: the direction
+// p lives in shared memory over the whole grid (zero boundary), x, r and A p
+// of a thread's points stay in registers, and each sum is one barrier (every
+// thread adds the warp partials itself).  Points are assigned to threads and
+// partial sums are added in the same order as k_cg_coarse<1> with 512
+// threads, so both kernels produce bitwise equal iterates; this one only
+// saves the global-memory round trips and barriers between the vector passes.
+constexpr int kCgThreads = 512, kCgPPT = 2;
+constexpr size_t kCgSmemMax = 200 * 1024;
+
+__global__ void __launch_bounds__(kCgThreads)
+    k_cg_coarse_onchip(Grid g, Op op, const double* __restrict__ cc,
+                       const double* __restrict__ fc, double* x, double* r, int itmax,
+                       double errtol, int* iters_out) {
+  extern __shared__ double ps[];
+  __shared__ double sh[2][32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nint = (nx - 2) * (ny - 2) * (nz - 2);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (size_t q = threadIdx.x; q < g.n(); q += blockDim.x) ps[q] = 0.0;
+  size_t id[kCgPPT];
+  bool own[kCgPPT];
+  double rl[kCgPPT], xl[kCgPPT], dg[kCgPPT], al[kCgPPT];
+  double acc = 0.0;
+  // r = f - (A + cc) x   (x = 0 on entry)
+#pragma unroll
+  for (int m = 0; m < kCgPPT; m++) {
+    const int q = threadIdx.x + m * blockDim.x;
+    own[m] = q < nint;
+    id[m] = 0;
+    rl[m] = xl[m] = dg[m] = al[m] = 0.0;
+    if (!own[m]) continue;
+    const int i = 1 + q % (nx - 2);
+    const int j = 1 + (q / (nx - 2)) % (ny - 2);
+    const int k = 1 + q / ((nx - 2) * (ny - 2));
+    id[m] = g.idx(i, j, k);
+    double tO, tU, tD;
+    sum27<true>(op, g, x, id[m], tO, tU, tD);
+    xl[m] = __ldcg(x + id[m]);
+    dg[m] = op.c[OC][id[m]] + cc[id[m]];
+    const double rv = fc[id[m]] + tO + tU + tD - (op.c[OC][id[m]] + cc[id[m]]) * xl[m];
+    rl[m] = rv;
+    acc += rv * rv;
+  }
+  int phase = 0;
+  auto bsum = [&](double v) {
+    v = warp_sum(v);
+    if (lane == 0) sh[phase][wid] = v;
+    __syncthreads();
+    double b = 0.0;
+    for (int w = 0; w < nw; w++) b += sh[phase][w];
+    phase ^= 1;
+    return b;
+  };
+  const double denom = sqrt(bsum(acc));
+  int iters = 0;
+  if (denom != 0.0) {
+    double rhok1 = 0.0;
+    for (;;) {
+      acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < kCgPPT; m++)
+        if (own[m]) acc += rl[m] * rl[m];
+      const double rhok2 = bsum(acc);
+      if (sqrt(rhok2) / denom <= errtol) break;
+      if (iters >= itmax) break;
+      if (iters == 0) {
+#pragma unroll
+        for (int m = 0; m < kCgPPT; m++)
+          if (own[m]) ps[id[m]] = rl[m];
+      } else {
+        const double beta = rhok2 / rhok1;
+        const double alpha = 1.0 / beta;
+#pragma unroll
+        for (int m = 0; m < kCgPPT; m++) {
+          if (!own[m]) continue;
+          double pv = ps[id[m]];
+          pv += alpha * rl[m];
+          pv *= beta;
+          ps[id[m]] = pv;
+        }
+      }
+      __syncthreads();
+      acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < kCgPPT; m++) {
+        if (!own[m]) continue;
+        double tO, tU, tD;
+        sum27<false>(op, g, ps, id[m], tO, tU, tD);
+        const double pv = ps[id[m]];
+        const double av = -tO - tU - tD + dg[m] * pv;
+        al[m] = av;
+        acc += pv * av;
+      }
+      const double pAp = bsum(acc);
+      const double alpha = rhok2 / pAp;
+      rhok1 = rhok2;
+#pragma unroll
+      for (int m = 0; m < kCgPPT; m++) {
+        if (!own[m]) continue;
+        xl[m] = xl[m] + alpha * ps[id[m]];
+        rl[m] = rl[m] + (-alpha) * al[m];
+      }
+      iters++;
+      // the next direction update writes only this thread's points of p; the
+      // two barriers of the sums order it after every read of the matvec
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < kCgPPT; m++) {
+    if (!own[m]) continue;
+    x[id[m]] = xl[m];
+    r[id[m]] = rl[m];
+  }
+  if (threadIdx.x == 0 && iters_out) iters_out[0] = iters;
+}
+
+// The same iteration on a larger coarsest level, one cluster of CL CTAs:
+// CTA `rank` owns the slab of planes k0 .. k1-1 and keeps p over its slab and
+// one halo plane on either side in shared memory (zero boundary); after each
+// direction update it copies the two halo planes from its neighbours' shared
+// memory (distributed shared memory) behind a cluster barrier.  x, r and A p
+// of its points stay in registers.  Sums go block by block in rank order, so
+// every CTA sees the same scalars and the iteration is deterministic.
+constexpr int kSlabThreads = 512, kSlabPPT = 4;
+
+// tmpO + tmpU + tmpD of sum27 with x read from xs at the offset of xid - id
+__device__ __forceinline__ void sum27_at(const Op& op, Grid g, const double* xs,
+                                         ptrdiff_t off, size_t id, double& tO, double& tU,
+                                         double& tD) {
+  const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
+  auto X = [&](size_t p) -> double { return xs[(ptrdiff_t)p + off]; };
+  const double* const* c = op.c;
+  tO = +c[ON][id] * X(id + sy) + c[ON][id - sy] * X(id - sy) + c[OE][id] * X(id + 1) +
+       c[OE][id - 1] * X(id - 1) + c[ONE][id] * X(id + sy + 1) +
+       c[ONW][id] * X(id + sy - 1) + c[ONW][id - sy + 1] * X(id - sy + 1) +
+       c[ONE][id - sy - 1] * X(id - sy - 1);
+  tU = +c[UC][id] * X(id + sz) + c[UN][id] * X(id + sz + sy) + c[US][id] * X(id + sz - sy) +
+       c[UE][id] * X(id + sz + 1) + c[UW][id] * X(id + sz - 1) +
+       c[UNE][id] * X(id + sz + sy + 1) + c[UNW][id] * X(id + sz + sy - 1) +
+       c[USE][id] * X(id + sz - sy + 1) + c[USW][id] * X(id + sz - sy - 1);
+  tD = +c[UC][id - sz] * X(id - sz) + c[US][id - sz + sy] * X(id - sz + sy) +
+       c[UN][id - sz - sy] * X(id - sz - sy) + c[UW][id - sz + 1] * X(id - sz + 1) +
+       c[UE][id - sz - 1] * X(id - sz - 1) + c[USW][id - sz + sy + 1] * X(id - sz + sy + 1) +
+       c[USE][id - sz + sy - 1] * X(id - sz + sy - 1) +
+       c[UNW][id - sz - sy + 1] * X(id - sz - sy + 1) +
+       c[UNE][id - sz - sy - 1] * X(id - sz - sy - 1);
+}
+
+template <int CL>
+__global__ void __launch_bounds__(kSlabThreads)
+    k_cg_coarse_slab(Grid g, Op op, const double* __restrict__ cc,
+                     const double* __restrict__ fc, double* x, double* r, int itmax,
+                     double errtol, int* iters_out) {
+  extern __shared__ double ps[];  // planes k0-1 .. k1 of p
+  __shared__ double sh[32];
+  __shared__ double slots[2];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t pl = (size_t)nx * ny;
+  const int per = (nz - 2 + CL - 1) / CL;
+  const int k0 = 1 + rank * per;
+  const int k1 = min(k0 + per, nz - 1);
+  const int nown = (k1 > k0) ? (k1 - k0) * (nx - 2) * (ny - 2) : 0;
+  const ptrdiff_t off = -(ptrdiff_t)((size_t)(k0 - 1) * pl);  // global id -> ps index
+  for (size_t q = threadIdx.x; q < (size_t)(per + 2) * pl; q += blockDim.x) ps[q] = 0.0;
+  size_t id[kSlabPPT];
+  bool own[kSlabPPT];
+  double rl[kSlabPPT], xl[kSlabPPT], dg[kSlabPPT], al[kSlabPPT];
+  double acc = 0.0;
+#pragma unroll
+  for (int m = 0; m < kSlabPPT; m++) {
+    const int q = threadIdx.x + m * blockDim.x;
+    own[m] = q < nown;
+    id[m] = 0;
+    rl[m] = xl[m] = dg[m] = al[m] = 0.0;
+    if (!own[m]) continue;
+    const int i = 1 + q % (nx - 2);
+    const int j = 1 + (q / (nx - 2)) % (ny - 2);
+    const int k = k0 + q / ((nx - 2) * (ny - 2));
+    id[m] = g.idx(i, j, k);
+    double tO, tU, tD;
+    sum27<true>(op, g, x, id[m], tO, tU, tD);
+    xl[m] = __ldcg(x + id[m]);
+    dg[m] = op.c[OC][id[m]] + cc[id[m]];
+    const double rv = fc[id[m]] + tO + tU + tD - (op.c[OC][id[m]] + cc[id[m]]) * xl[m];
+    rl[m] = rv;
+    acc += rv * rv;
+  }
+  int phase = 0;
+  auto csum = [&](double v) {
+    const double t = cluster_sum<CL>(v, sh, slots, phase);
+    phase ^= 1;
+    return t;
+  };
+  const double denom = sqrt(csum(acc));
+  int iters = 0;
+  if (denom != 0.0) {
+    double rhok1 = 0.0;
+    for (;;) {
+      acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < kSlabPPT; m++)
+        if (own[m]) acc += rl[m] * rl[m];
+      const double rhok2 = csum(acc);
+      if (sqrt(rhok2) / denom <= errtol) break;
+      if (iters >= itmax) break;
+      if (iters == 0) {
+#pragma unroll
+        for (int m = 0; m < kSlabPPT; m++)
+          if (own[m]) ps[(ptrdiff_t)id[m] + off] = rl[m];
+      } else {
+        const double beta = rhok2 / rhok1;
+        const double alpha = 1.0 / beta;
+#pragma unroll
+        for (int m = 0; m < kSlabPPT; m++) {
+          if (!own[m]) continue;
+          double pv = ps[(ptrdiff_t)id[m] + off];
+          pv += alpha * rl[m];
+          pv *= beta;
+          ps[(ptrdiff_t)id[m] + off] = pv;
+        }
+      }
+      cl.sync();
+      // halo planes: k0-1 is the last owned plane of rank-1, k1 the first of rank+1
+      if (k1 > k0) {
+        if (rank > 0) {
+          const double* src = cl.map_shared_rank(ps, rank - 1) + (size_t)per * pl;
+          for (size_t q = threadIdx.x; q < pl; q += blockDim.x) ps[q] = src[q];
+        }
+        if (rank < CL - 1 && k1 < nz - 1) {
+          const double* src = cl.map_shared_rank(ps, rank + 1) + pl;
+          double* dst = ps + (size_t)(k1 - k0 + 1) * pl;
+          for (size_t q = threadIdx.x; q < pl; q += blockDim.x) dst[q] = src[q];
+        }
+      }
+      __syncthreads();
+      acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < kSlabPPT; m++) {
+        if (!own[m]) continue;
+        double tO, tU, tD;
+        sum27_at(op, g, ps, off, id[m], tO, tU, tD);
+        const double pv = ps[(ptrdiff_t)id[m] + off];
+        const double av = -tO - tU - tD + dg[m] * pv;
+        al[m] = av;
+        acc += pv * av;
+      }
+      const double pAp = csum(acc);
+      const double alpha = rhok2 / pAp;
+      rhok1 = rhok2;
+#pragma unroll
+      for (int m = 0; m < kSlabPPT; m++) {
+        if (!own[m]) continue;
+        xl[m] = xl[m] + alpha * ps[(ptrdiff_t)id[m] + off];
+        rl[m] = rl[m] + (-alpha) * al[m];
+      }
+      iters++;
+      // a neighbour's halo copy of this slab ends before it reaches the next
+      // sum's cluster barrier, which precedes the next direction update here
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < kSlabPPT; m++) {
+    if (!own[m]) continue;
+    x[id[m]] = xl[m];
+    r[id[m]] = rl[m];
+  }
+  if (rank == 0 && threadIdx.x == 0 && iters_out) iters_out[0] = iters;
+  cl.sync();  // no CTA may exit while a neighbour can still read its shared memory
+}
+
+template <int CL>
+static int launch_cg_slab(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                          double* x, double* r, int itmax, double errtol, int* iters_dev,
+                          size_t smem) {
+  static const cudaError_t attr_ok = [] {
+    cudaError_t e = cudaFuncSetAttribute(k_cg_coarse_slab<CL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kCgSmemMax);
+    if (e == cudaSuccess && CL > 8)
+      e = cudaFuncSetAttribute(k_cg_coarse_slab<CL>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+  }();
+  if (attr_ok != cudaSuccess) return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CL, 1, 1);
+  cfg.blockDim = dim3(kSlabThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_cg_coarse_slab<CL>, g, op, cc, fc, x, r, itmax, errtol,
+                            iters_dev) == cudaSuccess;
+}
+
 int launch_cg_coarse(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, double* p, double* ap, int itmax, double errtol,
-                     int* iters_dev) {
+                     int* iters_dev, int want_cluster) {
   const int nint = (g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  const size_t smem = g.n() * sizeof(double);
+  if (nint <= kCgThreads * kCgPPT && smem <= kCgSmemMax) {
+    static const cudaError_t attr_ok = cudaFuncSetAttribute(
+        k_cg_coarse_onchip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCgSmemMax);
+    if (attr_ok != cudaSuccess) return 0;
+    k_cg_coarse_onchip<<<1, kCgThreads, smem, s>>>(g, op, cc, fc, x, r, itmax, errtol,
+                                                   iters_dev);
+    return cudaGetLastError() == cudaSuccess;
+  }
+  // slab clusters: the smallest size whose slabs give each thread at most two
+  // points, else at most kSlabPPT, within one CTA's shared memory (or the
+  // size asked for, if its slabs fit)
+  for (int pass = 0; pass < 2; pass++) {
+    static const int max_cl = [] {
+      int dev = 0, ok = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&ok, cudaDevAttrClusterLaunch, dev);
+      return ok ? 16 : 1;
+    }();
+    const int plane_pts = (g.nx - 2) * (g.ny - 2);
+    const int limit = kSlabThreads * (pass == 0 ? 2 : kSlabPPT);
+    for (int cl = 4; cl <= max_cl; cl *= 2) {
+      if (want_cluster > 0 && cl != want_cluster) continue;
+      const int per = (g.nz - 2 + cl - 1) / cl;
+      const size_t sm = (size_t)(per + 2) * g.nx * g.ny * sizeof(double);
+      if (per * plane_pts > limit || sm > kCgSmemMax) continue;
+      switch (cl) {
+        case 4: return launch_cg_slab<4>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm);
+        case 8: return launch_cg_slab<8>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm);
+        case 16:
+          if (launch_cg_slab<16>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm)) return 1;
+          cudaGetLastError();  // no 16-CTA clusters here: the strided kernel below
+          break;
+      }
+    }
+  }
   int cluster = 1;
   if (nint > 4096) cluster = 8;
   else if (nint > 1024) cluster = 4;
-  const int threads = 512;
+  const int threads = kCgThreads;
   if (cluster == 1) {
     k_cg_coarse<1><<<1, threads, 0, s>>>(g, op, cc, fc, x, r, p, ap, itmax, errtol, iters_dev);
     return cudaGetLastError() == cudaSuccess;

@@ -46,6 +46,17 @@ struct Gs27Plan {
 };
 // Sets kernel attributes; returns the largest usable GS27 cluster size.
 int mg_init();
+// One CTA per interior plane, neighbour planes synchronised by step counters
+// (kWavePlanesMax counters per level, never reset between launches; *err
+// counts waits that ran out).  wave_planes_fit: the level has few enough
+// planes for one resident CTA each.
+constexpr int kWavePlanesMax = 1024;
+constexpr int kWaveCounterBase = 16;  // words before level 0's counters
+constexpr size_t kWaveWords = kWaveCounterBase + 16 * (size_t)kWavePlanesMax;
+int wave_planes_fit(Grid g);
+int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                       double* x, double* r, int nsweep, int first_parity, unsigned* counters,
+                       int* err);
 int launch_gs27_wave(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, int nsweep, int first_parity, Gs27Plan plan);
 
@@ -69,7 +80,7 @@ void launch_band_solve(cudaStream_t s, Grid g, const double* abd, int n, int m, 
 // CG on the coarsest level (Vcghs), all iterations in one cluster launch.
 int launch_cg_coarse(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, double* p, double* ap, int itmax, double errtol,
-                     int* iters_dev);
+                     int* iters_dev, int want_cluster = 0);
 
 // ---- nonlinear (Newton) -----------------------------------------------------
 struct IonTable {

@@ -319,6 +319,8 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
   if (ok) ok &= (cudaMalloc(&s->d_iters, 16 * sizeof(int)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_info, 16 * sizeof(int)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_npts, sizeof(int)) == cudaSuccess);
+  if (ok) ok &= (cudaMalloc(&s->d_wave, kWaveWords * sizeof(unsigned)) == cudaSuccess);
+  if (ok) ok &= (cudaMemset(s->d_wave, 0, kWaveWords * sizeof(unsigned)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_opptrs, sizeof(double*) * 14 * 16) == cudaSuccess);
   if (ok) {
     // the operator arrays never move, so the pointer table is written once
@@ -377,6 +379,9 @@ static int set_geometry(pmgb_solver* s) {
     cudaMemcpy(s->wx, wx.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice);
     cudaMemcpy(s->wy, wy.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice);
     cudaStream_t st = s->stream;
+    // plane counts per level change with the grid: restart the wavefront
+    // step counters so every level's counters start equal
+    if (s->d_wave) cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), st);
     CK(cudaMemcpyAsync(s->xf, xf.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->yf, yf.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->zf, zf.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice, st));
@@ -477,7 +482,8 @@ extern "C" size_t pmgb_footprint(const pmgb_params* params, int precision, int n
   }
   const double pi = 3.14159265358979323846;
   const double nref = 4.0 * pi * (3.0 + p.srad) * (3.0 + p.srad) * (p.sdens > 0 ? p.sdens : 10.0);
-  bytes += (size_t)natoms * ((size_t)nref + 64 + 18 * sizeof(double) + 2 * sizeof(int));
+  bytes += (size_t)natoms * ((size_t)nref * sizeof(unsigned) + 64 + 18 * sizeof(double) +
+                            2 * sizeof(int));
   return bytes;
 }
 
@@ -497,12 +503,12 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   }
   dfree(s->w1); dfree(s->w2); dfree(s->w3); dfree(s->xs);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
-  dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts);
+  dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts); dfree(s->d_wave);
   dfree(s->d_opptrs);
   dfree(s->band);
   dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
-  dfree(s->cell_sorted); dfree(s->sas_flags); dfree(s->d_ref); dfree(s->atom_terms);
+  dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->d_ref); dfree(s->atom_terms);
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
   cudaStreamDestroy(s->own_stream);
@@ -594,10 +600,15 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
       launch_cell_build(st, C, natoms, s->d_xyz, s->cell_count, s->cell_start,
                         s->cell_fillpos, s->cell_of, s->cell_sorted);
       note_launches(3);
-      const size_t nflags = (size_t)natoms * nref;
-      if (!grow(&s->sas_flags, &s->sas_flags_alloc, nflags, st)) return 0;
+      const size_t npairs = (size_t)natoms * nref;
+      if (npairs >= 0x7fffffffu) {
+        set_error("fillco: %d atoms x %d surface points exceed the 2^31 point list", natoms,
+                  nref);
+        return 0;
+      }
+      if (!grow(&s->sas_list, &s->sas_list_alloc, npairs, st)) return 0;
       launch_sas(st, s->G, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
-                 s->cell_start, s->cell_sorted, s->sas_flags, s->d_npts, s->epsx, s->epsy,
+                 s->cell_start, s->cell_sorted, s->sas_list, s->d_npts, s->epsx, s->epsy,
                  s->epsz);
       note_launches(2);
     }
@@ -833,6 +844,24 @@ int pmgb::solver_build(pmgb_solver* s) { return build_ops(s); }
 // ===========================================================================
 // one V-cycle (body of the do-loop of Vmvcs, src/pmgc/mgcsd.c:312-562)
 // ===========================================================================
+// ordered 27-point smoothing of level l (two sweeps, optional residual):
+// the plane-parallel wavefront on levels of at least kPlanesMin planes that
+// fit it, else the one-cluster wavefront (PMGB_TUNE_GS27_PLANES: 1 = always
+// the latter, 2 = the former on every level that fits)
+constexpr int kPlanesMin = 24;
+static int gs27_smooth(pmgb_solver* s, cudaStream_t st, int l, const double* cc,
+                       const double* fc, double* x, double* r, int first_parity) {
+  const Level& L = s->lev[l];
+  const int mode = s->tune[PMGB_TUNE_GS27_PLANES];
+  if ((mode == 2 || (mode == 0 && L.g.nz - 2 >= kPlanesMin)) && wave_planes_fit(L.g)) {
+    s->wave_used = 1;
+    return launch_gs27_planes(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
+                              s->d_wave + kWaveCounterBase + (size_t)l * kWavePlanesMax,
+                              reinterpret_cast<int*>(s->d_wave));
+  }
+  return launch_gs27_wave(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity, s->plan[l]);
+}
+
 static int vcycle_body(pmgb_solver* s, int newton) {
   cudaStream_t st = s->stream;
   const int nlev = s->nlev;
@@ -876,7 +905,7 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     k++;
     if (l != nlev - 1) {
       launch_zero(st, X(l), C.g.n());
-      if (!launch_gs27_wave(st, C.g, C.ops(), CC(l), C.w0, X(l), s->w1, 2, 1, s->plan[l])) {
+      if (!gs27_smooth(s, st, l, CC(l), C.w0, X(l), s->w1, 1)) {
         set_error("gs27 launch failed at level %d", l);
         return 0;
       }
@@ -895,7 +924,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     } else {
       launch_zero(st, X(nlev - 1), C.g.n());
       if (!launch_cg_coarse(st, C.g, C.ops(), CC(nlev - 1), C.w0, X(nlev - 1), s->w1, s->w2,
-                            s->w3, 100, 2.220446049250313e-16, s->d_iters)) {
+                            s->w3, 100, 2.220446049250313e-16, s->d_iters,
+                            s->tune[PMGB_TUNE_CG_CLUSTER])) {
         set_error("coarse CG launch failed");
         return 0;
       }
@@ -934,7 +964,7 @@ static int vcycle_body(pmgb_solver* s, int newton) {
         k += 2;
       }
     } else {
-      if (!launch_gs27_wave(st, P.g, P.ops(), CC(l), P.w0, X(l), nullptr, 2, 0, s->plan[l])) {
+      if (!gs27_smooth(s, st, l, CC(l), P.w0, X(l), nullptr, 0)) {
         set_error("gs27 launch failed at level %d", l);
         return 0;
       }
@@ -1094,6 +1124,22 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
   return 1;
 }
 
+// Reads (and clears) the count of plane-wavefront waits that ran out; a
+// nonzero count fails the solve (the iterates are not the ordered sweep's).
+static int wave_check(pmgb_solver* s) {
+  if (!s->wave_used) return 1;
+  s->wave_used = 0;
+  int nerr = 0;
+  CK(cudaMemcpyAsync(&nerr, s->d_wave, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (nerr) {
+    CK(cudaMemsetAsync(s->d_wave, 0, sizeof(int), s->stream));
+    set_error("gs27 plane wavefront: %d waits for a neighbour plane ran out", nerr);
+    return 0;
+  }
+  return 1;
+}
+
 extern "C" int pmgb_solve(pmgb_solver* s) {
   if (!s) return 0;
   if (!s->filled) {
@@ -1128,6 +1174,7 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
   launch_fbound(st, s->g, s->lev[0].x, s->gx, s->gy, s->gz);
   note_launches(1);
   CK(cudaEventRecord(s->ev[4], st));
+  if (!wave_check(s)) return 0;
   CK(cudaStreamSynchronize(st));
   CK(cudaGetLastError());
   s->st.t_setup_ms = elapsed_ms(s->ev[2], s->ev[3]);
@@ -1303,7 +1350,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         if (s->nlev < 3) { set_error("pmgb_time_kernel: needs >= 3 levels"); return 0; }
         Level& C = s->lev[1];
         const double cint = (double)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
-        if (!launch_gs27_wave(st, C.g, C.ops(), C.cc, C.w0, C.x, s->w1, 2, 1, s->plan[1]))
+        if (!gs27_smooth(s, st, 1, C.cc, C.w0, C.x, s->w1, 1))
           return 0;
         // 14 coefficients + cc + f read, x read and written: 144 B per point
         // per sweep; the residual pass reads the same and writes r
@@ -1318,7 +1365,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         Level& C = s->lev[s->nlev - 1];
         const double cint = (double)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
         if (!launch_cg_coarse(st, C.g, C.ops(), C.cc, C.w0, C.x, s->w1, s->w2, s->w3, 100,
-                              2.220446049250313e-16, s->d_iters))
+                              2.220446049250313e-16, s->d_iters, s->tune[PMGB_TUNE_CG_CLUSTER]))
           return 0;
         b = 100.0 * (16.0 + 2.0 + 6.0) * 8.0 * cint;
         break;
@@ -1393,6 +1440,10 @@ extern "C" int pmgb_solver_set_tuning(pmgb_solver* s, int key, int value) {
   if ((key == PMGB_TUNE_MIXED_COARSE_SWEEPS || key == PMGB_TUNE_MIXED_FINE_SWEEPS) &&
       (value < 1 || value > 4)) {
     set_error("pmgb_solver_set_tuning: sweeps must be 1..4");
+    return 0;
+  }
+  if (key == PMGB_TUNE_CG_CLUSTER && value != 0 && value != 4 && value != 8 && value != 16) {
+    set_error("pmgb_solver_set_tuning: CG cluster must be 0, 4, 8 or 16");
     return 0;
   }
   if (s->tune[key] == value) return 1;

@@ -91,12 +91,17 @@ struct pmgb_solver {
   // fill work, grown stream-ordered and geometrically (never shrinks)
   int *cell_count, *cell_start, *cell_fillpos, *cell_of, *cell_sorted;
   size_t ncell_alloc, cellof_alloc;
-  unsigned char* sas_flags;
-  size_t sas_flags_alloc;
+  unsigned* sas_list;  // accessible SAS points, (atom * nref + point)
+  size_t sas_list_alloc;
   double* d_ref;
   int nref;
   size_t ref_alloc;
   int* d_npts;
+  // step counters of the plane-parallel GS27 wavefront: word 0 counts waits
+  // that ran out, level l's counters start at kWaveCounterBase + l *
+  // kWavePlanesMax
+  unsigned* d_wave;
+  int wave_used;  // a solve launched the plane kernel since the last check
   double* atom_terms;  // 13 x natoms sdh moment terms
   size_t terms_alloc;
   // focusing: faces set from a coarse solution, energies outside the domain

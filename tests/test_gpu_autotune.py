@@ -7,8 +7,8 @@ import pytest
 
 from apbs_b200 import autotune, synth
 from apbs_b200.vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
-                            TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_TAIL_MAX_POINTS,
-                            Vpmg)
+                            TUNE_GS27_PLANES, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK,
+                            TUNE_TAIL_MAX_POINTS, Vpmg)
 
 pytestmark = pytest.mark.gpu
 
@@ -23,10 +23,15 @@ def _solve(p, m, prec, tune):
 
 
 def test_fp64_launch_shapes_do_not_change_the_solve():
+    """The plane-parallel and one-cluster GS27 wavefronts, cluster sizes and
+    fine-smoother shapes: bitwise the same FP64 solve (NPBE, 129^3: GS27 on
+    the 65^3, 33^3 and 17^3 levels)."""
     m = synth.cluster(400, 11.0, seed=12, net_charge=2.0)
     p = synth.mg_manual(129, 0.4, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
     e0, u0, h0 = _solve(p, m, FP64, {})
-    for tune in ({TUNE_GS27_CLUSTER: 4}, {TUNE_GS27_CLUSTER_MID: 16},
+    for tune in ({TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2},
+                 {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER: 4},
+                 {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER_MID: 16},
                  {TUNE_GS7_SWEEP_KCHUNK: 8}, {TUNE_GS7_COLOUR_PASSES: 1}):
         e, u, h = _solve(p, m, FP64, tune)
         assert e == e0 and np.array_equal(u, u0) and np.array_equal(h, h0), tune
