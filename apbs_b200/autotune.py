@@ -1,8 +1,8 @@
 """Autotuner for the launch shapes of the PMG kernels.
 
 Each calculation carries its own launch-shape tunables (PMGB_TUNE_* in
-include/apbs_b200.h): the cluster size of the ordered 27-point wavefront on
-the large and middle levels, the fine smoother's kernel and its plane chunk,
+include/apbs_b200.h): which ordered 27-point wavefront runs on which levels
+(one CTA per plane or one cluster) and the cluster size on the middle levels, the fine smoother's kernel and its plane chunk,
 and the size limit of the one-cluster coarse V-cycle tail of the
 mixed-precision path, and the smoothing counts of the mixed path's inner FP32
 V-cycle.  The FP64 keys change no result at all; the mixed keys change the
@@ -28,7 +28,7 @@ import os
 from typing import Callable
 
 from . import vpmg
-from .vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
+from .vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID, TUNE_GS27_PLANES,
                    TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_MC_COOPERATIVE,
                    TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS, TUNE_TAIL_MAX_POINTS)
 
@@ -38,7 +38,7 @@ DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
 # candidate values per key; the first value of each list is the default
 CANDIDATES = {
     FP64: {
-        TUNE_GS27_CLUSTER: [0, 8, 4],
+        TUNE_GS27_PLANES: [0, 2, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
         TUNE_GS7_SWEEP_KCHUNK: [16, 8, 32],
@@ -54,6 +54,7 @@ CANDIDATES = {
 }
 
 KEY_NAMES = {TUNE_GS27_CLUSTER: "gs27_cluster", TUNE_GS27_CLUSTER_MID: "gs27_cluster_mid",
+             TUNE_GS27_PLANES: "gs27_planes",
              TUNE_GS7_COLOUR_PASSES: "gs7_colour_passes", TUNE_GS7_SWEEP_KCHUNK: "gs7_sweep_kchunk",
              TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative",
              TUNE_MIXED_COARSE_SWEEPS: "mixed_coarse_sweeps",

@@ -640,6 +640,7 @@ __device__ __forceinline__ void sum27_pre(const Coef27& C, const double* x, size
 
 constexpr int kPlanesThreads = 384;  // a step's items never exceed the CTA
 
+template <bool POLL_ALL>
 __global__ void __launch_bounds__(kPlanesThreads, 1)
     k_gs27_planes(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ fc,
                   double* x, double* r, int nhalf, int first_parity, int do_resid,
@@ -655,7 +656,7 @@ __global__ void __launch_bounds__(kPlanesThreads, 1)
   const int c = blockIdx.x, k = 1 + c;  // this CTA's plane
   const int ncta = gridDim.x;
   __shared__ unsigned base_sh;
-  __shared__ int failed_sh;
+  __shared__ volatile int failed_sh;
   if (threadIdx.x == 0) {
     base_sh = counters[c];
     failed_sh = 0;
@@ -692,25 +693,36 @@ __global__ void __launch_bounds__(kPlanesThreads, 1)
   int kind = (nsteps > 0) ? item_of(0, id) : 0;
   Coef27 C;
   if (kind) load_coef27(op, cc, fc, id, sy, sz, C);
-  for (int s = 0; s < nsteps; s++) {
-    if (s > 0) {
-      if (threadIdx.x == 0 && !failed_sh) {
-        const unsigned need = base + (unsigned)s;
-        const unsigned long long t0 = global_ns();
-        for (int nb = -1; nb <= 1; nb += 2) {
-          if (c + nb < 0 || c + nb >= ncta) continue;
-          const unsigned* f = counters + c + nb;
-          while ((int)(ld_acquire(f) - need) < 0) {
-            if ((long long)(global_ns() - t0) > kWaveWaitNs) {
-              failed_sh = 1;
-              atomicAdd(err, 1);
-              break;
-            }
-          }
-          if (failed_sh) break;
+  volatile int* verr = err;
+  // waits for the neighbour planes to finish step s-1 (every thread or only
+  // thread 0); once any CTA has given up, nobody waits any more
+  auto wait_neighbours = [&](int s) {
+    const unsigned need = base + (unsigned)s;
+    const unsigned long long t0 = global_ns();
+    for (int nb = -1; nb <= 1; nb += 2) {
+      if (c + nb < 0 || c + nb >= ncta) continue;
+      const unsigned* f = counters + c + nb;
+      while ((int)(ld_acquire(f) - need) < 0) {
+        if (failed_sh || *verr) {
+          failed_sh = 1;
+          return;
+        }
+        if ((long long)(global_ns() - t0) > kWaveWaitNs) {
+          failed_sh = 1;
+          atomicAdd(err, 1);
+          return;
         }
       }
-      __syncthreads();
+    }
+  };
+  for (int s = 0; s < nsteps; s++) {
+    if (s > 0) {
+      if (POLL_ALL) {
+        if (!failed_sh) wait_neighbours(s);
+      } else {
+        if (threadIdx.x == 0 && !failed_sh) wait_neighbours(s);
+        __syncthreads();
+      }
     }
     if (kind) {
       double tO, tU, tD;
@@ -722,17 +734,18 @@ __global__ void __launch_bounds__(kPlanesThreads, 1)
       }
     }
     // the next step's coefficients do not depend on this step: fetch them
-    // while the neighbour planes finish
+    // while the neighbour planes finish.  Thread 0 publishes the step, and a
+    // release waits for the thread's own loads, so it fetches after that.
     size_t nid = 0;
     const int nkind = (s + 1 < nsteps) ? item_of(s + 1, nid) : 0;
-    if (nkind) load_coef27(op, cc, fc, nid, sy, sz, C);
-    kind = nkind;
-    id = nid;
+    if (nkind && threadIdx.x != 0) load_coef27(op, cc, fc, nid, sy, sz, C);
     __syncthreads();
     if (threadIdx.x == 0) {
-      __threadfence();
       st_release(counters + c, base + (unsigned)(s + 1));
+      if (nkind) load_coef27(op, cc, fc, nid, sy, sz, C);
     }
+    kind = nkind;
+    id = nid;
   }
 }
 
@@ -741,7 +754,7 @@ int wave_planes_fit(Grid g) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs27_planes, kPlanesThreads,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs27_planes<false>, kPlanesThreads,
                                                       0) != cudaSuccess)
       per_sm = 0;
     return sms * per_sm;
@@ -754,7 +767,7 @@ int wave_planes_fit(Grid g) {
 
 int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, double* r, int nsweep, int first_parity, unsigned* counters,
-                       int* err) {
+                       int* err, int poll_all) {
   int nhalf = 2 * nsweep;
   int do_resid = (r != nullptr) ? 1 : 0;
   const int hr = (g.nx - 1) / 2;
@@ -762,8 +775,9 @@ int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const do
   if (items > kPlanesThreads) return 0;
   const int threads = std::max(64, (items + 31) / 32 * 32);
   void* args[] = {&g, &op, &cc, &fc, &x, &r, &nhalf, &first_parity, &do_resid, &counters, &err};
-  return cudaLaunchCooperativeKernel((void*)k_gs27_planes, dim3(g.nz - 2), dim3(threads), args,
-                                     0, s) == cudaSuccess;
+  void* fn = poll_all ? (void*)k_gs27_planes<true> : (void*)k_gs27_planes<false>;
+  return cudaLaunchCooperativeKernel(fn, dim3(g.nz - 2), dim3(threads), args, 0, s) ==
+         cudaSuccess;
 }
 
 int mg_init() {
@@ -1333,12 +1347,16 @@ __global__ void __launch_bounds__(kCgThreads)
 
 // The same iteration on a larger coarsest level, one cluster of CL CTAs:
 // CTA `rank` owns the slab of planes k0 .. k1-1 and keeps p over its slab and
-// one halo plane on either side in shared memory (zero boundary); after each
-// direction update it copies the two halo planes from its neighbours' shared
-// memory (distributed shared memory) behind a cluster barrier.  x, r and A p
-// of its points stay in registers.  Sums go block by block in rank order, so
-// every CTA sees the same scalars and the iteration is deterministic.
-constexpr int kSlabThreads = 512, kSlabPPT = 4;
+// one halo plane on either side in shared memory (zero boundary).  A
+// direction update writes the slab's first and last planes into the
+// neighbours' halo planes as well (stores to distributed shared memory ahead
+// of the cluster barrier), and each CTA writes its block partial of a sum
+// into every CTA's slot for it, so after the barrier every CTA adds the same
+// partials in rank order from its own shared memory.  x, r and A p of the
+// CTA's points stay in registers; where shared memory allows, the 26
+// off-diagonal coefficients of its points are loaded once into it.
+constexpr int kSlabThreads = 512, kSlabPPT = 2;
+constexpr size_t kSlabSmemMax = 220 * 1024;
 
 // tmpO + tmpU + tmpD of sum27 with x read from xs at the offset of xid - id
 __device__ __forceinline__ void sum27_at(const Op& op, Grid g, const double* xs,
@@ -1367,21 +1385,27 @@ template <int CL>
 __global__ void __launch_bounds__(kSlabThreads)
     k_cg_coarse_slab(Grid g, Op op, const double* __restrict__ cc,
                      const double* __restrict__ fc, double* x, double* r, int itmax,
-                     double errtol, int* iters_out) {
-  extern __shared__ double ps[];  // planes k0-1 .. k1 of p
+                     double errtol, int* iters_out, int cache_coef) {
+  extern __shared__ double ps[];  // planes k0-1 .. k1 of p, then the coefficients
   __shared__ double sh[32];
-  __shared__ double slots[2];
+  __shared__ double slots[2][CL];
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t pl = (size_t)nx * ny;
+  const size_t sy = nx, pl = (size_t)nx * ny;
   const int per = (nz - 2 + CL - 1) / CL;
   const int k0 = 1 + rank * per;
   const int k1 = min(k0 + per, nz - 1);
   const int nown = (k1 > k0) ? (k1 - k0) * (nx - 2) * (ny - 2) : 0;
+  const int ncap = per * (nx - 2) * (ny - 2);             // coefficient slots
+  double* cf = ps + (size_t)(per + 2) * pl;              // [26][ncap]
   const ptrdiff_t off = -(ptrdiff_t)((size_t)(k0 - 1) * pl);  // global id -> ps index
+  double* below = (rank > 0) ? cl.map_shared_rank(ps, rank - 1) + (size_t)(per + 1) * pl
+                             : nullptr;                  // rank-1's upper halo plane
+  double* above = (rank < CL - 1 && k1 < nz - 1) ? cl.map_shared_rank(ps, rank + 1) : nullptr;
   for (size_t q = threadIdx.x; q < (size_t)(per + 2) * pl; q += blockDim.x) ps[q] = 0.0;
   size_t id[kSlabPPT];
+  int kk[kSlabPPT];
   bool own[kSlabPPT];
   double rl[kSlabPPT], xl[kSlabPPT], dg[kSlabPPT], al[kSlabPPT];
   double acc = 0.0;
@@ -1390,11 +1414,13 @@ __global__ void __launch_bounds__(kSlabThreads)
     const int q = threadIdx.x + m * blockDim.x;
     own[m] = q < nown;
     id[m] = 0;
+    kk[m] = 0;
     rl[m] = xl[m] = dg[m] = al[m] = 0.0;
     if (!own[m]) continue;
     const int i = 1 + q % (nx - 2);
     const int j = 1 + (q / (nx - 2)) % (ny - 2);
     const int k = k0 + q / ((nx - 2) * (ny - 2));
+    kk[m] = k;
     id[m] = g.idx(i, j, k);
     double tO, tU, tD;
     sum27<true>(op, g, x, id[m], tO, tU, tD);
@@ -1403,12 +1429,33 @@ __global__ void __launch_bounds__(kSlabThreads)
     const double rv = fc[id[m]] + tO + tU + tD - (op.c[OC][id[m]] + cc[id[m]]) * xl[m];
     rl[m] = rv;
     acc += rv * rv;
+    if (cache_coef) {
+      Coef27 C;
+      load_coef27(op, cc, fc, id[m], sy, pl, C);
+#pragma unroll
+      for (int t = 0; t < 8; t++) cf[(size_t)t * ncap + q] = C.o[t];
+#pragma unroll
+      for (int t = 0; t < 9; t++) cf[(size_t)(8 + t) * ncap + q] = C.u[t];
+#pragma unroll
+      for (int t = 0; t < 9; t++) cf[(size_t)(17 + t) * ncap + q] = C.d[t];
+    }
   }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int phase = 0;
   auto csum = [&](double v) {
-    const double t = cluster_sum<CL>(v, sh, slots, phase);
+    v = warp_sum(v);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (threadIdx.x < CL) {
+      double b = 0.0;
+      for (int w = 0; w < nw; w++) b += sh[w];
+      cl.map_shared_rank(&slots[0][0], (int)threadIdx.x)[phase * CL + rank] = b;
+    }
+    cl.sync();
+    double tot = 0.0;
+    for (int q = 0; q < CL; q++) tot += slots[phase][q];
     phase ^= 1;
-    return t;
+    return tot;
   };
   const double denom = sqrt(csum(acc));
   int iters = 0;
@@ -1422,59 +1469,64 @@ __global__ void __launch_bounds__(kSlabThreads)
       const double rhok2 = csum(acc);
       if (sqrt(rhok2) / denom <= errtol) break;
       if (iters >= itmax) break;
-      if (iters == 0) {
+      const double beta = (iters == 0) ? 0.0 : rhok2 / rhok1;
+      const double alpha = (iters == 0) ? 0.0 : 1.0 / beta;
 #pragma unroll
-        for (int m = 0; m < kSlabPPT; m++)
-          if (own[m]) ps[(ptrdiff_t)id[m] + off] = rl[m];
-      } else {
-        const double beta = rhok2 / rhok1;
-        const double alpha = 1.0 / beta;
-#pragma unroll
-        for (int m = 0; m < kSlabPPT; m++) {
-          if (!own[m]) continue;
-          double pv = ps[(ptrdiff_t)id[m] + off];
+      for (int m = 0; m < kSlabPPT; m++) {
+        if (!own[m]) continue;
+        double pv;
+        if (iters == 0) {
+          pv = rl[m];
+        } else {
+          pv = ps[(ptrdiff_t)id[m] + off];
           pv += alpha * rl[m];
           pv *= beta;
-          ps[(ptrdiff_t)id[m] + off] = pv;
         }
+        ps[(ptrdiff_t)id[m] + off] = pv;
+        const size_t inplane = id[m] % pl;
+        if (kk[m] == k0 && below) below[inplane] = pv;
+        if (kk[m] == k1 - 1 && above) above[inplane] = pv;
       }
       cl.sync();
-      // halo planes: k0-1 is the last owned plane of rank-1, k1 the first of rank+1
-      if (k1 > k0) {
-        if (rank > 0) {
-          const double* src = cl.map_shared_rank(ps, rank - 1) + (size_t)per * pl;
-          for (size_t q = threadIdx.x; q < pl; q += blockDim.x) ps[q] = src[q];
-        }
-        if (rank < CL - 1 && k1 < nz - 1) {
-          const double* src = cl.map_shared_rank(ps, rank + 1) + pl;
-          double* dst = ps + (size_t)(k1 - k0 + 1) * pl;
-          for (size_t q = threadIdx.x; q < pl; q += blockDim.x) dst[q] = src[q];
-        }
-      }
-      __syncthreads();
       acc = 0.0;
 #pragma unroll
       for (int m = 0; m < kSlabPPT; m++) {
         if (!own[m]) continue;
         double tO, tU, tD;
-        sum27_at(op, g, ps, off, id[m], tO, tU, tD);
+        if (cache_coef) {
+          const int q = threadIdx.x + m * blockDim.x;
+          const double* ps0 = ps + ((ptrdiff_t)id[m] + off);
+          auto X = [&](ptrdiff_t d) -> double { return ps0[d]; };
+          auto A = [&](int t) -> double { return cf[(size_t)t * ncap + q]; };
+          const ptrdiff_t Y = (ptrdiff_t)sy, Z = (ptrdiff_t)pl;
+          tO = +A(0) * X(Y) + A(1) * X(-Y) + A(2) * X(1) + A(3) * X(-1) + A(4) * X(Y + 1) +
+               A(5) * X(Y - 1) + A(6) * X(-Y + 1) + A(7) * X(-Y - 1);
+          tU = +A(8) * X(Z) + A(9) * X(Z + Y) + A(10) * X(Z - Y) + A(11) * X(Z + 1) +
+               A(12) * X(Z - 1) + A(13) * X(Z + Y + 1) + A(14) * X(Z + Y - 1) +
+               A(15) * X(Z - Y + 1) + A(16) * X(Z - Y - 1);
+          tD = +A(17) * X(-Z) + A(18) * X(-Z + Y) + A(19) * X(-Z - Y) + A(20) * X(-Z + 1) +
+               A(21) * X(-Z - 1) + A(22) * X(-Z + Y + 1) + A(23) * X(-Z + Y - 1) +
+               A(24) * X(-Z - Y + 1) + A(25) * X(-Z - Y - 1);
+        } else {
+          sum27_at(op, g, ps, off, id[m], tO, tU, tD);
+        }
         const double pv = ps[(ptrdiff_t)id[m] + off];
         const double av = -tO - tU - tD + dg[m] * pv;
         al[m] = av;
         acc += pv * av;
       }
       const double pAp = csum(acc);
-      const double alpha = rhok2 / pAp;
+      const double alpha2 = rhok2 / pAp;
       rhok1 = rhok2;
 #pragma unroll
       for (int m = 0; m < kSlabPPT; m++) {
         if (!own[m]) continue;
-        xl[m] = xl[m] + alpha * ps[(ptrdiff_t)id[m] + off];
-        rl[m] = rl[m] + (-alpha) * al[m];
+        xl[m] = xl[m] + alpha2 * ps[(ptrdiff_t)id[m] + off];
+        rl[m] = rl[m] + (-alpha2) * al[m];
       }
       iters++;
-      // a neighbour's halo copy of this slab ends before it reaches the next
-      // sum's cluster barrier, which precedes the next direction update here
+      // a neighbour reads this slab's halo copy in its matvec, before the
+      // next sum's cluster barrier; this CTA writes it again only after that
     }
   }
 #pragma unroll
@@ -1484,17 +1536,17 @@ __global__ void __launch_bounds__(kSlabThreads)
     r[id[m]] = rl[m];
   }
   if (rank == 0 && threadIdx.x == 0 && iters_out) iters_out[0] = iters;
-  cl.sync();  // no CTA may exit while a neighbour can still read its shared memory
+  cl.sync();  // no CTA may exit while a neighbour can still write its shared memory
 }
 
 template <int CL>
 static int launch_cg_slab(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                           double* x, double* r, int itmax, double errtol, int* iters_dev,
-                          size_t smem) {
+                          size_t smem, int cache_coef) {
   static const cudaError_t attr_ok = [] {
     cudaError_t e = cudaFuncSetAttribute(k_cg_coarse_slab<CL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kCgSmemMax);
+                                         (int)kSlabSmemMax);
     if (e == cudaSuccess && CL > 8)
       e = cudaFuncSetAttribute(k_cg_coarse_slab<CL>,
                                cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -1514,7 +1566,7 @@ static int launch_cg_slab(cudaStream_t s, Grid g, Op op, const double* cc, const
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, k_cg_coarse_slab<CL>, g, op, cc, fc, x, r, itmax, errtol,
-                            iters_dev) == cudaSuccess;
+                            iters_dev, cache_coef) == cudaSuccess;
 }
 
 int launch_cg_coarse(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
@@ -1545,13 +1597,19 @@ int launch_cg_coarse(cudaStream_t s, Grid g, Op op, const double* cc, const doub
     for (int cl = 4; cl <= max_cl; cl *= 2) {
       if (want_cluster > 0 && cl != want_cluster) continue;
       const int per = (g.nz - 2 + cl - 1) / cl;
-      const size_t sm = (size_t)(per + 2) * g.nx * g.ny * sizeof(double);
-      if (per * plane_pts > limit || sm > kCgSmemMax) continue;
+      size_t sm = (size_t)(per + 2) * g.nx * g.ny * sizeof(double);
+      if (per * plane_pts > limit || sm > kSlabSmemMax) continue;
+      const size_t sm_coef = sm + (size_t)26 * per * plane_pts * sizeof(double);
+      const int cache = sm_coef <= kSlabSmemMax;
+      if (cache) sm = sm_coef;
       switch (cl) {
-        case 4: return launch_cg_slab<4>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm);
-        case 8: return launch_cg_slab<8>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm);
+        case 4:
+          return launch_cg_slab<4>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm, cache);
+        case 8:
+          return launch_cg_slab<8>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm, cache);
         case 16:
-          if (launch_cg_slab<16>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm)) return 1;
+          if (launch_cg_slab<16>(s, g, op, cc, fc, x, r, itmax, errtol, iters_dev, sm, cache))
+            return 1;
           cudaGetLastError();  // no 16-CTA clusters here: the strided kernel below
           break;
       }

@@ -56,7 +56,7 @@ constexpr size_t kWaveWords = kWaveCounterBase + 16 * (size_t)kWavePlanesMax;
 int wave_planes_fit(Grid g);
 int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, double* r, int nsweep, int first_parity, unsigned* counters,
-                       int* err);
+                       int* err, int poll_all);
 int launch_gs27_wave(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, int nsweep, int first_parity, Gs27Plan plan);
 

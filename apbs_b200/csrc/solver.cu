@@ -857,7 +857,8 @@ static int gs27_smooth(pmgb_solver* s, cudaStream_t st, int l, const double* cc,
     s->wave_used = 1;
     return launch_gs27_planes(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
                               s->d_wave + kWaveCounterBase + (size_t)l * kWavePlanesMax,
-                              reinterpret_cast<int*>(s->d_wave));
+                              reinterpret_cast<int*>(s->d_wave),
+                              s->tune[PMGB_TUNE_GS27_PLANES_POLL]);
   }
   return launch_gs27_wave(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity, s->plan[l]);
 }

@@ -37,6 +37,7 @@ TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS = 10, 11
 TUNE_GS7_SWEEP_STAGED = 12
 TUNE_GS27_PLANES = 13
 TUNE_CG_CLUSTER = 14
+TUNE_GS27_PLANES_POLL = 15
 TUNE_NKEYS = 16
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

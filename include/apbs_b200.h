@@ -180,6 +180,9 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_CG_CLUSTER 14       /* coarsest-level CG of the FP64 NPBE path: CTAs per
                                           cluster of the slab kernel (0 = smallest that fits;
                                           4, 8 or 16) */
+#define PMGB_TUNE_GS27_PLANES_POLL 15 /* plane-parallel GS27: 0 = one thread of a CTA waits
+                                          for the neighbour planes, then a block barrier;
+                                          1 = every thread waits itself */
 #define PMGB_TUNE_NKEYS 16
 int pmgb_set_tuning(int key, int value);
 int pmgb_get_tuning(int key);

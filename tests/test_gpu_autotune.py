@@ -7,7 +7,8 @@ import pytest
 
 from apbs_b200 import autotune, synth
 from apbs_b200.vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
-                            TUNE_GS27_PLANES, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK,
+                            TUNE_GS27_PLANES, TUNE_GS27_PLANES_POLL, TUNE_GS7_COLOUR_PASSES,
+                            TUNE_GS7_SWEEP_KCHUNK,
                             TUNE_TAIL_MAX_POINTS, Vpmg)
 
 pytestmark = pytest.mark.gpu
@@ -29,7 +30,7 @@ def test_fp64_launch_shapes_do_not_change_the_solve():
     m = synth.cluster(400, 11.0, seed=12, net_charge=2.0)
     p = synth.mg_manual(129, 0.4, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
     e0, u0, h0 = _solve(p, m, FP64, {})
-    for tune in ({TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2},
+    for tune in ({TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2}, {TUNE_GS27_PLANES_POLL: 1},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER: 4},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER_MID: 16},
                  {TUNE_GS7_SWEEP_KCHUNK: 8}, {TUNE_GS7_COLOUR_PASSES: 1}):
