@@ -440,44 +440,75 @@ __global__ void k_dense_build(Grid g, Op op, const double* __restrict__ cc, doub
 }
 
 // Inverse of the SPD coarsest matrix by Gauss-Jordan elimination (no
-// pivoting needed for SPD) in one CTA; the matrix lives in shared memory
-// when it fits.  M is replaced by its inverse.
-__global__ void k_dense_inverse(double* M, int n, int use_smem, int* info) {
-  // dynamic shared memory: [matrix (use_smem) | pivot row (n) | pivot column (n)]
+// pivoting needed for SPD) in one cluster of CL CTAs (CL = 1: one CTA).  CTA
+// `rank` keeps rows rank*rows_per .. +rows_per of M in shared memory; thread
+// (g, c) updates column c of the CTA's rows g, g+G, ... (G = blockDim / n row
+// groups).  The pivot row p is read from a double-buffered slot every CTA
+// holds: during step p the owner of row p+1 updates that row and stores the
+// result into every CTA's other slot, so one cluster barrier per pivot
+// suffices.  Each element sees the same operations as in a one-CTA
+// Gauss-Jordan sweep: A[r][c] -= A[r][p] A[p][c] / piv off row and column p,
+// column p becomes -A[r][p] / piv, row p A[p][c] / piv, the pivot 1/piv.
+// M is replaced by its inverse; info = first non-positive pivot + 1, else 0.
+template <int CL>
+__global__ void __launch_bounds__(1024) k_dense_inverse(double* M, int n, int rows_per,
+                                                        int* info) {
   extern __shared__ double sm[];
-  double* A = use_smem ? sm : M;
-  double* rowp = use_smem ? sm + (size_t)n * n : sm;
-  double* colp = rowp + n;
-  if (use_smem)
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = M[t];
-  __syncthreads();
+  double* A = sm;                          // [rows_per][n]
+  double* pb = A + (size_t)rows_per * n;   // [2][n] pivot rows
+  double* colp = pb + 2 * (size_t)n;       // [rows_per] column p before the step
+  const int rank = (CL > 1) ? (int)cg::this_cluster().block_rank() : 0;
+  auto csync = [&]() {
+    if (CL > 1) cg::this_cluster().sync();
+    else __syncthreads();
+  };
+  const int r0 = rank * rows_per;
+  const int nr = max(0, min(rows_per, n - r0));
+  const int G = max(1, (int)blockDim.x / n);
+  const int c = threadIdx.x % n, grp = threadIdx.x / n;
+  const bool active = grp < G && (int)threadIdx.x < G * n;
+  for (int t = threadIdx.x; t < nr * n; t += blockDim.x) A[t] = M[(size_t)r0 * n + t];
+  csync();  // every CTA runs and holds its rows before any slot is written
+  if (r0 == 0 && nr > 0)  // the owner of row 0 publishes it
+    for (int t = threadIdx.x; t < n; t += blockDim.x)
+      for (int q = 0; q < CL; q++) {
+        double* dst = (CL > 1) ? cg::this_cluster().map_shared_rank(pb, q) : pb;
+        dst[t] = A[t];
+      }
+  csync();
   int bad = 0;
   for (int p = 0; p < n; p++) {
-    // the pivot row and column before this step
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      rowp[t] = A[p * n + t];
-      colp[t] = A[t * n + p];
-    }
-    __syncthreads();
+    const double* rowp = pb + (size_t)(p & 1) * n;
     const double piv = rowp[p];
-    if (!(piv > 0.0)) {  // every thread reads the same value
+    if (!(piv > 0.0)) {  // every thread of every CTA reads the same value
       bad = p + 1;
       break;
     }
     const double ipiv = 1.0 / piv;
-    // Gauss-Jordan step: A[r][c] -= A[r][p] A[p][c] / piv off row and column
-    // p; column p becomes -A[r][p] / piv, row p A[p][c] / piv, the pivot 1/piv
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-      const int r = t / n, c = t - r * n;
-      if (r == p) A[t] = (c == p) ? ipiv : rowp[c] * ipiv;
-      else if (c == p) A[t] = -colp[r] * ipiv;
-      else A[t] -= colp[r] * rowp[c] * ipiv;
-    }
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) colp[r] = A[(size_t)r * n + p];
     __syncthreads();
+    if (active) {
+      const double rc = rowp[c];
+      double* nextslot = pb + (size_t)((p + 1) & 1) * n;
+      for (int r = grp; r < nr; r += G) {
+        const int gr = r0 + r;
+        double v;
+        if (gr == p) v = (c == p) ? ipiv : rc * ipiv;
+        else if (c == p) v = -colp[r] * ipiv;
+        else v = A[(size_t)r * n + c] - colp[r] * rc * ipiv;
+        A[(size_t)r * n + c] = v;
+        if (gr == p + 1)
+          for (int q = 0; q < CL; q++) {
+            double* dst = (CL > 1) ? cg::this_cluster().map_shared_rank(nextslot, q) : nextslot;
+            dst[c] = v;
+          }
+      }
+    }
+    csync();  // row p+1 is published and column p read everywhere
   }
-  if (use_smem)
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) M[t] = A[t];
-  if (threadIdx.x == 0) info[0] = bad;
+  for (int t = threadIdx.x; t < nr * n; t += blockDim.x) M[(size_t)r0 * n + t] = A[t];
+  if (rank == 0 && threadIdx.x == 0) info[0] = bad;
+  if (CL > 1) cg::this_cluster().sync();  // no CTA exits while a slot write may target it
 }
 
 // x = M^{-1} b on the coarsest level (FP32 in/out, FP64 product).
@@ -1347,6 +1378,58 @@ int mixed_refresh(pmgb_solver* s) {
 // restrict through the FP64 levels (where not already present) and convert.
 constexpr size_t kDenseSmemMax = 200 * 1024;
 
+// The dense inverse on the smallest cluster whose row blocks fit one CTA's
+// shared memory (rows, two pivot rows and a column).
+template <int CL>
+static cudaError_t dense_inverse_cl(cudaStream_t st, double* M, int n, int rows_per,
+                                    size_t smem, int* info) {
+  static const cudaError_t attr = [] {
+    cudaError_t e = cudaFuncSetAttribute(k_dense_inverse<CL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kDenseSmemMax);
+    if (e == cudaSuccess && CL > 8)
+      e = cudaFuncSetAttribute(k_dense_inverse<CL>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    return e;
+  }();
+  if (attr != cudaSuccess) return attr;
+  if (CL == 1) {
+    k_dense_inverse<1><<<1, 1024, smem, st>>>(M, n, rows_per, info);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(CL, 1, 1);
+  cfg.blockDim = dim3(1024, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_dense_inverse<CL>, M, n, rows_per, info);
+}
+
+static int launch_dense_inverse(cudaStream_t st, double* M, int n, int* info) {
+  for (int cl = 1; cl <= 16; cl *= 2) {
+    const int rows_per = (n + cl - 1) / cl;
+    const size_t smem = ((size_t)rows_per * n + 2 * (size_t)n + rows_per) * sizeof(double);
+    if (smem > kDenseSmemMax) continue;
+    cudaError_t e;
+    switch (cl) {
+      case 1: e = dense_inverse_cl<1>(st, M, n, rows_per, smem, info); break;
+      case 2: e = dense_inverse_cl<2>(st, M, n, rows_per, smem, info); break;
+      case 4: e = dense_inverse_cl<4>(st, M, n, rows_per, smem, info); break;
+      case 8: e = dense_inverse_cl<8>(st, M, n, rows_per, smem, info); break;
+      default: e = dense_inverse_cl<16>(st, M, n, rows_per, smem, info); break;
+    }
+    return e == cudaSuccess;
+  }
+  return 0;
+}
+
 int mixed_set_cc(pmgb_solver* s, int newton) {
   MixedState* m = s->mixed;
   cudaStream_t st = s->stream;
@@ -1376,15 +1459,10 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       const int nd = m->nd;
       k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, st>>>(L.g, L.ops64(), src,
                                                                        m->dense, nd);
-      const size_t smem_all = ((size_t)nd * nd + 2 * (size_t)nd) * sizeof(double);
-      const int use_smem = smem_all <= kDenseSmemMax;
-      const size_t smem = use_smem ? smem_all : 2 * (size_t)nd * sizeof(double);
-      // the attribute is set once, to the largest size any call uses: calls
-      // from concurrent host threads would otherwise race on it
-      static const cudaError_t attr = cudaFuncSetAttribute(
-          k_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmemMax);
-      (void)attr;
-      k_dense_inverse<<<1, 1024, smem, st>>>(m->dense, nd, use_smem, m->dinfo);
+      if (!launch_dense_inverse(st, m->dense, nd, m->dinfo)) {
+        set_error("mixed: dense coarsest inverse launch failed (%d unknowns)", nd);
+        return 0;
+      }
       note_launches(2);
     }
   }

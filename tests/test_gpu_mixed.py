@@ -22,8 +22,15 @@ def _cases():
     m4 = synth.cluster(120, 6.0, seed=11, net_charge=-2.0)
     p4 = synth.mg_manual(33, 0.6, m4.center(), npbe=True, ions=((2, 0.05, 2.0), (-1, 0.1, 1.8)))
     p5 = synth.mg_manual(49, 0.8, m2.center(), npbe=True)
+    # three levels: the mixed hierarchy is extended to a 6^3 (216 unknowns)
+    # or 7^3 (343) coarsest level whose dense inverse runs on a 2- or 8-CTA
+    # cluster (the matrix does not fit one CTA's shared memory)
+    p6 = synth.mg_manual(57, 0.6, m1.center(), npbe=True, nlev=3,
+                         ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    p7 = synth.mg_manual(65, 0.5, m0.center(), nlev=3)
     return [("lpbe65", m0, p0), ("npbe65", m1, p1), ("lpbe97", m2, p2),
-            ("npbe33_2to1", m4, p4), ("npbe49", m2, p5)]
+            ("npbe33_2to1", m4, p4), ("npbe49", m2, p5), ("npbe57_dense216", m1, p6),
+            ("lpbe65_dense343", m0, p7)]
 
 
 CASES = _cases()
