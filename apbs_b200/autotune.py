@@ -38,7 +38,7 @@ DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
 # candidate values per key; the first value of each list is the default
 CANDIDATES = {
     FP64: {
-        TUNE_GS27_PLANES: [0, 2, 1],
+        TUNE_GS27_PLANES: [0, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
         TUNE_GS7_SWEEP_KCHUNK: [16, 8, 32],

@@ -845,15 +845,12 @@ int pmgb::solver_build(pmgb_solver* s) { return build_ops(s); }
 // one V-cycle (body of the do-loop of Vmvcs, src/pmgc/mgcsd.c:312-562)
 // ===========================================================================
 // ordered 27-point smoothing of level l (two sweeps, optional residual):
-// the plane-parallel wavefront on levels of at least kPlanesMin planes that
-// fit it, else the one-cluster wavefront (PMGB_TUNE_GS27_PLANES: 1 = always
-// the latter, 2 = the former on every level that fits)
-constexpr int kPlanesMin = 24;
+// the plane-parallel wavefront on every level that fits it, else the
+// one-cluster wavefront (PMGB_TUNE_GS27_PLANES = 1: always the latter)
 static int gs27_smooth(pmgb_solver* s, cudaStream_t st, int l, const double* cc,
                        const double* fc, double* x, double* r, int first_parity) {
   const Level& L = s->lev[l];
-  const int mode = s->tune[PMGB_TUNE_GS27_PLANES];
-  if ((mode == 2 || (mode == 0 && L.g.nz - 2 >= kPlanesMin)) && wave_planes_fit(L.g)) {
+  if (s->tune[PMGB_TUNE_GS27_PLANES] != 1 && wave_planes_fit(L.g)) {
     s->wave_used = 1;
     return launch_gs27_planes(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
                               s->d_wave + kWaveCounterBase + (size_t)l * kWavePlanesMax,

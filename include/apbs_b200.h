@@ -172,11 +172,10 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_MIXED_FINE_SWEEPS 11 /* mixed: red-black sweeps on the fine level (default 2) */
 #define PMGB_TUNE_GS7_SWEEP_STAGED 12 /* single-pass sweep with plane tiles staged through
                                           shared memory by asynchronous copies (1) */
-#define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 = one CTA per plane synchronised
-                                          with its neighbour planes on levels of >= 24
-                                          planes that fit on the device, 1 = one cluster with
-                                          a barrier per wavefront everywhere, 2 = planes on
-                                          every level that fits */
+#define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
+                                          synchronised with its neighbour planes on every
+                                          level whose planes fit on the device, 1 = one
+                                          cluster with a barrier per wavefront everywhere */
 #define PMGB_TUNE_CG_CLUSTER 14       /* coarsest-level CG of the FP64 NPBE path: CTAs per
                                           cluster of the slab kernel (0 = smallest that fits;
                                           4, 8 or 16) */
