@@ -8,6 +8,7 @@
 #include <cooperative_groups.h>
 
 #include "gs7_pipe.cuh"
+#include "gs7_march.cuh"
 #include "gs7_sweep.cuh"
 #include "mg_kernels.cuh"
 
@@ -380,15 +381,14 @@ int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
-                       int staged) {
+                       int kernel) {
   Gs7Sweep<double> a;
   a.g = g;
   a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
   a.c1 = first_parity;
   a.kchunk = kchunk;
-  if (staged) return launch_gs7_sweep_async<double, 32, 8>(s, a) == cudaSuccess;
-  return launch_gs7_sweep<double, 32, 8>(s, a) == cudaSuccess;
+  return launch_gs7_sweep_kernel<double>(s, a, kernel) == cudaSuccess;
 }
 
 

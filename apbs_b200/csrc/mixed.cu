@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "gs7_pipe.cuh"
+#include "gs7_march.cuh"
 #include "gs7_sweep.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
@@ -1129,12 +1130,9 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
     a.c1 = first_parity;
     a.kchunk = tune[6];
     a.xin = x; a.xout = xs;
-    cudaError_t e = tune[12] ? launch_gs7_sweep_async<float, 32, 8>(st, a)
-                             : launch_gs7_sweep<float, 32, 8>(st, a);
+    cudaError_t e = launch_gs7_sweep_kernel<float>(st, a, tune[12]);
     a.xin = xs; a.xout = x;
-    if (e == cudaSuccess)
-      e = tune[12] ? launch_gs7_sweep_async<float, 32, 8>(st, a)
-                   : launch_gs7_sweep<float, 32, 8>(st, a);
+    if (e == cudaSuccess) e = launch_gs7_sweep_kernel<float>(st, a, tune[12]);
     if (r && e == cudaSuccess) {
       const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
       k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, opf(F), F.cc, F.w0, x, r);
@@ -1688,8 +1686,7 @@ int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
   a.cc = F.cc; a.fc = F.w0; a.xin = F.x; a.xout = m->xs;
   a.c1 = 1;
   a.kchunk = s->tune[6];
-  if ((s->tune[12] ? launch_gs7_sweep_async<float, 32, 8>(s->stream, a)
-                   : launch_gs7_sweep<float, 32, 8>(s->stream, a)) != cudaSuccess) {
+  if (launch_gs7_sweep_kernel<float>(s->stream, a, s->tune[12]) != cudaSuccess) {
     set_error("FP32 sweep launch failed");
     return 0;
   }

@@ -34,7 +34,8 @@ TUNE_GS7_COLOUR_PASSES = 5
 TUNE_GS7_SWEEP_KCHUNK, TUNE_GS27_CLUSTER_MID, TUNE_TAIL_MAX_POINTS = 6, 7, 8
 TUNE_MC_COOPERATIVE = 9
 TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS = 10, 11
-TUNE_GS7_SWEEP_STAGED = 12
+TUNE_GS7_SWEEP_KERNEL = 12
+TUNE_GS7_SWEEP_STAGED = TUNE_GS7_SWEEP_KERNEL
 TUNE_GS27_PLANES = 13
 TUNE_CG_CLUSTER = 14
 TUNE_GS27_PLANES_POLL = 15

@@ -170,8 +170,11 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_MIXED_COARSE_SWEEPS 10 /* mixed: 8-colour GS sweeps before and after each
                                             coarse correction on 27-point levels (default 2) */
 #define PMGB_TUNE_MIXED_FINE_SWEEPS 11 /* mixed: red-black sweeps on the fine level (default 2) */
-#define PMGB_TUNE_GS7_SWEEP_STAGED 12 /* single-pass sweep with plane tiles staged through
-                                          shared memory by asynchronous copies (1) */
+#define PMGB_TUNE_GS7_SWEEP_KERNEL 12 /* single-pass sweep kernel: 0 = ring tiles, 1 = ring
+                                          tiles staged through shared memory by asynchronous
+                                          copies, 2 = one thread per column marching up k on
+                                          32x16 tiles, 3 = the same on 32x8 tiles */
+#define PMGB_TUNE_GS7_SWEEP_STAGED PMGB_TUNE_GS7_SWEEP_KERNEL
 #define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
                                           synchronised with its neighbour planes on every
                                           level whose planes fit on the device, 1 = one

@@ -126,27 +126,44 @@ def test_exact_coarse_solve_matches_band():
 
 
 def test_single_pass_sweep_matches_colour_passes():
-    """The fine smoother's single-pass sweep kernel (default), its variant with
-    shared-memory staged planes and the one-launch-per-colour kernels compute
-    the same red-black sweep: bitwise equal results."""
-    from apbs_b200.vpmg import (TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_STAGED, get_tuning,
-                                set_tuning)
+    """The fine smoother's single-pass sweep kernels (ring tiles, the default;
+    ring tiles staged by cp.async; one thread per column marching up k, on
+    32x16 and 32x8 tiles) and the one-launch-per-colour kernels compute the
+    same red-black sweep: bitwise equal FP64 solves, and bitwise equal FP32
+    inner cycles of the mixed path."""
+    from apbs_b200.vpmg import (MIXED, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KERNEL,
+                                TUNE_MIXED_FINE_SWEEPS, get_tuning, set_tuning)
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
     out = {}
     old = get_tuning(TUNE_GS7_COLOUR_PASSES)
+    kernels = (0, 1, 2, 3)
     try:
         for npbe in (False, True):
             p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
-            for passes, staged in ((1, 0), (0, 0), (0, 1)):
+            for passes, kern in ((1, 0),) + tuple((0, k) for k in kernels):
                 set_tuning(TUNE_GS7_COLOUR_PASSES, passes)
                 with Vpmg(p, FP64) as pmg:
-                    pmg.set_tuning(TUNE_GS7_SWEEP_STAGED, staged)
+                    pmg.set_tuning(TUNE_GS7_SWEEP_KERNEL, kern)
                     pmg.fillco(m)
                     pmg.solve()
-                    out[(npbe, passes, staged)] = (pmg.u, pmg.residual_history())
+                    out[(npbe, passes, kern)] = (pmg.u, pmg.residual_history())
     finally:
         set_tuning(TUNE_GS7_COLOUR_PASSES, old)
     for npbe in (False, True):
-        for var in ((0, 0), (0, 1)):
+        for var in tuple((0, k) for k in kernels):
             assert np.array_equal(out[(npbe,) + var][0], out[(npbe, 1, 0)][0]), var
             assert np.array_equal(out[(npbe,) + var][1], out[(npbe, 1, 0)][1]), var
+    # FP32 (mixed inner cycles): every sweep kernel gives the same iterates
+    p = synth.mg_manual(65, 0.5, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    res = {}
+    for kern in kernels:
+        with Vpmg(p, MIXED) as pmg:
+            pmg.set_tuning(TUNE_GS7_COLOUR_PASSES, 2)
+            pmg.set_tuning(TUNE_MIXED_FINE_SWEEPS, 2)
+            pmg.set_tuning(TUNE_GS7_SWEEP_KERNEL, kern)
+            pmg.fillco(m)
+            pmg.solve()
+            res[kern] = (pmg.u, pmg.residual_history())
+    for kern in kernels[1:]:
+        assert np.array_equal(res[kern][0], res[0][0]), kern
+        assert np.array_equal(res[kern][1], res[0][1]), kern
