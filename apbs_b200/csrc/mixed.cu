@@ -80,6 +80,7 @@ struct MixedState {
   cudaGraphExec_t exec[2];
   long long kernels[2];
   int cc_ready;
+  int info_pending;  // dense factor status not read yet (read with the next residual)
   int lo;             // lowest level with FP32 storage (0, or the FP64 coarsest)
   int zero_cc;        // levels >= lo carry no Helmholtz term (band operator)
   int* d_flag;        // device flag of the band restencil check
@@ -1428,7 +1429,7 @@ static int launch_dense_inverse(cudaStream_t st, double* M, int n, int* info) {
   return 0;
 }
 
-int mixed_set_cc(pmgb_solver* s, int newton) {
+int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
   MixedState* m = s->mixed;
   cudaStream_t st = s->stream;
   for (int l = 0; l < m->nlev; l++) {
@@ -1464,6 +1465,12 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
       note_launches(2);
     }
   }
+  m->cc_ready = 1;
+  if (defer_check) {
+    // the caller's next read of the residual also reads the factor's status
+    m->info_pending = 1;
+    return 1;
+  }
   int info = 0;
   CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKM(cudaStreamSynchronize(st));
@@ -1471,7 +1478,6 @@ int mixed_set_cc(pmgb_solver* s, int newton) {
     set_error("mixed: coarsest operator not positive definite (pivot %d)", info);
     return 0;
   }
-  m->cc_ready = 1;
   return 1;
 }
 
@@ -1585,7 +1591,18 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
 
 int read_scal(pmgb_solver* s, int slot, double* v) {
   CKM(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  MixedState* m = s->mixed;
+  int info = 0;
+  const int check = m && m->info_pending;
+  if (check) CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CKM(cudaStreamSynchronize(s->stream));
+  if (check) {
+    m->info_pending = 0;
+    if (info != 0) {
+      set_error("mixed: coarsest operator not positive definite (pivot %d)", info);
+      return 0;
+    }
+  }
   return 1;
 }
 
@@ -1604,14 +1621,16 @@ int refine(pmgb_solver* s, int newton, const double* cc64, const double* fc64, d
                                      s->part);
   k_sum_parts<<<1, 256, 0, st>>>(s->part, nb, s->scal + S_RSNRM);
   note_launches(2);
-  double rsden = 1.0, rsnrm;
+  double rsden = 1.0, rsnrm = 0.0;
   if (!istop0) {
     launch_nrm1(st, g, fc64, s->part + 2368, s->scal + S_RSDEN);
     note_launches(2);
     if (!read_scal(s, S_RSDEN, &rsden)) return 0;
     if (rsden == 0.0) rsden = 1.0;
+    if (!read_scal(s, S_RSNRM, &rsnrm)) return 0;
   }
-  if (!read_scal(s, S_RSNRM, &rsnrm)) return 0;
+  // the Newton inner solve logs 1 and always runs a cycle: its initial
+  // residual norm is not needed on the host
   s->reslog.push_back(istop0 ? 1.0 : rsnrm / rsden);
   if (!m->exec[newton]) {
     cudaGraph_t graph;
@@ -1654,7 +1673,7 @@ int refine(pmgb_solver* s, int newton, const double* cc64, const double* fc64, d
 // ||rhs - J xt||_1 <= errtol_s.
 int mixed_newton_inner(pmgb_solver* s, double errtol_s) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
-  if (!mixed_set_cc(s, 1)) return 0;
+  if (!mixed_set_cc(s, 1, 1)) return 0;
   Level& F = s->lev[0];
   CKM(cudaMemsetAsync(F.xt, 0, s->n * sizeof(double), s->stream));
   int it = 0;
