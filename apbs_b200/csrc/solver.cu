@@ -243,6 +243,10 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     set_error("pmgb_create: chgm %d not implemented (spl0 and spl2 are)", p.chgm);
     return 0;
   }
+  if (p.srfm != PMGB_SRFM_MOL && p.srfm != PMGB_SRFM_SMOL && p.srfm != PMGB_SRFM_SPL2) {
+    set_error("pmgb_create: srfm %d not implemented (mol, smol and spl2 are)", p.srfm);
+    return 0;
+  }
   if (p.nion > 8) {
     set_error("pmgb_create: at most 8 ion species");
     return 0;
@@ -503,7 +507,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   }
   dfree(s->w1); dfree(s->w2); dfree(s->w3); dfree(s->xs);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
-  dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts); dfree(s->d_wave);
+  dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts); dfree(s->d_wave); dfree(s->d_forces);
   dfree(s->d_opptrs);
   dfree(s->band);
   dfree(s->focus_w);
@@ -546,7 +550,14 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
   note_launches(1);
   const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
-  if (!islap) {
+  if (!islap && p.srfm == PMGB_SRFM_SPL2) {
+    // spline surface: kappa and the dielectric maps together (fillcoCoefSpline)
+    const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
+    launch_spline_fill(st, s->G, natoms, s->d_xyz, s->d_r, s->maxIonRadius,
+                       (p.swin > 0.0) ? p.swin : 0.3, ionmask, p.pdie, p.sdie, s->kappa,
+                       s->epsx, s->epsy, s->epsz);
+    note_launches(1);
+  } else if (!islap) {
     // dielectric (fillcoCoefMolDielNoSmooth)
     launch_fill_value(st, s->epsx, n, p.sdie);
     launch_fill_value(st, s->epsy, n, p.sdie);

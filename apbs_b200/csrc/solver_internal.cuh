@@ -100,6 +100,8 @@ struct pmgb_solver {
   // step counters of the plane-parallel GS27 wavefront: word 0 counts waits
   // that ran out, level l's counters start at kWaveCounterBase + l *
   // kWavePlanesMax
+  double* d_forces;         // pmgb_forces: 9 doubles and a status word per atom
+  size_t forces_alloc;
   unsigned* d_wave;
   int wave_used;  // a solve launched the plane kernel since the last check
   double* atom_terms;  // 13 x natoms sdh moment terms

@@ -1,0 +1,608 @@
+// Spline-based molecular surfaces (srfm spl2) and the forces on the atoms.
+//
+// Surface: fillcoCoefSpline (src/mg/vpmg.c:4631-4854).  kappa, epsx, epsy
+// and epsz start at 1 everywhere; for every on-mesh atom with a positive
+// radius, in atom order, each grid point inside the atom's search box has
+// its values multiplied by the cubic spline accessibility of the point (0
+// well inside the atom, 1 outside the window, 0.75 s^2/w^2 - 0.25 s^3/w^3
+// between), each map only while it is above VPMGSMALL; kappa uses the
+// radius inflated by the largest ion radius, the eps maps are evaluated at
+// the staggered points (i+1/2, j, k), (i, j+1/2, k), (i, j, k+1/2).  Then
+// kappa *= ionmask and eps = (epsw - epsp) eps + epsp.
+//
+// The reference scatters atom by atom; here a CTA owns a block of grid
+// points, scans the atoms in index order and keeps those whose search box
+// (the reference's own imin..kmax) meets the block, in order, in shared
+// memory.  Each thread applies them to its points in that order with the
+// reference's expressions, so each point sees the same factors in the same
+// order and the maps are bitwise equal.
+//
+// Forces: Vpmg_qfForce (vpmg.c:5862-5904 with qfForceSpline1 5906-6041 and
+// qfForceSpline2 6043-6154), Vpmg_dbForce (5605-5860) and Vpmg_ibForce
+// (5440-5603) with Vacc_splineAccGradAtomNorm (src/generic/vacc.c:314-373).
+// One thread per atom walks the reference's loops in their order, so each
+// sum is taken in the reference's order.
+#include <algorithm>
+#include <vector>
+
+#include "apbs_b200.h"
+#include "fill_kernels.cuh"
+#include "solver_internal.cuh"
+
+namespace pmgb {
+
+namespace {
+
+constexpr double kPmgSmall = 1e-12;  // VPMGSMALL (src/generic/vhal.h)
+constexpr double kVSmall = 1e-9;     // VSMALL (maloc)
+constexpr double kExpMax = 85.0;     // EXPMAX / -EXPMIN (src/generic/vcap.h)
+
+// ---------------------------------------------------------------------------
+// srfm spl2 fill
+// ---------------------------------------------------------------------------
+struct SplineArgs {
+  FillGeom G;
+  int natoms;
+  const double* xyz;
+  const double* r;
+  double irad;      // largest ion radius
+  double win;       // spline window
+  double ionmask;   // 1 if the ionic strength is positive
+  double epsp, epsw;
+  double *kappa, *epsx, *epsy, *epsz;
+};
+
+struct SplAtom {
+  double pos[3];  // position relative to the grid origin
+  double arad;
+  int box[6];     // imin, imax, jmin, jmax, kmin, kmax
+};
+
+constexpr int kBX = 8, kBY = 8, kBZ = 8;        // grid points per CTA block
+constexpr int kSplThreads = 256;                 // two points per thread
+constexpr int kSplCap = 512;                     // candidate atoms held at once
+
+// the search box of atom a (fillcoCoefSpline), or false if the atom is
+// skipped (off the mesh or of zero radius)
+__device__ __forceinline__ bool spline_atom(const SplineArgs& A, int a, SplAtom& s) {
+  const FillGeom& G = A.G;
+  const double* apos = A.xyz + 3 * a;
+  const double arad = A.r[a];
+  if ((apos[0] <= G.xmin[0]) || (apos[0] >= G.xmax[0]) || (apos[1] <= G.xmin[1]) ||
+      (apos[1] >= G.xmax[1]) || (apos[2] <= G.xmin[2]) || (apos[2] >= G.xmax[2]))
+    return false;
+  if (!(arad > kPmgSmall)) return false;
+  for (int d = 0; d < 3; d++) s.pos[d] = apos[d] - G.xmin[d];
+  s.arad = arad;
+  const double itot = A.irad + arad + A.win;
+  const double stot = arad + A.win;
+  const double rtot = (itot > stot) ? itot : stot;
+  const int n[3] = {G.g.nx, G.g.ny, G.g.nz};
+  for (int d = 0; d < 3; d++) {
+    const double dd = rtot + 0.5 * G.h[d];
+    s.box[2 * d] = max(0, (int)floor((s.pos[d] - dd) / G.h[d]));
+    s.box[2 * d + 1] = min(n[d] - 1, (int)ceil((s.pos[d] + dd) / G.h[d]));
+  }
+  return true;
+}
+
+__device__ __forceinline__ double spline_value(double dist, double rad, double win, double w2i,
+                                               double w3i) {
+  const double sm = dist - rad + win;
+  const double sm2 = sm * sm;
+  return 0.75 * sm2 * w2i - 0.25 * sm * sm2 * w3i;
+}
+
+__global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
+  __shared__ SplAtom cand[kSplCap];
+  __shared__ int wcount[kSplThreads / 32];
+  __shared__ int ncand;
+  const FillGeom& G = A.G;
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  const int bi = blockIdx.x * kBX, bj = blockIdx.y * kBY, bk = blockIdx.z * kBZ;
+  const int tx = threadIdx.x % kBX, ty = (threadIdx.x / kBX) % kBY, tz = threadIdx.x / (kBX * kBY);
+  const int i = bi + tx, j = bj + ty;
+  const int kk[2] = {bk + tz, bk + tz + kBZ / 2};
+  const bool on[2] = {i < nx && j < ny && kk[0] < nz, i < nx && j < ny && kk[1] < nz};
+  double kap[2] = {1.0, 1.0}, ex[2] = {1.0, 1.0}, ey[2] = {1.0, 1.0}, ez[2] = {1.0, 1.0};
+  const double win = A.win;
+  const double w2i = 1.0 / (win * win);
+  const double w3i = 1.0 / (win * win * win);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) ncand = 0;
+  __syncthreads();
+
+  auto apply = [&](int count) {
+    for (int c = 0; c < count; c++) {
+      const SplAtom& s = cand[c];
+      if (i < s.box[0] || i > s.box[1] || j < s.box[2] || j > s.box[3]) continue;
+      const double arad = s.arad;
+      const double itot = A.irad + arad + win, itot2 = itot * itot;
+      const double ictot = fmax(0.0, (A.irad + arad - win)), ictot2 = ictot * ictot;
+      const double stot = arad + win, stot2 = stot * stot;
+      const double sctot = fmax(0.0, (arad - win)), sctot2 = sctot * sctot;
+      const double dx2 = (s.pos[0] - hx * i) * (s.pos[0] - hx * i);
+      const double dy2 = (s.pos[1] - hy * j) * (s.pos[1] - hy * j);
+      for (int p = 0; p < 2; p++) {
+        const int k = kk[p];
+        if (!on[p] || k < s.box[4] || k > s.box[5]) continue;
+        const double dz2 = (s.pos[2] - k * hz) * (s.pos[2] - k * hz);
+        if (kap[p] > kPmgSmall) {
+          const double dist2 = dz2 + dy2 + dx2;
+          if (dist2 <= ictot2) kap[p] = 0.0;
+          if ((dist2 < itot2) && (dist2 > ictot2))
+            kap[p] *= spline_value(sqrt(dist2), arad + A.irad, win, w2i, w3i);
+        }
+        if (ex[p] > kPmgSmall) {
+          const double t = s.pos[0] - (i + 0.5) * hx;
+          const double dist2 = dz2 + dy2 + t * t;
+          if (dist2 <= sctot2) ex[p] = 0.0;
+          if ((dist2 > sctot2) && (dist2 < stot2))
+            ex[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+        }
+        if (ey[p] > kPmgSmall) {
+          const double t = s.pos[1] - (j + 0.5) * hy;
+          const double dist2 = dz2 + dx2 + t * t;
+          if (dist2 <= sctot2) ey[p] = 0.0;
+          if ((dist2 > sctot2) && (dist2 < stot2))
+            ey[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+        }
+        if (ez[p] > kPmgSmall) {
+          const double t = s.pos[2] - (k + 0.5) * hz;
+          const double dist2 = dy2 + dx2 + t * t;
+          if (dist2 <= sctot2) ez[p] = 0.0;
+          if ((dist2 > sctot2) && (dist2 < stot2))
+            ez[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+        }
+      }
+    }
+  };
+
+  const int ilast = min(bi + kBX, nx) - 1, jlast = min(bj + kBY, ny) - 1,
+            klast = min(bk + kBZ, nz) - 1;
+  for (int base = 0; base < A.natoms; base += kSplThreads) {
+    // the atoms base .. base+255 whose search box meets this block, appended
+    // in atom order
+    const int a = base + threadIdx.x;
+    SplAtom s;
+    bool keep = false;
+    if (a < A.natoms && spline_atom(A, a, s))
+      keep = !(s.box[1] < bi || s.box[0] > ilast || s.box[3] < bj || s.box[2] > jlast ||
+               s.box[5] < bk || s.box[4] > klast);
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) wcount[wid] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < kSplThreads / 32; w++) {
+      if (w < wid) before += wcount[w];
+      total += wcount[w];
+    }
+    const int start = ncand;
+    if (start + total > kSplCap) {
+      // no room: apply what is held, then start a new list
+      apply(start);
+      __syncthreads();
+      if (keep) cand[before + __popc(m & ((1u << lane) - 1u))] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) ncand = total;
+    } else {
+      if (keep) cand[start + before + __popc(m & ((1u << lane) - 1u))] = s;
+      __syncthreads();
+      if (threadIdx.x == 0) ncand = start + total;
+    }
+    __syncthreads();
+  }
+  apply(ncand);
+  for (int p = 0; p < 2; p++) {
+    if (!on[p]) continue;
+    const size_t id = G.g.idx(i, j, kk[p]);
+    A.kappa[id] = A.ionmask * kap[p];
+    A.epsx[id] = (A.epsw - A.epsp) * ex[p] + A.epsp;
+    A.epsy[id] = (A.epsw - A.epsp) * ey[p] + A.epsp;
+    A.epsz[id] = (A.epsw - A.epsp) * ez[p] + A.epsp;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forces
+// ---------------------------------------------------------------------------
+struct ForceArgs {
+  FillGeom G;
+  int natoms;
+  const double *xyz, *q, *r;
+  const double* u;
+  const double *epsx, *epsy, *epsz, *kappa;
+  int chgm;         // PMGB_CHGM_*
+  int boundary;     // compute the dielectric and ionic boundary forces
+  int nonlin;
+  double win, irad, srad, epsp, epsw, zkappa2, izmagic, ionstr;
+  int nion;
+  double ion_q[8], ion_conc[8];
+  double* out;      // 9 per atom: qf, db, ib
+  int* status;      // per atom: 1, or 0 if the dielectric boundary force failed
+};
+
+__device__ __forceinline__ double bspline2d(double x) {
+  double m2m, m2, m3;
+  if ((x >= 0.0) && (x <= 2.0)) m2m = 1.0 - fabs(x - 1.0);
+  else m2m = 0.0;
+  if ((x >= 1.0) && (x <= 3.0)) m2 = 1.0 - fabs(x - 2.0);
+  else m2 = 0.0;
+  if ((x >= 0.0) && (x <= 3.0)) m3 = 0.5 * x * m2m + 0.5 * (3.0 - x) * m2;
+  else m3 = 0.0;
+  return m3;
+}
+// derivative of the quadratic B-spline (dbspline2, vpmg.c:5107-5120)
+__device__ __forceinline__ double dbspline2d(double x) {
+  double m2m, m2;
+  if ((x >= 0.0) && (x <= 2.0)) m2m = 1.0 - fabs(x - 1.0);
+  else m2m = 0.0;
+  if ((x >= 1.0) && (x <= 3.0)) m2 = 1.0 - fabs(x - 2.0);
+  else m2 = 0.0;
+  return m2m - m2;
+}
+
+// gradient of the log of one atom's spline accessibility at a point
+// (Vacc_splineAccGradAtomNorm, vacc.c:314-373)
+__device__ __forceinline__ void spline_grad(const double* center, double win, double infrad,
+                                            const double* apos, double radius, double* grad) {
+  const double w2i = 1.0 / (win * win);
+  const double w3i = 1.0 / (win * win * win);
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (!(radius > 0.0)) return;
+  const double arad = radius + infrad;
+  const double d0 = apos[0] - center[0], d1 = apos[1] - center[1], d2 = apos[2] - center[2];
+  const double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  double mychi, mygrad;
+  if (dist < (arad - win)) return;
+  else if (dist > (arad + win)) return;
+  else if ((fabs(dist - (arad - win)) < kVSmall) || (fabs(dist - (arad + win)) < kVSmall)) return;
+  else {
+    const double sm = dist - arad + win;
+    const double sm2 = sm * sm;
+    mychi = 0.75 * sm2 * w2i - 0.25 * sm * sm2 * w3i;
+    mygrad = 1.5 * sm * w2i - 0.75 * sm2 * w3i;
+  }
+  for (int d = 0; d < 3; d++) grad[d] = -(mygrad / mychi) * ((center[d] - apos[d]) / dist);
+}
+
+// Vcap_exp (src/generic/vcap.c:59-73)
+__device__ __forceinline__ double cap_exp(double x) {
+  if (x > kExpMax) return exp(kExpMax);
+  if (x < -kExpMax) return exp(-kExpMax);
+  return exp(x);
+}
+
+__global__ void k_forces(ForceArgs A) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= A.natoms) return;
+  const FillGeom& G = A.G;
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const double hx = G.h[0], hy = G.h[1], hzed = G.h[2];
+  const double xmin = G.xmin[0], ymin = G.xmin[1], zmin = G.xmin[2];
+  const double xmax = G.xmax[0], ymax = G.xmax[1], zmax = G.xmax[2];
+  const double* apos = A.xyz + 3 * a;
+  const double charge = A.q[a], radius = A.r[a];
+  const double* u = A.u;
+  auto IJK = [&](int i, int j, int k) { return ((size_t)k * ny + j) * nx + i; };
+  double* out = A.out + 9 * (size_t)a;
+  for (int d = 0; d < 9; d++) out[d] = 0.0;
+  int status = 1;
+
+  // partition flag of Vpmg_setPart (vpmg.c:673-720) for the domain box
+  double part_id = 1.0;
+  for (int d = 0; d < 3; d++) {
+    const double lo = G.xmin[d], hi = G.xmax[d];
+    double ok;
+    if ((apos[d] < hi) && (apos[d] > lo)) ok = 1;
+    else if (fabs(apos[d] - lo) < kPmgSmall) ok = 1;
+    else if (fabs(apos[d] - hi) < kPmgSmall) ok = 1;
+    else ok = 0;
+    part_id = (d == 0) ? ok : part_id * ok;
+  }
+
+  // ---- charge-field force
+  if (part_id != 0.0) {
+    double* f = out;
+    if (A.chgm == PMGB_CHGM_SPL2) {
+      if (!((apos[0] <= (xmin + hx)) || (apos[0] >= (xmax - hx)) || (apos[1] <= (ymin + hy)) ||
+            (apos[1] >= (ymax - hy)) || (apos[2] <= (zmin + hzed)) ||
+            (apos[2] >= (zmax - hzed)))) {
+        const double ifloat = (apos[0] - xmin) / hx;
+        const double jfloat = (apos[1] - ymin) / hy;
+        const double kfloat = (apos[2] - zmin) / hzed;
+        const int ip2 = min((int)ceil(ifloat) + 1, nx - 1);
+        const int im2 = max((int)floor(ifloat) - 1, 0);
+        const int jp2 = min((int)ceil(jfloat) + 1, ny - 1);
+        const int jm2 = max((int)floor(jfloat) - 1, 0);
+        const int kp2 = min((int)ceil(kfloat) + 1, nz - 1);
+        const int km2 = max((int)floor(kfloat) - 1, 0);
+        for (int ii = im2; ii <= ip2; ii++) {
+          const double mx = bspline2d(1.5 + ((double)ii - ifloat));
+          const double dmx = dbspline2d(1.5 + ((double)ii - ifloat));
+          for (int jj = jm2; jj <= jp2; jj++) {
+            const double my = bspline2d(1.5 + ((double)jj - jfloat));
+            const double dmy = dbspline2d(1.5 + ((double)jj - jfloat));
+            for (int kk = km2; kk <= kp2; kk++) {
+              const double mz = bspline2d(1.5 + ((double)kk - kfloat));
+              const double dmz = dbspline2d(1.5 + ((double)kk - kfloat));
+              const double uv = u[IJK(ii, jj, kk)];
+              f[0] += (charge * dmx * my * mz * uv) / hx;
+              f[1] += (charge * mx * dmy * mz * uv) / hy;
+              f[2] += (charge * mx * my * dmz * uv) / hzed;
+            }
+          }
+        }
+      }
+    } else if (!((apos[0] <= xmin) || (apos[0] >= xmax) || (apos[1] <= ymin) ||
+                 (apos[1] >= ymax) || (apos[2] <= zmin) || (apos[2] >= zmax))) {
+      // trilinear charges (qfForceSpline1)
+      const double ifloat = (apos[0] - xmin) / hx;
+      const double jfloat = (apos[1] - ymin) / hy;
+      const double kfloat = (apos[2] - zmin) / hzed;
+      const int ihi = (int)ceil(ifloat), ilo = (int)floor(ifloat);
+      const int jhi = (int)ceil(jfloat), jlo = (int)floor(jfloat);
+      const int khi = (int)ceil(kfloat), klo = (int)floor(kfloat);
+      const double dx = ifloat - (double)(ilo);
+      const double dy = jfloat - (double)(jlo);
+      const double dz = kfloat - (double)(klo);
+      if ((dx > kPmgSmall) && (fabs(1.0 - dx) > kPmgSmall)) {
+        f[0] = -charge *
+               (dy * dz * u[IJK(ihi, jhi, khi)] + dy * (1 - dz) * u[IJK(ihi, jhi, klo)] +
+                (1 - dy) * dz * u[IJK(ihi, jlo, khi)] +
+                (1 - dy) * (1 - dz) * u[IJK(ihi, jlo, klo)] - dy * dz * u[IJK(ilo, jhi, khi)] -
+                dy * (1 - dz) * u[IJK(ilo, jhi, klo)] - (1 - dy) * dz * u[IJK(ilo, jlo, khi)] -
+                (1 - dy) * (1 - dz) * u[IJK(ilo, jlo, klo)]) /
+               hx;
+      }
+      if ((dy > kPmgSmall) && (fabs(1.0 - dy) > kPmgSmall)) {
+        f[1] = -charge *
+               (dx * dz * u[IJK(ihi, jhi, khi)] + dx * (1 - dz) * u[IJK(ihi, jhi, klo)] -
+                dx * dz * u[IJK(ihi, jlo, khi)] - dx * (1 - dz) * u[IJK(ihi, jlo, klo)] +
+                (1 - dx) * dz * u[IJK(ilo, jhi, khi)] +
+                (1 - dx) * (1 - dz) * u[IJK(ilo, jhi, klo)] -
+                (1 - dx) * dz * u[IJK(ilo, jlo, khi)] -
+                (1 - dx) * (1 - dz) * u[IJK(ilo, jlo, klo)]) /
+               hy;
+      }
+      if ((dz > kPmgSmall) && (fabs(1.0 - dz) > kPmgSmall)) {
+        f[2] = -charge *
+               (dy * dx * u[IJK(ihi, jhi, khi)] - dy * dx * u[IJK(ihi, jhi, klo)] +
+                (1 - dy) * dx * u[IJK(ihi, jlo, khi)] - (1 - dy) * dx * u[IJK(ihi, jlo, klo)] +
+                dy * (1 - dx) * u[IJK(ilo, jhi, khi)] - dy * (1 - dx) * u[IJK(ilo, jhi, klo)] +
+                (1 - dy) * (1 - dx) * u[IJK(ilo, jlo, khi)] -
+                (1 - dy) * (1 - dx) * u[IJK(ilo, jlo, klo)]) /
+               hzed;
+      }
+    }
+  }
+  if (!A.boundary || part_id == 0.0) {
+    A.status[a] = status;
+    return;
+  }
+
+  // ---- dielectric boundary force
+  if (!(fabs(A.epsp - A.epsw) < kPmgSmall)) {
+    const double deps = (A.epsw - A.epsp);
+    const double depsi = 1.0 / deps;
+    const double rtot = (radius + A.win + A.srad);
+    if (!((apos[0] <= xmin + rtot) || (apos[0] >= xmax - rtot) || (apos[1] <= ymin + rtot) ||
+          (apos[1] >= ymax - rtot) || (apos[2] <= zmin + rtot) || (apos[2] >= zmax - rtot))) {
+      const double position[3] = {apos[0] - xmin, apos[1] - ymin, apos[2] - zmin};
+      const int imin = (int)floor((position[0] - rtot) / hx);
+      const int imax = (int)ceil((position[0] + rtot) / hx);
+      const int jmin = (int)floor((position[1] - rtot) / hy);
+      const int jmax = (int)ceil((position[1] + rtot) / hy);
+      const int kmin = (int)floor((position[2] - rtot) / hzed);
+      const int kmax = (int)ceil((position[2] + rtot) / hzed);
+      if (imin < 1 || imax > nx - 2 || jmin < 1 || jmax > ny - 2 || kmin < 1 || kmax > nz - 2) {
+        status = 0;  // "Atom off grid": the reference returns 0 here
+      } else {
+        double dbF[3] = {0.0, 0.0, 0.0};
+        for (int i = imin; i <= imax; i++) {
+          for (int j = jmin; j <= jmax; j++) {
+            for (int k = kmin; k <= kmax; k++) {
+              double gpos[3], dHx[3], dHy[3], dHz[3], dHxm[3], dHym[3], dHzm[3];
+              gpos[0] = (i + 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
+              const double Hxijk = (A.epsx[IJK(i, j, k)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHx);
+              for (int l = 0; l < 3; l++) dHx[l] *= Hxijk;
+              gpos[0] = i * hx + xmin; gpos[1] = (j + 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
+              const double Hyijk = (A.epsy[IJK(i, j, k)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHy);
+              for (int l = 0; l < 3; l++) dHy[l] *= Hyijk;
+              gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k + 0.5) * hzed + zmin;
+              const double Hzijk = (A.epsz[IJK(i, j, k)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHz);
+              for (int l = 0; l < 3; l++) dHz[l] *= Hzijk;
+              gpos[0] = (i - 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
+              const double Hxim1jk = (A.epsx[IJK(i - 1, j, k)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHxm);
+              for (int l = 0; l < 3; l++) dHxm[l] *= Hxim1jk;
+              gpos[0] = i * hx + xmin; gpos[1] = (j - 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
+              const double Hyijm1k = (A.epsy[IJK(i, j - 1, k)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHym);
+              for (int l = 0; l < 3; l++) dHym[l] *= Hyijm1k;
+              gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k - 0.5) * hzed + zmin;
+              const double Hzijkm1 = (A.epsz[IJK(i, j, k - 1)] - A.epsp) * depsi;
+              spline_grad(gpos, A.win, 0., apos, radius, dHzm);
+              for (int l = 0; l < 3; l++) dHzm[l] *= Hzijkm1;
+              const double u0 = u[IJK(i, j, k)];
+              const double dbFmag = u0;
+              const double uxp = u[IJK(i + 1, j, k)], uxm = u[IJK(i - 1, j, k)];
+              const double uyp = u[IJK(i, j + 1, k)], uym = u[IJK(i, j - 1, k)];
+              const double uzp = u[IJK(i, j, k + 1)], uzm = u[IJK(i, j, k - 1)];
+              for (int l = 0; l < 3; l++) {
+                const double tg = (dHx[l] * (uxp - u0) + dHxm[l] * (uxm - u0)) / (hx * hx) +
+                                  (dHy[l] * (uyp - u0) + dHym[l] * (uym - u0)) / (hy * hy) +
+                                  (dHz[l] * (uzp - u0) + dHzm[l] * (uzm - u0)) / (hzed * hzed);
+                dbF[l] += (dbFmag * tg);
+              }
+            }
+          }
+        }
+        for (int l = 0; l < 3; l++)
+          out[3 + l] = -dbF[l] * hx * hy * hzed * deps * 0.5 * A.izmagic;
+      }
+    }
+  }
+
+  // ---- ionic boundary force
+  if (!(A.zkappa2 < kPmgSmall) &&
+      !((apos[0] <= xmin) || (apos[0] >= xmax) || (apos[1] <= ymin) || (apos[1] >= ymax) ||
+        (apos[2] <= zmin) || (apos[2] >= zmax))) {
+    const double position[3] = {apos[0] - xmin, apos[1] - ymin, apos[2] - zmin};
+    const double rtot = (A.irad + radius + A.win);
+    const double rtot2 = rtot * rtot;
+    double ibF[3] = {0.0, 0.0, 0.0};
+    const double ddx = rtot + 0.5 * hx;
+    const int imin = max(0, (int)ceil((position[0] - ddx) / hx));
+    const int imax = min(nx - 1, (int)floor((position[0] + ddx) / hx));
+    for (int i = imin; i <= imax; i++) {
+      const double dx2 = (position[0] - hx * i) * (position[0] - hx * i);
+      double dy;
+      if (rtot2 > dx2) dy = sqrt(rtot2 - dx2) + 0.5 * hy;
+      else dy = 0.5 * hy;
+      const int jmin = max(0, (int)ceil((position[1] - dy) / hy));
+      const int jmax = min(ny - 1, (int)floor((position[1] + dy) / hy));
+      for (int j = jmin; j <= jmax; j++) {
+        const double dy2 = (position[1] - hy * j) * (position[1] - hy * j);
+        double dz;
+        if (rtot2 > (dx2 + dy2)) dz = sqrt(rtot2 - dx2 - dy2) + 0.5 * hzed;
+        else dz = 0.5 * hzed;
+        const int kmin = max(0, (int)ceil((position[2] - dz) / hzed));
+        const int kmax = min(nz - 1, (int)floor((position[2] + dz) / hzed));
+        for (int k = kmin; k <= kmax; k++) {
+          const double dz2 = (k * hzed - position[2]) * (k * hzed - position[2]);
+          if ((dz2 + dy2 + dx2) <= rtot2) {
+            double gpos[3], tgrad[3];
+            gpos[0] = i * hx + xmin;
+            gpos[1] = j * hy + ymin;
+            gpos[2] = k * hzed + zmin;
+            spline_grad(gpos, A.win, A.irad, apos, radius, tgrad);
+            const double uv = u[IJK(i, j, k)], kv = A.kappa[IJK(i, j, k)];
+            double fmag;
+            if (A.nonlin) {
+              fmag = 0.0;
+              for (int m = 0; m < A.nion; m++)
+                fmag += kv * A.ion_conc[m] * (cap_exp(-A.ion_q[m] * uv) - 1.0) / A.ionstr;
+            } else {
+              fmag = (uv * uv) * kv;
+            }
+            for (int l = 0; l < 3; l++) ibF[l] += (A.zkappa2 * fmag * tgrad[l]);
+          }
+        }
+      }
+    }
+    for (int l = 0; l < 3; l++) out[6 + l] = ibF[l] * 0.5 * hx * hy * hzed * A.izmagic;
+  }
+  A.status[a] = status;
+}
+
+}  // namespace
+
+void launch_spline_fill(cudaStream_t st, const FillGeom& G, int natoms, const double* xyz,
+                        const double* r, double irad, double win, double ionmask, double epsp,
+                        double epsw, double* kappa, double* epsx, double* epsy, double* epsz) {
+  SplineArgs A;
+  A.G = G;
+  A.natoms = natoms;
+  A.xyz = xyz;
+  A.r = r;
+  A.irad = irad;
+  A.win = win;
+  A.ionmask = ionmask;
+  A.epsp = epsp;
+  A.epsw = epsw;
+  A.kappa = kappa;
+  A.epsx = epsx;
+  A.epsy = epsy;
+  A.epsz = epsz;
+  dim3 grid((G.g.nx + kBX - 1) / kBX, (G.g.ny + kBY - 1) / kBY, (G.g.nz + kBZ - 1) / kBZ);
+  k_spline_fill<<<grid, kSplThreads, 0, st>>>(A);
+}
+
+}  // namespace pmgb
+
+using namespace pmgb;
+
+// Per-atom forces of the last solve (Vpmg_qfForce, Vpmg_dbForce, Vpmg_ibForce).
+extern "C" int pmgb_forces(pmgb_solver* s, double* qf, double* db, double* ib) {
+  if (!s || !s->solved) {
+    set_error("pmgb_forces: no solution (call pmgb_solve first)");
+    return 0;
+  }
+  const pmgb_params& p = s->p;
+  const int natoms = s->natoms;
+  const int boundary = (db || ib) ? 1 : 0;
+  if (boundary && p.srfm != PMGB_SRFM_SPL2) {
+    set_error("pmgb_forces: the boundary forces need srfm spl2 (spline-based surfaces)");
+    return 0;
+  }
+  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL) {
+    set_error("pmgb_forces: chgm %d has no charge-field force", p.chgm);
+    return 0;
+  }
+  if (natoms <= 0) return 1;
+  cudaStream_t st = s->stream;
+  const size_t need = (size_t)natoms * 10;  // 9 doubles and a status word per atom
+  if (!s->d_forces || s->forces_alloc < need) {
+    if (s->d_forces) cudaFreeAsync(s->d_forces, st);
+    s->d_forces = nullptr;
+    s->forces_alloc = 0;
+    PMGB_CUDA_OK(cudaMallocAsync((void**)&s->d_forces, need * sizeof(double), st));
+    s->forces_alloc = need;
+  }
+  ForceArgs A;
+  A.G = s->G;
+  A.natoms = natoms;
+  A.xyz = s->d_xyz;
+  A.q = s->d_q;
+  A.r = s->d_r;
+  A.u = s->lev[0].x;
+  A.epsx = s->epsx;
+  A.epsy = s->epsy;
+  A.epsz = s->epsz;
+  A.kappa = s->kappa;
+  A.chgm = p.chgm;
+  A.boundary = boundary;
+  A.nonlin = p.nonlin;
+  A.win = (p.swin > 0.0) ? p.swin : 0.3;
+  A.irad = s->maxIonRadius;
+  A.srad = p.srad;
+  A.epsp = p.pdie;
+  A.epsw = p.sdie;
+  A.zkappa2 = s->zkappa2;
+  A.izmagic = 1.0 / s->zmagic;
+  A.ionstr = s->ionstr;
+  A.nion = p.nion;
+  for (int i = 0; i < 8; i++) {
+    A.ion_q[i] = (i < p.nion) ? p.ion_q[i] : 0.0;
+    A.ion_conc[i] = (i < p.nion) ? p.ion_conc[i] : 0.0;
+  }
+  A.out = s->d_forces;
+  A.status = reinterpret_cast<int*>(s->d_forces + 9 * (size_t)natoms);
+  k_forces<<<(natoms + 127) / 128, 128, 0, st>>>(A);
+  note_launches(1);
+  std::vector<double> h(9 * (size_t)natoms);
+  std::vector<int> stat(natoms);
+  PMGB_CUDA_OK(cudaMemcpyAsync(h.data(), A.out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+  PMGB_CUDA_OK(cudaMemcpyAsync(stat.data(), A.status, sizeof(int) * natoms, cudaMemcpyDeviceToHost, st));
+  PMGB_CUDA_OK(cudaStreamSynchronize(st));
+  PMGB_CUDA_OK(cudaGetLastError());
+  for (int a = 0; a < natoms; a++)
+    for (int d = 0; d < 3; d++) {
+      if (qf) qf[3 * a + d] = h[9 * (size_t)a + d];
+      if (db) db[3 * a + d] = h[9 * (size_t)a + 3 + d];
+      if (ib) ib[3 * a + d] = h[9 * (size_t)a + 6 + d];
+    }
+  if (boundary)
+    for (int a = 0; a < natoms; a++)
+      if (!stat[a]) {
+        set_error("pmgb_forces: atom %d too close to the grid edge for the dielectric "
+                  "boundary force (Vpmg_dbForce off grid)", a);
+        return 0;
+      }
+  return 1;
+}

@@ -20,7 +20,7 @@ from dataclasses import dataclass
 import numpy as np
 
 PMGB_MAXION = 8
-SRFM_MOL, SRFM_SMOL = 0, 1
+SRFM_MOL, SRFM_SMOL, SRFM_SPL2 = 0, 1, 2
 CHGM_TRIL, CHGM_SPL2 = 0, 1
 BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS = 0, 1, 2, 4
 
@@ -42,6 +42,7 @@ class PmgbParams(ctypes.Structure):
         ("ion_q", ctypes.c_double * PMGB_MAXION),
         ("ion_conc", ctypes.c_double * PMGB_MAXION),
         ("ion_radius", ctypes.c_double * PMGB_MAXION),
+        ("swin", ctypes.c_double),
     ]
 
 

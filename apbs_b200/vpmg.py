@@ -87,6 +87,7 @@ def lib():
         L.pmgb_focus.argtypes = [vp, vp, ctypes.c_int]
         L.pmgb_solve.argtypes = [vp]
         L.pmgb_energy.argtypes = [vp, dp]
+        L.pmgb_forces.argtypes = [vp, dp, dp, dp]
         L.pmgb_get_potential.argtypes = [vp, dp]
         L.pmgb_get_maps.argtypes = [vp, dp, dp]
         L.pmgb_get_stats.argtypes = [vp, ctypes.POINTER(PmgbStats)]
@@ -170,6 +171,7 @@ class Vpmg:
 
     def fillco_device(self, natoms, d_xyz, d_q, d_r):
         """Fill from atom arrays already in device memory (raw pointers)."""
+        self._natoms = int(natoms)
         _check(lib().pmgb_fillco_device(self._h, natoms, ctypes.c_void_p(d_xyz),
                                         ctypes.c_void_p(d_q), ctypes.c_void_p(d_r)),
                "pmgb_fillco_device")
@@ -177,6 +179,7 @@ class Vpmg:
     def fillco(self, mol):
         xyz, q, r = _atoms(mol)
         self._keep = (xyz, q, r)
+        self._natoms = int(mol.natoms)
         _check(lib().pmgb_fillco(self._h, mol.natoms, _dp(xyz), _dp(q), _dp(r)), "pmgb_fillco")
 
     def focus(self, coarse: "Vpmg", calc_energy: bool = True):
@@ -204,6 +207,22 @@ class Vpmg:
         e = np.zeros(1)
         _check(lib().pmgb_energy(self._h, _dp(e)), "pmgb_energy")
         return float(e[0])
+
+    def forces(self, boundary: bool = True) -> dict:
+        """Per-atom forces of the last solve in kT/A, as Vpmg_force builds
+        them per atom: ``qf`` (charge field) and, with ``boundary`` (needs
+        srfm spl2), ``db`` (dielectric boundary) and ``ib`` (ionic
+        boundary); each an (natoms, 3) array."""
+        n = getattr(self, "_natoms", 0)
+        qf = np.zeros((n, 3))
+        db = np.zeros((n, 3)) if boundary else None
+        ib = np.zeros((n, 3)) if boundary else None
+        _check(lib().pmgb_forces(self._h, _dp(qf), _dp(db) if boundary else None,
+                                 _dp(ib) if boundary else None), "pmgb_forces")
+        out = {"qf": qf}
+        if boundary:
+            out.update(db=db, ib=ib)
+        return out
 
     @property
     def u(self) -> np.ndarray:

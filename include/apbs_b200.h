@@ -109,6 +109,19 @@ int pmgb_solve(pmgb_solver *s);
 /* Vpmg_energy(extFlag = 1) of a non-focused calculation, in kT. */
 int pmgb_energy(pmgb_solver *s, double *energy_kT);
 
+/* Forces on every atom of the last fill, from the last solve, in kT/A
+ * (arrays of 3 doubles per atom; any may be NULL):
+ *   qf  charge-field force, Vpmg_qfForce (src/mg/vpmg.c:5862-6154), for
+ *       chgm spl2 or spl0;
+ *   db  dielectric boundary force, Vpmg_dbForce (vpmg.c:5605-5860);
+ *   ib  ionic boundary force, Vpmg_ibForce (vpmg.c:5440-5603);
+ * db and ib need srfm spl2 (the reference's rule: forces need spline-based
+ * surfaces).  Atoms outside the domain get zero, as in the reference; an
+ * atom whose dielectric-boundary window crosses the grid edge fails the call
+ * (the reference's Vpmg_dbForce returns 0 for it).  One call replaces the
+ * per-atom Vpmg_force loop of forceMG (src/routines.c). */
+int pmgb_forces(pmgb_solver *s, double *qf, double *db, double *ib);
+
 /* Copy the potential (thee->u, Dirichlet values restored) to host memory. */
 int pmgb_get_potential(pmgb_solver *s, double *u);
 

@@ -5,7 +5,7 @@
  * PBEparm, Vpmgp and Vpbe for a single mg-manual ELEC block:
  *   dime/grid/gcent/nlev  (src/generic/mgparm.h:114-203, keyword parser
  *                          src/generic/mgparm.c:916-969)
- *   lpbe|npbe, bcfl, pdie, sdie, srfm, srad, sdens, temp, ion, chgm
+ *   lpbe|npbe, bcfl, pdie, sdie, srfm, srad, sdens, swin, temp, ion, chgm
  *                         (src/generic/pbeparm.c:1215-1285)
  * It is shared by the CUDA library's C ABI (apbs_b200.h) and by the CPU
  * oracle, so both sides of every parity test are driven by identical input.
@@ -18,6 +18,7 @@
 /* Surface method codes (values of Vsurf_Meth, src/generic/vhal.h:103-107). */
 #define PMGB_SRFM_MOL 0
 #define PMGB_SRFM_SMOL 1
+#define PMGB_SRFM_SPL2 2   /* cubic-spline surface (fillcoCoefSpline) */
 /* Charge method codes (Vchrg_Meth, src/generic/vhal.h:231-234). */
 #define PMGB_CHGM_TRIL 0   /* chgm spl0: trilinear to the 8 nearest points */
 #define PMGB_CHGM_SPL2 1
@@ -46,6 +47,8 @@ typedef struct pmgb_params {
     double ion_q[PMGB_MAXION];      /* valence (e) */
     double ion_conc[PMGB_MAXION];   /* bulk concentration (M) */
     double ion_radius[PMGB_MAXION]; /* radius (Angstrom) */
+    double swin;            /* spline window of srfm spl2 and of the boundary
+                               forces ("swin"); <= 0 -> 0.3 */
 } pmgb_params;
 
 #endif /* PMGB_PARAMS_H */

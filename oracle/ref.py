@@ -23,7 +23,8 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         _lib.ref_pmg_run.restype = ctypes.c_int
         _lib.ref_pmg_run.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
-                                     dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
+                                     dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int,
+                                     dp, ctypes.POINTER(ctypes.c_int)]
         _lib.ref_pmg_focus.restype = ctypes.c_int
         _lib.ref_pmg_focus.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
                                      dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
@@ -36,11 +37,13 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=4096):
+def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=4096,
+        want_forces=False):
     """Run ctor+fillco+solve+energy of the reference on one calculation.
 
     Returns a dict with u (nz,ny,nx), energy_kT, progress-message count,
-    residual log, phase timings and, on request, the fill maps and faces.
+    residual log, phase timings and, on request, the fill maps and faces and
+    the per-atom forces (qf, db, ib: (natoms, 3) each, and their status).
     """
     n = params.nx * params.ny * params.nz
     u = np.zeros(n)
@@ -52,9 +55,13 @@ def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=40
     xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
     q = np.ascontiguousarray(mol.charge, dtype=np.float64)
     r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    forces = np.zeros(9 * mol.natoms) if want_forces else None
+    fstatus = np.zeros(mol.natoms, dtype=np.int32) if want_forces else None
     rc = lib().ref_pmg_run(ctypes.byref(params), mol.natoms, _ptr(xyz), _ptr(q), _ptr(r),
                            _ptr(u), _ptr(maps), _ptr(faces), _ptr(out), _ptr(reslog),
-                           reslog_cap, verbose)
+                           reslog_cap, verbose, _ptr(forces),
+                           fstatus.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+                           if fstatus is not None else None)
     if rc != 1:
         raise RuntimeError("reference PMG run failed")
     shape = (params.nz, params.ny, params.nx)
@@ -71,6 +78,9 @@ def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=40
         res.update(charge=m[0], epsx=m[1], epsy=m[2], epsz=m[3], kappa=m[4])
     if faces is not None:
         res["faces"] = faces
+    if forces is not None:
+        f = forces.reshape(mol.natoms, 3, 3)
+        res.update(qf=f[:, 0].copy(), db=f[:, 1].copy(), ib=f[:, 2].copy(), fstatus=fstatus)
     return res
 
 

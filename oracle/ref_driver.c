@@ -30,6 +30,9 @@ int oracle_shim_log_count(void);
 int oracle_shim_iter_count(void);
 void oracle_shim_set_verbose(int v);
 
+/* spline window passed to Vpmg_fillco (the deck's swin, default 0.3) */
+#define SWIN(p) (((p)->swin > 0.0) ? (p)->swin : 0.3)
+
 static double now_s(void) {
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -100,12 +103,15 @@ static MGparm *make_mgparm(const pmgb_params *p) {
  *          [2] residual-log entries [3] t_ctor [4] t_fillco [5] t_solve
  *          [6] t_energy (seconds) [7] qf [8] diel [9] qm (kT, NPBE only)
  *   reslog (out, optional) relative residual of every progress message
+ *   forces (out, optional) 9 doubles per atom: Vpmg_qfForce, Vpmg_dbForce,
+ *          Vpmg_ibForce (kT/A), the last two for srfm spl2 only
+ *   fstatus (out, optional) per atom, 1 if both boundary forces succeeded
  * Returns 1 on success (Vpmg convention), 0 on failure.
  */
 int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
                 const double *q, const double *r, double *u, double *maps,
                 double *faces, double *out, double *reslog, int reslog_cap,
-                int verbose) {
+                int verbose, double *forces, int *fstatus) {
     int i, n, rc;
     double t0, t1, t2, t3, t4;
     double ionc[PMGB_MAXION], ionr[PMGB_MAXION], ionq[PMGB_MAXION];
@@ -136,7 +142,7 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
     pmgp->zcent = p->center[2];
     pmg = Vpmg_ctor(pmgp, pbe, 0, VNULL, mg, PCE_NO);
     t1 = now_s();
-    rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, 0.3, (Vchrg_Meth)p->chgm,
+    rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
                      0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
                      VNULL);
     t2 = now_s();
@@ -165,6 +171,24 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
         partMax[i] = mg->center[i] + 0.5 * mg->glen[i];
     }
     Vpmg_setPart(pmg, partMin, partMax, mg->partDisjOwnSide);
+    if (forces) {
+        /* per atom: charge-field, dielectric-boundary and ionic-boundary
+         * forces as Vpmg_force assembles them (vpmg.c:5418-5438); the two
+         * boundary forces only for spline surfaces (their status, 1/0, in
+         * fstatus) */
+        for (i = 0; i < natoms; i++) {
+            int rcf = 1;
+            Vpmg_qfForce(pmg, forces + 9 * (size_t)i, i, (Vchrg_Meth)p->chgm);
+            if (p->srfm == PMGB_SRFM_SPL2) {
+                rcf &= Vpmg_dbForce(pmg, forces + 9 * (size_t)i + 3, i, (Vsurf_Meth)p->srfm);
+                rcf &= Vpmg_ibForce(pmg, forces + 9 * (size_t)i + 6, i, (Vsurf_Meth)p->srfm);
+            } else {
+                int d;
+                for (d = 3; d < 9; d++) forces[9 * (size_t)i + d] = 0.0;
+            }
+            if (fstatus) fstatus[i] = rcf;
+        }
+    }
     out[0] = Vpmg_energy(pmg, 1);
     t4 = now_s();
     out[1] = (double)oracle_shim_iter_count();
@@ -230,7 +254,7 @@ int ref_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
     pmgpc->ycent = pc->center[1];
     pmgpc->zcent = pc->center[2];
     pmgc = Vpmg_ctor(pmgpc, pbec, 0, VNULL, mgc, PCE_NO);
-    rc = Vpmg_fillco(pmgc, (Vsurf_Meth)pc->srfm, 0.3, (Vchrg_Meth)pc->chgm,
+    rc = Vpmg_fillco(pmgc, (Vsurf_Meth)pc->srfm, SWIN(pc), (Vchrg_Meth)pc->chgm,
                      0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
                      VNULL);
     if (rc != 1) return 0;
@@ -261,7 +285,7 @@ int ref_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
     Vpbe_dtor(&pbec);
     MGparm_dtor(&mgc);
     t1 = now_s();
-    rc = Vpmg_fillco(pmgf, (Vsurf_Meth)pf->srfm, 0.3, (Vchrg_Meth)pf->chgm,
+    rc = Vpmg_fillco(pmgf, (Vsurf_Meth)pf->srfm, SWIN(pf), (Vchrg_Meth)pf->chgm,
                      0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
                      VNULL);
     t2 = now_s();
