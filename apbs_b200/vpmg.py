@@ -28,6 +28,7 @@ MIXED = 1
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
 K_GS7_PIPE_FP64, K_GS7_PIPE_FP32, K_VCYCLE_TAIL = 5, 6, 7
 K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
+DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX, DX_DIELY, DX_DIELZ = range(6)
 TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5
@@ -88,6 +89,8 @@ def lib():
         L.pmgb_solve.argtypes = [vp]
         L.pmgb_energy.argtypes = [vp, dp]
         L.pmgb_forces.argtypes = [vp, dp, dp, dp]
+        L.pmgb_write_dx.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.c_char_p]
         L.pmgb_get_potential.argtypes = [vp, dp]
         L.pmgb_get_maps.argtypes = [vp, dp, dp]
         L.pmgb_get_stats.argtypes = [vp, ctypes.POINTER(PmgbStats)]
@@ -207,6 +210,14 @@ class Vpmg:
         e = np.zeros(1)
         _check(lib().pmgb_energy(self._h, _dp(e)), "pmgb_energy")
         return float(e[0])
+
+    def write_dx(self, path, which: int = 0, title: str | None = None,
+                 package: str | None = None):
+        """Write one map (DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX/Y/Z) as the
+        OpenDX file writedataMG writes."""
+        _check(lib().pmgb_write_dx(self._h, which, str(path).encode(),
+                                   title.encode() if title else None,
+                                   package.encode() if package else None), "pmgb_write_dx")
 
     def forces(self, boundary: bool = True) -> dict:
         """Per-atom forces of the last solve in kT/A, as Vpmg_force builds

@@ -122,6 +122,25 @@ int pmgb_energy(pmgb_solver *s, double *energy_kT);
  * per-atom Vpmg_force loop of forceMG (src/routines.c). */
 int pmgb_forces(pmgb_solver *s, double *qf, double *db, double *ib);
 
+/* OpenDX output, byte for byte the file writedataMG writes through
+ * Vgrid_writeDX (src/routines.c:2620-2920, src/mg/vgrid.c:1206-1420):
+ * pmgb_write_dx writes one map of a calculation with its partition weights
+ * (which = PMGB_DX_*; title NULL = the reference's title for that map;
+ * package NULL = "APBS 3.4.1" for the "# Data from" line);
+ * pmgb_write_dx_host writes a caller's host array (pvec NULL = every
+ * point).  The values are formatted by several host threads. */
+#define PMGB_DX_POT 0     /* u (kT/e) */
+#define PMGB_DX_CHARGE 1  /* charge / zmagic (e) */
+#define PMGB_DX_KAPPA 2
+#define PMGB_DX_DIELX 3
+#define PMGB_DX_DIELY 4
+#define PMGB_DX_DIELZ 5
+int pmgb_write_dx(pmgb_solver *s, int which, const char *path, const char *title,
+                  const char *package);
+int pmgb_write_dx_host(const char *path, int nx, int ny, int nz, double hx, double hy,
+                       double hz, double xmin, double ymin, double zmin, const double *data,
+                       const double *pvec, const char *title, const char *package);
+
 /* Copy the potential (thee->u, Dirichlet values restored) to host memory. */
 int pmgb_get_potential(pmgb_solver *s, double *u);
 

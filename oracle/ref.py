@@ -25,6 +25,9 @@ def lib():
         _lib.ref_pmg_run.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
                                      dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int,
                                      dp, ctypes.POINTER(ctypes.c_int)]
+        _lib.ref_write_dx.restype = ctypes.c_int
+        _lib.ref_write_dx.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [
+            dp, dp, ctypes.c_char_p, ctypes.c_char_p]
         _lib.ref_pmg_focus.restype = ctypes.c_int
         _lib.ref_pmg_focus.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
                                      dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
@@ -113,3 +116,17 @@ def focus(coarse, fine, mol, want_faces=False, reslog_cap=8192):
     if faces is not None:
         res["faces"] = faces
     return res
+
+
+def write_dx(path, data, h, origin, pvec=None, title="POTENTIAL (kT/e)"):
+    """The reference's Vgrid_writeDX on data (nz, ny, nx): the OpenDX file
+    writedataMG writes.  PACKAGE_STRING of this build is
+    "APBS 3.4.1 (reference oracle build)"."""
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    nz, ny, nx = d.shape
+    pv = None if pvec is None else np.ascontiguousarray(pvec, dtype=np.float64)
+    rc = lib().ref_write_dx(nx, ny, nz, h[0], h[1], h[2], origin[0], origin[1], origin[2],
+                            _ptr(d.reshape(-1)), _ptr(None if pv is None else pv.reshape(-1)),
+                            str(path).encode(), title.encode())
+    if rc != 1:
+        raise RuntimeError("reference DX write failed")

@@ -12,6 +12,7 @@
  * list instead of a PQR file (Valist_readPQR, src/generic/valist.c:606, is
  * replaced by filling the Valist directly and calling Valist_getStatistics).
  */
+#include <stdio.h>
 #include <time.h>
 #include "apbscfg.h"
 #include "maloc/maloc.h"
@@ -21,6 +22,7 @@
 #include "generic/vpbe.h"
 #include "generic/mgparm.h"
 #include "generic/pbeparm.h"
+#include "mg/vgrid.h"
 #include "mg/vpmgp.h"
 #include "mg/vpmg.h"
 #include "pmgb_params.h"
@@ -325,5 +327,20 @@ int ref_pmg_focus(const pmgb_params *pc, const pmgb_params *pf, int natoms,
     Vpbe_dtor(&pbef);
     MGparm_dtor(&mgf);
     Valist_dtor(&alist);
+    return 1;
+}
+
+/* Vgrid_writeDX (src/mg/vgrid.c:1206-1420) on a caller array: the OpenDX
+ * file writedataMG writes for a map (routines.c:2620-2800), with pvec the
+ * partition weights (NULL: every point).  Returns 1. */
+int ref_write_dx(int nx, int ny, int nz, double hx, double hy, double hz, double xmin,
+                 double ymin, double zmin, double *data, double *pvec, const char *path,
+                 const char *title) {
+    char t[256];
+    Vgrid *grid = Vgrid_ctor(nx, ny, nz, hx, hy, hz, xmin, ymin, zmin, data);
+    if (grid == VNULL) return 0;
+    snprintf(t, sizeof(t), "%s", title);
+    Vgrid_writeDX(grid, "FILE", "ASC", VNULL, path, t, pvec);
+    Vgrid_dtor(&grid);
     return 1;
 }

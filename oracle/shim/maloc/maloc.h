@@ -110,9 +110,10 @@ VEXTERNC double Vnm_epsmac(void);
 VEXTERNC void Vnm_redirect(int flag);
 VEXTERNC int Vnm_system(char *cmd);
 
-/* ---- Vio: byte streams (input-deck parsing only; not on the solve path) */
+/* ---- Vio: byte streams.  Only "FILE" sockets opened for writing do
+ * anything (the OpenDX writer, Vgrid_writeDX); the rest are inert. */
 typedef struct sVio {
-    int unused;
+    void *fp;   /* FILE* of a "FILE" socket opened with "w", else NULL */
 } Vio;
 
 VEXTERNC Vio *Vio_ctor(const char *socktype, const char *datafrmt,

@@ -9,6 +9,11 @@
  * ("iteration = N", "relative residual = R") so the checker can compare
  * V-cycle counts and residual histories with the CUDA solver.
  */
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
 #include "maloc/maloc.h"
 
 /* ---------------------------------------------------------------------- */
@@ -159,21 +164,46 @@ void Vnm_redirect(int flag) { (void)flag; }
 int Vnm_system(char *cmd) { (void)cmd; return -1; }
 
 /* ---------------------------------------------------------------------- */
-/* Vio: not reached by the solve path; present so the parser objects link  */
+/* Vio: "FILE" sockets opened for writing go to a stdio stream (used by    */
+/* the OpenDX writer); everything else is inert                            */
 /* ---------------------------------------------------------------------- */
 Vio *Vio_ctor(const char *socktype, const char *datafrmt, const char *hostname,
               const char *filename, const char *rwkey) {
-    (void)socktype; (void)datafrmt; (void)hostname; (void)filename; (void)rwkey;
-    return NULL;
+    Vio *v;
+    FILE *fp;
+    (void)datafrmt; (void)hostname;
+    if (!socktype || !filename || !rwkey || strcmp(socktype, "FILE") != 0 ||
+        strcmp(rwkey, "w") != 0)
+        return NULL;
+    fp = fopen(filename, "w");
+    if (!fp) return NULL;
+    v = (Vio *)calloc(1, sizeof(Vio));
+    if (!v) { fclose(fp); return NULL; }
+    v->fp = fp;
+    return v;
 }
-void Vio_dtor(Vio **thee) { if (thee) *thee = NULL; }
+void Vio_dtor(Vio **thee) {
+    if (thee && *thee) {
+        if ((*thee)->fp) fclose((FILE *)(*thee)->fp);
+        free(*thee);
+    }
+    if (thee) *thee = NULL;
+}
 int Vio_scanf(Vio *thee, char *parms, ...) { (void)thee; (void)parms; return 0; }
-int Vio_printf(Vio *thee, char *parms, ...) { (void)thee; (void)parms; return 0; }
+int Vio_printf(Vio *thee, char *parms, ...) {
+    va_list ap;
+    int n;
+    if (!thee || !thee->fp) return 0;
+    va_start(ap, parms);
+    n = vfprintf((FILE *)thee->fp, parms, ap);
+    va_end(ap);
+    return n;
+}
 void Vio_setWhiteChars(Vio *thee, char *w) { (void)thee; (void)w; }
 void Vio_setCommChars(Vio *thee, char *c) { (void)thee; (void)c; }
 int Vio_accept(Vio *thee, int nonblock) { (void)thee; (void)nonblock; return -1; }
 void Vio_acceptFree(Vio *thee) { (void)thee; }
-int Vio_connect(Vio *thee, int nonblock) { (void)thee; (void)nonblock; return -1; }
+int Vio_connect(Vio *thee, int nonblock) { (void)nonblock; return (thee && thee->fp) ? 0 : -1; }
 void Vio_connectFree(Vio *thee) { (void)thee; }
 Vio *Vio_socketOpen(char *key, const char *iodev, const char *iofmt,
                     const char *iohost, const char *iofile) {
