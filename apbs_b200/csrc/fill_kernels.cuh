@@ -66,9 +66,10 @@ void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* q, double* terms, double* mom, const double* xf, const double* yf,
                 const double* zf, double* gx, double* gy, double* gz);
 void launch_ccf(cudaStream_t s, size_t n, const double* kappa, double zkappa2, double* ccf);
-// srfm spl2 kappa and dielectric maps (fillcoCoefSpline), spline.cu
-void launch_spline_fill(cudaStream_t st, const FillGeom& G, int natoms, const double* xyz,
-                        const double* r, double irad, double win, double ionmask, double epsp,
-                        double epsw, double* kappa, double* epsx, double* epsy, double* epsz);
+// srfm spl2/spl4 kappa and dielectric maps (fillcoCoefSpline, fillcoCoefSpline4), spline.cu
+void launch_spline_fill(cudaStream_t st, int order, const FillGeom& G, int natoms,
+                        const double* xyz, const double* r, double irad, double win,
+                        double ionmask, double epsp, double epsw, double* kappa, double* epsx,
+                        double* epsy, double* epsz);
 
 }  // namespace pmgb

@@ -243,8 +243,9 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     set_error("pmgb_create: chgm %d not implemented (spl0 and spl2 are)", p.chgm);
     return 0;
   }
-  if (p.srfm != PMGB_SRFM_MOL && p.srfm != PMGB_SRFM_SMOL && p.srfm != PMGB_SRFM_SPL2) {
-    set_error("pmgb_create: srfm %d not implemented (mol, smol and spl2 are)", p.srfm);
+  if (p.srfm != PMGB_SRFM_MOL && p.srfm != PMGB_SRFM_SMOL && p.srfm != PMGB_SRFM_SPL2 &&
+      p.srfm != PMGB_SRFM_SPL4) {
+    set_error("pmgb_create: srfm %d not implemented (mol, smol, spl2 and spl4 are)", p.srfm);
     return 0;
   }
   if (p.nion > 8) {
@@ -550,10 +551,12 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
   note_launches(1);
   const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
-  if (!islap && p.srfm == PMGB_SRFM_SPL2) {
-    // spline surface: kappa and the dielectric maps together (fillcoCoefSpline)
+  if (!islap && (p.srfm == PMGB_SRFM_SPL2 || p.srfm == PMGB_SRFM_SPL4)) {
+    // spline surface: kappa and the dielectric maps together
+    // (fillcoCoefSpline, fillcoCoefSpline4)
     const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
-    launch_spline_fill(st, s->G, natoms, s->d_xyz, s->d_r, s->maxIonRadius,
+    launch_spline_fill(st, p.srfm == PMGB_SRFM_SPL4 ? 4 : 2, s->G, natoms, s->d_xyz, s->d_r,
+                       s->maxIonRadius,
                        (p.swin > 0.0) ? p.swin : 0.3, ionmask, p.pdie, p.sdie, s->kappa,
                        s->epsx, s->epsy, s->epsz);
     note_launches(1);

@@ -1,6 +1,7 @@
-// Spline-based molecular surfaces (srfm spl2) and the forces on the atoms.
+// Spline-based molecular surfaces (srfm spl2, spl4) and the forces on the atoms.
 //
-// Surface: fillcoCoefSpline (src/mg/vpmg.c:4631-4854).  kappa, epsx, epsy
+// Surface: fillcoCoefSpline (src/mg/vpmg.c:4631-4854); fillcoCoefSpline4
+// (7052-7366) is the same with a 7th-order polynomial on the window.  kappa, epsx, epsy
 // and epsz start at 1 everywhere; for every on-mesh atom with a positive
 // radius, in atom order, each grid point inside the atom's search box has
 // its values multiplied by the cubic spline accessibility of the point (0
@@ -93,6 +94,40 @@ __device__ __forceinline__ double spline_value(double dist, double rad, double w
   return 0.75 * sm2 * w2i - 0.25 * sm * sm2 * w3i;
 }
 
+// Coefficients of the 7th-order accessibility polynomial on the window
+// [rad - win, rad + win] (fillcoCoefSpline4, vpmg.c:7119-7175, and
+// Vacc_splineAccGradAtomNorm4, vacc.c:1004-1095): 0 and 1 with three
+// vanishing derivatives at the ends.
+__device__ __forceinline__ void spline7_coef(double rad, double win, double* c) {
+  const double b = rad - win, e = rad + win;
+  const double e2 = e * e, e3 = e2 * e, e4 = e3 * e, e5 = e4 * e, e6 = e5 * e, e7 = e6 * e;
+  const double b2 = b * b, b3 = b2 * b, b4 = b3 * b, b5 = b4 * b, b6 = b5 * b, b7 = b6 * b;
+  const double denom = e7 - 7.0 * b * e6 + 21.0 * b2 * e5 - 35.0 * e4 * b3 + 35.0 * e3 * b4 -
+                       21.0 * b5 * e2 + 7.0 * e * b6 - b7;
+  c[0] = b4 * (35.0 * e3 - 21.0 * b * e2 + 7 * e * b2 - b3) / denom;
+  c[1] = -140.0 * b3 * e3 / denom;
+  c[2] = 210.0 * e2 * b2 * (e + b) / denom;
+  c[3] = -140.0 * e * b * (e2 + 3.0 * b * e + b2) / denom;
+  c[4] = 35.0 * (e3 + 9.0 * b * e2 + 9.0 * e * b2 + b3) / denom;
+  c[5] = -84.0 * (e2 + 3.0 * b * e + b2) / denom;
+  c[6] = 70.0 * (e + b) / denom;
+  c[7] = -20.0 / denom;
+}
+
+// the 7th-order accessibility at distance sm (sm2 as the reference forms it
+// for that map), clamped to [0, 1]
+__device__ __forceinline__ double spline7_value(const double* c, double sm, double sm2) {
+  const double sm3 = sm2 * sm, sm4 = sm3 * sm, sm5 = sm4 * sm, sm6 = sm5 * sm, sm7 = sm6 * sm;
+  double value = c[0] + c[1] * sm + c[2] * sm2 + c[3] * sm3 + c[4] * sm4 + c[5] * sm5 +
+                 c[6] * sm6 + c[7] * sm7;
+  if (value > 1.0) value = 1.0;
+  else if (value < 0.0) value = 0.0;
+  return value;
+}
+
+// ORDER 2: cubic window (srfm spl2, fillcoCoefSpline); ORDER 4: 7th-order
+// polynomial (srfm spl4, fillcoCoefSpline4, vpmg.c:7052-7366)
+template <int ORDER>
 __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
   __shared__ SplAtom cand[kSplCap];
   __shared__ int wcount[kSplThreads / 32];
@@ -131,29 +166,61 @@ __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
         if (kap[p] > kPmgSmall) {
           const double dist2 = dz2 + dy2 + dx2;
           if (dist2 <= ictot2) kap[p] = 0.0;
-          if ((dist2 < itot2) && (dist2 > ictot2))
-            kap[p] *= spline_value(sqrt(dist2), arad + A.irad, win, w2i, w3i);
+          if ((dist2 < itot2) && (dist2 > ictot2)) {
+            const double dist = sqrt(dist2);
+            if (ORDER == 2) {
+              kap[p] *= spline_value(dist, arad + A.irad, win, w2i, w3i);
+            } else {
+              double c[8];
+              spline7_coef(A.irad + arad, win, c);
+              kap[p] *= spline7_value(c, dist, dist2);
+            }
+          }
         }
         if (ex[p] > kPmgSmall) {
           const double t = s.pos[0] - (i + 0.5) * hx;
           const double dist2 = dz2 + dy2 + t * t;
           if (dist2 <= sctot2) ex[p] = 0.0;
-          if ((dist2 > sctot2) && (dist2 < stot2))
-            ex[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+          if ((dist2 > sctot2) && (dist2 < stot2)) {
+            const double dist = sqrt(dist2);
+            if (ORDER == 2) {
+              ex[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else {
+              double c[8];
+              spline7_coef(arad, win, c);
+              ex[p] *= spline7_value(c, dist, dist * dist);
+            }
+          }
         }
         if (ey[p] > kPmgSmall) {
           const double t = s.pos[1] - (j + 0.5) * hy;
           const double dist2 = dz2 + dx2 + t * t;
           if (dist2 <= sctot2) ey[p] = 0.0;
-          if ((dist2 > sctot2) && (dist2 < stot2))
-            ey[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+          if ((dist2 > sctot2) && (dist2 < stot2)) {
+            const double dist = sqrt(dist2);
+            if (ORDER == 2) {
+              ey[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else {
+              double c[8];
+              spline7_coef(arad, win, c);
+              ey[p] *= spline7_value(c, dist, dist * dist);
+            }
+          }
         }
         if (ez[p] > kPmgSmall) {
           const double t = s.pos[2] - (k + 0.5) * hz;
           const double dist2 = dy2 + dx2 + t * t;
           if (dist2 <= sctot2) ez[p] = 0.0;
-          if ((dist2 > sctot2) && (dist2 < stot2))
-            ez[p] *= spline_value(sqrt(dist2), arad, win, w2i, w3i);
+          if ((dist2 > sctot2) && (dist2 < stot2)) {
+            const double dist = sqrt(dist2);
+            if (ORDER == 2) {
+              ez[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else {
+              double c[8];
+              spline7_coef(arad, win, c);
+              ez[p] *= spline7_value(c, dist, dist2);
+            }
+          }
         }
       }
     }
@@ -215,6 +282,7 @@ struct ForceArgs {
   const double *epsx, *epsy, *epsz, *kappa;
   int chgm;         // PMGB_CHGM_*
   int boundary;     // compute the dielectric and ionic boundary forces
+  int order;        // surface: 2 = spl2, 4 = spl4 (Vpmg_splineSelect)
   int nonlin;
   double win, irad, srad, epsp, epsw, zkappa2, izmagic, ionstr;
   int nion;
@@ -267,11 +335,46 @@ __device__ __forceinline__ void spline_grad(const double* center, double win, do
   for (int d = 0; d < 3; d++) grad[d] = -(mygrad / mychi) * ((center[d] - apos[d]) / dist);
 }
 
+// the same for the 7th-order polynomial (Vacc_splineAccGradAtomNorm4,
+// vacc.c:1004-1095)
+__device__ __forceinline__ void spline_grad4(const double* center, double win, double infrad,
+                                             const double* apos, double radius, double* grad) {
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (!(radius > 0.0)) return;
+  const double arad = radius + infrad;
+  double c[8];
+  spline7_coef(arad, win, c);
+  const double d0 = apos[0] - center[0], d1 = apos[1] - center[1], d2 = apos[2] - center[2];
+  const double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  double mychi, mygrad;
+  if (dist < (arad - win)) return;
+  else if (dist > (arad + win)) return;
+  else if ((fabs(dist - (arad - win)) < kVSmall) || (fabs(dist - (arad + win)) < kVSmall)) return;
+  else {
+    const double sm = dist, sm2 = sm * sm, sm3 = sm2 * sm, sm4 = sm3 * sm, sm5 = sm4 * sm,
+                 sm6 = sm5 * sm, sm7 = sm6 * sm;
+    mychi = c[0] + c[1] * sm + c[2] * sm2 + c[3] * sm3 + c[4] * sm4 + c[5] * sm5 + c[6] * sm6 +
+            c[7] * sm7;
+    mygrad = c[1] + 2.0 * c[2] * sm + 3.0 * c[3] * sm2 + 4.0 * c[4] * sm3 + 5.0 * c[5] * sm4 +
+             6.0 * c[6] * sm5 + 7.0 * c[7] * sm6;
+    if (mychi <= 0.0) return;
+    else if (mychi > 1.0) mychi = 1.0;
+  }
+  for (int d = 0; d < 3; d++) grad[d] = -(mygrad / mychi) * ((center[d] - apos[d]) / dist);
+}
+
 // Vcap_exp (src/generic/vcap.c:59-73)
 __device__ __forceinline__ double cap_exp(double x) {
   if (x > kExpMax) return exp(kExpMax);
   if (x < -kExpMax) return exp(-kExpMax);
   return exp(x);
+}
+
+__device__ __forceinline__ void surf_grad(const ForceArgs& A, const double* center,
+                                          double infrad, const double* apos, double radius,
+                                          double* grad) {
+  if (A.order == 4) spline_grad4(center, A.win, infrad, apos, radius, grad);
+  else spline_grad(center, A.win, infrad, apos, radius, grad);
 }
 
 __global__ void k_forces(ForceArgs A) {
@@ -406,27 +509,27 @@ __global__ void k_forces(ForceArgs A) {
               double gpos[3], dHx[3], dHy[3], dHz[3], dHxm[3], dHym[3], dHzm[3];
               gpos[0] = (i + 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hxijk = (A.epsx[IJK(i, j, k)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHx);
+              surf_grad(A, gpos, 0., apos, radius, dHx);
               for (int l = 0; l < 3; l++) dHx[l] *= Hxijk;
               gpos[0] = i * hx + xmin; gpos[1] = (j + 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hyijk = (A.epsy[IJK(i, j, k)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHy);
+              surf_grad(A, gpos, 0., apos, radius, dHy);
               for (int l = 0; l < 3; l++) dHy[l] *= Hyijk;
               gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k + 0.5) * hzed + zmin;
               const double Hzijk = (A.epsz[IJK(i, j, k)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHz);
+              surf_grad(A, gpos, 0., apos, radius, dHz);
               for (int l = 0; l < 3; l++) dHz[l] *= Hzijk;
               gpos[0] = (i - 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hxim1jk = (A.epsx[IJK(i - 1, j, k)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHxm);
+              surf_grad(A, gpos, 0., apos, radius, dHxm);
               for (int l = 0; l < 3; l++) dHxm[l] *= Hxim1jk;
               gpos[0] = i * hx + xmin; gpos[1] = (j - 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hyijm1k = (A.epsy[IJK(i, j - 1, k)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHym);
+              surf_grad(A, gpos, 0., apos, radius, dHym);
               for (int l = 0; l < 3; l++) dHym[l] *= Hyijm1k;
               gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k - 0.5) * hzed + zmin;
               const double Hzijkm1 = (A.epsz[IJK(i, j, k - 1)] - A.epsp) * depsi;
-              spline_grad(gpos, A.win, 0., apos, radius, dHzm);
+              surf_grad(A, gpos, 0., apos, radius, dHzm);
               for (int l = 0; l < 3; l++) dHzm[l] *= Hzijkm1;
               const double u0 = u[IJK(i, j, k)];
               const double dbFmag = u0;
@@ -480,7 +583,7 @@ __global__ void k_forces(ForceArgs A) {
             gpos[0] = i * hx + xmin;
             gpos[1] = j * hy + ymin;
             gpos[2] = k * hzed + zmin;
-            spline_grad(gpos, A.win, A.irad, apos, radius, tgrad);
+            surf_grad(A, gpos, A.irad, apos, radius, tgrad);
             const double uv = u[IJK(i, j, k)], kv = A.kappa[IJK(i, j, k)];
             double fmag;
             if (A.nonlin) {
@@ -502,9 +605,10 @@ __global__ void k_forces(ForceArgs A) {
 
 }  // namespace
 
-void launch_spline_fill(cudaStream_t st, const FillGeom& G, int natoms, const double* xyz,
-                        const double* r, double irad, double win, double ionmask, double epsp,
-                        double epsw, double* kappa, double* epsx, double* epsy, double* epsz) {
+void launch_spline_fill(cudaStream_t st, int order, const FillGeom& G, int natoms,
+                        const double* xyz, const double* r, double irad, double win,
+                        double ionmask, double epsp, double epsw, double* kappa, double* epsx,
+                        double* epsy, double* epsz) {
   SplineArgs A;
   A.G = G;
   A.natoms = natoms;
@@ -520,7 +624,8 @@ void launch_spline_fill(cudaStream_t st, const FillGeom& G, int natoms, const do
   A.epsy = epsy;
   A.epsz = epsz;
   dim3 grid((G.g.nx + kBX - 1) / kBX, (G.g.ny + kBY - 1) / kBY, (G.g.nz + kBZ - 1) / kBZ);
-  k_spline_fill<<<grid, kSplThreads, 0, st>>>(A);
+  if (order == 4) k_spline_fill<4><<<grid, kSplThreads, 0, st>>>(A);
+  else k_spline_fill<2><<<grid, kSplThreads, 0, st>>>(A);
 }
 
 }  // namespace pmgb
@@ -536,8 +641,8 @@ extern "C" int pmgb_forces(pmgb_solver* s, double* qf, double* db, double* ib) {
   const pmgb_params& p = s->p;
   const int natoms = s->natoms;
   const int boundary = (db || ib) ? 1 : 0;
-  if (boundary && p.srfm != PMGB_SRFM_SPL2) {
-    set_error("pmgb_forces: the boundary forces need srfm spl2 (spline-based surfaces)");
+  if (boundary && p.srfm != PMGB_SRFM_SPL2 && p.srfm != PMGB_SRFM_SPL4) {
+    set_error("pmgb_forces: the boundary forces need srfm spl2 or spl4 (spline-based surfaces)");
     return 0;
   }
   if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL) {
@@ -567,6 +672,7 @@ extern "C" int pmgb_forces(pmgb_solver* s, double* qf, double* db, double* ib) {
   A.kappa = s->kappa;
   A.chgm = p.chgm;
   A.boundary = boundary;
+  A.order = (p.srfm == PMGB_SRFM_SPL4) ? 4 : 2;
   A.nonlin = p.nonlin;
   A.win = (p.swin > 0.0) ? p.swin : 0.3;
   A.irad = s->maxIonRadius;

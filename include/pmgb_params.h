@@ -19,6 +19,7 @@
 #define PMGB_SRFM_MOL 0
 #define PMGB_SRFM_SMOL 1
 #define PMGB_SRFM_SPL2 2   /* cubic-spline surface (fillcoCoefSpline) */
+#define PMGB_SRFM_SPL4 4   /* 7th-order polynomial surface (fillcoCoefSpline4) */
 /* Charge method codes (Vchrg_Meth, src/generic/vhal.h:231-234). */
 #define PMGB_CHGM_TRIL 0   /* chgm spl0: trilinear to the 8 nearest points */
 #define PMGB_CHGM_SPL2 1

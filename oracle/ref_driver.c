@@ -181,7 +181,7 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
         for (i = 0; i < natoms; i++) {
             int rcf = 1;
             Vpmg_qfForce(pmg, forces + 9 * (size_t)i, i, (Vchrg_Meth)p->chgm);
-            if (p->srfm == PMGB_SRFM_SPL2) {
+            if (p->srfm == PMGB_SRFM_SPL2 || p->srfm == PMGB_SRFM_SPL4) {
                 rcf &= Vpmg_dbForce(pmg, forces + 9 * (size_t)i + 3, i, (Vsurf_Meth)p->srfm);
                 rcf &= Vpmg_ibForce(pmg, forces + 9 * (size_t)i + 6, i, (Vsurf_Meth)p->srfm);
             } else {

@@ -1,9 +1,10 @@
-"""Spline-based surfaces (srfm spl2, fillcoCoefSpline) and the per-atom
-forces (Vpmg_qfForce, Vpmg_dbForce, Vpmg_ibForce) on the device against the
-reference compiled from source (oracle/_ref): the kappa and dielectric maps
-bitwise, the potential and energy to 1e-9, every force component to 1e-8 of
-the largest force of its kind (the forces difference the potential, whose
-two solves agree to round-off, not bit for bit)."""
+"""Spline-based surfaces (srfm spl2 and spl4: fillcoCoefSpline,
+fillcoCoefSpline4) and the per-atom forces (Vpmg_qfForce, Vpmg_dbForce,
+Vpmg_ibForce) on the device against the reference compiled from source
+(oracle/_ref): the kappa and dielectric maps bitwise, the potential and
+energy to 1e-9, every force component to 1e-8 of the largest force of its
+kind (the forces difference the potential, whose two solves agree to
+round-off, not bit for bit)."""
 import numpy as np
 import pytest
 
@@ -31,8 +32,10 @@ def _cases():
     p3.chgm = synth.CHGM_TRIL
     p4 = synth.mg_manual(49, 0.55, m3.center(), srfm=synth.SRFM_SPL2, ions=())
     p4.swin = 0.4
+    p5 = synth.mg_manual(65, 0.5, m1.center(), srfm=synth.SRFM_SPL4, ions=IONS)
+    p6 = synth.mg_manual(57, 0.5, m3.center(), srfm=synth.SRFM_SPL4, npbe=True, ions=IONS)
     return [("lpbe65", m1, p1), ("npbe65", m1, p2), ("lpbe_box_spl0", m3, p3),
-            ("lpbe49_noions_swin04", m3, p4)]
+            ("lpbe49_noions_swin04", m3, p4), ("lpbe65_spl4", m1, p5), ("npbe57_spl4", m3, p6)]
 
 
 CASES = _cases()
