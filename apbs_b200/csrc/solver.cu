@@ -515,6 +515,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
   dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->d_ref); dfree(s->atom_terms);
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
+  free_maps(s);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
   cudaStreamDestroy(s->own_stream);
   delete s;
@@ -545,13 +546,21 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   CK(cudaMemsetAsync(s->d_npts, 0, sizeof(int), st));
   // charge (fillcoChargeSpline2)
   CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
-  if (p.chgm == PMGB_CHGM_TRIL)
+  if (uses_charge_map(s)) {
+    // the charge map is read below (fillcoChargeMap)
+  } else if (p.chgm == PMGB_CHGM_TRIL) {
     launch_charge_tril(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
-  else
+  } else {
     launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+  }
   note_launches(1);
-  const int islap = (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
-  if (!islap && (p.srfm == PMGB_SRFM_SPL2 || p.srfm == PMGB_SRFM_SPL4)) {
+  // with coefficient maps the operator is never a plain Laplacian
+  // (Vpmg_fillco, vpmg.c:5354-5361)
+  const int coef_maps = uses_coef_maps(s);
+  const int islap = !coef_maps && (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
+  if (coef_maps) {
+    // the maps are read below (fillcoCoefMap)
+  } else if (!islap && (p.srfm == PMGB_SRFM_SPL2 || p.srfm == PMGB_SRFM_SPL4)) {
     // spline surface: kappa and the dielectric maps together
     // (fillcoCoefSpline, fillcoCoefSpline4)
     const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
@@ -651,6 +660,7 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     launch_fill_value(st, s->epsz, n, p.pdie);
     note_launches(4);
   }
+  if (!fill_from_maps(s)) return 0;
   // boundary values (bcCalc), except when focusing (vpmg.c:5404-5409): the
   // faces were set from the coarse solution by pmgb_focus
   if (p.bcfl == PMGB_BCFL_FOCUS) {
@@ -1229,7 +1239,7 @@ extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
   CK(cudaStreamSynchronize(st));
   const pmgb_params& p = s->p;
   double qf = sums[0] * p.hx * p.hy * p.hz / s->zmagic;
-  if (p.chgm == PMGB_CHGM_TRIL) {
+  if (p.chgm == PMGB_CHGM_TRIL && !uses_charge_map(s)) {
     // Vpmg_qfEnergyPoint (vpmg.c:1704-1789): charges at the atoms
     if (s->natoms <= 0 || !s->d_xyz) {
       set_error("pmgb_energy: chgm spl0 needs the atom list (pmgb_fillco)");

@@ -17,6 +17,12 @@ namespace pmgb {
 // calculation's stream and its statistics are read when first asked for.
 int fillco_issue(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
                  const double* radius);
+// usemap (maps.cu): whether coefficient / charge maps replace the atom
+// fill, the map fill itself (synchronous, checks off-map reads), cleanup
+int uses_coef_maps(const pmgb_solver* s);
+int uses_charge_map(const pmgb_solver* s);
+int fill_from_maps(pmgb_solver* s);
+void free_maps(pmgb_solver* s);
 }  // namespace pmgb
 
 namespace pmgb {
@@ -47,6 +53,13 @@ enum Scal { S_RSDEN = 0, S_RSNRM, S_XNUM, S_XDEN, S_NRM, S_E0, S_E1, S_E2, S_E3,
 }  // namespace pmgb
 
 using namespace pmgb;
+
+// A coefficient or charge map on its own grid (pmgb_set_map), on the device.
+struct UserMap {
+  int n[3];
+  double h[3], origin[3];
+  double* data;  // IJK, NULL when the map is not used
+};
 
 struct pmgb_solver {
   // (types from namespace pmgb)
@@ -100,6 +113,8 @@ struct pmgb_solver {
   // step counters of the plane-parallel GS27 wavefront: word 0 counts waits
   // that ran out, level l's counters start at kWaveCounterBase + l *
   // kWavePlanesMax
+  UserMap maps[PMGB_MAP_COUNT];  // usemap diel/kappa/charge
+  double* map_scratch;      // kappa-map maximum and error counts
   double* d_forces;         // pmgb_forces: 9 doubles and a status word per atom
   size_t forces_alloc;
   unsigned* d_wave;

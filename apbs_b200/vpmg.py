@@ -29,6 +29,7 @@ K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
 K_GS7_PIPE_FP64, K_GS7_PIPE_FP32, K_VCYCLE_TAIL = 5, 6, 7
 K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
 DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX, DX_DIELY, DX_DIELZ = range(6)
+MAP_DIELX, MAP_DIELY, MAP_DIELZ, MAP_KAPPA, MAP_CHARGE = range(5)
 TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5
@@ -91,6 +92,12 @@ def lib():
         L.pmgb_forces.argtypes = [vp, dp, dp, dp]
         L.pmgb_write_dx.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
                                     ctypes.c_char_p]
+        L.pmgb_set_map.argtypes = [vp, ctypes.c_int] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 6 + [dp]
+        L.pmgb_read_dx_host.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), dp, dp,
+                                        dp]
+        L.pmgb_write_dx_host.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 3 + \
+            [ctypes.c_double] * 6 + [dp, dp, ctypes.c_char_p, ctypes.c_char_p]
         L.pmgb_get_potential.argtypes = [vp, dp]
         L.pmgb_get_maps.argtypes = [vp, dp, dp]
         L.pmgb_get_stats.argtypes = [vp, ctypes.POINTER(PmgbStats)]
@@ -211,6 +218,20 @@ class Vpmg:
         _check(lib().pmgb_energy(self._h, _dp(e)), "pmgb_energy")
         return float(e[0])
 
+    def set_map(self, which: int, data, h, origin):
+        """Use a map (MAP_DIELX..MAP_CHARGE) given on its own grid, as the
+        deck's "usemap": data (nz, ny, nx), spacing h, origin; data None
+        stops using it.  Takes effect at the next fillco."""
+        if data is None:
+            _check(lib().pmgb_set_map(self._h, which, 0, 0, 0, 0, 0, 0, 0, 0, 0, None),
+                   "pmgb_set_map")
+            return
+        d = np.ascontiguousarray(data, dtype=np.float64)
+        nz, ny, nx = d.shape
+        _check(lib().pmgb_set_map(self._h, which, nx, ny, nz, *[float(v) for v in h],
+                                  *[float(v) for v in origin], _dp(d.reshape(-1))),
+               "pmgb_set_map")
+
     def write_dx(self, path, which: int = 0, title: str | None = None,
                  package: str | None = None):
         """Write one map (DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX/Y/Z) as the
@@ -323,3 +344,27 @@ def solve_molecule(params, mol, precision=FP64, want_u=False):
                                      _dp(q), _dp(r), _dp(e), _dp(u), ctypes.byref(st)),
            "pmgb_solve_molecule")
     return float(e[0]), u, st.as_dict()
+
+
+def read_dx(path):
+    """OpenDX file -> (data (nz, ny, nx), h (3,), origin (3,)), as
+    Vgrid_readDX reads it."""
+    dims = (ctypes.c_int * 3)()
+    h, origin = np.zeros(3), np.zeros(3)
+    _check(lib().pmgb_read_dx_host(str(path).encode(), dims, _dp(h), _dp(origin), None),
+           "pmgb_read_dx_host")
+    data = np.zeros((dims[2], dims[1], dims[0]))
+    _check(lib().pmgb_read_dx_host(str(path).encode(), dims, _dp(h), _dp(origin), _dp(data)),
+           "pmgb_read_dx_host")
+    return data, h, origin
+
+
+def write_dx(path, data, h, origin, title="", package=None, pvec=None):
+    """(nz, ny, nx) array -> OpenDX file, byte for byte as Vgrid_writeDX."""
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    nz, ny, nx = d.shape
+    pv = None if pvec is None else np.ascontiguousarray(pvec, dtype=np.float64)
+    _check(lib().pmgb_write_dx_host(str(path).encode(), nx, ny, nz, *[float(v) for v in h],
+                                    *[float(v) for v in origin], _dp(d.reshape(-1)), _dp(pv),
+                                    title.encode(), package.encode() if package else None),
+           "pmgb_write_dx_host")

@@ -141,6 +141,28 @@ int pmgb_write_dx_host(const char *path, int nx, int ny, int nz, double hx, doub
                        double hz, double xmin, double ymin, double zmin, const double *data,
                        const double *pvec, const char *title, const char *package);
 
+/* OpenDX reader (Vgrid_readDX, src/mg/vgrid.c:586-790): counts, spacings
+ * and origin of the file's grid, and with data non-NULL its values in the
+ * x-fastest IJK layout (nx*ny*nz doubles). */
+int pmgb_read_dx_host(const char *path, int *dims, double *h, double *origin, double *data);
+
+/* Maps given on their own grids, as the deck's "usemap" (Vpmg_fillco's
+ * dielXMap..chargeMap arguments, src/mg/vpmg.c:5250-5316): from the next
+ * pmgb_fillco the dielectric and kappa maps replace the surface
+ * (fillcoCoefMap, vpmg.c:4098-4221; all three dielectric maps are needed,
+ * and the kappa map when there are ions), the charge map replaces the atom
+ * charges (fillcoChargeMap, 4938-4984, and the energy then integrates the
+ * charge map as Vpmg_qfEnergyVolume does).  Values are interpolated as
+ * Vgrid_value does.  data (host, IJK) is copied; NULL stops using the map. */
+#define PMGB_MAP_DIELX 0
+#define PMGB_MAP_DIELY 1
+#define PMGB_MAP_DIELZ 2
+#define PMGB_MAP_KAPPA 3
+#define PMGB_MAP_CHARGE 4
+#define PMGB_MAP_COUNT 5
+int pmgb_set_map(pmgb_solver *s, int which, int nx, int ny, int nz, double hx, double hy,
+                 double hz, double xmin, double ymin, double zmin, const double *data);
+
 /* Copy the potential (thee->u, Dirichlet values restored) to host memory. */
 int pmgb_get_potential(pmgb_solver *s, double *u);
 

@@ -25,6 +25,10 @@ def lib():
         _lib.ref_pmg_run.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
                                      dp, dp, dp, dp, dp, ctypes.c_int, ctypes.c_int,
                                      dp, ctypes.POINTER(ctypes.c_int)]
+        _lib.ref_pmg_run_maps.restype = ctypes.c_int
+        _lib.ref_pmg_run_maps.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
+                                          ctypes.POINTER(ctypes.c_int), dp,
+                                          ctypes.POINTER(dp), dp, dp, dp]
         _lib.ref_write_dx.restype = ctypes.c_int
         _lib.ref_write_dx.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 6 + [
             dp, dp, ctypes.c_char_p, ctypes.c_char_p]
@@ -130,3 +134,37 @@ def write_dx(path, data, h, origin, pvec=None, title="POTENTIAL (kT/e)"):
                             str(path).encode(), title.encode())
     if rc != 1:
         raise RuntimeError("reference DX write failed")
+
+
+def run_maps(params, mol, maps):
+    """The reference with "usemap" maps: maps is {index 0..4 (dielx, diely,
+    dielz, kappa, charge): (data (nz, ny, nx), h (3,), origin (3,))}.
+    Returns u, energy_kT and the fill maps as run() does."""
+    n = params.nx * params.ny * params.nz
+    u = np.zeros(n)
+    fill = np.zeros(5 * n)
+    out = np.zeros(16)
+    dims = (ctypes.c_int * 15)()
+    geom = np.zeros(30)
+    ptrs = (ctypes.POINTER(ctypes.c_double) * 5)()
+    keep = []
+    for m in range(5):
+        if m in maps:
+            data, h, origin = maps[m]
+            d = np.ascontiguousarray(data, dtype=np.float64)
+            keep.append(d)
+            dims[3 * m], dims[3 * m + 1], dims[3 * m + 2] = d.shape[2], d.shape[1], d.shape[0]
+            geom[6 * m:6 * m + 3] = h
+            geom[6 * m + 3:6 * m + 6] = origin
+            ptrs[m] = _ptr(d.reshape(-1))
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(mol.charge, dtype=np.float64)
+    r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    rc = lib().ref_pmg_run_maps(ctypes.byref(params), mol.natoms, _ptr(xyz), _ptr(q), _ptr(r),
+                                dims, _ptr(geom), ptrs, _ptr(u), _ptr(fill), _ptr(out))
+    if rc != 1:
+        raise RuntimeError("reference PMG run with maps failed")
+    shape = (params.nz, params.ny, params.nx)
+    f = fill.reshape(5, *shape)
+    return {"u": u.reshape(shape), "energy_kT": out[0], "charge": f[0], "epsx": f[1],
+            "epsy": f[2], "epsz": f[3], "kappa": f[4]}

@@ -110,10 +110,45 @@ static MGparm *make_mgparm(const pmgb_params *p) {
  *   fstatus (out, optional) per atom, 1 if both boundary forces succeeded
  * Returns 1 on success (Vpmg convention), 0 on failure.
  */
+static int run_impl(const pmgb_params *p, int natoms, const double *xyz,
+                    const double *q, const double *r, double *u, double *maps,
+                    double *faces, double *out, double *reslog, int reslog_cap,
+                    int verbose, double *forces, int *fstatus, Vgrid **umap);
+
 int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
                 const double *q, const double *r, double *u, double *maps,
                 double *faces, double *out, double *reslog, int reslog_cap,
                 int verbose, double *forces, int *fstatus) {
+    return run_impl(p, natoms, xyz, q, r, u, maps, faces, out, reslog, reslog_cap, verbose,
+                    forces, fstatus, NULL);
+}
+
+/* ref_pmg_run with "usemap" maps given to Vpmg_fillco (vpmg.c:5250-5316):
+ * map m (0..4 = dielx, diely, dielz, kappa, charge) is used when data[m] is
+ * non-NULL, on the grid dims[3m..3m+2], spacing geom[6m..6m+2] and origin
+ * geom[6m+3..6m+5] (the Vgrid a map file would give). */
+int ref_pmg_run_maps(const pmgb_params *p, int natoms, const double *xyz, const double *q,
+                     const double *r, const int *dims, const double *geom, double **data,
+                     double *u, double *maps, double *out) {
+    Vgrid *g[5];
+    int m, rc;
+    for (m = 0; m < 5; m++) {
+        g[m] = VNULL;
+        if (data[m])
+            g[m] = Vgrid_ctor(dims[3 * m], dims[3 * m + 1], dims[3 * m + 2], geom[6 * m],
+                              geom[6 * m + 1], geom[6 * m + 2], geom[6 * m + 3],
+                              geom[6 * m + 4], geom[6 * m + 5], data[m]);
+    }
+    rc = run_impl(p, natoms, xyz, q, r, u, maps, NULL, out, NULL, 0, 0, NULL, NULL, g);
+    for (m = 0; m < 5; m++)
+        if (g[m]) Vgrid_dtor(&g[m]);
+    return rc;
+}
+
+static int run_impl(const pmgb_params *p, int natoms, const double *xyz,
+                    const double *q, const double *r, double *u, double *maps,
+                    double *faces, double *out, double *reslog, int reslog_cap,
+                    int verbose, double *forces, int *fstatus, Vgrid **umap) {
     int i, n, rc;
     double t0, t1, t2, t3, t4;
     double ionc[PMGB_MAXION], ionr[PMGB_MAXION], ionq[PMGB_MAXION];
@@ -144,9 +179,15 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
     pmgp->zcent = p->center[2];
     pmg = Vpmg_ctor(pmgp, pbe, 0, VNULL, mg, PCE_NO);
     t1 = now_s();
-    rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
-                     0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
-                     VNULL);
+    if (umap)
+        rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
+                         umap[0] != VNULL, umap[0], umap[1] != VNULL, umap[1],
+                         umap[2] != VNULL, umap[2], umap[3] != VNULL, umap[3], 0, VNULL,
+                         umap[4] != VNULL, umap[4]);
+    else
+        rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
+                         0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,
+                         VNULL);
     t2 = now_s();
     if (rc != 1) return 0;
     n = p->nx * p->ny * p->nz;

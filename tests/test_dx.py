@@ -61,3 +61,16 @@ def test_dx_partition_subset_matches_reference(tmp_path):
     _ours(tmp_path / "ours.dx", data, h, origin, pvec)
     ref.write_dx(tmp_path / "ref.dx", data, h, origin, pvec)
     assert (tmp_path / "ours.dx").read_bytes() == (tmp_path / "ref.dx").read_bytes()
+
+
+def test_dx_read_round_trip(tmp_path):
+    """The reader returns the values the writer printed (six digits), the
+    grid counts, spacings and origin."""
+    data = _values((6, 5, 7), 3)
+    h, origin = (0.5, 0.25, 0.75), (-3.0, 1.5, 2.25)
+    vpmg.write_dx(tmp_path / "m.dx", data, h, origin, title="KAPPA MAP")
+    got, gh, go = vpmg.read_dx(tmp_path / "m.dx")
+    assert got.shape == data.shape
+    printed = np.array([float("%12.6e" % v) for v in data.reshape(-1)]).reshape(data.shape)
+    assert np.array_equal(got, printed)
+    assert np.allclose(gh, h) and np.allclose(go, origin)
