@@ -302,3 +302,54 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
   fine->solved = 0;
   return 1;
 }
+
+// bcfl map (bcCalc, vpmg.c:4086-4089): the faces from a potential map, by
+// the same interpolation focusFillBound applies to a coarse solution (it is
+// called with the map standing in for the coarse grid, vpmg.c:2010-2025).
+int pmgb::map_faces(pmgb_solver* s) {
+  const UserMap& m = s->maps[PMGB_MAP_POT];
+  if (!m.data) {
+    set_error("pmgb_fillco: bcfl map needs a potential map (pmgb_set_map PMGB_MAP_POT)");
+    return 0;
+  }
+  const pmgb_params& pf = s->p;
+  FocusArgs a;
+  for (int d = 0; d < 3; d++) {
+    a.mnO[d] = m.origin[d];
+    a.mxO[d] = m.origin[d] + (m.n[d] - 1) * m.h[d];  // Vgrid_ctor's xmax
+  }
+  domain(pf, a.mnN, a.mxN);
+  for (int d = 0; d < 3; d++) {
+    if (fabs(a.mnO[d] - a.mnN[d]) < 1.0e-9) a.mnN[d] = a.mnO[d];
+    if (fabs(a.mxO[d] - a.mxN[d]) < 1.0e-9) a.mxN[d] = a.mxO[d];
+  }
+  for (int d = 0; d < 3; d++)
+    if (a.mxN[d] > a.mxO[d] || a.mnO[d] > a.mnN[d]) {
+      set_error("pmgb_fillco: grid [%g, %g] on axis %d not contained in the potential map "
+                "[%g, %g]", a.mnN[d], a.mxN[d], d, a.mnO[d], a.mxO[d]);
+      return 0;
+    }
+  a.uc = m.data;
+  a.ncx = m.n[0]; a.ncy = m.n[1]; a.ncz = m.n[2];
+  a.hcx = m.h[0]; a.hcy = m.h[1]; a.hcz = m.h[2];
+  a.nfx = pf.nx; a.nfy = pf.ny; a.nfz = pf.nz;
+  a.hfx = pf.hx; a.hfy = pf.hy; a.hfz = pf.hz;
+  a.gx = s->gx; a.gy = s->gy; a.gz = s->gz;
+  a.status = s->d_info + 8;
+  cudaStream_t st = s->stream;
+  FCK(cudaMemsetAsync(a.status, 0, sizeof(int), st));
+  const long long total = 2LL * (pf.ny * (long long)pf.nz + pf.nx * (long long)pf.nz +
+                                 pf.nx * (long long)pf.ny);
+  const int blocks = (int)((total + 255) / 256 < 4 * 148 ? (total + 255) / 256 : 4 * 148);
+  k_focus_faces<<<blocks, 256, 0, st>>>(a);
+  note_launches(1);
+  FCK(cudaGetLastError());
+  int bad = 0;
+  FCK(cudaMemcpyAsync(&bad, a.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FCK(cudaStreamSynchronize(st));
+  if (bad) {
+    set_error("pmgb_fillco: a boundary point lies off the potential map");
+    return 0;
+  }
+  return 1;
+}

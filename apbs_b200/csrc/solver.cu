@@ -663,7 +663,9 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   if (!fill_from_maps(s)) return 0;
   // boundary values (bcCalc), except when focusing (vpmg.c:5404-5409): the
   // faces were set from the coarse solution by pmgb_focus
-  if (p.bcfl == PMGB_BCFL_FOCUS) {
+  if (p.bcfl == PMGB_BCFL_MAP) {
+    if (!map_faces(s)) return 0;
+  } else if (p.bcfl == PMGB_BCFL_FOCUS) {
     if (!s->focused) {
       set_error("pmgb_fillco: bcfl focus needs pmgb_focus with a solved coarse calculation first");
       return 0;
@@ -705,8 +707,10 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     A.xkappa = s->xkappa;
     launch_mdh(st, A, natoms, s->d_xyz, s->d_q, s->d_r);
     note_launches(1);
-  } else if (p.bcfl != PMGB_BCFL_ZERO && p.bcfl != PMGB_BCFL_FOCUS) {
-    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh, mdh and focus are)", p.bcfl);
+  } else if (p.bcfl != PMGB_BCFL_ZERO && p.bcfl != PMGB_BCFL_FOCUS &&
+             p.bcfl != PMGB_BCFL_MAP) {
+    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh, mdh, focus and map are)",
+              p.bcfl);
     return 0;
   }
   CK(cudaEventRecord(s->ev[1], st));

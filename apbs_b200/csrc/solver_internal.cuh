@@ -23,6 +23,8 @@ int uses_coef_maps(const pmgb_solver* s);
 int uses_charge_map(const pmgb_solver* s);
 int fill_from_maps(pmgb_solver* s);
 void free_maps(pmgb_solver* s);
+// bcfl map: the faces from the potential map (focus.cu)
+int map_faces(pmgb_solver* s);
 }  // namespace pmgb
 
 namespace pmgb {

@@ -22,7 +22,7 @@ import numpy as np
 PMGB_MAXION = 8
 SRFM_MOL, SRFM_SMOL, SRFM_SPL2, SRFM_SPL4 = 0, 1, 2, 4
 CHGM_TRIL, CHGM_SPL2 = 0, 1
-BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS = 0, 1, 2, 4
+BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS, BCFL_MAP = 0, 1, 2, 4, 6
 
 
 class PmgbParams(ctypes.Structure):

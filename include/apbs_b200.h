@@ -159,7 +159,9 @@ int pmgb_read_dx_host(const char *path, int *dims, double *h, double *origin, do
 #define PMGB_MAP_DIELZ 2
 #define PMGB_MAP_KAPPA 3
 #define PMGB_MAP_CHARGE 4
-#define PMGB_MAP_COUNT 5
+#define PMGB_MAP_POT 5    /* boundary values of bcfl map (bcfl_map + focusFillBound,
+                             vpmg.c:3953-3993, 1914-2414) */
+#define PMGB_MAP_COUNT 6
 int pmgb_set_map(pmgb_solver *s, int which, int nx, int ny, int nz, double hx, double hy,
                  double hz, double xmin, double ymin, double zmin, const double *data);
 

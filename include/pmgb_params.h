@@ -28,6 +28,7 @@
 #define PMGB_BCFL_SDH 1
 #define PMGB_BCFL_MDH 2
 #define PMGB_BCFL_FOCUS 4
+#define PMGB_BCFL_MAP 6     /* faces from a potential map (pmgb_set_map PMGB_MAP_POT) */
 
 typedef struct pmgb_params {
     int nx, ny, nz;         /* grid points per axis ("dime") */

@@ -137,18 +137,18 @@ def write_dx(path, data, h, origin, pvec=None, title="POTENTIAL (kT/e)"):
 
 
 def run_maps(params, mol, maps):
-    """The reference with "usemap" maps: maps is {index 0..4 (dielx, diely,
-    dielz, kappa, charge): (data (nz, ny, nx), h (3,), origin (3,))}.
+    """The reference with "usemap" maps: maps is {index 0..5 (dielx, diely,
+    dielz, kappa, charge, pot): (data (nz, ny, nx), h (3,), origin (3,))}.
     Returns u, energy_kT and the fill maps as run() does."""
     n = params.nx * params.ny * params.nz
     u = np.zeros(n)
     fill = np.zeros(5 * n)
     out = np.zeros(16)
-    dims = (ctypes.c_int * 15)()
-    geom = np.zeros(30)
-    ptrs = (ctypes.POINTER(ctypes.c_double) * 5)()
+    dims = (ctypes.c_int * 18)()
+    geom = np.zeros(36)
+    ptrs = (ctypes.POINTER(ctypes.c_double) * 6)()
     keep = []
-    for m in range(5):
+    for m in range(6):
         if m in maps:
             data, h, origin = maps[m]
             d = np.ascontiguousarray(data, dtype=np.float64)

@@ -124,15 +124,15 @@ int ref_pmg_run(const pmgb_params *p, int natoms, const double *xyz,
 }
 
 /* ref_pmg_run with "usemap" maps given to Vpmg_fillco (vpmg.c:5250-5316):
- * map m (0..4 = dielx, diely, dielz, kappa, charge) is used when data[m] is
- * non-NULL, on the grid dims[3m..3m+2], spacing geom[6m..6m+2] and origin
- * geom[6m+3..6m+5] (the Vgrid a map file would give). */
+ * map m (0..5 = dielx, diely, dielz, kappa, charge, pot) is used when
+ * data[m] is non-NULL, on the grid dims[3m..3m+2], spacing geom[6m..6m+2]
+ * and origin geom[6m+3..6m+5] (the Vgrid a map file would give). */
 int ref_pmg_run_maps(const pmgb_params *p, int natoms, const double *xyz, const double *q,
                      const double *r, const int *dims, const double *geom, double **data,
                      double *u, double *maps, double *out) {
-    Vgrid *g[5];
+    Vgrid *g[6];
     int m, rc;
-    for (m = 0; m < 5; m++) {
+    for (m = 0; m < 6; m++) {
         g[m] = VNULL;
         if (data[m])
             g[m] = Vgrid_ctor(dims[3 * m], dims[3 * m + 1], dims[3 * m + 2], geom[6 * m],
@@ -140,7 +140,7 @@ int ref_pmg_run_maps(const pmgb_params *p, int natoms, const double *xyz, const 
                               geom[6 * m + 4], geom[6 * m + 5], data[m]);
     }
     rc = run_impl(p, natoms, xyz, q, r, u, maps, NULL, out, NULL, 0, 0, NULL, NULL, g);
-    for (m = 0; m < 5; m++)
+    for (m = 0; m < 6; m++)
         if (g[m]) Vgrid_dtor(&g[m]);
     return rc;
 }
@@ -182,8 +182,8 @@ static int run_impl(const pmgb_params *p, int natoms, const double *xyz,
     if (umap)
         rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
                          umap[0] != VNULL, umap[0], umap[1] != VNULL, umap[1],
-                         umap[2] != VNULL, umap[2], umap[3] != VNULL, umap[3], 0, VNULL,
-                         umap[4] != VNULL, umap[4]);
+                         umap[2] != VNULL, umap[2], umap[3] != VNULL, umap[3],
+                         umap[5] != VNULL, umap[5], umap[4] != VNULL, umap[4]);
     else
         rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm,
                          0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0,

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from apbs_b200 import synth, vpmg
-from apbs_b200.vpmg import FP64, MAP_CHARGE, MAP_DIELX, MAP_KAPPA, PmgbError, Vpmg
+from apbs_b200.vpmg import FP64, MAP_DIELX, MAP_KAPPA, MAP_POT, PmgbError, Vpmg
 from oracle import ref
 
 pytestmark = [pytest.mark.gpu,
@@ -80,4 +80,28 @@ def test_usemap_off_the_map_fails(tmp_path):
             pmg.set_map(m, *maps[m])
         with pytest.raises(PmgbError):
             pmg.fillco(mol)
-    _ = MAP_CHARGE
+
+
+def test_bcfl_map_matches_reference(tmp_path):
+    """bcfl map: the faces interpolated from a potential map (a coarse
+    solve over a larger box, through a DX file), as focusFillBound does with
+    the map in place of the coarse grid."""
+    mol = synth.cluster(150, 8.0, seed=13, net_charge=1.0)
+    pc = synth.mg_manual(49, 1.0, mol.center(), ions=IONS)
+    rc = ref.run(pc, mol)
+    h = (pc.hx, pc.hy, pc.hz)
+    origin = [pc.center[d] - 0.5 * (n - 1) * hd for d, (n, hd) in
+              enumerate(zip((pc.nx, pc.ny, pc.nz), h))]
+    vpmg.write_dx(tmp_path / "pot.dx", rc["u"], h, origin, title="POTENTIAL (kT/e)")
+    pot = vpmg.read_dx(tmp_path / "pot.dx")
+    p = synth.mg_manual(33, 0.9, mol.center(), ions=IONS, bcfl=synth.BCFL_MAP)
+    want = ref.run_maps(p, mol, {MAP_POT: pot})
+    with Vpmg(p, FP64) as pmg:
+        pmg.set_map(MAP_POT, *pot)
+        pmg.fillco(mol)
+        pmg.solve()
+        u, e = pmg.u, pmg.energy()
+    assert np.abs(u - want["u"]).max() <= REL_U * np.abs(want["u"]).max()
+    assert abs(e - want["energy_kT"]) <= REL_E * abs(want["energy_kT"])
+    # the boundary is the map's, not a Debye-Hueckel one
+    assert np.abs(u[0] - want["u"][0]).max() <= 1e-12 * np.abs(want["u"][0]).max()
