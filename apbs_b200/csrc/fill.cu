@@ -197,12 +197,63 @@ __global__ void k_cell_fill(int natoms, const int* __restrict__ cell_of, int* fi
   atoms_sorted[p] = a;
 }
 
+// The atoms that can exclude a surface point of atom a: a point lies at
+// r_a + srad from a, and b excludes it only within r_b + srad, so b is
+// within r_a + r_b + 2 srad of a.  One warp per atom collects them from the
+// cells within two cell edges (the cell edge is max r + srad) into a list of
+// up to kNbrCap entries; a longer list is only counted, and its atom's
+// points fall back to the cell search.  Any superset of the possible
+// excluders gives the same exclusion decisions.
+constexpr int kNbrCap = 512;
+
+__global__ void k_sas_nbr(CellGrid C, int natoms, const double* __restrict__ xyz,
+                          const double* __restrict__ r, double srad,
+                          const int* __restrict__ start, const int* __restrict__ atoms_sorted,
+                          int* nbr, int* ncount) {
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (a >= natoms) return;
+  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2];
+  int c[3];
+  const double pp[3] = {ax, ay, az};
+  for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
+  int count = 0;
+  for (int dz = -2; dz <= 2; dz++)
+    for (int dy = -2; dy <= 2; dy++)
+      for (int dx = -2; dx <= 2; dx++) {
+        const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+        if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
+          continue;
+        const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
+        const int s0 = start[cell], s1 = start[cell + 1];
+        for (int base = s0; base < s1; base += 32) {
+          const int s = base + lane;
+          bool keep = false;
+          int b = -1;
+          if (s < s1) {
+            b = atoms_sorted[s];
+            if (b != a) {
+              const double d0 = ax - xyz[3 * b], d1 = ay - xyz[3 * b + 1], d2 = az - xyz[3 * b + 2];
+              const double cut = r[a] + r[b] + 2.0 * srad + 1.0e-6;
+              keep = (d0 * d0 + d1 * d1 + d2 * d2) < cut * cut;
+            }
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, keep);
+          const int slot = count + __popc(m & ((1u << lane) - 1u));
+          if (keep && slot < kNbrCap) nbr[(size_t)a * kNbrCap + slot] = b;
+          count += __popc(m);
+        }
+      }
+  if (lane == 0) ncount[a] = count;
+}
+
 // One thread per (atom, reference point); the accessible points are appended
 // to a list (warp-aggregated), so the marking pass runs over them only.
 __global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xyz,
                            const double* __restrict__ r, const double* __restrict__ ref,
                            int nref, double srad, const int* __restrict__ start,
-                           const int* __restrict__ atoms_sorted, unsigned* list, int* npts) {
+                           const int* __restrict__ atoms_sorted, const int* __restrict__ nbr,
+                           const int* __restrict__ ncount, unsigned* list, int* npts) {
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   bool acc = false;
   if (tid < (long long)natoms * nref) {
@@ -213,30 +264,42 @@ __global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xy
       const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
       const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
       const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
-      int c[3];
-      const double pp[3] = {px, py, pz};
-      for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
+      auto excludes = [&](int b) {
+        const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1], d2 = pz - xyz[3 * b + 2];
+        const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+        const double rr = r[b] + srad;
+        return dist2 < rr * rr;
+      };
       acc = true;
-      for (int dz = -1; dz <= 1 && acc; dz++)
-        for (int dy = -1; dy <= 1 && acc; dy++)
-          for (int dx = -1; dx <= 1 && acc; dx++) {
-            const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
-            if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
-              continue;
-            const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
-            for (int s = start[cell]; s < start[cell + 1]; s++) {
-              const int b = atoms_sorted[s];
-              if (b == a) continue;
-              const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1],
-                           d2 = pz - xyz[3 * b + 2];
-              const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
-              const double rr = r[b] + srad;
-              if (dist2 < rr * rr) {
-                acc = false;
-                break;
+      const int cnt = ncount[a];
+      if (cnt <= kNbrCap) {
+        const int* lst = nbr + (size_t)a * kNbrCap;
+        for (int s = 0; s < cnt; s++)
+          if (excludes(lst[s])) {
+            acc = false;
+            break;
+          }
+      } else {
+        int c[3];
+        const double pp[3] = {px, py, pz};
+        for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
+        for (int dz = -1; dz <= 1 && acc; dz++)
+          for (int dy = -1; dy <= 1 && acc; dy++)
+            for (int dx = -1; dx <= 1 && acc; dx++) {
+              const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+              if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
+                continue;
+              const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
+              for (int s = start[cell]; s < start[cell + 1]; s++) {
+                const int b = atoms_sorted[s];
+                if (b == a) continue;
+                if (excludes(b)) {
+                  acc = false;
+                  break;
+                }
               }
             }
-          }
+      }
     }
   }
   const unsigned m = __ballot_sync(0xffffffffu, acc);
@@ -675,15 +738,20 @@ void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const doub
   cudaMemcpyAsync(fillpos, start, sizeof(int) * ncell, cudaMemcpyDeviceToDevice, s);
   k_cell_fill<<<(natoms + 255) / 256, 256, 0, s>>>(natoms, cell_of, fillpos, sorted);
 }
+size_t sas_nbr_ints(int natoms) { return (size_t)natoms * (kNbrCap + 1); }
+
 void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
                 const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, unsigned* list,
+                double epsw, const int* start, const int* sorted, int* nbr, unsigned* list,
                 int* npts, double* epsx, double* epsy, double* epsz) {
   const long long tot = (long long)natoms * nref;
   if (tot <= 0) return;
   cudaMemsetAsync(npts, 0, sizeof(int), s);
+  int* ncount = nbr + (size_t)natoms * kNbrCap;
+  k_sas_nbr<<<(natoms + 7) / 8, 256, 0, s>>>(C, natoms, xyz, r, srad, start, sorted, nbr, ncount);
   k_sas_test<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(C, natoms, xyz, r, ref, nref, srad,
-                                                           start, sorted, list, npts);
+                                                           start, sorted, nbr, ncount, list,
+                                                           npts);
   static const int nblocks = [] {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);

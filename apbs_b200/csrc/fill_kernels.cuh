@@ -56,9 +56,11 @@ void launch_mark_atoms_kappa(cudaStream_t s, const FillGeom& G, int natoms, cons
                              const double* r, double irad, double* kappa);
 void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
                        int* count, int* start, int* fillpos, int* cell_of, int* sorted);
+// ints of the per-atom excluder lists launch_sas needs (nbr)
+size_t sas_nbr_ints(int natoms);
 void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
                 const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, unsigned* list,
+                double epsw, const int* start, const int* sorted, int* nbr, unsigned* list,
                 int* npts, double* epsx, double* epsy, double* epsz);
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
                    const double* a3, double* epsx, double* epsy, double* epsz);

@@ -488,7 +488,7 @@ extern "C" size_t pmgb_footprint(const pmgb_params* params, int precision, int n
   const double pi = 3.14159265358979323846;
   const double nref = 4.0 * pi * (3.0 + p.srad) * (3.0 + p.srad) * (p.sdens > 0 ? p.sdens : 10.0);
   bytes += (size_t)natoms * ((size_t)nref * sizeof(unsigned) + 64 + 18 * sizeof(double) +
-                            2 * sizeof(int));
+                            2 * sizeof(int) + 513 * sizeof(int));
   return bytes;
 }
 
@@ -513,7 +513,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->band);
   dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
-  dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->d_ref); dfree(s->atom_terms);
+  dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->sas_nbr); dfree(s->d_ref); dfree(s->atom_terms);
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   free_maps(s);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
@@ -630,10 +630,12 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
         return 0;
       }
       if (!grow(&s->sas_list, &s->sas_list_alloc, npairs, st)) return 0;
+      if (!grow(&s->sas_nbr, &s->sas_nbr_alloc, sas_nbr_ints(natoms), st)) return 0;
       launch_sas(st, s->G, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
-                 s->cell_start, s->cell_sorted, s->sas_list, s->d_npts, s->epsx, s->epsy,
+                 s->cell_start, s->cell_sorted, s->sas_nbr, s->sas_list, s->d_npts, s->epsx,
+                 s->epsy,
                  s->epsz);
-      note_launches(2);
+      note_launches(3);
     }
     if (p.srfm == PMGB_SRFM_SMOL) {
       CK(cudaMemcpyAsync(s->tmp3, s->epsx, n * sizeof(double), cudaMemcpyDeviceToDevice, st));

@@ -107,6 +107,8 @@ struct pmgb_solver {
   int *cell_count, *cell_start, *cell_fillpos, *cell_of, *cell_sorted;
   size_t ncell_alloc, cellof_alloc;
   unsigned* sas_list;  // accessible SAS points, (atom * nref + point)
+  int* sas_nbr;        // per-atom lists of possible excluders, then their counts
+  size_t sas_nbr_alloc;
   size_t sas_list_alloc;
   double* d_ref;
   int nref;
