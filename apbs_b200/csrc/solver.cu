@@ -192,7 +192,16 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
 
 int read_scalar(pmgb_solver* s, int slot, double* v) {
   CK(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  // a plane-wavefront wait that ran out leaves the iterates undefined: stop
+  // at the next read instead of iterating on them (pmgb_solve reports it)
+  int nerr = 0;
+  if (s->wave_used)
+    CK(cudaMemcpyAsync(&nerr, s->d_wave, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
+  if (nerr) {
+    set_error("gs27 plane wavefront: %d waits for a neighbour plane ran out", nerr);
+    return 0;
+  }
   return 1;
 }
 
@@ -1155,16 +1164,34 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
 // Reads (and clears) the count of plane-wavefront waits that ran out; a
 // nonzero count fails the solve (the iterates are not the ordered sweep's).
 static int wave_check(pmgb_solver* s) {
+  // wave_used stays set: graphs captured with the plane kernel replay it in
+  // every later solve without passing through gs27_smooth again
   if (!s->wave_used) return 1;
-  s->wave_used = 0;
   int nerr = 0;
   CK(cudaMemcpyAsync(&nerr, s->d_wave, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   if (nerr) {
-    CK(cudaMemsetAsync(s->d_wave, 0, sizeof(int), s->stream));
+    // the counters of the levels may now disagree: restart them all
+    CK(cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), s->stream));
+    CK(cudaStreamSynchronize(s->stream));
     set_error("gs27 plane wavefront: %d waits for a neighbour plane ran out", nerr);
     return 0;
   }
+  return 1;
+}
+
+// Testing hook: shift one plane's step counter so that its neighbours'
+// waits run out on the next solve (a failure made without a device fault).
+extern "C" int pmgb_debug_shift_wave_counter(pmgb_solver* s, int level, int plane, int delta) {
+  if (!s || level < 0 || level >= s->nlev || plane < 0 || plane >= kWavePlanesMax) {
+    set_error("pmgb_debug_shift_wave_counter: bad arguments");
+    return 0;
+  }
+  unsigned* c = s->d_wave + kWaveCounterBase + (size_t)level * kWavePlanesMax + plane;
+  unsigned v = 0;
+  CK(cudaMemcpy(&v, c, sizeof(v), cudaMemcpyDeviceToHost));
+  v += (unsigned)delta;
+  CK(cudaMemcpy(c, &v, sizeof(v), cudaMemcpyHostToDevice));
   return 1;
 }
 
@@ -1197,7 +1224,12 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
       ok = newton_driver(s, errtol, 200, 0);
     }
   }
-  if (!ok) return 0;
+  if (!ok) {
+    // a wavefront wait that ran out is the cause to report (and its
+    // counters are restarted)
+    wave_check(s);
+    return 0;
+  }
   // restore Dirichlet values (VfboundPMG, mgdrvd.c:557)
   launch_fbound(st, s->g, s->lev[0].x, s->gx, s->gy, s->gz);
   note_launches(1);

@@ -122,7 +122,7 @@ struct pmgb_solver {
   double* d_forces;         // pmgb_forces: 9 doubles and a status word per atom
   size_t forces_alloc;
   unsigned* d_wave;
-  int wave_used;  // a solve launched the plane kernel since the last check
+  int wave_used;  // the plane kernel has been launched or captured (stays set)
   double* atom_terms;  // 13 x natoms sdh moment terms
   size_t terms_alloc;
   // focusing: faces set from a coarse solution, energies outside the domain

@@ -90,6 +90,7 @@ def lib():
         L.pmgb_solve.argtypes = [vp]
         L.pmgb_energy.argtypes = [vp, dp]
         L.pmgb_forces.argtypes = [vp, dp, dp, dp]
+        L.pmgb_debug_shift_wave_counter.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.pmgb_write_dx.argtypes = [vp, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
                                     ctypes.c_char_p]
         L.pmgb_set_map.argtypes = [vp, ctypes.c_int] + [ctypes.c_int] * 3 + \

@@ -122,6 +122,13 @@ int pmgb_energy(pmgb_solver *s, double *energy_kT);
  * per-atom Vpmg_force loop of forceMG (src/routines.c). */
 int pmgb_forces(pmgb_solver *s, double *qf, double *db, double *ib);
 
+/* Testing hook for the failure path of the plane-parallel GS27 wavefront:
+ * shifts the step counter of one plane of one level, so that the next solve
+ * has its neighbours' bounded waits run out (no device fault).  That solve
+ * fails with an error naming the waits and restarts the counters; the one
+ * after it runs normally.  No reference counterpart. */
+int pmgb_debug_shift_wave_counter(pmgb_solver *s, int level, int plane, int delta);
+
 /* OpenDX output, byte for byte the file writedataMG writes through
  * Vgrid_writeDX (src/routines.c:2620-2920, src/mg/vgrid.c:1206-1420):
  * pmgb_write_dx writes one map of a calculation with its partition weights
