@@ -29,6 +29,7 @@
 
 #include "common.cuh"
 #include "gs7_sweep.cuh"
+#include "gs7_pairs.cuh"
 
 namespace pmgb {
 
@@ -187,9 +188,18 @@ inline cudaError_t launch_gs7_march(cudaStream_t st, const Gs7Sweep<T>& a0) {
 // The single-pass sweep kernels by PMGB_TUNE_GS7_SWEEP_KERNEL: 0 = ring tiles
 // (k_gs7_sweep), 1 = ring tiles staged by cp.async, 2 = column march on 32x16
 // tiles (32x8 in FP64, whose window needs more registers), 3 = column march
-// on 32x8 tiles.
+// on 32x8 tiles, 4 = whole-row pair tiles (k_gs7_sweep_pairs), 5 = the same
+// with the next plane's coefficients loaded one step ahead.  A grid the pair
+// kernel does not take (even row length, rows of more than 1534 points,
+// arrays not pair-aligned) runs the ring-tile kernel.
 template <typename T>
 inline cudaError_t launch_gs7_sweep_kernel(cudaStream_t st, const Gs7Sweep<T>& a, int kernel) {
+  if (kernel == 4 || kernel == 5) {
+    const cudaError_t e = kernel == 4 ? launch_gs7_sweep_pairs<T, false>(st, a)
+                                      : launch_gs7_sweep_pairs<T, true>(st, a);
+    if (e != cudaErrorNotSupported) return e;
+    kernel = 0;
+  }
   switch (kernel) {
     case 1: return launch_gs7_sweep_async<T, 32, 8>(st, a);
     case 2: return sizeof(T) == 8 ? launch_gs7_march<T, 32, 8>(st, a)

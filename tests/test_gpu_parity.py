@@ -128,7 +128,8 @@ def test_exact_coarse_solve_matches_band():
 def test_single_pass_sweep_matches_colour_passes():
     """The fine smoother's single-pass sweep kernels (ring tiles, the default;
     ring tiles staged by cp.async; one thread per column marching up k, on
-    32x16 and 32x8 tiles) and the one-launch-per-colour kernels compute the
+    32x16 and 32x8 tiles; whole-row pair tiles, with and without the next
+    plane's coefficients loaded ahead) and the one-launch-per-colour kernels compute the
     same red-black sweep: bitwise equal FP64 solves, and bitwise equal FP32
     inner cycles of the mixed path."""
     from apbs_b200.vpmg import (MIXED, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KERNEL,
@@ -136,7 +137,7 @@ def test_single_pass_sweep_matches_colour_passes():
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
     out = {}
     old = get_tuning(TUNE_GS7_COLOUR_PASSES)
-    kernels = (0, 1, 2, 3)
+    kernels = (0, 1, 2, 3, 4, 5)
     try:
         for npbe in (False, True):
             p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
