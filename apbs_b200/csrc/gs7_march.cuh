@@ -30,6 +30,7 @@
 #include "common.cuh"
 #include "gs7_sweep.cuh"
 #include "gs7_pairs.cuh"
+#include "gs7_bulk.cuh"
 
 namespace pmgb {
 
@@ -188,15 +189,29 @@ inline cudaError_t launch_gs7_march(cudaStream_t st, const Gs7Sweep<T>& a0) {
 // The single-pass sweep kernels by PMGB_TUNE_GS7_SWEEP_KERNEL: 0 = ring tiles
 // (k_gs7_sweep), 1 = ring tiles staged by cp.async, 2 = column march on 32x16
 // tiles (32x8 in FP64, whose window needs more registers), 3 = column march
-// on 32x8 tiles, 4 = whole-row pair tiles (k_gs7_sweep_pairs), 5 = the same
-// with the next plane's coefficients loaded one step ahead.  A grid the pair
+// on 32x8 tiles, 4 = whole-row pair tiles (k_gs7_sweep_pairs) of up to 768
+// threads, 5 = the same with the next plane's coefficients loaded one step
+// ahead, 6 and 7 = pair tiles of 4 and 5 rows (2 tile rows and 3, several
+// CTAs per SM), 8 and 9 = FP64 pair tiles staged by bulk asynchronous row
+// copies (k_gs7_sweep_bulk; 4 x planes and 2 coefficient planes resident, or
+// 5 and 3; FP32 runs kernel 4).  A grid the pair
 // kernel does not take (even row length, rows of more than 1534 points,
 // arrays not pair-aligned) runs the ring-tile kernel.
 template <typename T>
 inline cudaError_t launch_gs7_sweep_kernel(cudaStream_t st, const Gs7Sweep<T>& a, int kernel) {
-  if (kernel == 4 || kernel == 5) {
-    const cudaError_t e = kernel == 4 ? launch_gs7_sweep_pairs<T, false>(st, a)
-                                      : launch_gs7_sweep_pairs<T, true>(st, a);
+  if (kernel == 8 || kernel == 9) {
+    cudaError_t e = cudaErrorNotSupported;
+    if constexpr (sizeof(T) == 8)
+      e = kernel == 8 ? launch_gs7_sweep_bulk<4, 2>(st, a, a.err)
+                      : launch_gs7_sweep_bulk<5, 3>(st, a, a.err);
+    if (e != cudaErrorNotSupported) return e;
+    kernel = 4;
+  }
+  if (kernel >= 4 && kernel <= 7) {
+    const cudaError_t e = kernel == 5   ? launch_gs7_sweep_pairs<T, true>(st, a)
+                          : kernel == 6 ? launch_gs7_sweep_pairs<T, false>(st, a, 4)
+                          : kernel == 7 ? launch_gs7_sweep_pairs<T, false>(st, a, 5)
+                                        : launch_gs7_sweep_pairs<T, false>(st, a);
     if (e != cudaErrorNotSupported) return e;
     kernel = 0;
   }

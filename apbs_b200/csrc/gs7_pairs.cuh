@@ -230,11 +230,12 @@ struct PairShape {
   int rw, ny_blk, ty;
 };
 
-inline bool pair_shape(const Grid& g, PairShape* s) {
+inline bool pair_shape(const Grid& g, int rows_cap, PairShape* s) {
   if ((g.nx & 1) == 0 || (g.ny & 1) == 0 || g.nx < 5 || g.ny < 5 || g.nz < 3) return false;
   const int w = (g.nx + 1) / 2;
   s->rw = (w + 31) / 32 * 32;
   s->ny_blk = kPairThreads / s->rw;
+  if (rows_cap > 0 && s->ny_blk > rows_cap) s->ny_blk = rows_cap;
   if (s->ny_blk < 3) return false;
   s->ty = s->ny_blk - 2;
   if (s->ty > g.ny - 2) {
@@ -255,13 +256,15 @@ inline bool pair_aligned(const Gs7Sweep<T>& a) {
 
 // Launches the pair sweep; returns cudaErrorNotSupported (nothing launched)
 // when the grid has an even row length, rows too long for one CTA, or
-// arrays that are not pair-aligned.  The plane chunk is chosen so that the
-// CTAs fill the device in one wave.
+// arrays that are not pair-aligned.  rows_cap > 0 limits the rows of a CTA
+// (tile plus ring) so that several CTAs fit on an SM.  The plane chunk is
+// chosen so that the CTAs fill the device in one wave.
 template <typename T, bool PF>
-inline cudaError_t launch_gs7_sweep_pairs(cudaStream_t st, const Gs7Sweep<T>& a0) {
+inline cudaError_t launch_gs7_sweep_pairs(cudaStream_t st, const Gs7Sweep<T>& a0,
+                                          int rows_cap = 0) {
   using V = typename PairOf<T>::type;
   PairShape ps;
-  if (!pair_shape(a0.g, &ps) || !pair_aligned(a0)) return cudaErrorNotSupported;
+  if (!pair_shape(a0.g, rows_cap, &ps) || !pair_aligned(a0)) return cudaErrorNotSupported;
   const size_t smem = (size_t)6 * ps.ny_blk * ps.rw * sizeof(V);
   static thread_local int dev_cached = -1, sms = 0;
   int dev = 0;
@@ -277,10 +280,15 @@ inline cudaError_t launch_gs7_sweep_pairs(cudaStream_t st, const Gs7Sweep<T>& a0
     }
     dev_cached = dev;
   }
+  int per_sm = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs7_sweep_pairs<T, 0, PF>,
+                                                    ps.rw * ps.ny_blk, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorNotSupported;
   Gs7Sweep<T> a = a0;
   const Grid g = a.g;
   const int rowblocks = (g.ny - 2 + ps.ty - 1) / ps.ty;
-  int nchunks = sms / rowblocks;
+  int nchunks = sms * per_sm / rowblocks;
   if (nchunks < 1) nchunks = 1;
   a.kchunk = (g.nz - 2 + nchunks - 1) / nchunks;
   nchunks = (g.nz - 2 + a.kchunk - 1) / a.kchunk;

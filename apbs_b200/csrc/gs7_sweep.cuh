@@ -40,6 +40,7 @@ struct Gs7Sweep {
   T* xout;
   int c1;      // colour updated first: (i + j + k) & 1 == c1
   int kchunk;  // planes per CTA
+  int* err = nullptr;  // staged sweeps: count of bounded waits that ran out
 };
 
 template <typename T, int TX, int TY>

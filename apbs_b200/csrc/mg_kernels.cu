@@ -381,13 +381,14 @@ int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
-                       int kernel) {
+                       int kernel, int* err) {
   Gs7Sweep<double> a;
   a.g = g;
   a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
   a.c1 = first_parity;
   a.kchunk = kchunk;
+  a.err = err;
   return launch_gs7_sweep_kernel<double>(s, a, kernel) == cudaSuccess;
 }
 

@@ -28,7 +28,7 @@ void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const do
 // one full red-black sweep in one pass, xin -> xout (boundaries of both zero)
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
-                       int kernel);
+                       int kernel, int* err = nullptr);
 int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                       double* x, double* r, int nsweep, int first_parity, const int* tune);
 extern int g_tune[16];

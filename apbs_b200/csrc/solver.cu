@@ -190,6 +190,14 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
+// Error word of the bounded device waits for a fine sweep launch: the sweeps
+// staged by bulk copies (sweep kernels 8 and 9) count waits that ran out in
+// the same word as the plane wavefront, which every residual read checks.
+static int* wave_err(pmgb_solver* s) {
+  if (s->tune[12] == 8 || s->tune[12] == 9) s->wave_used = 1;
+  return reinterpret_cast<int*>(s->d_wave);
+}
+
 int read_scalar(pmgb_solver* s, int slot, double* v) {
   CK(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   // a plane-wavefront wait that ran out leaves the iterates undefined: stop
@@ -199,7 +207,7 @@ int read_scalar(pmgb_solver* s, int slot, double* v) {
     CK(cudaMemcpyAsync(&nerr, s->d_wave, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   if (nerr) {
-    set_error("gs27 plane wavefront: %d waits for a neighbour plane ran out", nerr);
+    set_error("%d bounded device waits ran out (gs27 plane wavefront or staged gs7 sweep)", nerr);
     return 0;
   }
   return 1;
@@ -924,8 +932,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     k += 1;
   } else {
     // two single-pass sweeps, x -> xs -> x
-    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6], s->tune[12]) ||
-        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6], s->tune[12])) {
+    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6], s->tune[12], wave_err(s)) ||
+        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6], s->tune[12], wave_err(s))) {
       set_error("gs7 sweep launch failed");
       return 0;
     }
@@ -993,8 +1001,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
           k += 2;
         }
       } else {
-        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6], s->tune[12]) ||
-            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6], s->tune[12])) {
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6], s->tune[12], wave_err(s)) ||
+            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6], s->tune[12], wave_err(s))) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1174,7 +1182,7 @@ static int wave_check(pmgb_solver* s) {
     // the counters of the levels may now disagree: restart them all
     CK(cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    set_error("gs27 plane wavefront: %d waits for a neighbour plane ran out", nerr);
+    set_error("%d bounded device waits ran out (gs27 plane wavefront or staged gs7 sweep)", nerr);
     return 0;
   }
   return 1;
@@ -1450,7 +1458,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_SWEEP_FP64:
         // one full sweep: oE oN uC oC cc fc and x read, x written: 56 B per point
         if (!launch_gs7_sweep64(st, F.g, F.ops(), F.cc, F.fc, (r & 1) ? s->xs : F.x,
-                                (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12])) {
+                                (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12], wave_err(s))) {
           set_error("gs7 sweep launch failed");
           return 0;
         }

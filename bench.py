@@ -278,6 +278,10 @@ def main():
     ap.add_argument("--only", choices=["mixed", "fp64", "batch"], default=None,
                     help="profiling mode: run the steps of one precision (or the batched "
                          "kernel on the binding sweep's ligands) and nothing else")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="override one launch-shape tunable of the benchmark calculations "
+                         "after the tuning table (names as in the JSON line's config.tuning, "
+                         "e.g. gs7_sweep_kernel=8)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -344,6 +348,13 @@ def main():
     for name, prec in precisions:
         s = vpmg.Vpmg(params, prec)
         tuned[name] = autotune.apply(s, table)   # launch shapes from the autotuner's table
+        for kv in args.tune:
+            key, val = kv.split("=")
+            ids = [k for k, n in autotune.KEY_NAMES.items() if n == key]
+            if not ids:
+                raise SystemExit("--tune: unknown key %r" % key)
+            s.set_tuning(ids[0], int(val))
+            tuned[name][ids[0]] = int(val)
         s.set_stream(stream.cuda_stream)
         solvers[name] = s
 

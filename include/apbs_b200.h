@@ -236,7 +236,14 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_GS7_SWEEP_KERNEL 12 /* single-pass sweep kernel: 0 = ring tiles, 1 = ring
                                           tiles staged through shared memory by asynchronous
                                           copies, 2 = one thread per column marching up k on
-                                          32x16 tiles, 3 = the same on 32x8 tiles */
+                                          32x16 tiles, 3 = the same on 32x8 tiles, 4 = whole-row
+                                          tiles of 16-byte (red, black) pairs, 5 = the same with
+                                          the next plane loaded ahead, 6 and 7 = pair tiles of 4
+                                          and 5 rows, 8 and 9 = FP64 pair tiles whose plane rows
+                                          are staged by bulk asynchronous copies (4 x planes and
+                                          2 coefficient planes resident, or 5 and 3; FP32 runs
+                                          4).  Pair kernels need odd nx and ny, as PMG grids
+                                          have; other grids run 0. */
 #define PMGB_TUNE_GS7_SWEEP_STAGED PMGB_TUNE_GS7_SWEEP_KERNEL
 #define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
                                           synchronised with its neighbour planes on every

@@ -137,7 +137,7 @@ def test_single_pass_sweep_matches_colour_passes():
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
     out = {}
     old = get_tuning(TUNE_GS7_COLOUR_PASSES)
-    kernels = (0, 1, 2, 3, 4, 5)
+    kernels = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9)
     try:
         for npbe in (False, True):
             p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
