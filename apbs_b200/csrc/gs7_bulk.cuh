@@ -6,7 +6,10 @@
 // bitwise the colour-pass result of Vgsrb7x (src/pmgc/gsd.c:95-164).
 //
 // A row of pairs starts at an even flat index, so it is a 16-byte-aligned
-// run of W = (nx+1)/2 pairs (W * 16 bytes): one copy per row and array.  The
+// run of W = (nx+1)/2 pairs, and consecutive rows start nx - 1 or nx + 1
+// elements apart: the rows of a CTA in one plane form one contiguous,
+// 16-byte-aligned range, brought in by one copy per array and plane.  Shared
+// memory is indexed by the flat offset from the start of that range.  The
 // last row of the last plane would run one element past the array and is
 // never needed (no update reads it), so it is not copied.
 //
@@ -72,10 +75,15 @@ __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// pairs of one staged plane of one array: rows 0 .. ny_blk-1 from the pair
+// base of row 0
+inline int bulk_stage_pairs(int ny_blk, int nx) { return ((ny_blk - 1) * nx + 1) / 2 + (nx + 1) / 2; }
+
 template <int DX, int DC>
-inline size_t bulk_smem_bytes(int ny_blk, int w) {
-  const size_t rowp = (size_t)w * 16;
-  return (size_t)(DX + 6 * DC) * ny_blk * rowp + 4 * (size_t)ny_blk * w * 8 + (DX + DC) * 8;
+inline size_t bulk_smem_bytes(int ny_blk, int nx) {
+  const int w = (nx + 1) / 2;
+  return (size_t)(DX + 6 * DC) * bulk_stage_pairs(ny_blk, nx) * 16 +
+         4 * (size_t)ny_blk * w * 8 + (DX + DC) * 8;
 }
 
 template <int C1, int DX, int DC>
@@ -89,11 +97,11 @@ __global__ void __launch_bounds__(kPairThreads, 1)
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long sy = nx, sz = (long long)nx * ny;
   const int W = (nx + 1) / 2;
-  const int plane = NY * W;  // pairs per staged plane
-  V* XS = reinterpret_cast<V*>(smem_raw);                 // [DX][NY][W]
-  V* CS = XS + DX * plane;                                // [DC][6][NY][W]
-  double* R = reinterpret_cast<double*>(CS + DC * 6 * plane);  // [4][NY][W]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(R + 4 * plane);  // [DX + DC]
+  const int SP = ((NY - 1) * nx + 1) / 2 + W;  // pairs per staged plane of one array
+  V* XS = reinterpret_cast<V*>(smem_raw);                 // [DX][SP]
+  V* CS = XS + DX * SP;                                   // [DC][6][SP]
+  double* R = reinterpret_cast<double*>(CS + DC * 6 * SP);  // [4][NY][W]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(R + 4 * NY * W);  // [DX + DC]
   const int q = threadIdx.x, y = threadIdx.y;
   const int lane = threadIdx.x & 31;
   const bool warp0 = (y == 0) && (threadIdx.x < 32);
@@ -107,7 +115,6 @@ __global__ void __launch_bounds__(kPairThreads, 1)
   const int xfirst = max(k0 - 2, 0), xlast = min(k1 + 1, nz - 1);
   const int cfirst = k0 - 1, clast = k1;
   const double* __restrict__ X = a.xin;
-  const double* const src[6] = {a.fc, a.oC, a.cc, a.oE, a.oN, a.uC};
 
   auto base = [&](int p, int jj, int qq) -> long long {
     return (long long)p * sz + (long long)jj * sy + 2 * qq - ((jj + p) & 1);
@@ -116,45 +123,51 @@ __global__ void __launch_bounds__(kPairThreads, 1)
     const int i = 2 * q - ((j + p) & 1) + e;
     return row_int && p >= 1 && p <= nz - 2 && i >= 1 && i <= nx - 2;
   };
+  // pair offset of (row, col) in a staged plane p
+  auto off = [&](int p, int row, int col) -> int {
+    return ((row * nx - ((jb + row + p) & 1) + ((jb + p) & 1)) >> 1) + col;
+  };
   auto xs_at = [&](int p, int row, int col) -> const V& {
-    return XS[((p - xfirst) % DX * NY + row) * W + col];
+    return XS[(p - xfirst) % DX * SP + off(p, row, col)];
   };
   auto cs_at = [&](int p, int arr, int row, int col) -> const V& {
-    return CS[(((p - cfirst) % DC * 6 + arr) * NY + row) * W + col];
+    return CS[((p - cfirst) % DC * 6 + arr) * SP + off(p, row, col)];
   };
   auto r_at = [&](int p, int row, int col) -> double& {
     return R[(p % 4 * NY + row) * W + col];
   };
-  // rows of plane p that are staged: rows of the grid, less the last row of
-  // the last plane
-  auto row_copied = [&](int p, int r) {
-    const int jj = jb + r;
-    return jj <= ny - 1 && !(jj == ny - 1 && p == nz - 1);
-  };
-  const unsigned rowbytes = (unsigned)W * 16u;
-  // warp 0: stage x (narr = 1) or the coefficients (narr = 6) of plane p
+  // warp 0: stage x (narr = 1) or the coefficients (narr = 6) of plane p:
+  // rows jb .. jlast (rows of the grid, less the last row of the last plane)
+  // as one contiguous range per array
   auto issue = [&](int p, int narr, V* dst, uint64_t* b) {
-    unsigned rows = 0;
-    for (int r = 0; r < NY; r++) rows += row_copied(p, r) ? 1u : 0u;
+    int jlast = min(jb + NY - 1, ny - 1);
+    if (p == nz - 1 && jlast == ny - 1) jlast--;
+    const long long start = base(p, jb, 0);
+    const unsigned bytes =
+        jlast >= jb ? (unsigned)((base(p, jlast, 0) + 2 * W - start) * 8) : 0u;
     fence_async_shared();
-    if (lane == 0) mbar_arrive_tx(b, rows * rowbytes * narr);
+    if (lane == 0) mbar_arrive_tx(b, bytes * narr);
     __syncwarp();
-    for (int t = lane; t < narr * NY; t += 32) {
-      const int ai = t / NY, r = t - ai * NY;
-      if (!row_copied(p, r)) continue;
-      const double* s0 = narr == 1 ? X : src[ai];
-      bulk_copy_g2s(dst + (size_t)(ai * NY + r) * W, s0 + base(p, jb + r, 0), rowbytes, b);
+    if (bytes && lane < narr) {
+      const double* s0 = narr == 1 ? X
+                         : lane == 0 ? a.fc
+                         : lane == 1 ? a.oC
+                         : lane == 2 ? a.cc
+                         : lane == 3 ? a.oE
+                         : lane == 4 ? a.oN
+                                     : a.uC;
+      bulk_copy_g2s(dst + (size_t)lane * SP, s0 + start, bytes, b);
     }
   };
   auto issue_x = [&](int p) {
     if (p < xfirst || p > xlast) return;
     const int sl = (p - xfirst) % DX;
-    issue(p, 1, XS + (size_t)sl * plane, bar + sl);
+    issue(p, 1, XS + (size_t)sl * SP, bar + sl);
   };
   auto issue_c = [&](int p) {
     if (p < cfirst || p > clast) return;
     const int sl = (p - cfirst) % DC;
-    issue(p, 6, CS + (size_t)sl * 6 * plane, bar + DX + sl);
+    issue(p, 6, CS + (size_t)sl * 6 * SP, bar + DX + sl);
   };
   bool failed = false;
   auto wait = [&](uint64_t* b, unsigned parity) {
@@ -321,11 +334,11 @@ inline cudaError_t launch_gs7_sweep_bulk(cudaStream_t st, const Gs7Sweep<double>
     if (e != cudaSuccess) return e;
     dev_cached = dev;
   }
-  const int w = (a0.g.nx + 1) / 2;
-  while (ps.ny_blk >= 3 && bulk_smem_bytes<DX, DC>(ps.ny_blk, w) > (size_t)smem_max) ps.ny_blk--;
+  const int nx = a0.g.nx;
+  while (ps.ny_blk >= 3 && bulk_smem_bytes<DX, DC>(ps.ny_blk, nx) > (size_t)smem_max) ps.ny_blk--;
   if (ps.ny_blk < 3) return cudaErrorNotSupported;
   ps.ty = ps.ny_blk - 2;
-  const size_t smem = bulk_smem_bytes<DX, DC>(ps.ny_blk, w);
+  const size_t smem = bulk_smem_bytes<DX, DC>(ps.ny_blk, nx);
   Gs7Sweep<double> a = a0;
   const Grid g = a.g;
   const int rowblocks = (g.ny - 2 + ps.ty - 1) / ps.ty;

@@ -21,7 +21,7 @@ def test_wavefront_wait_runs_out_and_recovers():
         e0, u0 = pmg.energy(), pmg.u
         # level 1 (33^3) runs the plane kernel; shift plane 10's counter back
         assert lib().pmgb_debug_shift_wave_counter(pmg._h, 1, 10, -1000) == 1
-        with pytest.raises(PmgbError, match="waits for a neighbour plane ran out"):
+        with pytest.raises(PmgbError, match="bounded device waits ran out"):
             pmg.solve()
         pmg.solve()
         assert pmg.energy() == e0
