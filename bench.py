@@ -175,16 +175,23 @@ def serving_measurements(args):
                            % args.serve_n,
                "server": "8 worker streams, mixed LPBE up to 65^3 batched up to 16 per "
                          "persistent kernel, budget 80%% of free HBM, warm pools (the stream "
-                         "replayed once untimed so every grid shape is resident)"}
+                         "replayed once untimed so every grid shape is resident)",
+               "timed_replays": "%d, the median one reported" % args.serve_reps}
         for name, prec in (("mixed", MIXED), ("fp64", FP64)):
             with serve.Server(prec, max_inflight=8) as srv:
                 srv.apply_table(autotune.load_table(), prec)
                 serve.replay(srv, stream, time_scale=0.0)     # resident calculations
-                r = serve.replay(srv, stream)
+                # the makespan of one replay hangs on where the largest requests
+                # land: replay several times and keep the median run
+                runs = [serve.replay(srv, stream) for _ in range(max(1, args.serve_reps))]
+                runs.sort(key=lambda x: x["solves_per_s"])
+                r = runs[len(runs) // 2]
                 st = srv.stats()
             pts = sum(q.params.nx * q.params.ny * q.params.nz for q in stream)
             errors = sorted({x["error"] for x in r["results"] if x["status"] != 1})
-            rec[name] = {"solves_per_s": r["solves_per_s"], "p50_ms": r["p50_ms"],
+            rec[name] = {"solves_per_s": r["solves_per_s"],
+                         "solves_per_s_runs": [x["solves_per_s"] for x in runs],
+                         "p50_ms": r["p50_ms"],
                          "p99_ms": r["p99_ms"], "failed": r["failed"], "errors": errors,
                          "wall_s": r["wall_s"],
                          "grid_points_per_s": pts / r["wall_s"],
@@ -273,6 +280,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-n", type=int, default=300,
                     help="requests in the serving-stream measurement (0 skips it)")
+    ap.add_argument("--serve-reps", type=int, default=3,
+                    help="timed replays of the request stream (the median one is reported)")
     ap.add_argument("--sweep-poses", type=int, default=64,
                     help="poses of the binding-energy sweep measurement (0 skips it)")
     ap.add_argument("--only", choices=["mixed", "fp64", "batch"], default=None,
