@@ -1,16 +1,19 @@
 // Energy of a solved potential without any device allocation.
 //
 // For callers that cannot allocate device memory at the point where they
-// need the energy: code running inside another framework's memory pool or a
-// captured work stream, where a cudaMalloc would synchronise the device or
-// is forbidden, and embedded or real-time callers whose device footprint is
-// fixed up front.  They already hold the potential and the coefficient maps
-// in device memory; this entry point only reads them.
+// need the energy: code running inside another framework's memory pool,
+// whose device memory belongs to that pool and where a cudaMalloc would
+// synchronise the device, and embedded or real-time callers whose device
+// footprint is fixed up front.  They already hold the potential and the
+// coefficient maps in device memory; this entry point only reads them.
+// The call copies the partition weights in from host memory and waits for
+// its own result on the stream before it returns.
 //
 // The per-block partial sums and the partition weights live in one
 // file-scope device array of fixed size.  Its device address is looked up
 // once per device (cudaGetSymbolAddress, with that device current) on the
-// first call made there, so make that first call before any stream capture.
+// first call made there, so make that first call before any stream capture
+// on that device.
 // Every call on a device uses the same array: calls that overlap on the GPU
 // (different streams, or host threads calling concurrently) race on it and
 // must be serialised by the caller.  Nothing in the array needs to start at
@@ -83,6 +86,10 @@ extern "C" int pmgb_energy_noalloc(const pmgb_params* p, const double* d_u,
               p->nz, PMGB_NOALLOC_MAX_DIM);
     return 0;
   }
+  if (p->nion < 0 || p->nion > PMGB_MAXION) {
+    set_error("pmgb_energy_noalloc: %d ion species outside 0..%d", p->nion, PMGB_MAXION);
+    return 0;
+  }
   if (p->chgm != PMGB_CHGM_SPL2) {
     set_error("pmgb_energy_noalloc: the charge-map energy needs chgm spl2");
     return 0;
@@ -149,7 +156,7 @@ extern "C" int pmgb_energy_noalloc(const pmgb_params* p, const double* d_u,
   a.hz = p->hz;
   a.nonlin = (p->nonlin && ionstr > 0.) ? 1 : 0;
   a.ions.nion = p->nion;
-  for (int i = 0; i < p->nion && i < 8; i++) {
+  for (int i = 0; i < p->nion; i++) {
     a.ions.q[i] = p->ion_q[i];
     a.ions.sconc[i] = p->ion_conc[i];
   }

@@ -102,14 +102,26 @@ struct pmgb_server {
     for (const Pooled& q : idle) b += q.bytes;
     return b;
   }
-  bool has_idle(const Shape& sh) const {
-    for (const Pooled& q : idle)
-      if (q.shape == sh) return true;
-    return false;
+  // the idle calculation admit_at reuses for this shape (most recently
+  // used), or -1
+  int pick_idle(const Shape& sh) const {
+    int pick = -1;
+    for (int i = 0; i < (int)idle.size(); i++)
+      if (idle[i].shape == sh && (pick < 0 || idle[i].last_used > idle[pick].last_used))
+        pick = i;
+    return pick;
   }
-  // a request can start now
+  // a request can start now.  A pooled calculation is reused when one of
+  // the shape is idle; its footprint grows to the request's when the
+  // request has more atoms (the fill buffers grow with natoms), and that
+  // growth must fit beside everything not evictable.
   bool admissible(const Request* h) const {
-    if (has_idle(shape_of(h->p))) return true;
+    const int pick = pick_idle(shape_of(h->p));
+    if (pick >= 0) {
+      const size_t b = idle[pick].bytes;
+      if (h->bytes <= b) return true;
+      return in_use - (idle_bytes() - b) + (h->bytes - b) <= budget;
+    }
     return in_use - idle_bytes() + h->bytes <= budget;
   }
   bool head_admissible() const { return !queue.empty() && admissible(queue.front()); }
@@ -162,27 +174,27 @@ pmgb_server::Slot pmgb_server::admit_at(size_t pos, std::vector<void*>& release)
   queue.erase(queue.begin() + pos);
   const Shape sh = shape_of(sl.rq->p);
   // a resident calculation of this shape, most recently used first
-  int pick = -1;
-  for (int i = 0; i < (int)idle.size(); i++)
-    if (idle[i].shape == sh && (pick < 0 || idle[i].last_used > idle[pick].last_used)) pick = i;
+  const int pick = pick_idle(sh);
+  size_t grow = sl.rq->bytes;  // bytes in_use must take on
   if (pick >= 0) {
     sl.calc = idle[pick].calc;
-    sl.held = idle[pick].bytes;
+    sl.held = std::max(idle[pick].bytes, sl.rq->bytes);
+    grow = sl.held - idle[pick].bytes;
     idle.erase(idle.begin() + pick);
     reused++;
   } else {
-    // release idle calculations, least recently used first, until it fits
-    std::sort(idle.begin(), idle.end(),
-              [](const Pooled& a, const Pooled& b) { return a.last_used < b.last_used; });
-    while (in_use + sl.rq->bytes > budget && !idle.empty()) {
-      in_use -= idle.front().bytes;
-      release.push_back(idle.front().calc);
-      idle.erase(idle.begin());
-      evicted++;
-    }
-    in_use += sl.rq->bytes;
     sl.held = sl.rq->bytes;
   }
+  // release idle calculations, least recently used first, until it fits
+  std::sort(idle.begin(), idle.end(),
+            [](const Pooled& a, const Pooled& b) { return a.last_used < b.last_used; });
+  while (grow > 0 && in_use + grow > budget && !idle.empty()) {
+    in_use -= idle.front().bytes;
+    release.push_back(idle.front().calc);
+    idle.erase(idle.begin());
+    evicted++;
+  }
+  in_use += grow;
   peak = std::max(peak, in_use);
   inflight++;
   inflight_peak = std::max(inflight_peak, inflight);

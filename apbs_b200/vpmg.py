@@ -42,6 +42,7 @@ TUNE_GS27_PLANES = 13
 TUNE_CG_CLUSTER = 14
 TUNE_GS27_PLANES_POLL = 15
 TUNE_NKEYS = 16
+NOALLOC_MAX_DIM = 1025   # PMGB_NOALLOC_MAX_DIM
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libapbs_b200.so")

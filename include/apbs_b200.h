@@ -273,16 +273,18 @@ int pmgb_time_kernel(pmgb_solver *s, int which, int reps, double *ms_per_launch,
 /* Energy of a solved potential (as pmgb_energy) computed from device arrays
  * the caller already holds, without allocating any device memory.  It has
  * no counterpart in the reference; it serves callers that cannot allocate
- * at this point -- code inside another framework's memory pool or a
- * captured stream, where cudaMalloc would synchronise or is not allowed,
- * and fixed-footprint embedded callers.  d_u is the potential with its
- * boundary values, the maps are those of the fill (N = nx*ny*nz doubles;
- * the dielectric and kappa maps may be NULL for LPBE).  Grids up to
- * PMGB_NOALLOC_MAX_DIM points per axis; larger grids are rejected.  The
- * scratch is one fixed 64 KiB device array per device, shared by every
- * call: the first call on a device looks its address up (make that call
- * before any stream capture), and calls that overlap on the GPU race on it.
- * cuda_stream may be NULL (default stream); the call waits for its result. */
+ * at this point -- code inside another framework's memory pool, whose
+ * device memory belongs to that pool and where cudaMalloc would synchronise
+ * the device, and fixed-footprint embedded callers.  d_u is the potential
+ * with its boundary values, the maps are those of the fill (N = nx*ny*nz
+ * doubles; the dielectric and kappa maps may be NULL for LPBE).  Grids up
+ * to PMGB_NOALLOC_MAX_DIM points per axis and 0..PMGB_MAXION ion species;
+ * anything else is rejected before any device work.  The scratch is one
+ * fixed 64 KiB device array per device, shared by every call: the first
+ * call on a device looks its address up (make that call before any stream
+ * capture on that device), and calls that overlap on the GPU race on it.
+ * cuda_stream may be NULL (default stream); the call copies the partition
+ * weights from host memory and waits for its result on that stream. */
 int pmgb_energy_noalloc(const pmgb_params *params, const double *d_u, const double *d_charge,
                         const double *d_epsx, const double *d_epsy, const double *d_epsz,
                         const double *d_kappa, void *cuda_stream, double *energy_kT);

@@ -51,3 +51,29 @@ def test_nlev_rule():
     assert synth.mgparm_nlev(33) == 4
     assert synth.mgparm_nlev(49) == 3
     assert synth.mgparm_nlev(225) == 4
+
+
+@pytest.mark.skipif(not os.path.exists(vpmg.LIB_PATH), reason="library not built")
+@pytest.mark.parametrize("what,edit,msg", [
+    ("axis over the limit", lambda p: setattr(p, "nx", vpmg.NOALLOC_MAX_DIM + 2), "points per axis"),
+    ("axis too small", lambda p: setattr(p, "nz", 2), "points per axis"),
+    ("chgm spl0", lambda p: setattr(p, "chgm", synth.CHGM_TRIL), "chgm spl2"),
+    ("nion over the table", lambda p: setattr(p, "nion", 9), "ion species"),
+    ("negative nion", lambda p: setattr(p, "nion", -1), "ion species"),
+])
+def test_energy_noalloc_rejects_bad_arguments(what, edit, msg):
+    """pmgb_energy_noalloc checks its arguments before any CUDA call, so the
+    rejections run on a machine without a GPU (dummy device addresses are
+    never touched)."""
+    _, p = synth.config0()
+    edit(p)
+    with pytest.raises(vpmg.PmgbError, match=msg):
+        vpmg.energy_noalloc(p, 0x1000, 0x2000, 0x3000, 0x4000, 0x5000, 0x6000)
+
+
+@pytest.mark.skipif(not os.path.exists(vpmg.LIB_PATH), reason="library not built")
+def test_energy_noalloc_rejects_npbe_without_maps():
+    m = synth.cluster(50, 5.0, seed=1)
+    p = synth.mg_manual(33, 0.6, m.center(), npbe=True)
+    with pytest.raises(vpmg.PmgbError, match="NPBE needs"):
+        vpmg.energy_noalloc(p, 0x1000, 0x2000)

@@ -152,3 +152,30 @@ def test_serving_stream_is_seeded():
     assert all(r.params.nx in serve.DIMES for r in a)
     assert all(np.array_equal(x.mol.xyz, y.mol.xyz) for x, y in zip(a, b))
     assert all(np.diff([r.t_arrival for r in a]) > 0)
+
+
+def test_reused_calculation_takes_the_larger_footprint():
+    """A pooled calculation reused by a request with more atoms grows to that
+    request's footprint (the fill buffers grow with the atom count), and the
+    loop counts the growth against the budget."""
+    dev = FakeDevice(0.0)
+    per_atom = 4096
+
+    def footprint(ctx, pp, precision, natoms):
+        p = ctypes.cast(pp, ctypes.POINTER(PmgbParams)).contents
+        return p.nx * p.ny * p.nz * 8 + natoms * per_atom
+
+    dev._cb = (serve.FOOTPRINT(footprint),) + dev._cb[1:]
+    dev.backend = serve.Backend(None, *dev._cb)
+    grid = 33 ** 3 * 8
+    with serve.Server(max_inflight=1, hbm_budget_bytes=1 << 30, backend=dev.backend) as srv:
+        assert srv.wait(srv.submit(*_req(33, 10, 0)))["status"] == 1
+        assert srv.stats()["bytes_in_use"] == grid + 10 * per_atom
+        assert srv.wait(srv.submit(*_req(33, 500, 1)))["status"] == 1
+        st = srv.stats()
+        assert st["reused"] == 1
+        assert st["bytes_in_use"] == grid + 500 * per_atom
+        # a smaller request keeps the grown calculation's footprint
+        assert srv.wait(srv.submit(*_req(33, 20, 2)))["status"] == 1
+        st = srv.stats()
+        assert st["reused"] == 2 and st["bytes_in_use"] == grid + 500 * per_atom

@@ -2,8 +2,8 @@
 allocating one (pmgb_energy) on the same solved state.
 
 Callers that cannot allocate device memory when they need the energy --
-inside another framework's memory pool or a captured stream, or with a
-fixed device footprint -- hand in device arrays they already hold; the
+code inside another framework's memory pool, or with a fixed device
+footprint -- hand in device arrays they already hold; the
 result must equal what the solver's own energy call reports.  Two calls in
 a row check that the shared scratch array carries nothing over.  This file
 is collected last so a failure here never hides another test's result."""
