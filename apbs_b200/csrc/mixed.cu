@@ -1836,16 +1836,16 @@ int launch_coarse_exact(pmgb_solver* s, cudaStream_t st, const double* cc, const
   return 1;
 }
 
-int mixed_solve(pmgb_solver* s, double errtol) {
+int mixed_solve(pmgb_solver* s, double errtol, int itmax) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   CKM(cudaMemsetAsync(s->lev[0].x, 0, s->n * sizeof(double), s->stream));
   if (!s->p.nonlin) {
     if (!s->mixed->cc_ready && !mixed_set_cc(s, 0)) return 0;
     int it = 0;
     Level& F = s->lev[0];
-    return refine(s, 0, F.cc, F.fc, F.x, errtol, 200, 0, &it);
+    return refine(s, 0, F.cc, F.fc, F.x, errtol, itmax, 0, &it);
   }
-  return newton_driver(s, errtol, 200, 1);
+  return newton_driver(s, errtol, itmax, 1);
 }
 
 }  // namespace pmgb
@@ -1945,7 +1945,7 @@ extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_s
     B.e = m->lev[0].x;
     B.r = m->r;
     B.errtol = (s->p.etol > 0.0) ? s->p.etol : 1.0e-6;
-    B.itmax = 200;
+    B.itmax = (s->p.itmax > 0) ? s->p.itmax : 200;
     B.nlog = nlog;
     B.out = d_out + (size_t)(2 + nlog) * b;
   }
@@ -1993,6 +1993,7 @@ extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_s
     s->st.refinements = iters;
     s->st.newton_iters = 0;
     s->st.rel_residual = o[1];
+    s->st.converged = (o[1] <= ((s->p.etol > 0.0) ? s->p.etol : 1.0e-6)) ? 1 : 0;
     s->st.coarse_method = 2;
     s->st.t_setup_ms = 0.0;
     s->st.t_solve_ms = 0.0;

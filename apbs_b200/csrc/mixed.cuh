@@ -7,7 +7,7 @@ namespace pmgb {
 struct MixedState;
 // Solve the problem held by s (LPBE or NPBE) in mixed precision.  Leaves the
 // FP64 solution in s->lev[0].x (Dirichlet values not yet restored).
-int mixed_solve(pmgb_solver* s, double errtol);
+int mixed_solve(pmgb_solver* s, double errtol, int itmax);
 void mixed_destroy(MixedState* m);
 void mixed_mark_stale(MixedState* m);
 // Inner linear solve of one Newton step in mixed precision.

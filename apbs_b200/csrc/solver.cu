@@ -8,6 +8,8 @@
 // only the decisions the reference takes on scalar norms (stopping tests,
 // Newton damping), reading one scalar per decision.
 #include <math.h>
+
+#include <cmath>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -745,12 +747,32 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   return 1;
 }
 
+// Atom data must be finite: a NaN or infinite coordinate, charge or radius
+// would pass every on-mesh test of the fill and poison the maps.  The
+// calculation is left unfilled, so a following solve fails too.
+static int check_atoms(pmgb_solver* s, const char* who, int natoms, const double* xyz,
+                       const double* charge, const double* radius) {
+  for (int a = 0; a < natoms; a++) {
+    const double v[5] = {xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], charge[a], radius[a]};
+    for (int c = 0; c < 5; c++)
+      if (!std::isfinite(v[c])) {
+        static const char* what[5] = {"x", "y", "z", "charge", "radius"};
+        set_error("%s: atom %d has a non-finite %s", who, a, what[c]);
+        s->filled = 0;
+        s->solved = 0;
+        return 0;
+      }
+  }
+  return 1;
+}
+
 static int fillco_host(pmgb_solver* s, int natoms, const double* xyz, const double* charge,
                        const double* radius, int wait) {
   if (!s || natoms <= 0 || !xyz || !charge || !radius) {
     set_error("pmgb_fillco: bad arguments");
     return 0;
   }
+  if (!check_atoms(s, "pmgb_fillco", natoms, xyz, charge, radius)) return 0;
   {
     size_t c1 = 3 * s->atoms_cap, c2 = s->atoms_cap, c3 = s->atoms_cap;
     if (!grow(&s->a_xyz, &c1, 3 * (size_t)natoms, s->stream) ||
@@ -790,9 +812,11 @@ extern "C" int pmgb_fillco_device(pmgb_solver* s, int natoms, const double* d_xy
   }
   // host copies of positions and radii for the scalar setup (bounding box,
   // solute radius, sphere density)
-  std::vector<double> xyz(3 * (size_t)natoms), r(natoms);
+  std::vector<double> xyz(3 * (size_t)natoms), q(natoms), r(natoms);
   CK(cudaMemcpy(xyz.data(), d_xyz, sizeof(double) * 3 * natoms, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(q.data(), d_charge, sizeof(double) * natoms, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(r.data(), d_radius, sizeof(double) * natoms, cudaMemcpyDeviceToHost));
+  if (!check_atoms(s, "pmgb_fillco_device", natoms, xyz.data(), q.data(), r.data())) return 0;
   s->d_xyz = const_cast<double*>(d_xyz);
   s->d_q = const_cast<double*>(d_charge);
   s->d_r = const_cast<double*>(d_radius);
@@ -1219,17 +1243,20 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
   CK(cudaEventRecord(s->ev[3], st));
   s->st.coarse_method = (s->precision == PMGB_MIXED) ? 2 : (s->mgsolv == 2 ? 3 : s->mgsolv);
   const double errtol = (s->p.etol > 0.0) ? s->p.etol : 1.0e-6;
+  // Vpmgp itmax (vpmgp.c:131): V-cycles (LPBE) or Newton steps (NPBE)
+  const int itmax = (s->p.itmax > 0) ? s->p.itmax : 200;
+  s->st.converged = 0;
   int ok;
   if (s->precision == PMGB_MIXED) {
-    ok = mixed_solve(s, errtol);
+    ok = mixed_solve(s, errtol, itmax);
   } else {
     // u = 0 (Vazeros + VfboundPMG00, mgdrvd.c:462-483 / newdrvd.c:300)
     CK(cudaMemsetAsync(s->lev[0].x, 0, s->n * sizeof(double), st));
     if (!s->p.nonlin) {
       int iters = 0;
-      ok = vcycles(s, 0, errtol, 200, 0, &iters);
+      ok = vcycles(s, 0, errtol, itmax, 0, &iters);
     } else {
-      ok = newton_driver(s, errtol, 200, 0);
+      ok = newton_driver(s, errtol, itmax, 0);
     }
   }
   if (!ok) {
@@ -1247,6 +1274,9 @@ extern "C" int pmgb_solve(pmgb_solver* s) {
   CK(cudaGetLastError());
   s->st.t_setup_ms = elapsed_ms(s->ev[2], s->ev[3]);
   s->st.t_solve_ms = elapsed_ms(s->ev[3], s->ev[4]);
+  // like Vpmg_solve, a solve that stops at itmax still succeeds (the
+  // reference only sets ierror, mgcsd.c:564); the stats say so
+  s->st.converged = (s->st.rel_residual <= errtol) ? 1 : 0;
   s->solved = 1;
   return 1;
 }

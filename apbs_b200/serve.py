@@ -244,6 +244,18 @@ def serving_stream(n: int, seed: int = 4, rate: float = 200.0, dimes=DIMES,
     return out
 
 
+def stream_request(dime: int, natoms: int, npbe: bool, conc: float, seed: int):
+    """One calculation drawn by the rules of `serving_stream` with its grid,
+    size, equation and ionic strength given: a seeded `natoms`-atom cluster
+    (ball radius scaled to keep the atom density), the spacing that fits it
+    with 5 A of margin, 1:1 salt of concentration `conc` M."""
+    radius = 12.0 * (natoms / 500.0) ** (1.0 / 3.0)
+    mol = synth.cluster(natoms, radius, seed=seed)
+    span = float((mol.xyz.max(axis=0) - mol.xyz.min(axis=0)).max()) + 2 * 2.0 + 10.0
+    ions = ((1.0, conc, 2.0), (-1.0, conc, 2.0)) if conc > 0 else ()
+    return synth.mg_manual(dime, span / (dime - 1), mol.center(), npbe=npbe, ions=ions), mol
+
+
 def replay(server: Server, stream: list[StreamRequest], time_scale: float = 1.0) -> dict:
     """Submit each request at its arrival time and wait for all of them.
     Returns per-request results, the wall time from the first arrival to the

@@ -43,6 +43,7 @@ class PmgbParams(ctypes.Structure):
         ("ion_conc", ctypes.c_double * PMGB_MAXION),
         ("ion_radius", ctypes.c_double * PMGB_MAXION),
         ("swin", ctypes.c_double),
+        ("itmax", ctypes.c_int),
     ]
 
 

@@ -62,7 +62,7 @@ class PmgbStats(ctypes.Structure):
         ("diel", ctypes.c_double), ("qm", ctypes.c_double),
         ("sas_points", ctypes.c_int), ("status", ctypes.c_int),
         ("ext_qf", ctypes.c_double), ("ext_diel", ctypes.c_double),
-        ("ext_qm", ctypes.c_double),
+        ("ext_qm", ctypes.c_double), ("converged", ctypes.c_int),
     ]
 
     def as_dict(self):
@@ -261,6 +261,15 @@ class Vpmg:
     @property
     def u(self) -> np.ndarray:
         out = np.empty(self.shape)
+        _check(lib().pmgb_get_potential(self._h, _dp(out)), "pmgb_get_potential")
+        return out
+
+    def potential_into(self, out: np.ndarray) -> np.ndarray:
+        """Copy the potential into a caller's float64 array of nx*ny*nz
+        values (pinned host memory makes the copy a direct DMA)."""
+        if out.dtype != np.float64 or out.size != int(np.prod(self.shape)) or \
+                not out.flags.c_contiguous:
+            raise ValueError("potential_into: need a contiguous float64 array of nx*ny*nz")
         _check(lib().pmgb_get_potential(self._h, _dp(out)), "pmgb_get_potential")
         return out
 

@@ -136,26 +136,43 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(args):
-    """Reference CPU PMG timed on a bounded sample (one calculation)."""
+def cpu_baseline_sample(args, n=None):
+    """Reference CPU PMG timed on a bounded sample (n calculations of the
+    workload).  Returns the baseline record and the last calculation's
+    result (potential and energy), which the GPU results are checked
+    against."""
     ncores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
     try:
         from oracle import ref
         if not ref.available():
-            return None
+            return None, None
         mol, params, _ = workload(args.workload)
-        n = 2 if args.workload == "c1" else 10
+        if n is None:
+            n = 2 if args.workload == "c1" else 10
         t0 = time.perf_counter()
         for _ in range(n):
-            ref.run(params, mol)
+            res = ref.run(params, mol)
         dt = time.perf_counter() - t0
-        return {"value": n / dt, "unit": "solves/s",
-                "cores": int(os.environ.get("OMP_NUM_THREADS", ncores)), "kind": "reference",
-                "sample": "%d full calculations of the same workload" % n}
+        return ({"value": n / dt, "unit": "solves/s",
+                 "cores": int(os.environ.get("OMP_NUM_THREADS", ncores)), "kind": "reference",
+                 "sample": "%d full calculations of the same workload" % n}, res)
     except Exception as e:  # the baseline must not break the GPU line
-        return {"value": None, "unit": "solves/s", "cores": ncores, "kind": "reference",
-                "sample": "failed: %s" % e}
+        return ({"value": None, "unit": "solves/s", "cores": ncores, "kind": "reference",
+                 "sample": "failed: %s" % e}, None)
+
+
+def errors_vs_reference(u, e, want):
+    """Potential and energy error of one GPU result against the reference's
+    result for the same calculation (relative to max |u| and to |E|)."""
+    import numpy as np
+    ur = want["u"].reshape(-1)
+    d = np.abs(u.reshape(-1) - ur)
+    scale = float(np.abs(ur).max())
+    return {"u_rel_max": float(d.max()) / scale,
+            "u_rel_rms": float(np.sqrt(np.mean(d * d))) / scale,
+            "energy_rel": abs(e - want["energy_kT"]) / abs(want["energy_kT"]),
+            "energy_kT": e, "reference_energy_kT": want["energy_kT"]}
 
 
 def serving_measurements(args):
@@ -347,6 +364,7 @@ def main():
         return float(t.item())
 
     results = {}
+    potentials = {}
     precisions = [("fp64", vpmg.FP64), ("mixed", vpmg.MIXED)]
     if args.only:
         precisions = [p for p in precisions if p[0] == args.only]
@@ -396,6 +414,7 @@ def main():
         lat = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
         total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
         st = s.stats()
+        potentials[name] = s.u
         results[name] = {
             "solves_per_s": sum_over_ranks(args.steps) / (total_ms / 1e3),
             "ms_per_step": total_ms / args.steps,
@@ -426,6 +445,9 @@ def main():
         charge = h_q.numpy()
         radius = h_r.numpy()
     hm = _HostMol()
+    # the potential comes back every step, as Vpmg_solve leaves it in thee->u
+    h_u = torch.empty(params.nx * params.ny * params.nz, dtype=torch.float64).pin_memory()
+    h_u_np = h_u.numpy()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
@@ -434,12 +456,15 @@ def main():
             s.fillco(hm)
             s.solve()
             s.energy()
+            s.potential_into(h_u_np)
         ev1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
     e2e = {"value": sum_over_ranks(args.steps) / (e2e_ms / 1e3), "unit": "solves/s",
            "h2d_bytes_per_step": int(8 * (h_xyz.numel() + h_q.numel() + h_r.numel())),
-           "d2h_bytes_per_step": 8}
+           "d2h_bytes_per_step": int(8 + 8 * h_u.numel()),
+           "returns": "energy (8 B) and the potential grid (nx*ny*nz doubles) to pinned "
+                      "host memory every step"}
 
     # roofline of the dominant kernel of the headline path (largest share of
     # the ncu launch list in profiles/), timed live on the headline stream
@@ -477,9 +502,15 @@ def main():
             sv.close()
         extra = serving_measurements(args)
 
-    cpu = None
+    cpu, err_ref = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args)
+        cpu, want = cpu_baseline_sample(args)
+        if want is not None:
+            # error of every GPU result against the reference's own run of
+            # the same calculation
+            err_ref = {name: errors_vs_reference(potentials[name], results[name]["energy_kT"],
+                                                 want)
+                       for name in results}
 
     if rank == 0:
         line = {
@@ -502,6 +533,7 @@ def main():
             "mixed_vs_fp64": {"speedup": results["mixed"]["solves_per_s"] /
                               results["fp64"]["solves_per_s"],
                               "energy_rel_err": abs(emix - e64) / abs(e64)},
+            "err_vs_reference": err_ref,
             "e2e": e2e, "gpu_launches": head["gpu_launches"],
             "roofline": roofline, "smoothers": smoothers,
             "cpu_baseline": cpu, "clocks": clocks, **extra,

@@ -58,6 +58,9 @@ typedef struct pmgb_stats {
     int sas_points;       /* accessible surface points used by the fill */
     int status;           /* 0 ok, nonzero: last device-side status code */
     double ext_qf, ext_diel, ext_qm; /* energies outside the domain (focusing) */
+    int converged;        /* 1 if the last solve met its tolerance; 0 if it stopped at
+                             itmax (pmgb_params.itmax), which -- as Vpmg_solve --
+                             still returns success */
 } pmgb_stats;
 
 /* Vpmg_ctor: allocate device state for one calculation on the current CUDA
@@ -103,7 +106,11 @@ int pmgb_set_coefficients(pmgb_solver *s, const double *charge, const double *ep
                           const double *gxcf, const double *gycf, const double *gzcf);
 
 /* Vpmg_solve: build the operators and solve (LPBE: linear PMG; NPBE:
- * damped inexact Newton).  The potential stays on the device. */
+ * damped inexact Newton).  The potential stays on the device.  As in the
+ * reference, reaching the iteration limit (pmgb_params.itmax) without
+ * meeting the tolerance is not a failure: the call returns 1 with the last
+ * iterate and pmgb_stats.converged = 0.  A non-finite residual, a device
+ * error or a device wait that ran out returns 0. */
 int pmgb_solve(pmgb_solver *s);
 
 /* Vpmg_energy(extFlag = 1) of a non-focused calculation, in kT. */

@@ -51,6 +51,9 @@ typedef struct pmgb_params {
     double ion_radius[PMGB_MAXION]; /* radius (Angstrom) */
     double swin;            /* spline window of srfm spl2 and of the boundary
                                forces ("swin"); <= 0 -> 0.3 */
+    int itmax;              /* iteration limit of the solve (Vpmgp itmax: V-cycles of
+                               the LPBE solve, Newton steps of the NPBE solve);
+                               <= 0 -> 200, the reference's default (vpmgp.c:131) */
 } pmgb_params;
 
 #endif /* PMGB_PARAMS_H */

@@ -1788,10 +1788,11 @@ static int run_calc(const pmgb_params *p, int natoms, const double *xyz,
     s.mgsolv = p->nonlin ? 0 : 1;
     if (s.mgsolv == 1 && !build_band(&s, &s.lev[s.nlev - 1])) s.mgsolv = 0;
     /* solve: u = 0, then restore Dirichlet values (mgdrvd.c:462-557) */
+    /* Vpmgp itmax (vpmgp.c:131), 200 unless the parameters say otherwise */
     if (!p->nonlin) {
-        vcycles(&s, 0, errtol, 200, 0, &iters);
+        vcycles(&s, 0, errtol, p->itmax > 0 ? p->itmax : 200, 0, &iters);
     } else {
-        iters = newton(&s, p, &ph, errtol, 200);
+        iters = newton(&s, p, &ph, errtol, p->itmax > 0 ? p->itmax : 200);
     }
     t3 = now_s();
     {

@@ -173,6 +173,7 @@ static int run_impl(const pmgb_params *p, int natoms, const double *xyz,
                     p->sdie, p->srad, 0, p->sdens, 0.0, 0.0, 0.0, 0.0);
     if (pbe == VNULL) return 0;
     pmgp = Vpmgp_ctor(mg);
+    if (p->itmax > 0) pmgp->itmax = p->itmax;
     pmgp->bcfl = (Vbcfl)p->bcfl;
     pmgp->xcent = p->center[0];
     pmgp->ycent = p->center[1];

@@ -1,0 +1,84 @@
+"""Parity at the sizes that are benchmarked and served, against the
+reference compiled from source (oracle/_ref):
+
+* the 161^3 NPBE benchmark calculation itself (5000 atoms, net +12, 0.1 M),
+  whose coarsest 21^3 level runs the slab-cluster conjugate gradients;
+* a 97^3 NPBE calculation (coarsest 13^3, 1331 unknowns) through the slab
+  kernel and, forced by the tunable, through the strided cluster kernel;
+* serving-stream calculations at 129^3 (LPBE) and 225^3 (NPBE, coarsest
+  29^3, the strided 8-CTA kernel without forcing).
+
+FP64 must reproduce the reference's potential and energy to 1e-9 and its
+residual history; mixed precision must meet 1e-6 in energy and 1e-5 of
+max |u| in the potential against the same reference run."""
+import numpy as np
+import pytest
+
+from apbs_b200 import serve, synth
+from apbs_b200.vpmg import FP64, MIXED, TUNE_CG_CLUSTER, Vpmg
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+REL_U = 1e-9        # FP64 potential, relative to max |u|
+REL_E = 1e-9        # FP64 energy
+MIX_E = 1e-6        # mixed energy
+MIX_U = 1e-5        # mixed potential, relative to max |u|
+
+
+def _cases():
+    m1, p1 = synth.config1()
+    m97 = synth.cluster(1500, 17.0, seed=21, net_charge=5.0)
+    p97 = synth.mg_manual(97, 0.45, m97.center(), npbe=True,
+                          ions=((1.0, 0.1, 2.0), (-1.0, 0.1, 2.0)))
+    p129, m129 = serve.stream_request(129, 2600, False, 0.21, seed=129)
+    p225, m225 = serve.stream_request(225, 7400, True, 0.12, seed=225)
+    return [("config1_npbe161", m1, p1, None), ("npbe97_slab_cg", m97, p97, None),
+            ("npbe97_strided_cg", m97, p97, 2), ("stream129_lpbe", m129, p129, None),
+            ("stream225_npbe", m225, p225, None)]
+
+
+CASES = _cases()
+_REF = {}
+
+
+def _reference(name, mol, params):
+    key = name.replace("_strided_cg", "_slab_cg")   # same calculation
+    if key not in _REF:
+        _REF[key] = ref.run(params, mol)
+    return _REF[key]
+
+
+def _solve(params, mol, prec, cg_cluster):
+    with Vpmg(params, prec) as pmg:
+        if cg_cluster is not None:
+            pmg.set_tuning(TUNE_CG_CLUSTER, cg_cluster)
+        pmg.fillco(mol)
+        pmg.solve()
+        return pmg.energy(), pmg.u, pmg.residual_history(), pmg.stats()
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name,mol,params,cg", CASES, ids=[c[0] for c in CASES])
+def test_fp64_matches_reference(name, mol, params, cg):
+    want = _reference(name, mol, params)
+    e, u, hist, st = _solve(params, mol, FP64, cg)
+    scale = np.abs(want["u"]).max()
+    assert np.abs(u - want["u"]).max() <= REL_U * scale
+    assert abs(e - want["energy_kT"]) <= REL_E * abs(want["energy_kT"])
+    assert len(hist) == len(want["reslog"])
+    np.testing.assert_allclose(hist, want["reslog"], rtol=2e-6)
+    if params.nonlin:
+        assert st["coarse_method"] == 0          # conjugate gradients, as the reference
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name,mol,params,cg", [c for c in CASES if c[3] is None],
+                         ids=[c[0] for c in CASES if c[3] is None])
+def test_mixed_matches_reference(name, mol, params, cg):
+    want = _reference(name, mol, params)
+    e, u, _, st = _solve(params, mol, MIXED, cg)
+    scale = np.abs(want["u"]).max()
+    assert abs(e - want["energy_kT"]) <= MIX_E * abs(want["energy_kT"])
+    assert np.abs(u - want["u"]).max() <= MIX_U * scale
+    assert st["rel_residual"] <= 1e-6

@@ -75,3 +75,20 @@ def test_focusing_restatement_matches_reference(name, mol, pc, pf):
     assert abs(a["energy_kT"] - b["energy_kT"]) <= 1e-12 * abs(a["energy_kT"])
     # the focused energy differs from the plain one by the external term
     assert a["ext_qf"] != 0.0
+
+
+@pytest.mark.parametrize("npbe", [False, True], ids=["lpbe", "npbe"])
+def test_iteration_limit_restated(npbe):
+    """itmax below what convergence needs: the reference stops after itmax
+    V-cycles (LPBE) or Newton steps (NPBE) and returns its iterate; the
+    restatement stops at the same point."""
+    m = synth.cluster(120, 6.0, seed=11, net_charge=-2.0)
+    p = synth.mg_manual(33, 0.6, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    p.itmax = 1
+    a = ref.run(p, m)
+    b = port.run(p, m)
+    assert len(a["reslog"]) == len(b["reslog"])
+    assert a["reslog"][-1] > 1e-6          # not converged
+    np.testing.assert_allclose(b["reslog"], a["reslog"], rtol=2e-6)
+    scale = np.abs(a["u"]).max()
+    assert np.abs(a["u"] - b["u"]).max() <= 1e-12 * scale

@@ -179,3 +179,31 @@ def test_reused_calculation_takes_the_larger_footprint():
         assert srv.wait(srv.submit(*_req(33, 20, 2)))["status"] == 1
         st = srv.stats()
         assert st["reused"] == 2 and st["bytes_in_use"] == grid + 500 * per_atom
+
+
+def test_failed_request_leaves_the_others_alone():
+    """A request whose device run fails is reported failed with the others'
+    results untouched, and its calculation is not pooled."""
+    dev = FakeDevice(0.001)
+    bad_natoms = 13
+    inner = dev._cb[3]
+
+    def run(ctx, calc, natoms, xyz, q, r, energy):
+        if natoms == bad_natoms:
+            return 0
+        return inner(ctx, calc, natoms, xyz, q, r, energy)
+
+    dev._cb = dev._cb[:3] + (serve.RUN(run),) + dev._cb[4:]
+    dev.backend = serve.Backend(None, *dev._cb)
+    with serve.Server(max_inflight=3, hbm_budget_bytes=1 << 30, backend=dev.backend) as srv:
+        reqs = [_req(33, 10 + i, i) for i in range(10)]
+        ids = [srv.submit(p, m) for p, m in reqs]
+        res = [srv.wait(i) for i in ids]
+        st = srv.stats()
+    for (p, m), r in zip(reqs, res):
+        if m.natoms == bad_natoms:
+            assert r["status"] == -1 and r["error"]
+        else:
+            assert r["status"] == 1
+            assert r["energy_kT"] == pytest.approx(m.charge.sum() + m.natoms)
+    assert st["failed"] == 1 and st["done"] == 9
