@@ -9,17 +9,25 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libapbsref.so")
-_lib = None
+# the same reference objects and driver with Vpmg_solve replaced by the
+# drop-in binding apbs_b200/dropin/vpmg_b200.c (solve on the GPU)
+DROPIN_PATH = os.path.join(_HERE, "_ref", "libapbsref_b200.so")
+_libs = {}
 
 
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        _lib = ctypes.CDLL(LIB_PATH)
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_PATH)
+
+
+def lib(dropin=False):
+    path = DROPIN_PATH if dropin else LIB_PATH
+    if path not in _libs:
+        _lib = ctypes.CDLL(path)
+        _libs[path] = _lib
         dp = ctypes.POINTER(ctypes.c_double)
         _lib.ref_pmg_run.restype = ctypes.c_int
         _lib.ref_pmg_run.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
@@ -35,7 +43,10 @@ def lib():
         _lib.ref_pmg_focus.restype = ctypes.c_int
         _lib.ref_pmg_focus.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, dp, dp, dp,
                                      dp, dp, dp, dp, ctypes.c_int, ctypes.c_int]
-    return _lib
+        _lib.ref_pmg_chain.restype = ctypes.c_int
+        _lib.ref_pmg_chain.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, dp, dp,
+                                       dp, dp]
+    return _libs[path]
 
 
 def _ptr(a):
@@ -45,8 +56,9 @@ def _ptr(a):
 
 
 def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=4096,
-        want_forces=False):
-    """Run ctor+fillco+solve+energy of the reference on one calculation.
+        want_forces=False, dropin=False):
+    """Run ctor+fillco+solve+energy of the reference on one calculation
+    (with dropin=True, the same sequence with Vpmg_solve on the GPU).
 
     Returns a dict with u (nz,ny,nx), energy_kT, progress-message count,
     residual log, phase timings and, on request, the fill maps and faces and
@@ -64,7 +76,7 @@ def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=40
     r = np.ascontiguousarray(mol.radius, dtype=np.float64)
     forces = np.zeros(9 * mol.natoms) if want_forces else None
     fstatus = np.zeros(mol.natoms, dtype=np.int32) if want_forces else None
-    rc = lib().ref_pmg_run(ctypes.byref(params), mol.natoms, _ptr(xyz), _ptr(q), _ptr(r),
+    rc = lib(dropin).ref_pmg_run(ctypes.byref(params), mol.natoms, _ptr(xyz), _ptr(q), _ptr(r),
                            _ptr(u), _ptr(maps), _ptr(faces), _ptr(out), _ptr(reslog),
                            reslog_cap, verbose, _ptr(forces),
                            fstatus.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
@@ -91,7 +103,7 @@ def run(params, mol, want_maps=False, want_faces=False, verbose=0, reslog_cap=40
     return res
 
 
-def focus(coarse, fine, mol, want_faces=False, reslog_cap=8192):
+def focus(coarse, fine, mol, want_faces=False, reslog_cap=8192, dropin=False):
     """Two-block focusing chain (coarse solve, then the bcfl-focus block whose
     faces and external energy come from it), computed by the reference.
 
@@ -106,7 +118,7 @@ def focus(coarse, fine, mol, want_faces=False, reslog_cap=8192):
     faces = np.zeros(nfaces) if want_faces else None
     out = np.zeros(16)
     reslog = np.zeros(reslog_cap)
-    rc = lib().ref_pmg_focus(ctypes.byref(coarse), ctypes.byref(fine), mol.natoms, _ptr(xyz), _ptr(q),
+    rc = lib(dropin).ref_pmg_focus(ctypes.byref(coarse), ctypes.byref(fine), mol.natoms, _ptr(xyz), _ptr(q),
                   _ptr(r), _ptr(u), _ptr(faces), _ptr(out), _ptr(reslog), reslog_cap, 0)
     if rc != 1:
         raise RuntimeError("reference focusing run failed")
@@ -168,3 +180,22 @@ def run_maps(params, mol, maps):
     f = fill.reshape(5, *shape)
     return {"u": u.reshape(shape), "energy_kT": out[0], "charge": f[0], "epsx": f[1],
             "epsy": f[2], "epsz": f[3], "kappa": f[4]}
+
+
+def chain(levels, mol, dropin=False):
+    """An mg-auto focusing chain (a list of pmgb_params, coarse first, the
+    later ones bcfl focus) run by the reference as main.c runs it.  Returns
+    the total energy (kT) of every level and the finest potential."""
+    from apbs_b200.synth import PmgbParams
+    arr = (PmgbParams * len(levels))(*levels)
+    xyz = np.ascontiguousarray(mol.xyz, dtype=np.float64).reshape(-1)
+    q = np.ascontiguousarray(mol.charge, dtype=np.float64)
+    r = np.ascontiguousarray(mol.radius, dtype=np.float64)
+    e = np.zeros(len(levels))
+    f = levels[-1]
+    u = np.zeros(f.nx * f.ny * f.nz)
+    rc = lib(dropin).ref_pmg_chain(ctypes.byref(arr), len(levels), mol.natoms, _ptr(xyz), _ptr(q),
+                                   _ptr(r), _ptr(e), _ptr(u))
+    if rc != 1:
+        raise RuntimeError("reference focusing chain failed")
+    return {"energies_kT": e, "u": u.reshape(f.nz, f.ny, f.nx)}

@@ -386,3 +386,78 @@ int ref_write_dx(int nx, int ny, int nz, double hx, double hy, double hz, double
     Vgrid_dtor(&grid);
     return 1;
 }
+
+/* An mg-auto chain of nlevel mg-manual blocks on one molecule as main.c
+ * runs the calculations NOsh_setupCalcMGAUTO makes of it
+ * (src/generic/nosh.c:1828-2101): level 0 with its own boundary condition,
+ * every later level focused on the one before (Vpmg_ctor with focusFlag = 1
+ * and pmgOLD = the previous Vpmg, which it destroys), each filled, solved,
+ * partitioned on its own box and its total energy taken (energyMG with
+ * calcenergy total, src/routines.c:1726-1801).  energies[l] = Vpmg_energy of
+ * level l in kT; u (optional) = the finest potential.  Returns 1 or 0. */
+int ref_pmg_chain(const pmgb_params *levels, int nlevel, int natoms, const double *xyz,
+                  const double *q, const double *r, double *energies, double *u) {
+    int i, l, rc;
+    double ionc[PMGB_MAXION], ionr[PMGB_MAXION], ionq[PMGB_MAXION];
+    double partMin[3], partMax[3];
+    Valist *alist;
+    MGparm *mg = VNULL;
+    Vpbe *pbe = VNULL;
+    Vpmgp *pmgp = VNULL;
+    Vpmg *pmg = VNULL;
+
+    if (nlevel < 1) return 0;
+    oracle_shim_set_verbose(0);
+    oracle_shim_set_log(VNULL, 0);
+    alist = make_alist(natoms, xyz, q, r);
+    for (l = 0; l < nlevel; l++) {
+        const pmgb_params *p = &levels[l];
+        MGparm *mg_l;
+        Vpbe *pbe_l;
+        Vpmgp *pmgp_l;
+        Vpmg *pmg_l;
+        if ((l == 0) == (p->bcfl == PMGB_BCFL_FOCUS)) return 0;
+        for (i = 0; i < p->nion && i < PMGB_MAXION; i++) {
+            ionc[i] = p->ion_conc[i];
+            ionr[i] = p->ion_radius[i];
+            ionq[i] = p->ion_q[i];
+        }
+        mg_l = make_mgparm(p);
+        pbe_l = Vpbe_ctor(alist, p->nion, ionc, ionr, ionq, p->temp, p->pdie, p->sdie,
+                          p->srad, l > 0, p->sdens, 0.0, 0.0, 0.0, 0.0);
+        if (pbe_l == VNULL) return 0;
+        pmgp_l = Vpmgp_ctor(mg_l);
+        if (p->itmax > 0) pmgp_l->itmax = p->itmax;
+        pmgp_l->bcfl = (Vbcfl)p->bcfl;
+        pmgp_l->xcent = p->center[0];
+        pmgp_l->ycent = p->center[1];
+        pmgp_l->zcent = p->center[2];
+        /* the focused constructor destroys the previous Vpmg */
+        pmg_l = Vpmg_ctor(pmgp_l, pbe_l, l > 0, pmg, mg_l, PCE_TOTAL);
+        if (pmgp != VNULL) Vpmgp_dtor(&pmgp);
+        if (pbe != VNULL) Vpbe_dtor(&pbe);
+        if (mg != VNULL) MGparm_dtor(&mg);
+        pmg = pmg_l;
+        pmgp = pmgp_l;
+        pbe = pbe_l;
+        mg = mg_l;
+        rc = Vpmg_fillco(pmg, (Vsurf_Meth)p->srfm, SWIN(p), (Vchrg_Meth)p->chgm, 0, VNULL, 0,
+                         VNULL, 0, VNULL, 0, VNULL, 0, VNULL, 0, VNULL);
+        if (rc != 1) return 0;
+        if (Vpmg_solve(pmg) != 1) return 0;
+        for (i = 0; i < 3; i++) {
+            partMin[i] = mg->center[i] - 0.5 * mg->glen[i];
+            partMax[i] = mg->center[i] + 0.5 * mg->glen[i];
+        }
+        Vpmg_setPart(pmg, partMin, partMax, mg->partDisjOwnSide);
+        energies[l] = Vpmg_energy(pmg, 1);
+    }
+    if (u) memcpy(u, pmg->u, sizeof(double) * levels[nlevel - 1].nx * levels[nlevel - 1].ny *
+                                 levels[nlevel - 1].nz);
+    Vpmg_dtor(&pmg);
+    Vpmgp_dtor(&pmgp);
+    Vpbe_dtor(&pbe);
+    MGparm_dtor(&mg);
+    Valist_dtor(&alist);
+    return 1;
+}
