@@ -656,24 +656,37 @@ void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz,
 // weight (Vpmg_setPart's atom rule for the domain box, vpmg.c:673-720);
 // per-block partial sums, then one block adds them.
 // ---------------------------------------------------------------------------
+struct QfBox {
+  int complement;   // weight 1 - membership of [lo, hi] instead of membership of the domain
+  double lo[3], hi[3];
+};
+
 __global__ void __launch_bounds__(256) k_qf_point(FillGeom G, int natoms,
                                                  const double* __restrict__ xyz,
                                                  const double* __restrict__ q,
-                                                 const double* __restrict__ u, double* part) {
+                                                 const double* __restrict__ u, double* part,
+                                                 QfBox box) {
   __shared__ double sh[32];
   const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
   double acc = 0.0;
   for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < natoms; a += gridDim.x * blockDim.x) {
     const double* pos = xyz + 3 * a;
+    // Vpmg_setPart's atom weight (vpmg.c:680-723, no disjoint sides)
     double part_id = 1.0;
     for (int d = 0; d < 3; d++) {
-      const double lo = G.xmin[d], hi = G.xmax[d];
+      const double lo = box.complement ? box.lo[d] : G.xmin[d];
+      const double hi = box.complement ? box.hi[d] : G.xmax[d];
       double ok;
       if ((pos[d] < hi) && (pos[d] > lo)) ok = 1;
       else if (fabs(pos[d] - lo) < 1.0e-12) ok = 1;
       else if (fabs(pos[d] - hi) < 1.0e-12) ok = 1;
       else ok = 0;
       part_id = (d == 0) ? ok : part_id * ok;
+    }
+    if (box.complement) {
+      // extEnergy's flip (vpmg.c:2533-2534)
+      if (part_id > 1.0e-9) part_id = 1.0;
+      part_id = (1 - part_id) * (1.0 * 1.0 * 1.0);
     }
     const double fi = (pos[0] - G.xmin[0]) / G.h[0];
     const double fj = (pos[1] - G.xmin[1]) / G.h[1];
@@ -707,9 +720,16 @@ __global__ void k_qf_point_final(const double* __restrict__ part, int nparts, do
 }
 
 void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                     const double* q, const double* u, double* part, double* out) {
+                     const double* q, const double* u, double* part, double* out,
+                     const double* box) {
   const int nb = std::max(1, std::min(1184, (natoms + 255) / 256));
-  k_qf_point<<<nb, 256, 0, s>>>(G, natoms, xyz, q, u, part);
+  QfBox b;
+  b.complement = box ? 1 : 0;
+  for (int d = 0; d < 3; d++) {
+    b.lo[d] = box ? box[d] : 0.0;
+    b.hi[d] = box ? box[3 + d] : 0.0;
+  }
+  k_qf_point<<<nb, 256, 0, s>>>(G, natoms, xyz, q, u, part, b);
   k_qf_point_final<<<1, 256, 0, s>>>(part, nb, out);
 }
 

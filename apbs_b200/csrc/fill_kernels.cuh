@@ -45,8 +45,15 @@ void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz,
                 const double* r);
 // sum over atoms of the trilinearly interpolated potential x charge (part:
 // up to 1184 doubles of scratch; out: one double)
+// Vpmg_qfEnergyPoint (vpmg.c:1704-1789): sum of q u(atom) over the atoms on
+// the mesh, each weighted by its partition weight.  With box == NULL the
+// weight is the atom's membership of the calculation's own domain
+// (Vpmg_setPart with the mg-manual partition); with box = {lo[3], hi[3]} it
+// is 1 minus the membership of that box, the flipped weight extEnergy gives
+// the coarse calculation of a focusing step (vpmg.c:2525-2535).
 void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                     const double* q, const double* u, double* part, double* out);
+                     const double* q, const double* u, double* part, double* out,
+                     const double* box = nullptr);
 void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                         const double* q, double zmagic, double* charge);
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,

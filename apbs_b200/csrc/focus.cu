@@ -142,8 +142,11 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
     set_error("pmgb_focus: the fine calculation must be created with bcfl focus");
     return 0;
   }
-  if (fine->p.chgm != PMGB_CHGM_SPL2 || coarse->p.chgm != PMGB_CHGM_SPL2) {
-    set_error("pmgb_focus: focusing is implemented for chgm spl2");
+  // the coarse charge energy outside the fine box: a volume sum of the
+  // charge map (spl2, or a charge map) or a point sum at the atoms (spl0)
+  const int coarse_point_qf = coarse->p.chgm == PMGB_CHGM_TRIL && !uses_charge_map(coarse);
+  if (calc_energy && coarse_point_qf && (coarse->natoms <= 0 || !coarse->d_xyz)) {
+    set_error("pmgb_focus: chgm spl0 needs the coarse calculation's atom list (pmgb_fillco)");
     return 0;
   }
   if (!coarse->solved) {
@@ -210,6 +213,7 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
 
   double ext[3] = {0.0, 0.0, 0.0};
   double sums[4] = {0.0, 0.0, 0.0, 0.0};
+  double qf_point = 0.0;
   if (calc_energy) {
     // extEnergy: coarse weights of the fine box, flipped (vpmg.c:2462-2509)
     const int nw = pc.nx + pc.ny + pc.nz;
@@ -254,6 +258,16 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
     note_launches(2);
     FCK(cudaMemcpyAsync(sums, coarse->scal + S_E0, 4 * sizeof(double), cudaMemcpyDeviceToHost,
                         st));
+    if (coarse_point_qf) {
+      // Vpmg_qfEnergyPoint of the coarse calculation with the atoms' flipped
+      // partition weights (vpmg.c:2518-2539)
+      const double box[6] = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]};
+      launch_qf_point(st, coarse->G, coarse->natoms, coarse->d_xyz, coarse->d_q,
+                      coarse->lev[0].x, coarse->part, coarse->scal + S_TMP, box);
+      note_launches(2);
+      FCK(cudaMemcpyAsync(&qf_point, coarse->scal + S_TMP, sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+    }
   }
   int status = 0;
   FCK(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -280,8 +294,8 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
       qm = qm / coarse->zmagic;
       qm += coarse->ext_qm;
     }
-    // Vpmg_qfEnergyVolume (vpmg.c:1883-1888)
-    double qf = sums[0] * h3x * h3y * h3z / coarse->zmagic;
+    // Vpmg_qfEnergyVolume (vpmg.c:1883-1888) or Vpmg_qfEnergyPoint
+    double qf = coarse_point_qf ? qf_point : sums[0] * h3x * h3y * h3z / coarse->zmagic;
     qf += coarse->ext_qf;
     // Vpmg_dielEnergy (vpmg.c:1333-1337)
     double di = 0.5 * sums[1] * h3x * h3y * h3z;

@@ -7,9 +7,7 @@
 // global sums (norms, dot products) are reassociated (tree reductions).
 #include <cooperative_groups.h>
 
-#include "gs7_pipe.cuh"
-#include "gs7_march.cuh"
-#include "gs7_sweep.cuh"
+#include "gs7_rb.cuh"
 #include "mg_kernels.cuh"
 
 namespace cg = cooperative_groups;
@@ -377,32 +375,40 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {8, 0, 0, 0, 0, 0, 16, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
+int g_tune[16] = {0, 0, 0, 0, 0, 0, 8, 0, 70000, 0, 2, 2, 0, 0, 0, 0};
 
-int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
-                       int kernel, int* err) {
-  Gs7Sweep<double> a;
-  a.g = g;
-  a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
-  a.cc = cc; a.fc = fc; a.xin = xin; a.xout = xout;
-  a.c1 = first_parity;
-  a.kchunk = kchunk;
-  a.err = err;
-  return launch_gs7_sweep_kernel<double>(s, a, kernel) == cudaSuccess;
+                       int shape) {
+  Gs7Rb<double> a;
+  a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
+  a.D = diag; a.f = fc; a.xin = xin; a.xout = xout;
+  a.nx = g.nx; a.S = g.nx * g.ny; a.nz = g.nz;
+  a.kchunk = kchunk > 0 ? kchunk : 8;
+  return launch_gs7_rb<double>(s, a, first_parity, shape) == cudaSuccess;
 }
 
+int gs7_sweep_supported(Grid g) {
+  return (g.nx & 1) && (g.ny & 1) && (double)g.n() * sizeof(double) < 2147483647.0;
+}
 
-int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                      double* x, double* r, int nsweep, int first_parity, const int* tune) {
-  Gs7Args<double> a;
-  a.g = g;
-  a.oC = op.c[OC]; a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
-  a.cc = cc; a.fc = fc; a.x = x; a.r = r;
-  a.nhalf = 2 * nsweep;
-  a.first_parity = first_parity;
-  a.chunk = tune[0] > 0 ? tune[0] : 8;
-  return launch_gs7_pipe<double>(s, a, tune[1]) == cudaSuccess;
+// D = oC + cc on interior points (the FP64 sum the smoother divides by),
+// 1 on boundary points (the single-pass sweep's boundary update is then 0/1)
+__global__ void k_diag(Grid g, const double* __restrict__ oC, const double* __restrict__ cc,
+                       double* D) {
+  const size_t n = g.n();
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const int j = (int)((q / g.nx) % g.ny);
+    const int k = (int)(q / ((size_t)g.nx * g.ny));
+    const bool inner = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
+    D[q] = inner ? oC[q] + cc[q] : 1.0;
+  }
+}
+
+void launch_diag(cudaStream_t s, Grid g, const double* oC, const double* cc, double* D) {
+  k_diag<<<blocks_for(g.n()), kThreads, 0, s>>>(g, oC, cc, D);
 }
 
 void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,

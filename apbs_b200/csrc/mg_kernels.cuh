@@ -22,15 +22,15 @@ void launch_interp_axpy(cudaStream_t s, Grid gc, const double* xc, Grid gf, doub
 // ---- stencils ----------------------------------------------------------------
 void launch_gs7_colour(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, int parity);
-// nsweep red-black sweeps (+ residual into r unless r is null) as one
-// temporally blocked cooperative kernel; planes per chunk from
-// PMGB_GS7_CHUNK (default 8).
-// one full red-black sweep in one pass, xin -> xout (boundaries of both zero)
-int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+// one full red-black sweep in one pass, xin -> xout (boundaries of both
+// zero; diag from launch_diag; shape: PMGB_TUNE_GS7_SWEEP_SHAPE)
+int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
-                       int kernel, int* err = nullptr);
-int launch_gs7_smooth(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
-                      double* x, double* r, int nsweep, int first_parity, const int* tune);
+                       int shape);
+// the single-pass sweep handles this grid (odd nx and ny, 32-bit offsets)
+int gs7_sweep_supported(Grid g);
+// D = oC + cc inside, 1 on the boundary
+void launch_diag(cudaStream_t s, Grid g, const double* oC, const double* cc, double* D);
 extern int g_tune[16];
 void launch_resid(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                   const double* x, double* r);

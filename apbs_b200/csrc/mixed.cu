@@ -21,9 +21,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "gs7_pipe.cuh"
-#include "gs7_march.cuh"
-#include "gs7_sweep.cuh"
+#include "gs7_rb.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
 
@@ -73,6 +71,7 @@ struct MixedState {
   float* r;      // fine-sized FP32 scratch
   float* w2;     // fine-sized FP32 scratch
   float* xs;     // second fine FP32 iterate of the single-pass sweep (zero boundary)
+  float* d32;    // fine-level oC + cc in FP32, 1 on the boundary (single-pass sweep)
   double* dense;  // coarsest dense factor (n x n)
   double* dvec;   // coarsest rhs / solution in FP64
   int nd;
@@ -1120,20 +1119,26 @@ int gs27_mc(cudaStream_t s, const MLevel& L, float* x, int nsweep, int reverse, 
   return 1;
 }
 
+// FP32 single-pass sweep arguments for the fine level (xin, xout set by the caller)
+Gs7Rb<float> rb_f32(const MLevel& F, const float* d32, const int* tune) {
+  Gs7Rb<float> a;
+  a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
+  a.D = d32; a.f = F.w0;
+  a.nx = F.g.nx; a.S = F.g.nx * F.g.ny; a.nz = F.g.nz;
+  a.kchunk = tune[6] > 0 ? tune[6] : 8;
+  a.xin = nullptr; a.xout = nullptr;
+  return a;
+}
+
 cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
-                    float* xs, const int* tune) {
-  if (!tune[3] && tune[5] == 2 && tune[11] == 2 && xs) {
+                    float* xs, const float* d32, const int* tune) {
+  if (tune[5] == 2 && tune[11] == 2 && xs && d32 && (F.g.nx & 1) && (F.g.ny & 1)) {
     // two single-pass sweeps x -> xs -> x, then the residual
-    Gs7Sweep<float> a;
-    a.g = F.g;
-    a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
-    a.cc = F.cc; a.fc = F.w0;
-    a.c1 = first_parity;
-    a.kchunk = tune[6];
+    Gs7Rb<float> a = rb_f32(F, d32, tune);
     a.xin = x; a.xout = xs;
-    cudaError_t e = launch_gs7_sweep_kernel<float>(st, a, tune[12]);
+    cudaError_t e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
     a.xin = xs; a.xout = x;
-    if (e == cudaSuccess) e = launch_gs7_sweep_kernel<float>(st, a, tune[12]);
+    if (e == cudaSuccess) e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
     if (r && e == cudaSuccess) {
       const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
       k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, opf(F), F.cc, F.w0, x, r);
@@ -1141,29 +1146,33 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
     }
     return e;
   }
-  if (!tune[3] || tune[11] != 2) {
-    // colour passes: the sweeps, then the residual
-    const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
-    const OpF fo = opf(F);
-    for (int sw = 0; sw < tune[11]; sw++) {
-      k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, first_parity);
-      k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x,
-                                                         1 - first_parity);
-    }
-    if (r) {
-      const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
-      k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, r);
-    }
-    return cudaGetLastError();
+  // colour passes: the sweeps, then the residual
+  const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
+  const OpF fo = opf(F);
+  for (int sw = 0; sw < tune[11]; sw++) {
+    k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, first_parity);
+    k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x,
+                                                       1 - first_parity);
   }
-  Gs7Args<float> a;
-  a.g = F.g;
-  a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
-  a.cc = F.cc; a.fc = F.w0; a.x = x; a.r = r;
-  a.nhalf = 4;
-  a.first_parity = first_parity;
-  a.chunk = tune[0] > 0 ? tune[0] : 8;
-  return launch_gs7_pipe<float>(st, a, tune[1]);
+  if (r) {
+    const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
+    k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, r);
+  }
+  return cudaGetLastError();
+}
+
+// FP32 D = oC + cc inside, 1 on the boundary
+__global__ void k_diag_f32(Grid g, const float* __restrict__ oC, const float* __restrict__ cc,
+                           float* D) {
+  const size_t n = g.n();
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % g.nx);
+    const int j = (int)((q / g.nx) % g.ny);
+    const int k = (int)(q / ((size_t)g.nx * g.ny));
+    const bool inner = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
+    D[q] = inner ? oC[q] + cc[q] : 1.0f;
+  }
 }
 
 int falloc(float** p, size_t n) {
@@ -1212,6 +1221,7 @@ void mixed_destroy(MixedState* m) {
   if (m->r) cudaFree(m->r);
   if (m->w2) cudaFree(m->w2);
   if (m->xs) cudaFree(m->xs);
+  if (m->d32) cudaFree(m->d32);
   if (m->dense) cudaFree(m->dense);
   if (m->dvec) cudaFree(m->dvec);
   if (m->dinfo) cudaFree(m->dinfo);
@@ -1285,7 +1295,7 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
   m->stale = 1;
   const size_t nscr = m->lev[lo].g.n();
   if (!falloc(&m->r, nscr) || !falloc(&m->w2, nscr)) return 0;
-  if (lo == 0 && !falloc(&m->xs, nscr)) return 0;
+  if (lo == 0 && (!falloc(&m->xs, nscr) || !falloc(&m->d32, nscr))) return 0;
   const Grid gc = m->lev[nl - 1].g;
   m->nd = (gc.nx - 2) * (gc.ny - 2) * (gc.nz - 2);
   if (m->nd > 4096) {
@@ -1453,6 +1463,11 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
       to_f32(st, src, L.cc, L.g.n());
       note_launches(1);
     }
+    if (l == 0 && m->d32) {
+      // the FP32 single-pass sweep's divisor
+      k_diag_f32<<<blocks_for(L.g.n()), kThreads, 0, st>>>(L.g, L.op[OC], L.cc, m->d32);
+      note_launches(1);
+    }
     if (l == m->nlev - 1) {
       // dense factor of (A_c + cc) on the coarsest level
       const int nd = m->nd;
@@ -1528,11 +1543,11 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const OpF fo = opf(F);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, s->tune) != cudaSuccess) {
-    set_error("FP32 gs7 pipeline launch failed");
+  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, m->d32, s->tune) != cudaSuccess) {
+    set_error("FP32 fine smoother launch failed");
     return 0;
   }
-  k += (s->tune[3] && s->tune[11] == 2) ? 1 : 2 * s->tune[11] + 1;
+  k += 2 * s->tune[11] + 1;
   const int tf = m->tail_first > 0 ? m->tail_first : nl;
   for (int l = 1; l < tf; l++) {
     MLevel& C = m->lev[l];
@@ -1571,11 +1586,11 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
-      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, s->tune) != cudaSuccess) {
-        set_error("FP32 gs7 pipeline launch failed");
+      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, m->d32, s->tune) != cudaSuccess) {
+        set_error("FP32 fine smoother launch failed");
         return 0;
       }
-      k += (s->tune[3] && s->tune[11] == 2) ? 1 : 2 * s->tune[11];
+      k += 2 * s->tune[11];
     } else {
       if (!gs27_mc(st, P, P.x, s->tune[10], 1, k, s->tune[9])) return 0;
     }
@@ -1699,31 +1714,13 @@ int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
-  Gs7Sweep<float> a;
-  a.g = F.g;
-  a.oC = F.op[OC]; a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
-  a.cc = F.cc; a.fc = F.w0; a.xin = F.x; a.xout = m->xs;
-  a.c1 = 1;
-  a.kchunk = s->tune[6];
-  if (launch_gs7_sweep_kernel<float>(s->stream, a, s->tune[12]) != cudaSuccess) {
+  Gs7Rb<float> a = rb_f32(F, m->d32, s->tune);
+  a.xin = F.x; a.xout = m->xs;
+  if (launch_gs7_rb<float>(s->stream, a, 1, s->tune[12]) != cudaSuccess) {
     set_error("FP32 sweep launch failed");
     return 0;
   }
   *bytes = 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
-  return 1;
-}
-
-// One FP32 fine smoothing call (2 sweeps + residual) for kernel timing:
-// (2 x 28 + 28) B per point.
-int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes) {
-  if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
-  MixedState* m = s->mixed;
-  MLevel& F = m->lev[0];
-  if (gs7_f32(s->stream, F, F.x, m->r, 1, m->xs, s->tune) != cudaSuccess) {
-    set_error("FP32 gs7 pipeline launch failed");
-    return 0;
-  }
-  *bytes = 3.0 * 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   return 1;
 }
 

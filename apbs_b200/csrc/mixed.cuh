@@ -16,7 +16,6 @@ int mixed_newton_inner(pmgb_solver* s, double errtol_s);
 int newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed);
 void set_error(const char* fmt, ...);
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
-int mixed_time_gs7_pipe(pmgb_solver* s, double* bytes);
 int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes);
 int mixed_time_tail(pmgb_solver* s, double* bytes);
 // FP64 path, LPBE: exact-to-round-off solve of the FP64 coarsest level

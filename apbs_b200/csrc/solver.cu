@@ -192,14 +192,6 @@ float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-// Error word of the bounded device waits for a fine sweep launch: the sweeps
-// staged by bulk copies (sweep kernels 8 and 9) count waits that ran out in
-// the same word as the plane wavefront, which every residual read checks.
-static int* wave_err(pmgb_solver* s) {
-  if (s->tune[12] == 8 || s->tune[12] == 9) s->wave_used = 1;
-  return reinterpret_cast<int*>(s->d_wave);
-}
-
 int read_scalar(pmgb_solver* s, int slot, double* v) {
   CK(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   // a plane-wavefront wait that ran out leaves the iterates undefined: stop
@@ -209,7 +201,7 @@ int read_scalar(pmgb_solver* s, int slot, double* v) {
     CK(cudaMemcpyAsync(&nerr, s->d_wave, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   if (nerr) {
-    set_error("%d bounded device waits ran out (gs27 plane wavefront or staged gs7 sweep)", nerr);
+    set_error("%d bounded device waits ran out (gs27 plane wavefront)", nerr);
     return 0;
   }
   return 1;
@@ -337,6 +329,7 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     s->plan[l] = plan_for(L.g, s->tune);
   }
   ok &= dalloc(&s->w1, n) && dalloc(&s->w2, n) && dalloc(&s->w3, n) && dalloc(&s->xs, n);
+  ok &= dalloc(&s->dg[0], n) && dalloc(&s->dg[1], n);
   ok &= dalloc(&s->nw_r0, n) && dalloc(&s->nw_ws, n) && dalloc(&s->nw_keepx, n) &&
         dalloc(&s->nw_keepr, n);
   ok &= dalloc(&s->part, 4 * 1184 + 64) && dalloc(&s->scal, S_COUNT);
@@ -526,6 +519,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
     dfree(L.cc); dfree(L.fc); dfree(L.x); dfree(L.w0); dfree(L.cp); dfree(L.rhs); dfree(L.xt);
   }
   dfree(s->w1); dfree(s->w2); dfree(s->w3); dfree(s->xs);
+  dfree(s->dg[0]); dfree(s->dg[1]);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts); dfree(s->d_wave); dfree(s->d_forces);
   dfree(s->d_opptrs);
@@ -862,7 +856,9 @@ static int build_ops(pmgb_solver* s) {
   launch_build_fine(st, F.g, s->xf, s->yf, s->zf, s->epsx, s->epsy, s->epsz, s->ccf,
                     s->charge, s->gx, s->gy, s->gz, F.op[OC], F.op[OE], F.op[ON], F.op[UC],
                     F.cc, F.fc);
-  note_launches(2);
+  // the smoother's divisor oC + cc, summed once per operator
+  launch_diag(st, F.g, F.op[OC], F.cc, s->dg[0]);
+  note_launches(3);
   for (int l = 1; l < s->nlev; l++) {
     Level& C = s->lev[l];
     Level& P = s->lev[l - 1];
@@ -938,15 +934,11 @@ static int vcycle_body(pmgb_solver* s, int newton) {
   auto CC = [&](int l) -> double* { return newton ? s->lev[l].cp : s->lev[l].cc; };
   auto X = [&](int l) -> double* { return newton ? s->lev[l].xt : s->lev[l].x; };
   double* FC0 = newton ? F.rhs : F.fc;
+  const double* DG = s->dg[newton ? 1 : 0];
+  const int colour_passes = s->tune[5] == 1 || !gs7_sweep_supported(F.g);
   long long k = 0;
   // nu1 = 2 pre-smoothings on the fine level, then the residual
-  if (s->tune[3]) {
-    if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), s->w1, 2, 1, s->tune)) {
-      set_error("gs7 pipeline launch failed");
-      return 0;
-    }
-    k += 1;
-  } else if (s->tune[5] == 1) {
+  if (colour_passes) {
     for (int sw = 0; sw < 2; sw++) {
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
       launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
@@ -956,8 +948,8 @@ static int vcycle_body(pmgb_solver* s, int newton) {
     k += 1;
   } else {
     // two single-pass sweeps, x -> xs -> x
-    if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 1, s->tune[6], s->tune[12], wave_err(s)) ||
-        !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 1, s->tune[6], s->tune[12], wave_err(s))) {
+    if (!launch_gs7_sweep64(st, F.g, F.ops(), DG, FC0, X(0), s->xs, 1, s->tune[6], s->tune[12]) ||
+        !launch_gs7_sweep64(st, F.g, F.ops(), DG, FC0, s->xs, X(0), 1, s->tune[6], s->tune[12])) {
       set_error("gs7 sweep launch failed");
       return 0;
     }
@@ -1012,21 +1004,15 @@ static int vcycle_body(pmgb_solver* s, int newton) {
                        s->scal + S_XDEN_L + l);
     k += 6;
     if (l == 0) {
-      if (s->tune[3]) {
-        if (!launch_gs7_smooth(st, F.g, F.ops(), CC(0), FC0, X(0), nullptr, 2, 0, s->tune)) {
-          set_error("gs7 pipeline launch failed");
-          return 0;
-        }
-        k += 1;
-      } else if (s->tune[5] == 1) {
+      if (colour_passes) {
         for (int sw = 0; sw < 2; sw++) {
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 0);
           launch_gs7_colour(st, F.g, F.ops(), CC(0), FC0, X(0), 1);
           k += 2;
         }
       } else {
-        if (!launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, X(0), s->xs, 0, s->tune[6], s->tune[12], wave_err(s)) ||
-            !launch_gs7_sweep64(st, F.g, F.ops(), CC(0), FC0, s->xs, X(0), 0, s->tune[6], s->tune[12], wave_err(s))) {
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), DG, FC0, X(0), s->xs, 0, s->tune[6], s->tune[12]) ||
+            !launch_gs7_sweep64(st, F.g, F.ops(), DG, FC0, s->xs, X(0), 0, s->tune[6], s->tune[12])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1133,7 +1119,8 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
     // Vgetjac (newtond.c:550-598)
     launch_copy_interior(st, F.g, s->nw_r0, F.rhs);
     launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
-    note_launches(2);
+    launch_diag(st, F.g, F.op[OC], F.cp, s->dg[1]);
+    note_launches(3);
     for (int l = 1; l < s->nlev; l++) {
       launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].rhs, s->lev[l].g, s->lev[l].rhs);
       launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].cp, s->lev[l].g, s->lev[l].cp);
@@ -1206,7 +1193,7 @@ static int wave_check(pmgb_solver* s) {
     // the counters of the levels may now disagree: restart them all
     CK(cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    set_error("%d bounded device waits ran out (gs27 plane wavefront or staged gs7 sweep)", nerr);
+    set_error("%d bounded device waits ran out (gs27 plane wavefront)", nerr);
     return 0;
   }
   return 1;
@@ -1425,7 +1412,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
     set_error("pmgb_time_kernel: solve first");
     return 0;
   }
-  if ((which == PMGB_K_GS7_FP32 || which == PMGB_K_GS7_PIPE_FP32 ||
+  if ((which == PMGB_K_GS7_FP32 ||
        which == PMGB_K_VCYCLE_TAIL || which == PMGB_K_GS7_SWEEP_FP32) &&
       s->precision != PMGB_MIXED) {
     set_error("pmgb_time_kernel: kernel %d belongs to the mixed-precision path", which);
@@ -1471,24 +1458,13 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
       case PMGB_K_GS7_FP32:
         if (!mixed_time_gs7(s, r & 1, &b)) return 0;
         break;
-      case PMGB_K_GS7_PIPE_FP64:
-        if (!launch_gs7_smooth(st, F.g, F.ops(), F.cc, F.fc, F.x, s->w1, 2, 1, s->tune)) {
-          set_error("gs7 pipeline launch failed");
-          return 0;
-        }
-        // two sweeps (56 B per point each) + residual (56 B per point)
-        b = 3.0 * 56.0 * fint;
-        break;
-      case PMGB_K_GS7_PIPE_FP32:
-        if (!mixed_time_gs7_pipe(s, &b)) return 0;
-        break;
       case PMGB_K_VCYCLE_TAIL:
         if (!mixed_time_tail(s, &b)) return 0;
         break;
       case PMGB_K_GS7_SWEEP_FP64:
-        // one full sweep: oE oN uC oC cc fc and x read, x written: 56 B per point
-        if (!launch_gs7_sweep64(st, F.g, F.ops(), F.cc, F.fc, (r & 1) ? s->xs : F.x,
-                                (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12], wave_err(s))) {
+        // one full sweep: oE oN uC D=oC+cc fc and x read, x written: 56 B per point
+        if (!launch_gs7_sweep64(st, F.g, F.ops(), s->dg[0], F.fc, (r & 1) ? s->xs : F.x,
+                                (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12])) {
           set_error("gs7 sweep launch failed");
           return 0;
         }
@@ -1540,8 +1516,9 @@ extern "C" int pmgb_solver_set_tuning(pmgb_solver* s, int key, int value) {
     set_error("pmgb_solver_set_tuning: sweeps must be 1..4");
     return 0;
   }
-  if (key == PMGB_TUNE_CG_CLUSTER && value != 0 && value != 4 && value != 8 && value != 16) {
-    set_error("pmgb_solver_set_tuning: CG cluster must be 0, 4, 8 or 16");
+  if (key == PMGB_TUNE_CG_CLUSTER && value != 0 && value != 1 && value != 4 && value != 8 &&
+      value != 16) {
+    set_error("pmgb_solver_set_tuning: CG cluster must be 0, 1, 4, 8 or 16");
     return 0;
   }
   if (s->tune[key] == value) return 1;

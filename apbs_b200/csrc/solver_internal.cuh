@@ -92,6 +92,8 @@ struct pmgb_solver {
   Level lev[12];
   double *w1, *w2, *w3;
   double* xs;  // second fine iterate for the out-of-place sweep kernel (zero boundary)
+  double* dg[2];  // fine-level oC + cc (dg[0]) and oC + c'(u) of the Newton system
+                  // (dg[1]), 1 on the boundary: the single-pass sweep's divisor
   double *nw_r0, *nw_ws, *nw_keepx, *nw_keepr;  // Newton work vectors
   double* part;
   double* scal;

@@ -26,18 +26,17 @@ FP64 = 0
 MIXED = 1
 
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
-K_GS7_PIPE_FP64, K_GS7_PIPE_FP32, K_VCYCLE_TAIL = 5, 6, 7
+K_VCYCLE_TAIL = 7
 K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
 DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX, DX_DIELY, DX_DIELZ = range(6)
 MAP_DIELX, MAP_DIELY, MAP_DIELZ, MAP_KAPPA, MAP_CHARGE, MAP_POT = range(6)
-TUNE_GS7_CHUNK, TUNE_GS7_BLOCKS_PER_SM, TUNE_GS27_CLUSTER, TUNE_GS7_PIPELINED = 0, 1, 2, 3
+TUNE_GS27_CLUSTER = 2
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5
 TUNE_GS7_SWEEP_KCHUNK, TUNE_GS27_CLUSTER_MID, TUNE_TAIL_MAX_POINTS = 6, 7, 8
 TUNE_MC_COOPERATIVE = 9
 TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS = 10, 11
-TUNE_GS7_SWEEP_KERNEL = 12
-TUNE_GS7_SWEEP_STAGED = TUNE_GS7_SWEEP_KERNEL
+TUNE_GS7_SWEEP_SHAPE = 12
 TUNE_GS27_PLANES = 13
 TUNE_CG_CLUSTER = 14
 TUNE_GS27_PLANES_POLL = 15

@@ -307,7 +307,7 @@ def main():
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="override one launch-shape tunable of the benchmark calculations "
                          "after the tuning table (names as in the JSON line's config.tuning, "
-                         "e.g. gs7_sweep_kernel=8)")
+                         "e.g. gs7_sweep_shape=1)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -487,8 +487,8 @@ def main():
                 "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs, burst copy)"}
     # the fine-level smoothers (HBM-bound), FP64 and FP32
     smoothers = {}
-    for nm, sv, k in (("k_gs7_sweep<double>", solvers["fp64"], vpmg.K_GS7_SWEEP_FP64),
-                      ("k_gs7_sweep<float>", solvers["mixed"], vpmg.K_GS7_SWEEP_FP32),
+    for nm, sv, k in (("k_gs7_rb<double>", solvers["fp64"], vpmg.K_GS7_SWEEP_FP64),
+                      ("k_gs7_rb<float>", solvers["mixed"], vpmg.K_GS7_SWEEP_FP32),
                       ("k_gs7_colour", solvers["fp64"], vpmg.K_GS7_FP64),
                       ("k_gs7_f32", solvers["mixed"], vpmg.K_GS7_FP32)):
         ms_k, b_k = sv.time_kernel(k, 20)

@@ -206,8 +206,7 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_RESID_FP64 2  /* fine-level 7-point residual */
 #define PMGB_K_GS7_FP32 3    /* fine-level FP32 7-point GS half-sweep (mixed) */
 #define PMGB_K_CG_COARSE 4   /* coarsest-level CG (NPBE), up to 100 iterations */
-#define PMGB_K_GS7_PIPE_FP64 5  /* fine smoothing call: 2 sweeps + residual, FP64 */
-#define PMGB_K_GS7_PIPE_FP32 6  /* fine smoothing call: 2 sweeps + residual, FP32 */
+/* 5 and 6 are not used */
 #define PMGB_K_VCYCLE_TAIL 7    /* mixed: coarse-level V-cycle tail (one cluster kernel) */
 #define PMGB_K_GS7_SWEEP_FP64 8 /* fine-level 7-point GS, one full sweep in one pass, FP64 */
 #define PMGB_K_GS7_SWEEP_FP32 9 /* the same, FP32 (mixed) */
@@ -218,18 +217,16 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
  * The autotuner (apbs_b200/autotune.py) times whole solves per grid shape
  * and keeps the best values in a table.  No key changes a result beyond
  * round-off; the FP64 smoother and wavefront keys change none at all. */
-#define PMGB_TUNE_GS7_CHUNK 0          /* planes per pipeline chunk (default 8) */
-#define PMGB_TUNE_GS7_BLOCKS_PER_SM 1  /* CTAs per SM of the pipelined smoother (0 = max) */
+/* keys 0, 1 and 3 are not used */
 #define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 on levels with
                                           >= 60 interior points per axis (0 = device max) */
-#define PMGB_TUNE_GS7_PIPELINED 3      /* 1: temporally blocked fine smoother, 0: colour passes */
 #define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded
                                           Cholesky of the reference, 0: exact refinement
                                           above 512 unknowns */
 #define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
                                           kernel, FP32 one launch per colour), 1 = one launch
                                           per colour, 2 = single-pass sweeps in FP32 too */
-#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 16) */
+#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 8) */
 #define PMGB_TUNE_GS27_CLUSTER_MID 7   /* the same as key 2 for levels with 28-59 interior
                                           points per axis (0 = 8) */
 #define PMGB_TUNE_TAIL_MAX_POINTS 8    /* mixed: largest level (interior points) run inside
@@ -240,25 +237,18 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_MIXED_COARSE_SWEEPS 10 /* mixed: 8-colour GS sweeps before and after each
                                             coarse correction on 27-point levels (default 2) */
 #define PMGB_TUNE_MIXED_FINE_SWEEPS 11 /* mixed: red-black sweeps on the fine level (default 2) */
-#define PMGB_TUNE_GS7_SWEEP_KERNEL 12 /* single-pass sweep kernel: 0 = ring tiles, 1 = ring
-                                          tiles staged through shared memory by asynchronous
-                                          copies, 2 = one thread per column marching up k on
-                                          32x16 tiles, 3 = the same on 32x8 tiles, 4 = whole-row
-                                          tiles of 16-byte (red, black) pairs, 5 = the same with
-                                          the next plane loaded ahead, 6 and 7 = pair tiles of 4
-                                          and 5 rows, 8 and 9 = FP64 pair tiles whose plane rows
-                                          are staged by bulk asynchronous copies (4 x planes and
-                                          2 coefficient planes resident, or 5 and 3; FP32 runs
-                                          4).  Pair kernels need odd nx and ny, as PMG grids
-                                          have; other grids run 0. */
-#define PMGB_TUNE_GS7_SWEEP_STAGED PMGB_TUNE_GS7_SWEEP_KERNEL
+#define PMGB_TUNE_GS7_SWEEP_SHAPE 12 /* single-pass sweep launch shape: bits 0-3 threads per
+                                          CTA (0 = 256, 1 = 512, 2 = 1024), bits 4-7 pair
+                                          slots per thread (0 = 2); a CTA owns a flat range
+                                          of 2 x (slots - nx - 3) points of each plane */
 #define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
                                           synchronised with its neighbour planes on every
                                           level whose planes fit on the device, 1 = one
                                           cluster with a barrier per wavefront everywhere */
 #define PMGB_TUNE_CG_CLUSTER 14       /* coarsest-level CG of the FP64 NPBE path: CTAs per
                                           cluster of the slab kernel (0 = smallest that fits;
-                                          4, 8 or 16) */
+                                          4, 8 or 16); 1 = the strided cluster kernel that
+                                          levels too large for slabs use */
 #define PMGB_TUNE_GS27_PLANES_POLL 15 /* plane-parallel GS27: 0 = one thread of a CTA waits
                                           for the neighbour planes, then a block barrier;
                                           1 = every thread waits itself */

@@ -8,8 +8,8 @@ import pytest
 from apbs_b200 import autotune, synth
 from apbs_b200.vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
                             TUNE_GS27_PLANES, TUNE_GS27_PLANES_POLL, TUNE_GS7_COLOUR_PASSES,
-                            TUNE_GS7_SWEEP_KCHUNK,
-                            TUNE_TAIL_MAX_POINTS, Vpmg)
+                            TUNE_GS7_SWEEP_KCHUNK, TUNE_GS7_SWEEP_SHAPE,
+                            TUNE_TAIL_MAX_POINTS, Vpmg, get_tuning)
 
 pytestmark = pytest.mark.gpu
 
@@ -33,7 +33,9 @@ def test_fp64_launch_shapes_do_not_change_the_solve():
     for tune in ({TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2}, {TUNE_GS27_PLANES_POLL: 1},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER: 4},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER_MID: 16},
-                 {TUNE_GS7_SWEEP_KCHUNK: 8}, {TUNE_GS7_COLOUR_PASSES: 1}):
+                 {TUNE_GS7_SWEEP_KCHUNK: 3}, {TUNE_GS7_SWEEP_KCHUNK: 32},
+                 {TUNE_GS7_SWEEP_SHAPE: 1}, {TUNE_GS7_SWEEP_SHAPE: 2},
+                 {TUNE_GS7_SWEEP_SHAPE: 0x41}, {TUNE_GS7_COLOUR_PASSES: 1}):
         e, u, h = _solve(p, m, FP64, tune)
         assert e == e0 and np.array_equal(u, u0) and np.array_equal(h, h0), tune
 
@@ -51,9 +53,10 @@ def test_tuning_is_per_calculation():
     m = synth.cluster(200, 9.0, seed=3)
     p = synth.mg_manual(65, 0.5, m.center())
     with Vpmg(p, FP64) as a, Vpmg(p, FP64) as b:
-        a.set_tuning(TUNE_GS7_SWEEP_KCHUNK, 8)
-        assert a.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == 8
-        assert b.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == 16
+        default = get_tuning(TUNE_GS7_SWEEP_KCHUNK)
+        a.set_tuning(TUNE_GS7_SWEEP_KCHUNK, default + 4)
+        assert a.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == default + 4
+        assert b.get_tuning(TUNE_GS7_SWEEP_KCHUNK) == default
         for s in (a, b):
             s.fillco(m)
             s.solve()

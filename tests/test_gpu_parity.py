@@ -126,45 +126,53 @@ def test_exact_coarse_solve_matches_band():
 
 
 def test_single_pass_sweep_matches_colour_passes():
-    """The fine smoother's single-pass sweep kernels (ring tiles, the default;
-    ring tiles staged by cp.async; one thread per column marching up k, on
-    32x16 and 32x8 tiles; whole-row pair tiles, with and without the next
-    plane's coefficients loaded ahead) and the one-launch-per-colour kernels compute the
-    same red-black sweep: bitwise equal FP64 solves, and bitwise equal FP32
-    inner cycles of the mixed path."""
-    from apbs_b200.vpmg import (MIXED, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KERNEL,
-                                TUNE_MIXED_FINE_SWEEPS, get_tuning, set_tuning)
+    """The fine smoother's single-pass sweep (gs7_rb.cuh: flat pair slots,
+    the first colour of the next plane in a shared-memory ring) computes the
+    same red-black sweep as one launch per colour: bitwise equal FP64 solves
+    (LPBE and NPBE) for every launch shape and plane chunk, including ranges
+    that split rows and chunks of one plane.  In FP32 (the mixed path's
+    inner cycles) every shape gives the same iterates and the solve meets
+    the mixed-precision tolerance."""
+    from apbs_b200.vpmg import (MIXED, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK,
+                                TUNE_GS7_SWEEP_SHAPE, TUNE_MIXED_FINE_SWEEPS)
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
-    out = {}
-    old = get_tuning(TUNE_GS7_COLOUR_PASSES)
-    kernels = (0, 1, 2, 3, 4, 5, 6, 7, 8, 9)
-    try:
-        for npbe in (False, True):
-            p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
-            for passes, kern in ((1, 0),) + tuple((0, k) for k in kernels):
-                set_tuning(TUNE_GS7_COLOUR_PASSES, passes)
-                with Vpmg(p, FP64) as pmg:
-                    pmg.set_tuning(TUNE_GS7_SWEEP_KERNEL, kern)
-                    pmg.fillco(m)
-                    pmg.solve()
-                    out[(npbe, passes, kern)] = (pmg.u, pmg.residual_history())
-    finally:
-        set_tuning(TUNE_GS7_COLOUR_PASSES, old)
+    shapes = ((0, 8), (1, 8), (2, 8), (0x41, 8), (0, 1), (1, 5), (2, 64))
     for npbe in (False, True):
-        for var in tuple((0, k) for k in kernels):
-            assert np.array_equal(out[(npbe,) + var][0], out[(npbe, 1, 0)][0]), var
-            assert np.array_equal(out[(npbe,) + var][1], out[(npbe, 1, 0)][1]), var
-    # FP32 (mixed inner cycles): every sweep kernel gives the same iterates
+        p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+        out = {}
+        for key in (("colour",),) + shapes:
+            with Vpmg(p, FP64) as pmg:
+                if key == ("colour",):
+                    pmg.set_tuning(TUNE_GS7_COLOUR_PASSES, 1)
+                else:
+                    pmg.set_tuning(TUNE_GS7_COLOUR_PASSES, 0)
+                    pmg.set_tuning(TUNE_GS7_SWEEP_SHAPE, key[0])
+                    pmg.set_tuning(TUNE_GS7_SWEEP_KCHUNK, key[1])
+                pmg.fillco(m)
+                pmg.solve()
+                out[key] = (pmg.u, pmg.residual_history(), pmg.energy())
+        for key in shapes:
+            assert np.array_equal(out[key][0], out[("colour",)][0]), (npbe, key)
+            assert np.array_equal(out[key][1], out[("colour",)][1]), (npbe, key)
+            assert out[key][2] == out[("colour",)][2], (npbe, key)
+    # FP32 inner cycles of the mixed path
     p = synth.mg_manual(65, 0.5, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
+    with Vpmg(p, FP64) as pmg:
+        pmg.fillco(m)
+        pmg.solve()
+        e64 = pmg.energy()
     res = {}
-    for kern in kernels:
+    for shape, kchunk in shapes:
         with Vpmg(p, MIXED) as pmg:
             pmg.set_tuning(TUNE_GS7_COLOUR_PASSES, 2)
             pmg.set_tuning(TUNE_MIXED_FINE_SWEEPS, 2)
-            pmg.set_tuning(TUNE_GS7_SWEEP_KERNEL, kern)
+            pmg.set_tuning(TUNE_GS7_SWEEP_SHAPE, shape)
+            pmg.set_tuning(TUNE_GS7_SWEEP_KCHUNK, kchunk)
             pmg.fillco(m)
             pmg.solve()
-            res[kern] = (pmg.u, pmg.residual_history())
-    for kern in kernels[1:]:
-        assert np.array_equal(res[kern][0], res[0][0]), kern
-        assert np.array_equal(res[kern][1], res[0][1]), kern
+            res[(shape, kchunk)] = (pmg.u, pmg.residual_history(), pmg.energy())
+    first = res[shapes[0]]
+    for key in shapes[1:]:
+        assert np.array_equal(res[key][0], first[0]), key
+        assert np.array_equal(res[key][1], first[1]), key
+    assert abs(first[2] - e64) <= 1e-6 * abs(e64)
