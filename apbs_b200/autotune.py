@@ -59,7 +59,8 @@ KEY_NAMES = {TUNE_GS27_CLUSTER: "gs27_cluster", TUNE_GS27_CLUSTER_MID: "gs27_clu
              TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative",
              TUNE_MIXED_COARSE_SWEEPS: "mixed_coarse_sweeps",
              TUNE_MIXED_FINE_SWEEPS: "mixed_fine_sweeps",
-             vpmg.TUNE_GS7_SWEEP_SHAPE: "gs7_sweep_shape"}
+             vpmg.TUNE_GS7_SWEEP_SHAPE: "gs7_sweep_shape",
+             vpmg.TUNE_MIXED_CHEBYSHEV: "mixed_chebyshev"}
 
 
 def shape_key(params, precision: int) -> str:

@@ -190,7 +190,8 @@ inline cudaError_t launch_gs7_rb_nt(cudaStream_t st, Gs7Rb<T> a, int c1, int q) 
   return cudaGetLastError();
 }
 
-// shape: bits 0-3 threads (0: 256, 1: 512, 2: 1024), bits 4-7 slots per thread (0: 2)
+// shape: bits 0-3 threads per CTA (0: 256, 1: 512, 2: 1024), bits 4-7 pair
+// slots per thread (0: 2); a CTA's widened range is threads x slots pairs
 template <typename T>
 inline cudaError_t launch_gs7_rb(cudaStream_t st, const Gs7Rb<T>& a, int c1, int shape) {
   const int nt = shape & 15, q = ((shape >> 4) & 15) ? ((shape >> 4) & 15) : 2;

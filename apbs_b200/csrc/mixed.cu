@@ -41,6 +41,8 @@ struct MLevel {
   float* cc;
   float* w0;
   float* x;
+  float* x2;         // Chebyshev smoothing: second iterate (zero boundary) and direction
+  float* d;
   Op ops64() const {
     Op o;
     for (int c = 0; c < 14; c++) o.c[c] = (c < nop) ? op64[c] : nullptr;
@@ -63,6 +65,9 @@ struct TLev {
   const float* cc;
   float* w0;
   float* x;
+  float* x2;
+  float* d;
+  const float* lam;  // Gershgorin bound of D^-1 A of this level
 };
 
 struct MixedState {
@@ -87,6 +92,7 @@ struct MixedState {
   int tail_first;     // first level run by the cluster tail kernel (0: none)
   int tail_cluster;
   TLev* d_tlev;       // device copies of the level descriptors
+  float* lam;         // per level: Gershgorin bound of D^-1 (A + cc) (Chebyshev smoothing)
 };
 
 namespace {
@@ -146,6 +152,88 @@ __device__ __forceinline__ T nb27g(const T* const* c, Grid g, const T* x, size_t
 
 __device__ __forceinline__ float nb27(const OpF& o, Grid g, const float* x, size_t id) {
   return nb27g<float>(o.c, g, x, id);
+}
+
+// ---------------------------------------------------------------------------
+// Chebyshev smoothing of the FP32 27-point levels (an option of the mixed
+// path's inner V-cycle, which is this project's own preconditioner; the
+// FP64 stopping test decides convergence).  Jacobi-preconditioned
+// Chebyshev iteration on the interval [b/16, b] of D^-1 (A + cc), b the
+// Gershgorin bound max_i sum_j |a_ij| / a_ii of the level, in the three-term
+// form of Adams, Brezina, Hu and Tuminaro (J. Comput. Phys. 188, 2003):
+//   r_i = (f - (A + cc) x_i) / a_ii,
+//   d_0 = r_0 / theta,  d_i = rho_i rho_{i-1} d_{i-1} + (2 rho_i / delta) r_i,
+//   x_{i+1} = x_i + d_i,
+// theta = (b + a)/2, delta = (b - a)/2, rho_0 = delta/theta,
+// rho_i = 1/(2 theta/delta - rho_{i-1}).  Every step updates all points
+// at once (one launch, or one barrier in the cluster tail) where the 8-colour
+// Gauss-Seidel needs eight.  x_i and x_{i+1} alternate between two buffers.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cheb_coef(float b, int i, float& alpha, float& beta) {
+  const float a = b * (1.0f / 16.0f);
+  const float theta = 0.5f * (b + a), delta = 0.5f * (b - a);
+  const float sigma = theta / delta;
+  float rho = 1.0f / sigma, rho_prev = 0.0f;
+  for (int s = 1; s <= i; s++) {
+    rho_prev = rho;
+    rho = 1.0f / (2.0f * sigma - rho_prev);
+  }
+  alpha = (i == 0) ? 0.0f : rho * rho_prev;
+  beta = (i == 0) ? 1.0f / theta : 2.0f * rho / delta;
+}
+
+__device__ __forceinline__ void cheb_point(const OpF& o, Grid g, const float* cc, const float* f,
+                                           const float* xin, float* xout, float* d, size_t id,
+                                           float alpha, float beta) {
+  const float dg = o.c[OC][id] + cc[id];
+  const float xv = xin[id];
+  const float r = (f[id] + nb27(o, g, xin, id) - dg * xv) / dg;
+  const float dn = alpha * d[id] + beta * r;
+  d[id] = dn;
+  xout[id] = xv + dn;
+}
+
+__global__ void k_cheb_step(Grid g, OpF o, const float* __restrict__ cc,
+                            const float* __restrict__ f, const float* __restrict__ xin,
+                            float* __restrict__ xout, float* __restrict__ d,
+                            const float* __restrict__ lam, int i) {
+  float alpha, beta;
+  cheb_coef(*lam, i, alpha, beta);
+  const int ex = g.nx - 2, ey = g.ny - 2;
+  const size_t nint = (size_t)ex * ey * (g.nz - 2);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i0 = 1 + (int)(q % ex), j0 = 1 + (int)((q / ex) % ey), k0 = 1 + (int)(q / ((size_t)ex * ey));
+    cheb_point(o, g, cc, f, xin, xout, d, g.idx(i0, j0, k0), alpha, beta);
+  }
+}
+
+// Gershgorin bound of D^-1 (A + cc) over the interior rows of a 27-point
+// level, as a float maximum (positive floats order like their bit patterns)
+__global__ void k_gersh(Grid g, OpF o, const float* __restrict__ cc, float* out) {
+  const int ex = g.nx - 2, ey = g.ny - 2;
+  const size_t nint = (size_t)ex * ey * (g.nz - 2);
+  const size_t sy = g.nx, sz = (size_t)g.nx * g.ny;
+  float mx = 0.0f;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(q % ex), j = 1 + (int)((q / ex) % ey), k = 1 + (int)(q / ((size_t)ex * ey));
+    const size_t id = g.idx(i, j, k);
+    const float* const* c = o.c;
+    float s = fabsf(c[ON][id]) + fabsf(c[ON][id - sy]) + fabsf(c[OE][id]) + fabsf(c[OE][id - 1]) +
+              fabsf(c[ONE][id]) + fabsf(c[ONW][id]) + fabsf(c[ONW][id - sy + 1]) +
+              fabsf(c[ONE][id - sy - 1]) + fabsf(c[UC][id]) + fabsf(c[UN][id]) +
+              fabsf(c[US][id]) + fabsf(c[UE][id]) + fabsf(c[UW][id]) + fabsf(c[UNE][id]) +
+              fabsf(c[UNW][id]) + fabsf(c[USE][id]) + fabsf(c[USW][id]) +
+              fabsf(c[UC][id - sz]) + fabsf(c[US][id - sz + sy]) + fabsf(c[UN][id - sz - sy]) +
+              fabsf(c[UW][id - sz + 1]) + fabsf(c[UE][id - sz - 1]) +
+              fabsf(c[USW][id - sz + sy + 1]) + fabsf(c[USE][id - sz + sy - 1]) +
+              fabsf(c[UNW][id - sz - sy + 1]) + fabsf(c[UNE][id - sz - sy - 1]);
+    const float dg = c[OC][id] + cc[id];
+    if (dg > 0.0f) mx = fmaxf(mx, 1.0f + s / dg);
+  }
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(out), __float_as_int(mx));
 }
 
 __device__ __forceinline__ float nb7(const OpF& o, Grid g, const float* x, size_t id) {
@@ -553,6 +641,7 @@ struct TailArgs {
   double* xnum;         // damping sums of the first -> first-1 correction
   double* xden;
   int nsweep;           // 8-colour sweeps before and after each coarse correction
+  int cheb = 0;         // > 0: Chebyshev smoothing of this (even) degree instead
 };
 
 __device__ __forceinline__ float nb27t(const TLev& L, const float* x, size_t id) {
@@ -628,6 +717,28 @@ __device__ void tail_smooth(const TLev& L, int reverse, int gtid, int nthr, int 
     }
 }
 
+// K Chebyshev steps on level L inside the cluster (K even: the result ends in L.x)
+template <int CLUSTER>
+__device__ void tail_cheb(const TLev& L, int gtid, int nthr, int K) {
+  const Grid g = L.g;
+  OpF o;
+#pragma unroll
+  for (int c = 0; c < 14; c++) o.c[c] = L.op[c];
+  o.nop = 14;
+  const int ex = g.nx - 2, ey = g.ny - 2, nint = ex * ey * (g.nz - 2);
+  const float b = *L.lam;
+  for (int i = 0; i < K; i++) {
+    float alpha, beta;
+    cheb_coef(b, i, alpha, beta);
+    const float* xin = (i & 1) ? L.x2 : L.x;
+    float* xout = (i & 1) ? L.x : L.x2;
+    for (int q = gtid; q < nint; q += nthr)
+      cheb_point(o, g, L.cc, L.w0, xin, xout, L.d, g.idx(1 + q % ex, 1 + (q / ex) % ey, 1 + q / (ex * ey)),
+                 alpha, beta);
+    tail_sync<CLUSTER>();
+  }
+}
+
 // restriction src (grid gs) -> level L's w0 (all points, boundary 0)
 __device__ void tail_restrict(Grid gs, const float* src, const TLev& L, bool zero_x, int gtid,
                               int nthr) {
@@ -694,7 +805,8 @@ __device__ void tail_cycle(const TailArgs& A, bool rhs_given, int gtid, int nthr
     }
     tail_sync<CLUSTER>();
     if (l != A.last) {
-      tail_smooth<CLUSTER>(L, 0, gtid, nthr, A.nsweep);
+      if (A.cheb > 0) tail_cheb<CLUSTER>(L, gtid, nthr, A.cheb);
+      else tail_smooth<CLUSTER>(L, 0, gtid, nthr, A.nsweep);
       const Grid g = L.g;
       const int ex = g.nx - 2, ey = g.ny - 2, nint = ex * ey * (g.nz - 2);
       for (int q = gtid; q < nint; q += nthr) {
@@ -742,7 +854,8 @@ __device__ void tail_cycle(const TailArgs& A, bool rhs_given, int gtid, int nthr
       P.x[gf.idx(i, j, k)] += xdamp * w;
     }
     tail_sync<CLUSTER>();
-    tail_smooth<CLUSTER>(P, 1, gtid, nthr, A.nsweep);
+    if (A.cheb > 0) tail_cheb<CLUSTER>(P, gtid, nthr, A.cheb);
+    else tail_smooth<CLUSTER>(P, 1, gtid, nthr, A.nsweep);
   }
 }
 
@@ -1217,7 +1330,10 @@ void mixed_destroy(MixedState* m) {
     if (L.cc) cudaFree(L.cc);
     if (L.w0) cudaFree(L.w0);
     if (L.x) cudaFree(L.x);
+    if (L.x2) cudaFree(L.x2);
+    if (L.d) cudaFree(L.d);
   }
+  if (m->lam) cudaFree(m->lam);
   if (m->r) cudaFree(m->r);
   if (m->w2) cudaFree(m->w2);
   if (m->xs) cudaFree(m->xs);
@@ -1291,7 +1407,9 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
     for (int c = 0; c < L.nop; c++)
       if (!falloc(&L.op[c], n)) return 0;
     if (!falloc(&L.cc, n) || !falloc(&L.w0, n) || !falloc(&L.x, n)) return 0;
+    if (l >= 1 && L.nop == 14 && (!falloc(&L.x2, n) || !falloc(&L.d, n))) return 0;
   }
+  if (!falloc(&m->lam, 16)) return 0;
   m->stale = 1;
   const size_t nscr = m->lev[lo].g.n();
   if (!falloc(&m->r, nscr) || !falloc(&m->w2, nscr)) return 0;
@@ -1323,6 +1441,9 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
       tl[l].cc = m->lev[l].cc;
       tl[l].w0 = m->lev[l].w0;
       tl[l].x = m->lev[l].x;
+      tl[l].x2 = m->lev[l].x2;
+      tl[l].d = m->lev[l].d;
+      tl[l].lam = m->lam + l;
     }
     CKM(cudaMalloc(&m->d_tlev, sizeof(TLev) * nl));
     CKM(cudaMemcpy(m->d_tlev, tl.data(), sizeof(TLev) * nl, cudaMemcpyHostToDevice));
@@ -1463,6 +1584,13 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
       to_f32(st, src, L.cc, L.g.n());
       note_launches(1);
     }
+    if (l >= 1 && l >= m->lo && !m->zero_cc && L.nop == 14 && L.x2) {
+      // the Chebyshev interval of this level
+      CKM(cudaMemsetAsync(m->lam + l, 0, sizeof(float), st));
+      const size_t nint = (size_t)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.nz - 2);
+      k_gersh<<<blocks_for(nint), kThreads, 0, st>>>(L.g, opf(L), L.cc, m->lam + l);
+      note_launches(1);
+    }
     if (l == 0 && m->d32) {
       // the FP32 single-pass sweep's divisor
       k_diag_f32<<<blocks_for(L.g.n()), kThreads, 0, st>>>(L.g, L.op[OC], L.cc, m->d32);
@@ -1496,6 +1624,30 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
   return 1;
 }
 
+// Chebyshev degree of the 27-point FP32 levels (PMGB_TUNE_MIXED_CHEBYSHEV,
+// rounded up to even), 0 for the 8-colour Gauss-Seidel
+int cheb_degree(const int* tune) {
+  const int k = tune[PMGB_TUNE_MIXED_CHEBYSHEV];
+  return k <= 0 ? 0 : (k + 1) & ~1;
+}
+
+// smoothing of a 27-point FP32 level outside the tail: K Chebyshev steps
+// (one launch each) or the 8-colour Gauss-Seidel
+int smooth27(cudaStream_t st, MLevel& L, MixedState* m, int l, int reverse, long long& k,
+             const int* tune) {
+  const int K = cheb_degree(tune);
+  if (K == 0 || !L.x2) return gs27_mc(st, L, L.x, tune[10], reverse, k, tune[9]);
+  const size_t nint = (size_t)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.nz - 2);
+  const OpF o = opf(L);
+  for (int i = 0; i < K; i++) {
+    k_cheb_step<<<blocks_for(nint), kThreads, 0, st>>>(L.g, o, L.cc, L.w0, (i & 1) ? L.x2 : L.x,
+                                                       (i & 1) ? L.x : L.x2, L.d, m->lam + l, i);
+    k++;
+  }
+  CKM(cudaGetLastError());
+  return 1;
+}
+
 int launch_tail(pmgb_solver* s, cudaStream_t st) {
   MixedState* m = s->mixed;
   const int nl = m->nlev, tf = m->tail_first;
@@ -1509,6 +1661,7 @@ int launch_tail(pmgb_solver* s, cudaStream_t st) {
   A.minv = m->dense;
   A.nd = m->nd;
   A.nsweep = s->tune[10];
+  A.cheb = cheb_degree(s->tune);
   A.xnum = s->scal + S_XNUM_L + ((tf - 1) & 15);
   A.xden = s->scal + S_XDEN_L + ((tf - 1) & 15);
   cudaLaunchConfig_t cfg = {};
@@ -1556,7 +1709,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     k++;
     if (l != nl - 1) {
       CKM(cudaMemsetAsync(C.x, 0, C.g.n() * sizeof(float), st));
-      if (!gs27_mc(st, C, C.x, s->tune[10], 0, k, s->tune[9])) return 0;
+      if (!smooth27(st, C, m, l, 0, k, s->tune)) return 0;
       const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
       k_resid_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.w0, C.x, m->r);
       k++;
@@ -1592,7 +1745,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
       }
       k += 2 * s->tune[11];
     } else {
-      if (!gs27_mc(st, P, P.x, s->tune[10], 1, k, s->tune[9])) return 0;
+      if (!smooth27(st, P, m, l, 1, k, s->tune)) return 0;
     }
   }
   // x64 += e ; r = f - (A + cc) x64 (FP64) -> FP32 rhs ; ||r||_1

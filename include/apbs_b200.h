@@ -217,7 +217,11 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
  * The autotuner (apbs_b200/autotune.py) times whole solves per grid shape
  * and keeps the best values in a table.  No key changes a result beyond
  * round-off; the FP64 smoother and wavefront keys change none at all. */
-/* keys 0, 1 and 3 are not used */
+#define PMGB_TUNE_MIXED_CHEBYSHEV 0   /* mixed: smoothing of the 27-point FP32 levels, 0 = the
+                                          8-colour Gauss-Seidel (PMGB_TUNE_MIXED_COARSE_SWEEPS
+                                          sweeps), K > 0 = Jacobi-preconditioned Chebyshev of
+                                          degree K (rounded up to even) */
+/* keys 1 and 3 are not used */
 #define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 on levels with
                                           >= 60 interior points per axis (0 = device max) */
 #define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded

@@ -136,7 +136,7 @@ def test_single_pass_sweep_matches_colour_passes():
     from apbs_b200.vpmg import (MIXED, TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK,
                                 TUNE_GS7_SWEEP_SHAPE, TUNE_MIXED_FINE_SWEEPS)
     m = synth.cluster(300, 10.0, seed=5, net_charge=3.0)
-    shapes = ((0, 8), (1, 8), (2, 8), (0x41, 8), (0, 1), (1, 5), (2, 64))
+    shapes = ((0x00, 8), (0x01, 8), (0x02, 8), (0x12, 18), (0x41, 8), (0x10, 1), (0x21, 5))
     for npbe in (False, True):
         p = synth.mg_manual(65, 0.5, m.center(), npbe=npbe, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
         out = {}
