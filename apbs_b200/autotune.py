@@ -29,8 +29,9 @@ from typing import Callable
 
 from . import vpmg
 from .vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID, TUNE_GS27_PLANES,
-                   TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_MC_COOPERATIVE,
-                   TUNE_MIXED_COARSE_SWEEPS, TUNE_MIXED_FINE_SWEEPS, TUNE_TAIL_MAX_POINTS)
+                   TUNE_GS7_COLOUR_PASSES, TUNE_GS7_SWEEP_KCHUNK, TUNE_GS7_SWEEP_SHAPE,
+                   TUNE_MC_COOPERATIVE, TUNE_MIXED_CHEBYSHEV, TUNE_MIXED_COARSE_SWEEPS,
+                   TUNE_MIXED_FINE_SWEEPS, TUNE_TAIL_MAX_POINTS)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
@@ -41,13 +42,14 @@ CANDIDATES = {
         TUNE_GS27_PLANES: [0, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
-        TUNE_GS7_SWEEP_KCHUNK: [16, 8, 32],
+        TUNE_GS7_SWEEP_SHAPE: [2, 0x12, 0x01, 0x31],
+        TUNE_GS7_SWEEP_KCHUNK: [8, 6, 12, 18],
     },
     MIXED: {
-        TUNE_MIXED_COARSE_SWEEPS: [2, 1, 3],
+        TUNE_MIXED_CHEBYSHEV: [2, 0, 4],
+        TUNE_TAIL_MAX_POINTS: [70000, 20000, 5000],
         TUNE_MIXED_FINE_SWEEPS: [2, 1, 3],
-        TUNE_TAIL_MAX_POINTS: [70000, 20000, 200000],
-        TUNE_MC_COOPERATIVE: [0, 1],
+        TUNE_MIXED_COARSE_SWEEPS: [2, 1, 3],
         TUNE_GS7_COLOUR_PASSES: [0, 2],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
     },
