@@ -209,7 +209,8 @@ __global__ void k_cheb_step(Grid g, OpF o, const float* __restrict__ cc,
 }
 
 // Gershgorin bound of D^-1 (A + cc) over the interior rows of a 27-point
-// level, as a float maximum (positive floats order like their bit patterns)
+// level (cc NULL: without the Helmholtz term), as a float maximum (positive
+// floats order like their bit patterns)
 __global__ void k_gersh(Grid g, OpF o, const float* __restrict__ cc, float* out) {
   const int ex = g.nx - 2, ey = g.ny - 2;
   const size_t nint = (size_t)ex * ey * (g.nz - 2);
@@ -229,7 +230,7 @@ __global__ void k_gersh(Grid g, OpF o, const float* __restrict__ cc, float* out)
               fabsf(c[UW][id - sz + 1]) + fabsf(c[UE][id - sz - 1]) +
               fabsf(c[USW][id - sz + sy + 1]) + fabsf(c[USE][id - sz + sy - 1]) +
               fabsf(c[UNW][id - sz - sy + 1]) + fabsf(c[UNE][id - sz - sy - 1]);
-    const float dg = c[OC][id] + cc[id];
+    const float dg = c[OC][id] + (cc ? cc[id] : 0.0f);
     if (dg > 0.0f) mx = fmaxf(mx, 1.0f + s / dg);
   }
   for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
@@ -1497,6 +1498,16 @@ int mixed_refresh(pmgb_solver* s) {
       to_f32(st, L.op64[c], L.op[c], L.g.n());
       note_launches(1);
     }
+    if (l >= 1 && L.nop == 14 && L.x2) {
+      // the Chebyshev interval of this level: the Gershgorin bound of
+      // D^-1 A without the Helmholtz term, which stays an upper bound for
+      // every cc >= 0 (the linear term and c'(u) of the Newton steps), so
+      // the bound follows operator rebuilds only
+      CKM(cudaMemsetAsync(m->lam + l, 0, sizeof(float), st));
+      const size_t nint = (size_t)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.nz - 2);
+      k_gersh<<<blocks_for(nint), kThreads, 0, st>>>(L.g, opf(L), nullptr, m->lam + l);
+      note_launches(1);
+    }
   }
   CKM(cudaGetLastError());
   m->stale = 0;
@@ -1584,14 +1595,7 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
       to_f32(st, src, L.cc, L.g.n());
       note_launches(1);
     }
-    if (l >= 1 && l >= m->lo && !m->zero_cc && L.nop == 14 && L.x2) {
-      // the Chebyshev interval of this level
-      CKM(cudaMemsetAsync(m->lam + l, 0, sizeof(float), st));
-      const size_t nint = (size_t)(L.g.nx - 2) * (L.g.ny - 2) * (L.g.nz - 2);
-      k_gersh<<<blocks_for(nint), kThreads, 0, st>>>(L.g, opf(L), L.cc, m->lam + l);
-      note_launches(1);
-    }
-    if (l == 0 && m->d32) {
+    if (l == 0 && m->d32 && s->tune[PMGB_TUNE_GS7_COLOUR_PASSES] == 2) {
       // the FP32 single-pass sweep's divisor
       k_diag_f32<<<blocks_for(L.g.n()), kThreads, 0, st>>>(L.g, L.op[OC], L.cc, m->d32);
       note_launches(1);
@@ -2079,6 +2083,7 @@ extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_s
     B.T.minv = m->dense;
     B.T.nd = m->nd;
     B.T.nsweep = s->tune[10];
+    B.T.cheb = cheb_degree(s->tune);  // the same smoothing as the calculation's own V-cycle
     B.fine_sweeps = s->tune[11];
     B.T.xnum = s->scal + S_TMP;
     B.T.xden = s->scal + S_TMP;

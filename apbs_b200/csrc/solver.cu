@@ -856,9 +856,12 @@ static int build_ops(pmgb_solver* s) {
   launch_build_fine(st, F.g, s->xf, s->yf, s->zf, s->epsx, s->epsy, s->epsz, s->ccf,
                     s->charge, s->gx, s->gy, s->gz, F.op[OC], F.op[OE], F.op[ON], F.op[UC],
                     F.cc, F.fc);
-  // the smoother's divisor oC + cc, summed once per operator
-  launch_diag(st, F.g, F.op[OC], F.cc, s->dg[0]);
-  note_launches(3);
+  // the FP64 smoother's divisor oC + cc, summed once per operator
+  if (s->precision == PMGB_FP64) {
+    launch_diag(st, F.g, F.op[OC], F.cc, s->dg[0]);
+    note_launches(1);
+  }
+  note_launches(2);
   for (int l = 1; l < s->nlev; l++) {
     Level& C = s->lev[l];
     Level& P = s->lev[l - 1];
@@ -1119,8 +1122,11 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
     // Vgetjac (newtond.c:550-598)
     launch_copy_interior(st, F.g, s->nw_r0, F.rhs);
     launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
-    launch_diag(st, F.g, F.op[OC], F.cp, s->dg[1]);
-    note_launches(3);
+    note_launches(2);
+    if (!mixed) {
+      launch_diag(st, F.g, F.op[OC], F.cp, s->dg[1]);
+      note_launches(1);
+    }
     for (int l = 1; l < s->nlev; l++) {
       launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].rhs, s->lev[l].g, s->lev[l].rhs);
       launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].cp, s->lev[l].g, s->lev[l].cp);
@@ -1463,6 +1469,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         break;
       case PMGB_K_GS7_SWEEP_FP64:
         // one full sweep: oE oN uC D=oC+cc fc and x read, x written: 56 B per point
+        if (r == 0 && s->precision != PMGB_FP64) launch_diag(st, F.g, F.op[OC], F.cc, s->dg[0]);
         if (!launch_gs7_sweep64(st, F.g, F.ops(), s->dg[0], F.fc, (r & 1) ? s->xs : F.x,
                                 (r & 1) ? F.x : s->xs, 1, s->tune[6], s->tune[12])) {
           set_error("gs7 sweep launch failed");
