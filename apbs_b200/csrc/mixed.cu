@@ -2007,6 +2007,9 @@ int mixed_solve(pmgb_solver* s, double errtol, int itmax) {
 // ---------------------------------------------------------------------------
 // Batched solve entry point
 // ---------------------------------------------------------------------------
+// largest level 1 (interior points) the batched kernel takes into its cluster
+constexpr int kBatchTailMax = 70000;
+
 extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_stream) {
   using namespace pmgb;
   if (!solvers || n < 1) {
@@ -2028,6 +2031,16 @@ extern "C" int pmgb_batch_solve(pmgb_solver* const* solvers, int n, void* cuda_s
   for (int b = 0; b < n; b++) {
     pmgb_solver* s = solvers[b];
     if (!s->built && !solver_build(s)) return 0;
+    // the persistent kernel runs every level from 1 down in its cluster: a
+    // calculation tuned to keep level 1 outside the one-cluster tail takes
+    // a tail limit that holds it (the FP32 hierarchy is rebuilt once)
+    if (s->nlev > 1) {
+      const Grid g1 = s->lev[1].g;
+      const int need = (g1.nx - 2) * (g1.ny - 2) * (g1.nz - 2);
+      if (need <= kBatchTailMax && s->tune[PMGB_TUNE_TAIL_MAX_POINTS] < need &&
+          !pmgb_solver_set_tuning(s, PMGB_TUNE_TAIL_MAX_POINTS, need))
+        return 0;
+    }
     if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
     if (!s->mixed->cc_ready && !mixed_set_cc(s, 0)) return 0;
     if (s->mixed->tail_first != 1) {

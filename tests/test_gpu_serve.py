@@ -87,3 +87,29 @@ def test_binding_sweep_through_the_loop_matches_fp64():
         dg_mx = e_mx[1 + 2 * k] - e_mx[0] - e_mx[2 + 2 * k]
         dg_64 = e_64[1 + 2 * k] - e_64[0] - e_64[2 + 2 * k]
         assert abs(dg_mx - dg_64) * KCAL_PER_KT <= 0.01
+
+
+def test_tuned_loop_matches_tuned_solves():
+    """With the B200 tuning table applied per grid shape (as the benchmark
+    runs the loop), every request succeeds and gives the energy of the same
+    calculation solved alone with the same table, in mixed precision: the
+    batched kernel takes the tuned calculations too (it widens a tail limit
+    that would keep level 1 outside its cluster)."""
+    from apbs_b200 import autotune
+    table = autotune.load_table()
+    jobs = _mix(10, seed=21)
+    alone = []
+    for p, m in jobs:
+        with Vpmg(p, MIXED) as pmg:
+            autotune.apply(pmg, table)
+            pmg.fillco(m)
+            pmg.solve()
+            alone.append(pmg.energy())
+    with serve.Server(MIXED, max_inflight=4) as srv:
+        srv.apply_table(table, MIXED)
+        res = [srv.wait(i) for i in [srv.submit(p, m) for p, m in jobs]]
+        st = srv.stats()
+    for r, e0 in zip(res, alone):
+        assert r["status"] == 1, r["error"]
+        assert abs(r["energy_kT"] - e0) <= 1e-9 * abs(e0)
+    assert st["failed"] == 0 and st["batched"] >= 2
