@@ -1694,6 +1694,63 @@ void launch_nresid(cudaStream_t s, Grid g, Op op, const double* cc, const double
   k_nresid<<<blocks_for(nint), kThreads, 0, s>>>(g, op, cc, fc, x, r, ions);
 }
 
+// k_nresid fused with the 1-norm of r (the partial sums of k_reduce_partial
+// with the same grid and traversal, so the norm is the same bits) and, when
+// cp is not null, c'(x) on the interior (the update of k_dcvec)
+__global__ void k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
+                             const double* __restrict__ fc, const double* __restrict__ x,
+                             double* r, IonTable ions, double* part, double* cp) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
+  double acc = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(q % (nx - 2));
+    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
+    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    const size_t id = g.idx(i, j, k);
+    const double c = cc[id], xv = x[id];
+    const double w = cvec_point(ions, c, xv, false);
+    const double rv = sum7(op, g, x, id, fc[id]) - op.c[OC][id] * xv - w;
+    r[id] = rv;
+    acc += fabs(rv);
+    if (cp) cp[id] = cvec_point(ions, c, xv, true);
+  }
+  const double t = block_sum<kRedThreads>(acc, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+void launch_nresid_nrm1(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                        const double* x, double* r, IonTable ions, double* part,
+                        double* out_dev, double* cp) {
+  const size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  const int nb = (int)reduce_parts(nint);
+  k_nresid_nrm<<<nb, kRedThreads, 0, s>>>(g, op, cc, fc, x, r, ions, part, cp);
+  k_reduce_final<<<1, kRedThreads, 0, s>>>(part, nb, out_dev);
+}
+
+// out = x + a y on interior points (the reference's copy then axpy, one pass)
+__global__ void k_xpay_interior(Grid g, const double* __restrict__ x, double a,
+                                const double* __restrict__ y, double* out) {
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(q % (nx - 2));
+    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
+    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    const size_t id = g.idx(i, j, k);
+    out[id] = x[id] + a * y[id];
+  }
+}
+
+void launch_xpay_interior(cudaStream_t s, Grid g, const double* x, double a, const double* y,
+                          double* out) {
+  size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  k_xpay_interior<<<blocks_for(nint), kThreads, 0, s>>>(g, x, a, y, out);
+}
+
 __global__ void k_dcvec(size_t n, const double* __restrict__ cc, const double* __restrict__ x,
                         double* cp, IonTable ions) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;

@@ -91,6 +91,14 @@ struct IonTable {
 // r = f + (off-diagonal stencil) x - oC x - c(x) on the fine level
 void launch_nresid(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                    const double* x, double* r, IonTable ions);
+// k_nresid and the 1-norm of r into out_dev (bitwise the launch_nrm1 value),
+// and c'(x) into cp on the interior when cp is not null
+void launch_nresid_nrm1(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                        const double* x, double* r, IonTable ions, double* part,
+                        double* out_dev, double* cp);
+// out = x + a y on interior points
+void launch_xpay_interior(cudaStream_t s, Grid g, const double* x, double a, const double* y,
+                          double* out);
 // cp = c'(x) on every point
 void launch_dcvec(cudaStream_t s, Grid g, const double* cc, const double* x, double* cp,
                   IonTable ions);

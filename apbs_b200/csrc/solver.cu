@@ -1092,11 +1092,13 @@ static int vcycles(pmgb_solver* s, int newton, double errtol, int itmax, int ist
   return 1;
 }
 
-static int nresid_norm(pmgb_solver* s, const double* x, double* r, double* out) {
+// ||N(x)||_1 with r = N(x); with cp not null also c'(x) (one pass)
+static int nresid_norm(pmgb_solver* s, const double* x, double* r, double* out,
+                       double* cp = nullptr) {
   Level& F = s->lev[0];
-  launch_nresid(s->stream, F.g, F.ops(), F.cc, F.fc, x, r, s->ions);
-  launch_nrm1(s->stream, F.g, r, s->part, s->scal + S_NRM);
-  note_launches(3);
+  launch_nresid_nrm1(s->stream, F.g, F.ops(), F.cc, F.fc, x, r, s->ions, s->part,
+                     s->scal + S_NRM, cp);
+  note_launches(2);
   return read_scalar(s, S_NRM, out);
 }
 
@@ -1117,20 +1119,28 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
   s->reslog.push_back(rsnrm / rsden);
   if (!nresid_norm(s, F.x, s->nw_r0, &xnorm_old)) return 0;
   int iters = 0, idamp = 1;
+  // work vectors of the damping loop: trial iterate and residual, and the
+  // best ones kept; "keep" is a swap of the two pairs (no copies)
+  double *ws = s->nw_ws, *r0 = s->nw_r0, *keepx = s->nw_keepx, *keepr = s->nw_keepr;
+  int cp_ready = 0;  // F.cp already holds c'(F.x) (computed with the last residual)
   for (;;) {
     iters++;
-    // Vgetjac (newtond.c:550-598)
-    launch_copy_interior(st, F.g, s->nw_r0, F.rhs);
-    launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
-    note_launches(2);
+    // Vgetjac (newtond.c:550-598).  Only the fine right-hand side is used:
+    // every coarse level's right-hand side is the restricted residual of
+    // the V-cycle itself.
+    launch_copy_interior(st, F.g, r0, F.rhs);
+    note_launches(1);
+    if (!cp_ready) {
+      launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
+      note_launches(1);
+    }
     if (!mixed) {
       launch_diag(st, F.g, F.op[OC], F.cp, s->dg[1]);
       note_launches(1);
     }
     for (int l = 1; l < s->nlev; l++) {
-      launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].rhs, s->lev[l].g, s->lev[l].rhs);
       launch_restrict(st, s->lev[l - 1].g, s->lev[l - 1].cp, s->lev[l].g, s->lev[l].cp);
-      note_launches(2);
+      note_launches(1);
     }
     const double errtol_s =
         (0.9 * xnorm_old <= 1.0 * pow(xnorm_old, 2.0)) ? 0.9 * xnorm_old : 1.0 * pow(xnorm_old, 2.0);
@@ -1141,39 +1151,42 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
     } else {
       if (!vcycles(s, 1, errtol_s, 1000, 1, &it_s)) return 0;
     }
+    cp_ready = 0;
     if (idamp == 1) {
       double damp = 1.0;
       int iter_d = 0, mode = 0;
-      launch_copy_interior(st, F.g, F.x, s->nw_ws);
-      launch_axpy_interior(st, F.g, nullptr, damp, F.xt, s->nw_ws);
-      note_launches(2);
-      if (!nresid_norm(s, s->nw_ws, s->nw_r0, &xnorm_new)) return 0;
+      // ws = x + damp xt (the reference's copy then axpy, newtond.c:430-445)
+      launch_xpay_interior(st, F.g, F.x, damp, F.xt, ws);
+      note_launches(1);
+      if (!nresid_norm(s, ws, r0, &xnorm_new)) return 0;
       while (iter_d < 10) {
         if (mode == 0) {
           if (xnorm_new < xnorm_old) mode = 1;
         } else if (xnorm_new > xnorm_med) {
           break;
         }
-        launch_copy_interior(st, F.g, s->nw_ws, s->nw_keepx);
-        launch_copy_interior(st, F.g, s->nw_r0, s->nw_keepr);
+        // keep this trial: its iterate and residual become the kept pair
+        std::swap(ws, keepx);
+        std::swap(r0, keepr);
         xnorm_med = xnorm_new;
-        launch_copy_interior(st, F.g, F.x, s->nw_ws);
         damp = damp / 2.0;
-        launch_axpy_interior(st, F.g, nullptr, damp, F.xt, s->nw_ws);
-        note_launches(4);
-        if (!nresid_norm(s, s->nw_ws, s->nw_r0, &xnorm_new)) return 0;
+        launch_xpay_interior(st, F.g, F.x, damp, F.xt, ws);
+        note_launches(1);
+        if (!nresid_norm(s, ws, r0, &xnorm_new)) return 0;
         iter_d++;
       }
-      launch_copy_interior(st, F.g, s->nw_keepx, F.x);
-      launch_copy_interior(st, F.g, s->nw_keepr, s->nw_r0);
-      note_launches(2);
+      launch_copy_interior(st, F.g, keepx, F.x);
+      note_launches(1);
+      std::swap(keepr, r0);
       xnorm_new = xnorm_med;
       xnorm_old = xnorm_new;
       if ((iter_d - 1) == 0) idamp = 0;
     } else {
       launch_axpy_interior(st, F.g, nullptr, 1.0, F.xt, F.x);
       note_launches(1);
-      if (!nresid_norm(s, F.x, s->nw_r0, &xnorm_new)) return 0;
+      // the residual pass also gives c'(x) for the next Jacobian
+      if (!nresid_norm(s, F.x, r0, &xnorm_new, F.cp)) return 0;
+      cp_ready = 1;
       xnorm_old = xnorm_new;
     }
     rsnrm = xnorm_new;
@@ -1181,6 +1194,10 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
     if ((rsnrm / rsden) <= errtol) break;
     if (iters >= itmax) break;
   }
+  s->nw_ws = ws;
+  s->nw_r0 = r0;
+  s->nw_keepx = keepx;
+  s->nw_keepr = keepr;
   s->st.rel_residual = rsnrm / rsden;
   s->st.newton_iters = iters;
   return 1;
