@@ -203,8 +203,26 @@ __global__ void k_cell_fill(int natoms, const int* __restrict__ cell_of, int* fi
 // cells within two cell edges (the cell edge is max r + srad) into a list of
 // up to kNbrCap entries; a longer list is only counted, and its atom's
 // points fall back to the cell search.  Any superset of the possible
-// excluders gives the same exclusion decisions.
+// excluders, in any order, gives the same exclusion decisions; the cells are
+// visited centre-out (kCellRing) so that the nearest atoms, which exclude
+// most buried points, come first in the list.
 constexpr int kNbrCap = 512;
+
+// the 125 cell offsets (dx, dy, dz) in -2..2, coded 25 (dz+2) + 5 (dy+2) + (dx+2),
+// sorted by dx^2 + dy^2 + dz^2
+struct CellRing {
+  int v[125];
+  constexpr CellRing() : v() {
+    int n = 0;
+    for (int d2 = 0; d2 <= 12; d2++)
+      for (int code = 0; code < 125; code++) {
+        const int dx = code % 5 - 2, dy = (code / 5) % 5 - 2, dz = code / 25 - 2;
+        if (dx * dx + dy * dy + dz * dz == d2) v[n++] = code;
+      }
+  }
+};
+__constant__ CellRing kCellRingTab = CellRing();
+#define kCellRing (kCellRingTab.v)
 
 __global__ void k_sas_nbr(CellGrid C, int natoms, const double* __restrict__ xyz,
                           const double* __restrict__ r, double srad,
@@ -218,10 +236,10 @@ __global__ void k_sas_nbr(CellGrid C, int natoms, const double* __restrict__ xyz
   const double pp[3] = {ax, ay, az};
   for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
   int count = 0;
-  for (int dz = -2; dz <= 2; dz++)
-    for (int dy = -2; dy <= 2; dy++)
-      for (int dx = -2; dx <= 2; dx++) {
-        const int cx = c[0] + dx, cy = c[1] + dy, cz = c[2] + dz;
+  for (int o = 0; o < 125; o++) {
+        const int code = kCellRing[o];
+        const int cx = c[0] + (code % 5) - 2, cy = c[1] + (code / 5) % 5 - 2,
+                  cz = c[2] + code / 25 - 2;
         if (cx < 0 || cy < 0 || cz < 0 || cx >= C.n[0] || cy >= C.n[1] || cz >= C.n[2])
           continue;
         const int cell = (cz * C.n[1] + cy) * C.n[0] + cx;
@@ -243,43 +261,60 @@ __global__ void k_sas_nbr(CellGrid C, int natoms, const double* __restrict__ xyz
           if (keep && slot < kNbrCap) nbr[(size_t)a * kNbrCap + slot] = b;
           count += __popc(m);
         }
-      }
+  }
   if (lane == 0) ncount[a] = count;
 }
 
 // One thread per (atom, reference point); the accessible points are appended
 // to a list (warp-aggregated), so the marking pass runs over them only.
-__global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xyz,
-                           const double* __restrict__ r, const double* __restrict__ ref,
-                           int nref, double srad, const int* __restrict__ start,
-                           const int* __restrict__ atoms_sorted, const int* __restrict__ nbr,
-                           const int* __restrict__ ncount, unsigned* list, int* npts) {
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  bool acc = false;
-  if (tid < (long long)natoms * nref) {
-    const int a = (int)(tid / nref), t = (int)(tid % nref);
+// Block row y takes atoms y, y + gridDim.y, ...: an atom's excluder list (coordinates and (r_b + srad)^2)
+// is staged in shared memory once for the row's points.  The test is the
+// reference's FP64 comparison, dist^2 < (r_b + srad)^2 (Vacc_atomSASPoints
+// via ivdwAccExclus, src/generic/vacc.c).
+__global__ void __launch_bounds__(256) k_sas_test(
+    CellGrid C, int natoms, const double* __restrict__ xyz, const double* __restrict__ r,
+    const double* __restrict__ ref, int nref, double srad, const int* __restrict__ start,
+    const int* __restrict__ atoms_sorted, const int* __restrict__ nbr,
+    const int* __restrict__ ncount, unsigned* list, int* npts) {
+  __shared__ double4 ex[kNbrCap];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int a = blockIdx.y; a < natoms; a += gridDim.y) {
     const double arad = r[a];
-    if (!(arad < 1.0e-9)) {
+    if (arad < 1.0e-9) continue;  // the whole block: no points on this atom
+    const int cnt = ncount[a];
+    const bool staged = cnt <= kNbrCap;
+    if (staged) {
+      const int* lst = nbr + (size_t)a * kNbrCap;
+      for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+        const int b = lst[q];
+        const double rr = r[b] + srad;
+        ex[q] = make_double4(xyz[3 * b], xyz[3 * b + 1], xyz[3 * b + 2], rr * rr);
+      }
+      __syncthreads();
+    }
+    bool acc = false;
+    if (t < nref) {
       const double rad = arad + srad;
       const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
       const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
       const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
-      auto excludes = [&](int b) {
-        const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1], d2 = pz - xyz[3 * b + 2];
-        const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
-        const double rr = r[b] + srad;
-        return dist2 < rr * rr;
-      };
       acc = true;
-      const int cnt = ncount[a];
-      if (cnt <= kNbrCap) {
-        const int* lst = nbr + (size_t)a * kNbrCap;
-        for (int s = 0; s < cnt; s++)
-          if (excludes(lst[s])) {
+      if (staged) {
+        for (int q = 0; q < cnt; q++) {
+          const double4 e = ex[q];
+          const double d0 = px - e.x, d1 = py - e.y, d2 = pz - e.z;
+          if (d0 * d0 + d1 * d1 + d2 * d2 < e.w) {
             acc = false;
             break;
           }
+        }
       } else {
+        auto excludes = [&](int b) {
+          const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1], d2 = pz - xyz[3 * b + 2];
+          const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+          const double rr = r[b] + srad;
+          return dist2 < rr * rr;
+        };
         int c[3];
         const double pp[3] = {px, py, pz};
         for (int d = 0; d < 3; d++) c[d] = (int)floor((pp[d] - C.lo[d]) / C.cs);
@@ -301,14 +336,15 @@ __global__ void k_sas_test(CellGrid C, int natoms, const double* __restrict__ xy
             }
       }
     }
-  }
-  const unsigned m = __ballot_sync(0xffffffffu, acc);
-  if (m) {
-    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(npts, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (acc) list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)tid;
+    const unsigned m = __ballot_sync(0xffffffffu, acc);
+    if (m) {
+      const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(npts, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (acc) list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)a * (unsigned)nref + t;
+    }
+    __syncthreads();  // the next atom restages ex
   }
 }
 
@@ -769,9 +805,9 @@ void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms
   cudaMemsetAsync(npts, 0, sizeof(int), s);
   int* ncount = nbr + (size_t)natoms * kNbrCap;
   k_sas_nbr<<<(natoms + 7) / 8, 256, 0, s>>>(C, natoms, xyz, r, srad, start, sorted, nbr, ncount);
-  k_sas_test<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(C, natoms, xyz, r, ref, nref, srad,
-                                                           start, sorted, nbr, ncount, list,
-                                                           npts);
+  k_sas_test<<<dim3((nref + 255) / 256, std::min(natoms, 65535)), 256, 0, s>>>(C, natoms, xyz, r, ref, nref,
+                                                              srad, start, sorted, nbr, ncount,
+                                                              list, npts);
   static const int nblocks = [] {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);

@@ -1672,6 +1672,38 @@ __device__ __forceinline__ double cvec_point(const IonTable& ions, double coef, 
   return out;
 }
 
+// cvec_point(..., false) and, where d is given, cvec_point(..., true) of the
+// same point: the two share the exponential wherever their arguments agree
+// (everywhere but where |zcf2 coef| is below 1e-20 for one of them), so the
+// values are those of two separate calls.
+__device__ __forceinline__ void cvec_pair(const IonTable& ions, double coef, double u,
+                                          double* c, double* d) {
+  double out = 0.0, dout = 0.0;
+  for (int s = 0; s < ions.nion; s++) {
+    const double zcf2 = -1.0 * ions.sconc[s] * ions.q[s];
+    const double zcf2d = ions.sconc[s] * ions.q[s] * ions.q[s];
+    const double zu2 = -1.0 * ions.q[s];
+    const double t = fabs(zcf2 * coef);
+    const double am_zero = (1.0e-20 <= t ? 1.0e-20 : t) * 1.0e20;
+    const double v = zu2 * u;
+    double am_neg = (v <= 0.0 ? v : 0.0);
+    double am_pos = (v >= 0.0 ? v : 0.0);
+    if (!(am_neg >= -85.0)) am_neg = -85.0;
+    if (!(am_pos <= 85.0)) am_pos = 85.0;
+    const double arg = am_zero * (am_neg + am_pos);
+    const double e = exp(arg);
+    out = out + zcf2 * coef * e;
+    if (d) {
+      const double td = fabs(zcf2d * coef);
+      const double am_zero_d = (1.0e-20 <= td ? 1.0e-20 : td) * 1.0e20;
+      const double argd = am_zero_d * (am_neg + am_pos);
+      dout = dout + zcf2d * coef * (argd == arg ? e : exp(argd));
+    }
+  }
+  *c = out;
+  if (d) *d = dout;
+}
+
 __global__ void k_nresid(Grid g, Op op, const double* __restrict__ cc,
                          const double* __restrict__ fc, const double* __restrict__ x, double* r,
                          IonTable ions) {
@@ -1711,11 +1743,12 @@ __global__ void k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
     const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
     const size_t id = g.idx(i, j, k);
     const double c = cc[id], xv = x[id];
-    const double w = cvec_point(ions, c, xv, false);
+    double w, dw;
+    cvec_pair(ions, c, xv, &w, cp ? &dw : nullptr);
     const double rv = sum7(op, g, x, id, fc[id]) - op.c[OC][id] * xv - w;
     r[id] = rv;
     acc += fabs(rv);
-    if (cp) cp[id] = cvec_point(ions, c, xv, true);
+    if (cp) cp[id] = dw;
   }
   const double t = block_sum<kRedThreads>(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = t;

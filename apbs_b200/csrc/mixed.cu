@@ -21,7 +21,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "gs7_rb.cuh"
+#include "gs7_rb_bulk.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
 
@@ -93,6 +93,10 @@ struct MixedState {
   int tail_cluster;
   TLev* d_tlev;       // device copies of the level descriptors
   float* lam;         // per level: Gershgorin bound of D^-1 (A + cc) (Chebyshev smoothing)
+  // the dense coarsest inverse runs on the solver's side stream: forked after
+  // the coarsest Helmholtz term is in place, done when dense_ev completes
+  cudaEvent_t dense_fork, dense_ev;
+  int* d_err;  // set by a bulk-staged fine sweep whose copies did not complete
 };
 
 namespace {
@@ -116,15 +120,46 @@ OpF opf(const MLevel& L) {
 // ---------------------------------------------------------------------------
 // conversions
 // ---------------------------------------------------------------------------
-__global__ void k_to_f32(const double* __restrict__ a, float* b, size_t n) {
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
-       q += (size_t)gridDim.x * blockDim.x)
-    b[q] = (float)a[q];
+// Many conversions in one launch: segment i converts a[i][0..n_i) into b[i].
+constexpr int kConvSegs = 32;
+struct ConvBatch {
+  const double* a[kConvSegs];
+  float* b[kConvSegs];
+  unsigned long long off[kConvSegs + 1];  // running sums of the lengths
+  int nseg;
+};
+
+__global__ void k_to_f32_batch(ConvBatch c) {
+  const unsigned long long tot = c.off[c.nseg];
+  int seg = 0;
+  for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       q < tot; q += (unsigned long long)gridDim.x * blockDim.x) {
+    while (q >= c.off[seg + 1]) seg++;  // q only grows along a thread's loop
+    const unsigned long long e = q - c.off[seg];
+    c.b[seg][e] = (float)c.a[seg][e];
+  }
 }
 
-void to_f32(cudaStream_t s, const double* a, float* b, size_t n) {
-  k_to_f32<<<blocks_for(n), kThreads, 0, s>>>(a, b, n);
-}
+// Collects conversions and issues them kConvSegs at a time.
+struct ConvQueue {
+  cudaStream_t st;
+  ConvBatch c{};
+  explicit ConvQueue(cudaStream_t s) : st(s) {}
+  void add(const double* a, float* b, size_t n) {
+    if (n == 0) return;
+    if (c.nseg == kConvSegs) flush();
+    c.a[c.nseg] = a;
+    c.b[c.nseg] = b;
+    c.off[c.nseg + 1] = c.off[c.nseg] + n;
+    c.nseg++;
+  }
+  void flush() {
+    if (c.nseg == 0) return;
+    k_to_f32_batch<<<blocks_for((size_t)c.off[c.nseg]), kThreads, 0, st>>>(c);
+    note_launches(1);
+    c = ConvBatch{};
+  }
+};
 
 // ---------------------------------------------------------------------------
 // FP32 stencils
@@ -276,21 +311,6 @@ __global__ void k_resid_f32(Grid g, OpF o, const float* __restrict__ cc,
   }
 }
 
-__global__ void k_matvec_f32(Grid g, OpF o, const float* __restrict__ cc,
-                             const float* __restrict__ x, float* y) {
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
-    const size_t id = g.idx(i, j, k);
-    const float nb = (o.nop == 4) ? nb7(o, g, x, id) : nb27(o, g, x, id);
-    y[id] = (o.c[OC][id] + cc[id]) * x[id] - nb;
-  }
-}
-
 // 8-colour Gauss-Seidel on a 27-point level: colour c = (i&1)|(j&1)<<1|(k&1)<<2.
 // One cluster runs nsweep sweeps (colour order ascending, or descending when
 // reverse) with a cluster barrier between colours.
@@ -420,24 +440,6 @@ __global__ void k_interp_axpy_f32(Grid gc, const float* __restrict__ xc, Grid gf
 }
 
 // dot product of FP32 vectors on interior points, FP64 accumulation
-__global__ void k_dot_f32(Grid g, const float* __restrict__ x, const float* __restrict__ y,
-                          double* part) {
-  __shared__ double sh[32];
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
-  double acc = 0.0;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
-    const size_t id = g.idx(i, j, k);
-    acc += (double)x[id] * (double)y[id];
-  }
-  const double t = block_sum<256>(acc, sh);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
 __global__ void k_sum_parts(const double* __restrict__ part, int n, double* out) {
   __shared__ double sh[32];
   double acc = 0.0;
@@ -446,12 +448,51 @@ __global__ void k_sum_parts(const double* __restrict__ part, int n, double* out)
   if (threadIdx.x == 0) out[0] = t;
 }
 
-void dot_f32(cudaStream_t s, Grid g, const float* x, const float* y, double* part,
-             double* out) {
+// The two sums of the interpolation damping on a coarse level, x.w0 and
+// x.((A + cc) x), in one pass over x: FP32 products (A + cc) x, FP64 sums,
+// partials per block (reduce_parts blocks) summed by k_sum_parts2.
+__global__ void k_damp_dots(Grid g, OpF o, const float* __restrict__ cc,
+                            const float* __restrict__ x, const float* __restrict__ w0,
+                            double* part_num, double* part_den) {
+  __shared__ double sh[32];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
+  double an = 0.0, ad = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(q % (nx - 2));
+    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
+    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    const size_t id = g.idx(i, j, k);
+    const float nb = (o.nop == 4) ? nb7(o, g, x, id) : nb27(o, g, x, id);
+    const float xv = x[id];
+    const float ax = (o.c[OC][id] + cc[id]) * xv - nb;
+    an += (double)xv * (double)w0[id];
+    ad += (double)xv * (double)ax;
+  }
+  const double tn = block_sum<256>(an, sh);
+  if (threadIdx.x == 0) part_num[blockIdx.x] = tn;
+  const double td = block_sum<256>(ad, sh);
+  if (threadIdx.x == 0) part_den[blockIdx.x] = td;
+}
+
+// k_sum_parts of two partial arrays (blocks 0 and 1)
+__global__ void k_sum_parts2(const double* __restrict__ p0, const double* __restrict__ p1,
+                             int n, double* out0, double* out1) {
+  __shared__ double sh[32];
+  const double* part = blockIdx.x ? p1 : p0;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+  const double t = block_sum<256>(acc, sh);
+  if (threadIdx.x == 0) (blockIdx.x ? out1 : out0)[0] = t;
+}
+
+void damp_dots(cudaStream_t s, Grid g, OpF o, const float* cc, const float* x, const float* w0,
+               double* part, double* num, double* den) {
   const size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
   const int nb = (int)reduce_parts(nint);
-  k_dot_f32<<<nb, 256, 0, s>>>(g, x, y, part);
-  k_sum_parts<<<1, 256, 0, s>>>(part, nb, out);
+  k_damp_dots<<<nb, 256, 0, s>>>(g, o, cc, x, w0, part, part + 2368);
+  k_sum_parts2<<<2, 256, 0, s>>>(part, part + 2368, nb, num, den);
 }
 
 // FP64 fine residual r = f - (A + cc) x written as the FP32 V-cycle rhs,
@@ -1244,18 +1285,34 @@ Gs7Rb<float> rb_f32(const MLevel& F, const float* d32, const int* tune) {
   return a;
 }
 
+// The fine-level FP32 smoothing: tune[11] red-black sweeps, then (r given)
+// the residual.  tune[5] 2 and 3 run single-pass sweeps out of place
+// (x -> xs -> x ...; after an odd count xs is copied back), 3 with the
+// operands staged by the bulk-copy engine; otherwise one launch per colour.
+// k counts the kernels launched.
 cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
-                    float* xs, const float* d32, const int* tune) {
-  if (tune[5] == 2 && tune[11] == 2 && xs && d32 && (F.g.nx & 1) && (F.g.ny & 1)) {
-    // two single-pass sweeps x -> xs -> x, then the residual
+                    float* xs, const float* d32, const int* tune, int* err, long long& k) {
+  const int mode = tune[5];
+  const int nsweep = tune[11];
+  if ((mode == 2 || mode == 3) && xs && d32 && (F.g.nx & 1) && (F.g.ny & 1)) {
     Gs7Rb<float> a = rb_f32(F, d32, tune);
-    a.xin = x; a.xout = xs;
-    cudaError_t e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
-    a.xin = xs; a.xout = x;
-    if (e == cudaSuccess) e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
+    float* buf[2] = {x, xs};
+    cudaError_t e = cudaSuccess;
+    for (int sw = 0; sw < nsweep && e == cudaSuccess; sw++) {
+      a.xin = buf[sw & 1];
+      a.xout = buf[(sw + 1) & 1];
+      e = cudaErrorNotSupported;
+      if (mode == 3) e = launch_gs7_rb_bulk<float>(st, a, first_parity, tune[12] & 15, err);
+      if (e == cudaErrorNotSupported)  // the windows do not fit shared memory
+        e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
+      k++;
+    }
+    if (e == cudaSuccess && (nsweep & 1))
+      e = cudaMemcpyAsync(x, xs, F.g.n() * sizeof(float), cudaMemcpyDeviceToDevice, st);
     if (r && e == cudaSuccess) {
       const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
       k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, opf(F), F.cc, F.w0, x, r);
+      k++;
       e = cudaGetLastError();
     }
     return e;
@@ -1263,14 +1320,16 @@ cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int fi
   // colour passes: the sweeps, then the residual
   const size_t nslots = (size_t)((F.g.nx - 1) / 2) * (F.g.ny - 2) * (F.g.nz - 2);
   const OpF fo = opf(F);
-  for (int sw = 0; sw < tune[11]; sw++) {
+  for (int sw = 0; sw < nsweep; sw++) {
     k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, first_parity);
     k_gs7_f32<<<blocks_for(nslots), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x,
                                                        1 - first_parity);
+    k += 2;
   }
   if (r) {
     const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
     k_resid_f32<<<blocks_for(fint), kThreads, 0, st>>>(F.g, fo, F.cc, F.w0, x, r);
+    k++;
   }
   return cudaGetLastError();
 }
@@ -1344,6 +1403,9 @@ void mixed_destroy(MixedState* m) {
   if (m->dinfo) cudaFree(m->dinfo);
   if (m->d_tlev) cudaFree(m->d_tlev);
   if (m->d_flag) cudaFree(m->d_flag);
+  if (m->dense_fork) cudaEventDestroy(m->dense_fork);
+  if (m->dense_ev) cudaEventDestroy(m->dense_ev);
+  if (m->d_err) cudaFree(m->d_err);
   delete m;
 }
 
@@ -1357,6 +1419,10 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
   s->mixed = m;
   m->lo = lo;
   cudaStream_t st = s->stream;
+  CKM(cudaEventCreateWithFlags(&m->dense_fork, cudaEventDisableTiming));
+  CKM(cudaEventCreateWithFlags(&m->dense_ev, cudaEventDisableTiming));
+  CKM(cudaMalloc((void**)&m->d_err, sizeof(int)));
+  CKM(cudaMemset(m->d_err, 0, sizeof(int)));
   // levels shared with the FP64 hierarchy
   int nl = 0;
   m->zero_cc = (lo > 0);
@@ -1492,12 +1558,14 @@ int mixed_refresh(pmgb_solver* s) {
                     s->d_opptrs + 14 * l);
     note_launches(1);
   }
+  ConvQueue conv(st);
   for (int l = m->lo; l < m->nlev; l++) {
     MLevel& L = m->lev[l];
-    for (int c = 0; c < L.nop; c++) {
-      to_f32(st, L.op64[c], L.op[c], L.g.n());
-      note_launches(1);
-    }
+    for (int c = 0; c < L.nop; c++) conv.add(L.op64[c], L.op[c], L.g.n());
+  }
+  conv.flush();
+  for (int l = m->lo; l < m->nlev; l++) {
+    MLevel& L = m->lev[l];
     if (l >= 1 && L.nop == 14 && L.x2) {
       // the Chebyshev interval of this level: the Gershgorin bound of
       // D^-1 A without the Helmholtz term, which stays an upper bound for
@@ -1574,6 +1642,9 @@ static int launch_dense_inverse(cudaStream_t st, double* M, int n, int* info) {
 int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
   MixedState* m = s->mixed;
   cudaStream_t st = s->stream;
+  // the previous dense inverse reads the coarsest term rewritten below
+  CKM(cudaStreamWaitEvent(st, m->dense_ev, 0));
+  ConvQueue conv(st);
   for (int l = 0; l < m->nlev; l++) {
     MLevel& L = m->lev[l];
     const double* src;
@@ -1591,26 +1662,32 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
       note_launches(1);
       src = L.cc64;
     }
-    if (l >= m->lo && !m->zero_cc) {
-      to_f32(st, src, L.cc, L.g.n());
-      note_launches(1);
-    }
-    if (l == 0 && m->d32 && s->tune[PMGB_TUNE_GS7_COLOUR_PASSES] == 2) {
-      // the FP32 single-pass sweep's divisor
-      k_diag_f32<<<blocks_for(L.g.n()), kThreads, 0, st>>>(L.g, L.op[OC], L.cc, m->d32);
-      note_launches(1);
-    }
+    if (l >= m->lo && !m->zero_cc) conv.add(src, L.cc, L.g.n());
     if (l == m->nlev - 1) {
-      // dense factor of (A_c + cc) on the coarsest level
+      // dense inverse of (A_c + cc) on the coarsest level, on the side stream:
+      // the V-cycle's finer levels run meanwhile and its coarsest solve waits
+      // for dense_ev
       const int nd = m->nd;
-      k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, st>>>(L.g, L.ops64(), src,
-                                                                       m->dense, nd);
-      if (!launch_dense_inverse(st, m->dense, nd, m->dinfo)) {
+      CKM(cudaEventRecord(m->dense_fork, st));
+      CKM(cudaStreamWaitEvent(s->side, m->dense_fork, 0));
+      k_dense_build<<<blocks_for((size_t)nd * nd), kThreads, 0, s->side>>>(
+          L.g, L.ops64(), src, m->dense, nd);
+      const int ok = launch_dense_inverse(s->side, m->dense, nd, m->dinfo);
+      CKM(cudaEventRecord(m->dense_ev, s->side));
+      if (!ok) {
         set_error("mixed: dense coarsest inverse launch failed (%d unknowns)", nd);
         return 0;
       }
       note_launches(2);
     }
+  }
+  // the FP32 Helmholtz terms of all levels in one launch
+  conv.flush();
+  MLevel& F = m->lev[0];
+  if (m->d32 && s->tune[PMGB_TUNE_GS7_COLOUR_PASSES] >= 2) {
+    // the FP32 single-pass sweep's divisor
+    k_diag_f32<<<blocks_for(F.g.n()), kThreads, 0, st>>>(F.g, F.op[OC], F.cc, m->d32);
+    note_launches(1);
   }
   m->cc_ready = 1;
   if (defer_check) {
@@ -1618,6 +1695,7 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
     m->info_pending = 1;
     return 1;
   }
+  CKM(cudaStreamWaitEvent(st, m->dense_ev, 0));
   int info = 0;
   CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKM(cudaStreamSynchronize(st));
@@ -1700,11 +1778,10 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const OpF fo = opf(F);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, m->d32, s->tune) != cudaSuccess) {
+  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, m->d32, s->tune, m->d_err, k) != cudaSuccess) {
     set_error("FP32 fine smoother launch failed");
     return 0;
   }
-  k += 2 * s->tune[11] + 1;
   const int tf = m->tail_first > 0 ? m->tail_first : nl;
   for (int l = 1; l < tf; l++) {
     MLevel& C = m->lev[l];
@@ -1719,6 +1796,8 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
       k++;
     }
   }
+  // the coarsest solve reads the dense inverse made on the side stream
+  CKM(cudaStreamWaitEvent(st, m->dense_ev, cudaEventWaitExternal));
   if (m->tail_first > 0) {
     if (!launch_tail(s, st)) return 0;
     k++;
@@ -1732,22 +1811,20 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     MLevel& C = m->lev[l + 1];
     MLevel& P = m->lev[l];
     if (l + 1 != tf || m->tail_first == 0) {
-      const size_t cint = (size_t)(C.g.nx - 2) * (C.g.ny - 2) * (C.g.nz - 2);
-      k_matvec_f32<<<blocks_for(cint), kThreads, 0, st>>>(C.g, opf(C), C.cc, C.x, m->w2);
-      dot_f32(st, C.g, C.x, C.w0, s->part, s->scal + S_XNUM_L + (l & 15));
-      dot_f32(st, C.g, C.x, m->w2, s->part + 2368, s->scal + S_XDEN_L + (l & 15));
-      k += 5;
+      damp_dots(st, C.g, opf(C), C.cc, C.x, C.w0, s->part, s->scal + S_XNUM_L + (l & 15),
+                s->scal + S_XDEN_L + (l & 15));
+      k += 2;
     }
     const size_t pint = (size_t)(P.g.nx - 2) * (P.g.ny - 2) * (P.g.nz - 2);
     k_interp_axpy_f32<<<blocks_for(pint), kThreads, 0, st>>>(
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
-      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, m->d32, s->tune) != cudaSuccess) {
+      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, m->d32, s->tune, m->d_err, k) !=
+          cudaSuccess) {
         set_error("FP32 fine smoother launch failed");
         return 0;
       }
-      k += 2 * s->tune[11];
     } else {
       if (!smooth27(st, P, m, l, 1, k, s->tune)) return 0;
     }
@@ -1764,10 +1841,20 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
 int read_scal(pmgb_solver* s, int slot, double* v) {
   CKM(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   MixedState* m = s->mixed;
+  int bulk_err = 0;
+  if (m) CKM(cudaMemcpyAsync(&bulk_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   int info = 0;
   const int check = m && m->info_pending;
-  if (check) CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (check) {
+    CKM(cudaStreamWaitEvent(s->stream, m->dense_ev, 0));
+    CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  }
   CKM(cudaStreamSynchronize(s->stream));
+  if (bulk_err) {
+    cudaMemsetAsync(m->d_err, 0, sizeof(int), s->stream);
+    set_error("mixed: a staged copy of the FP32 fine sweep did not complete");
+    return 0;
+  }
   if (check) {
     m->info_pending = 0;
     if (info != 0) {
@@ -1866,19 +1953,45 @@ int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
 }
 
 // One FP32 single-pass sweep for kernel timing: 28 B per point per sweep
-// (6 FP32 arrays read, x read and written once).
-int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
+// (6 FP32 arrays read, x read and written once); bulk selects the
+// bulk-staged kernel.  mixed_prepare_sweep makes the divisor first.
+int mixed_prepare_sweep(pmgb_solver* s) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
+  MixedState* m = s->mixed;
+  MLevel& F = m->lev[0];
+  if (!m->d32) {
+    set_error("pmgb_time_kernel: no FP32 fine sweep in this calculation");
+    return 0;
+  }
+  k_diag_f32<<<blocks_for(F.g.n()), kThreads, 0, s->stream>>>(F.g, F.op[OC], F.cc, m->d32);
+  CKM(cudaGetLastError());
+  return 1;
+}
+
+int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes, int bulk) {
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
   Gs7Rb<float> a = rb_f32(F, m->d32, s->tune);
   a.xin = F.x; a.xout = m->xs;
-  if (launch_gs7_rb<float>(s->stream, a, 1, s->tune[12]) != cudaSuccess) {
+  const cudaError_t e = bulk ? launch_gs7_rb_bulk<float>(s->stream, a, 1, s->tune[12] & 15,
+                                                         m->d_err)
+                             : launch_gs7_rb<float>(s->stream, a, 1, s->tune[12]);
+  if (e != cudaSuccess) {
     set_error("FP32 sweep launch failed");
     return 0;
   }
   *bytes = 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   return 1;
+}
+
+// the bulk sweep's error flag: 1 if a wait gave up since the last call
+int mixed_bulk_error(pmgb_solver* s) {
+  if (!s->mixed) return 0;
+  int v = 0;
+  cudaMemcpyAsync(&v, s->mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+  cudaMemsetAsync(s->mixed->d_err, 0, sizeof(int), s->stream);
+  cudaStreamSynchronize(s->stream);
+  return v;
 }
 
 // The coarse tail alone, for kernel timing.  Algorithmic bytes per tail

@@ -300,8 +300,16 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     return 0;
   }
   s->stream = s->own_stream;
+  if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("pmgb_create: stream creation failed");
+    cudaStreamDestroy(s->own_stream);
+    delete s;
+    return 0;
+  }
   for (int i = 0; i < 16; i++) s->tune[i] = g_tune[i];
   for (int i = 0; i < 8; i++) cudaEventCreate(&s->ev[i]);
+  cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming);
   const size_t n = s->n;
   int ok = 1;
   ok &= dalloc(&s->charge, n) && dalloc(&s->epsx, n) && dalloc(&s->epsy, n) &&
@@ -530,6 +538,9 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   free_maps(s);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
+  cudaEventDestroy(s->fork_ev);
+  cudaEventDestroy(s->join_ev);
+  cudaStreamDestroy(s->side);
   cudaStreamDestroy(s->own_stream);
   delete s;
 }
@@ -549,24 +560,91 @@ static int settle_fill(pmgb_solver* s) {
   return 1;
 }
 
+// sdh / mdh boundary values (bcCalc, vpmg.c:3369-3645 and 3289-3367) on
+// stream `sd`; the atom term buffer is already sized.
+static int side_boundary(pmgb_solver* s, cudaStream_t sd) {
+  const pmgb_params& p = s->p;
+  const int natoms = s->natoms;
+  const double pi = 3.14159265358979323846;
+  CK(cudaMemsetAsync(s->gx, 0, sizeof(double) * 2 * p.ny * p.nz, sd));
+  CK(cudaMemsetAsync(s->gy, 0, sizeof(double) * 2 * p.nx * p.nz, sd));
+  CK(cudaMemsetAsync(s->gz, 0, sizeof(double) * 2 * p.nx * p.ny, sd));
+  if (p.bcfl == PMGB_BCFL_SDH) {
+    SdhArgs A;
+    A.g = s->g;
+    for (int d = 0; d < 3; d++) A.center[d] = s->soluteCenter[d];
+    A.size = s->soluteRadius;
+    A.xkappa = s->xkappa;
+    A.eps_p = p.pdie;
+    A.eps_w = p.sdie;
+    A.pre = (1.6021773e-19 * 1.6021773e-19) /
+            (4 * pi * 8.8541878e-12 * 1.3806581e-23 * p.temp);
+    A.pre = A.pre * (1.0e10);
+    launch_sdh(sd, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf,
+               s->gx, s->gy, s->gz);
+    note_launches(3);
+  } else {
+    // bcflnew (vpmg.c:3289-3367)
+    MdhArgs A;
+    A.g = s->g;
+    A.xf = s->xf;
+    A.yf = s->yf;
+    A.zf = s->zf;
+    A.gx = s->gx;
+    A.gy = s->gy;
+    A.gz = s->gz;
+    A.pre1 = ((1.6021773e-19) / (4 * pi * 8.8541878e-12 * p.sdie * 1.3806581e-23 * p.temp)) *
+             (1.0e10);
+    A.xkappa = s->xkappa;
+    launch_mdh(sd, A, natoms, s->d_xyz, s->d_q, s->d_r);
+    note_launches(1);
+  }
+  CK(cudaGetLastError());
+  return 1;
+}
+
 static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int wait) {
   const pmgb_params& p = s->p;
   cudaStream_t st = s->stream;
   const size_t n = s->n;
   const int natoms = s->natoms;
   phys_setup(s, natoms, h_xyz, h_r);
+  const int side_bc = (p.bcfl == PMGB_BCFL_SDH || p.bcfl == PMGB_BCFL_MDH);
+  if (p.bcfl == PMGB_BCFL_SDH &&
+      !grow(&s->atom_terms, &s->terms_alloc, 13 * (size_t)natoms, st))
+    return 0;
   CK(cudaEventRecord(s->ev[0], st));
   CK(cudaMemsetAsync(s->d_npts, 0, sizeof(int), st));
+  // The charge map and the sdh/mdh boundary values depend on the atoms only:
+  // they run on the side stream while this stream builds the dielectric and
+  // ion maps, and every return from here on joins the two.
+  CK(cudaEventRecord(s->fork_ev, st));
+  CK(cudaStreamWaitEvent(s->side, s->fork_ev, 0));
+  struct SideJoin {
+    pmgb_solver* s;
+    int joined = 0;
+    cudaError_t join() {
+      if (joined) return cudaSuccess;
+      joined = 1;
+      cudaError_t e = cudaEventRecord(s->join_ev, s->side);
+      return e == cudaSuccess ? cudaStreamWaitEvent(s->stream, s->join_ev, 0) : e;
+    }
+    ~SideJoin() { join(); }
+  } side_join{s};
+  cudaStream_t sd = s->side;
   // charge (fillcoChargeSpline2)
-  CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
   if (uses_charge_map(s)) {
     // the charge map is read below (fillcoChargeMap)
-  } else if (p.chgm == PMGB_CHGM_TRIL) {
-    launch_charge_tril(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+    CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
   } else {
-    launch_charge_spl2(st, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+    CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), sd));
+    if (p.chgm == PMGB_CHGM_TRIL)
+      launch_charge_tril(sd, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+    else
+      launch_charge_spl2(sd, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
   }
   note_launches(1);
+  if (side_bc && !side_boundary(s, sd)) return 0;
   // with coefficient maps the operator is never a plain Laplacian
   // (Vpmg_fillco, vpmg.c:5354-5361)
   const int coef_maps = uses_coef_maps(s);
@@ -685,49 +763,17 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
       set_error("pmgb_fillco: bcfl focus needs pmgb_focus with a solved coarse calculation first");
       return 0;
     }
-  } else {
+  } else if (!side_bc) {
+    if (p.bcfl != PMGB_BCFL_ZERO) {
+      set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh, mdh, focus and map are)",
+                p.bcfl);
+      return 0;
+    }
     CK(cudaMemsetAsync(s->gx, 0, sizeof(double) * 2 * p.ny * p.nz, st));
     CK(cudaMemsetAsync(s->gy, 0, sizeof(double) * 2 * p.nx * p.nz, st));
     CK(cudaMemsetAsync(s->gz, 0, sizeof(double) * 2 * p.nx * p.ny, st));
   }
-  if (p.bcfl == PMGB_BCFL_SDH) {
-    SdhArgs A;
-    A.g = s->g;
-    for (int d = 0; d < 3; d++) A.center[d] = s->soluteCenter[d];
-    A.size = s->soluteRadius;
-    A.xkappa = s->xkappa;
-    A.eps_p = p.pdie;
-    A.eps_w = p.sdie;
-    const double pi = 3.14159265358979323846;
-    A.pre = (1.6021773e-19 * 1.6021773e-19) /
-            (4 * pi * 8.8541878e-12 * 1.3806581e-23 * p.temp);
-    A.pre = A.pre * (1.0e10);
-    if (!grow(&s->atom_terms, &s->terms_alloc, 13 * (size_t)natoms, st)) return 0;
-    launch_sdh(st, A, natoms, s->d_xyz, s->d_q, s->atom_terms, s->mom, s->xf, s->yf, s->zf, s->gx, s->gy,
-               s->gz);
-    note_launches(3);
-  } else if (p.bcfl == PMGB_BCFL_MDH) {
-    // bcflnew (vpmg.c:3289-3367)
-    MdhArgs A;
-    A.g = s->g;
-    A.xf = s->xf;
-    A.yf = s->yf;
-    A.zf = s->zf;
-    A.gx = s->gx;
-    A.gy = s->gy;
-    A.gz = s->gz;
-    const double pi = 3.14159265358979323846;
-    A.pre1 = ((1.6021773e-19) / (4 * pi * 8.8541878e-12 * p.sdie * 1.3806581e-23 * p.temp)) *
-             (1.0e10);
-    A.xkappa = s->xkappa;
-    launch_mdh(st, A, natoms, s->d_xyz, s->d_q, s->d_r);
-    note_launches(1);
-  } else if (p.bcfl != PMGB_BCFL_ZERO && p.bcfl != PMGB_BCFL_FOCUS &&
-             p.bcfl != PMGB_BCFL_MAP) {
-    set_error("pmgb_fillco: bcfl %d not implemented (zero, sdh, mdh, focus and map are)",
-              p.bcfl);
-    return 0;
-  }
+  CK(side_join.join());
   CK(cudaEventRecord(s->ev[1], st));
   CK(cudaGetLastError());
   s->filled = 1;
@@ -1435,8 +1481,8 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
     set_error("pmgb_time_kernel: solve first");
     return 0;
   }
-  if ((which == PMGB_K_GS7_FP32 ||
-       which == PMGB_K_VCYCLE_TAIL || which == PMGB_K_GS7_SWEEP_FP32) &&
+  if ((which == PMGB_K_GS7_FP32 || which == PMGB_K_VCYCLE_TAIL ||
+       which == PMGB_K_GS7_SWEEP_FP32 || which == PMGB_K_GS7_BULK_FP32) &&
       s->precision != PMGB_MIXED) {
     set_error("pmgb_time_kernel: kernel %d belongs to the mixed-precision path", which);
     return 0;
@@ -1445,6 +1491,9 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
   Level& F = s->lev[0];
   const double fint = (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   double b = 0.0;
+  if ((which == PMGB_K_GS7_SWEEP_FP32 || which == PMGB_K_GS7_BULK_FP32) &&
+      !mixed_prepare_sweep(s))
+    return 0;
   CK(cudaStreamSynchronize(st));
   CK(cudaEventRecord(s->ev[6], st));
   for (int r = 0; r < reps; r++) {
@@ -1495,7 +1544,8 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         b = 56.0 * fint;
         break;
       case PMGB_K_GS7_SWEEP_FP32:
-        if (!mixed_time_gs7_sweep(s, &b)) return 0;
+      case PMGB_K_GS7_BULK_FP32:
+        if (!mixed_time_gs7_sweep(s, &b, which == PMGB_K_GS7_BULK_FP32)) return 0;
         break;
       default:
         set_error("pmgb_time_kernel: unknown kernel %d", which);
@@ -1505,6 +1555,10 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
   CK(cudaEventRecord(s->ev[7], st));
   CK(cudaEventSynchronize(s->ev[7]));
   CK(cudaGetLastError());
+  if (which == PMGB_K_GS7_BULK_FP32 && mixed_bulk_error(s)) {
+    set_error("pmgb_time_kernel: a staged copy of the bulk sweep did not complete");
+    return 0;
+  }
   *ms = elapsed_ms(s->ev[6], s->ev[7]) / reps;
   *bytes = b;
   note_launches(reps);

@@ -70,6 +70,10 @@ struct pmgb_solver {
   int device;
   cudaStream_t stream;      // stream all work is issued on
   cudaStream_t own_stream;  // created with the solver
+  // second stream of the fill: the charge map and the boundary values run on
+  // it beside the dielectric and ion maps (forked from and joined to `stream`)
+  cudaStream_t side;
+  cudaEvent_t fork_ev, join_ev;
   size_t n;
   Grid g;
   // physics scalars (Vpbe_ctor2, src/generic/vpbe.c:264-450)
