@@ -42,6 +42,23 @@ __device__ inline double warp_sum(double v) {
   return v;
 }
 
+// Interior point q (i fastest) -> (i, j, k), 1-based interior indices, with
+// 32-bit divisions where the interior count allows (it does up to 1025^3).
+__device__ __forceinline__ void interior_ijk(size_t q, int nx, int ny, int& i, int& j, int& k) {
+  const unsigned ex = (unsigned)(nx - 2), ey = (unsigned)(ny - 2);
+  if (q <= 0xffffffffull) {
+    const unsigned u = (unsigned)q, t = u / ex, kk = t / ey;
+    i = 1 + (int)(u - t * ex);
+    j = 1 + (int)(t - kk * ey);
+    k = 1 + (int)kk;
+  } else {
+    const size_t t = q / ex, kk = t / ey;
+    i = 1 + (int)(q - t * ex);
+    j = 1 + (int)(t - kk * ey);
+    k = 1 + (int)kk;
+  }
+}
+
 template <int NT>
 __device__ inline double block_sum(double v, double* sh) {
   v = warp_sum(v);

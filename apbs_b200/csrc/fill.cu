@@ -12,9 +12,11 @@
 namespace pmgb {
 
 // ---------------------------------------------------------------------------
-// Charge: fillcoChargeSpline2 + bspline2 (vpmg.c:5091-5248).  One thread per
-// atom, 64 scatter-adds.  FP64 atomics make the per-point accumulation order
-// run-dependent (the sum is exact to round-off either way).
+// Charge: fillcoChargeSpline2 + bspline2 (vpmg.c:5091-5248) and the
+// trilinear fillcoChargeSpline1 (vpmg.c:4986-5121), gathered per tile of grid
+// points (k_charge_gather below) so that every point adds its atoms'
+// contributions in atom order, as the reference's atom loop does: the map is
+// the reference's bit for bit and the same on every run.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double bspline2(double x) {
   double m2m, m2, m3;
@@ -27,36 +29,12 @@ __device__ __forceinline__ double bspline2(double x) {
   return m3;
 }
 
-__global__ void k_charge_spl2(FillGeom G, int natoms, const double* __restrict__ xyz,
-                              const double* __restrict__ q, double zmagic, double* charge) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= natoms) return;
-  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
-  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
-  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2];
-  if ((ax <= (G.xmin[0] - hx)) || (ax >= (G.xmax[0] + hx)) || (ay <= (G.xmin[1] - hy)) ||
-      (ay >= (G.xmax[1] + hy)) || (az <= (G.xmin[2] - hz)) || (az >= (G.xmax[2] + hz)))
-    return;
-  const double px = ax - G.xmin[0], py = ay - G.xmin[1], pz = az - G.xmin[2];
-  const double c = q[a] * zmagic / (hx * hy * hz);
-  const double fi = px / hx, fj = py / hy, fk = pz / hz;
-  int ip1 = (int)ceil(fi), im1 = (int)floor(fi);
-  int jp1 = (int)ceil(fj), jm1 = (int)floor(fj);
-  int kp1 = (int)ceil(fk), km1 = (int)floor(fk);
-  int ip2 = ip1 + 1, im2 = im1 - 1, jp2 = jp1 + 1, jm2 = jm1 - 1, kp2 = kp1 + 1, km2 = km1 - 1;
-  ip2 = min(ip2, nx - 1); im2 = max(im2, 0);
-  jp2 = min(jp2, ny - 1); jm2 = max(jm2, 0);
-  kp2 = min(kp2, nz - 1); km2 = max(km2, 0);
-  for (int ii = im2; ii <= ip2; ii++) {
-    const double mx = bspline2(1.5 + ((double)ii - fi));
-    for (int jj = jm2; jj <= jp2; jj++) {
-      const double my = bspline2(1.5 + ((double)jj - fj));
-      for (int kk = km2; kk <= kp2; kk++) {
-        const double mz = bspline2(1.5 + ((double)kk - fk));
-        atomicAdd(charge + G.g.idx(ii, jj, kk), (c * mx * my * mz));
-      }
-    }
-  }
+// Products and sums rounded one by one, as the reference's C evaluates
+// them: the geometry tests below never fuse a multiply-add.
+__device__ __forceinline__ double sq_rn(double v) { return __dmul_rn(v, v); }
+// (pos - h f)^2 of markSphere
+__device__ __forceinline__ double off2_rn(double pos, double h, double f) {
+  return sq_rn(__dsub_rn(pos, __dmul_rn(h, f)));
 }
 
 // ---------------------------------------------------------------------------
@@ -69,7 +47,7 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
                                                   double* array, double markVal, int lane,
                                                   int nlanes) {
   const double posx = cx - xmin, posy = cy - ymin, posz = cz - zmin;
-  const double rtot2 = rtot * rtot;
+  const double rtot2 = __dmul_rn(rtot, rtot);
   const double xr = rtot + 0.5 * hx, yr = rtot + 0.5 * hy, zr = rtot + 0.5 * hz;
   const int imin = max(0, (int)ceil((posx - xr) / hx));
   const int jmin = max(0, (int)ceil((posy - yr) / hy));
@@ -86,15 +64,14 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
   for (int t = lane; t < ni * nj; t += nlanes) {
     const int ii = imin + t % ni, jj = jmin + t / ni;
     const double fi = (double)ii, fj = (double)jj;
-    const double dx2 = (posx - hx * fi) * (posx - hx * fi);
-    const double dy2 = (posy - hy * fj) * (posy - hy * fj);
-    if ((dx2 + dy2) > rtot2) continue;
+    const double dx2 = off2_rn(posx, hx, fi);
+    const double dy2 = off2_rn(posy, hy, fj);
+    if (__dadd_rn(dx2, dy2) > rtot2) continue;
     double* col = array + g.idx(ii, jj, 0);
     const size_t sz = (size_t)g.nx * g.ny;
     for (int kk = kmin; kk <= kmax; kk++) {
-      const double fk = (double)kk;
-      const double dz2 = (posz - hz * fk) * (posz - hz * fk);
-      if ((dz2 + dy2 + dx2) <= rtot2) col[kk * sz] = markVal;
+      const double dz2 = off2_rn(posz, hz, (double)kk);
+      if (__dadd_rn(__dadd_rn(dz2, dy2), dx2) <= rtot2) col[kk * sz] = markVal;
     }
   }
 }
@@ -164,25 +141,32 @@ __global__ void k_cell_count(CellGrid C, int natoms, const double* __restrict__ 
 }
 
 __global__ void k_scan_single(const int* count, int n, int* start) {
-  // one block: exclusive scan, serial per chunk (cell counts are small)
-  __shared__ int sums[1024];
-  const int t = threadIdx.x, nt = blockDim.x;
+  // one block: thread t sums a chunk of counts, the chunk sums are scanned
+  // with warp shuffles, then each thread writes its chunk's prefixes
+  __shared__ int wsum[32];
+  const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
   const int chunk = (n + nt - 1) / nt;
+  const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
   int s = 0;
-  for (int i = t * chunk; i < min(n, (t + 1) * chunk); i++) s += count[i];
-  sums[t] = s;
+  for (int i = lo; i < hi; i++) s += count[i];
+  int v = s;  // inclusive scan within the warp
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) wsum[w] = v;
   __syncthreads();
-  if (t == 0) {
-    int acc = 0;
-    for (int i = 0; i < nt; i++) {
-      int v = sums[i];
-      sums[i] = acc;
-      acc += v;
+  if (w == 0) {
+    int u = (lane < nt / 32) ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, u, o);
+      if (lane >= o) u += y;
     }
+    wsum[lane] = u;
   }
   __syncthreads();
-  int acc = sums[t];
-  for (int i = t * chunk; i < min(n, (t + 1) * chunk); i++) {
+  int acc = v - s + (w > 0 ? wsum[w - 1] : 0);
+  for (int i = lo; i < hi; i++) {
     start[i] = acc;
     acc += count[i];
   }
@@ -195,6 +179,22 @@ __global__ void k_cell_fill(int natoms, const int* __restrict__ cell_of, int* fi
   if (a >= natoms) return;
   const int p = atomicAdd(fillpos + cell_of[a], 1);
   atoms_sorted[p] = a;
+}
+
+// Surface point t of atom a: (r_a + srad) ref_t + x_a (Vacc_atomSurf,
+// vacc.c:889-891), rounded as the reference computes it.
+__device__ __forceinline__ void sas_point(const double* __restrict__ xyz,
+                                          const double* __restrict__ r,
+                                          const double* __restrict__ ref, int a, int t,
+                                          double srad, double& px, double& py, double& pz) {
+  const double rad = r[a] + srad;
+  px = __dadd_rn(__dmul_rn(rad, ref[3 * t + 0]), xyz[3 * a + 0]);
+  py = __dadd_rn(__dmul_rn(rad, ref[3 * t + 1]), xyz[3 * a + 1]);
+  pz = __dadd_rn(__dmul_rn(rad, ref[3 * t + 2]), xyz[3 * a + 2]);
+}
+// ivdwAccExclus's squared distance (vacc.c:118-119)
+__device__ __forceinline__ double dist2_rn(double d0, double d1, double d2) {
+  return __dadd_rn(__dadd_rn(sq_rn(d0), sq_rn(d1)), sq_rn(d2));
 }
 
 // The atoms that can exclude a surface point of atom a: a point lies at
@@ -288,32 +288,27 @@ __global__ void __launch_bounds__(256) k_sas_test(
       for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
         const int b = lst[q];
         const double rr = r[b] + srad;
-        ex[q] = make_double4(xyz[3 * b], xyz[3 * b + 1], xyz[3 * b + 2], rr * rr);
+        ex[q] = make_double4(xyz[3 * b], xyz[3 * b + 1], xyz[3 * b + 2], sq_rn(rr));
       }
       __syncthreads();
     }
     bool acc = false;
     if (t < nref) {
-      const double rad = arad + srad;
-      const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
-      const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
-      const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+      double px, py, pz;
+      sas_point(xyz, r, ref, a, t, srad, px, py, pz);
       acc = true;
       if (staged) {
         for (int q = 0; q < cnt; q++) {
           const double4 e = ex[q];
-          const double d0 = px - e.x, d1 = py - e.y, d2 = pz - e.z;
-          if (d0 * d0 + d1 * d1 + d2 * d2 < e.w) {
+          if (dist2_rn(px - e.x, py - e.y, pz - e.z) < e.w) {
             acc = false;
             break;
           }
         }
       } else {
         auto excludes = [&](int b) {
-          const double d0 = px - xyz[3 * b], d1 = py - xyz[3 * b + 1], d2 = pz - xyz[3 * b + 2];
-          const double dist2 = d0 * d0 + d1 * d1 + d2 * d2;
           const double rr = r[b] + srad;
-          return dist2 < rr * rr;
+          return dist2_rn(px - xyz[3 * b], py - xyz[3 * b + 1], pz - xyz[3 * b + 2]) < sq_rn(rr);
         };
         int c[3];
         const double pp[3] = {px, py, pz};
@@ -364,11 +359,9 @@ __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
   for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < n;
        w += nwarps) {
     const unsigned tid = list[w];
-    const int a = (int)(tid / (unsigned)nref), t = (int)(tid % (unsigned)nref);
-    const double rad = r[a] + srad;
-    const double px = rad * (ref[3 * t + 0]) + xyz[3 * a + 0];
-    const double py = rad * (ref[3 * t + 1]) + xyz[3 * a + 1];
-    const double pz = rad * (ref[3 * t + 2]) + xyz[3 * a + 2];
+    double px, py, pz;
+    sas_point(xyz, r, ref, (int)(tid / (unsigned)nref), (int)(tid % (unsigned)nref), srad, px,
+              py, pz);
     mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
                       G.xmin[2], epsx, epsw, lane, 32);
     mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
@@ -379,9 +372,19 @@ __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
 }
 
 // 9-point harmonic-mean smoothing, fillcoCoefMolDielSmooth (vpmg.c:4500-4628).
-// a1..a3 are the unsmoothed maps.
+// a1..a3 are the unsmoothed maps.  Their values are the two dielectric
+// constants v0 and v1 almost everywhere, so 1 / a comes from a table of the
+// two reciprocals (the same correctly rounded quotients) with a division
+// only for any other value.
+struct InvPair {
+  double v0, r0, v1, r1;
+  __device__ __forceinline__ double operator()(double a) const {
+    return a == v0 ? r0 : (a == v1 ? r1 : 1.0 / a);
+  }
+};
+
 __global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __restrict__ a2,
-                         const double* __restrict__ a3, double* epsx, double* epsy,
+                         const double* __restrict__ a3, InvPair inv, double* epsx, double* epsy,
                          double* epsz) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t n = g.n();
@@ -390,48 +393,48 @@ __global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __
     const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
     double frac;
     int np;
-    frac = 1.0 / a1[q];
-    frac += 1.0 / a2[q];
-    frac += 1.0 / a3[q];
+    frac = inv(a1[q]);
+    frac += inv(a2[q]);
+    frac += inv(a3[q]);
     np = 3;
-    if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k)]; np += 1; }
-    if (k > 0) { frac += 1.0 / a3[g.idx(i, j, k - 1)]; np += 1; }
+    if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k)]); np += 1; }
+    if (k > 0) { frac += inv(a3[g.idx(i, j, k - 1)]); np += 1; }
     if (i < (nx - 1)) {
-      frac += 1.0 / a2[g.idx(i + 1, j, k)];
-      frac += 1.0 / a3[g.idx(i + 1, j, k)];
+      frac += inv(a2[g.idx(i + 1, j, k)]);
+      frac += inv(a3[g.idx(i + 1, j, k)]);
       np += 2;
-      if (j > 0) { frac += 1.0 / a2[g.idx(i + 1, j - 1, k)]; np += 1; }
-      if (k > 0) { frac += 1.0 / a3[g.idx(i + 1, j, k - 1)]; np += 1; }
+      if (j > 0) { frac += inv(a2[g.idx(i + 1, j - 1, k)]); np += 1; }
+      if (k > 0) { frac += inv(a3[g.idx(i + 1, j, k - 1)]); np += 1; }
     }
     epsx[q] = np / frac;
 
-    frac = 1.0 / a2[q];
-    frac += 1.0 / a1[q];
-    frac += 1.0 / a3[q];
+    frac = inv(a2[q]);
+    frac += inv(a1[q]);
+    frac += inv(a3[q]);
     np = 3;
-    if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k)]; np += 1; }
-    if (k > 0) { frac += 1.0 / a3[g.idx(i, j, k - 1)]; np += 1; }
+    if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k)]); np += 1; }
+    if (k > 0) { frac += inv(a3[g.idx(i, j, k - 1)]); np += 1; }
     if (j < (ny - 1)) {
-      frac += 1.0 / a1[g.idx(i, j + 1, k)];
-      frac += 1.0 / a3[g.idx(i, j + 1, k)];
+      frac += inv(a1[g.idx(i, j + 1, k)]);
+      frac += inv(a3[g.idx(i, j + 1, k)]);
       np += 2;
-      if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j + 1, k)]; np += 1; }
-      if (k > 0) { frac += 1.0 / a3[g.idx(i, j + 1, k - 1)]; np += 1; }
+      if (i > 0) { frac += inv(a1[g.idx(i - 1, j + 1, k)]); np += 1; }
+      if (k > 0) { frac += inv(a3[g.idx(i, j + 1, k - 1)]); np += 1; }
     }
     epsy[q] = np / frac;
 
-    frac = 1.0 / a3[q];
-    frac += 1.0 / a1[q];
-    frac += 1.0 / a2[q];
+    frac = inv(a3[q]);
+    frac += inv(a1[q]);
+    frac += inv(a2[q]);
     np = 3;
-    if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k)]; np += 1; }
-    if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k)]; np += 1; }
+    if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k)]); np += 1; }
+    if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k)]); np += 1; }
     if (k < (nz - 1)) {
-      frac += 1.0 / a1[g.idx(i, j, k + 1)];
-      frac += 1.0 / a2[g.idx(i, j, k + 1)];
+      frac += inv(a1[g.idx(i, j, k + 1)]);
+      frac += inv(a2[g.idx(i, j, k + 1)]);
       np += 2;
-      if (i > 0) { frac += 1.0 / a1[g.idx(i - 1, j, k + 1)]; np += 1; }
-      if (j > 0) { frac += 1.0 / a2[g.idx(i, j - 1, k + 1)]; np += 1; }
+      if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k + 1)]); np += 1; }
+      if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k + 1)]); np += 1; }
     }
     epsz[q] = np / frac;
   }
@@ -580,40 +583,6 @@ void launch_fill_value(cudaStream_t s, double* a, size_t n, double v) {
 // grid points shared by several atoms sum in a different order than the
 // reference's atom loop).
 // ---------------------------------------------------------------------------
-__global__ void k_charge_tril(FillGeom G, int natoms, const double* __restrict__ xyz,
-                              const double* __restrict__ q, double zmagic, double* charge) {
-  const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= natoms) return;
-  const int nx = G.g.nx, ny = G.g.ny;
-  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
-  const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2];
-  if ((ax <= G.xmin[0]) || (ax >= G.xmax[0]) || (ay <= G.xmin[1]) || (ay >= G.xmax[1]) ||
-      (az <= G.xmin[2]) || (az >= G.xmax[2]))
-    return;
-  const double px = ax - G.xmin[0], py = ay - G.xmin[1], pz = az - G.xmin[2];
-  const double c = q[a] * zmagic / (hx * hy * hz);
-  const double fi = px / hx, fj = py / hy, fk = pz / hz;
-  const int ihi = (int)ceil(fi), ilo = (int)floor(fi);
-  const int jhi = (int)ceil(fj), jlo = (int)floor(fj);
-  const int khi = (int)ceil(fk), klo = (int)floor(fk);
-  const double dx = fi - (double)(ilo), dy = fj - (double)(jlo), dz = fk - (double)(klo);
-  auto at = [&](int i, int j, int k) { return ((size_t)k * ny + j) * nx + i; };
-  atomicAdd(&charge[at(ihi, jhi, khi)], (dx * dy * dz * c));
-  atomicAdd(&charge[at(ihi, jlo, khi)], (dx * (1.0 - dy) * dz * c));
-  atomicAdd(&charge[at(ihi, jhi, klo)], (dx * dy * (1.0 - dz) * c));
-  atomicAdd(&charge[at(ihi, jlo, klo)], (dx * (1.0 - dy) * (1.0 - dz) * c));
-  atomicAdd(&charge[at(ilo, jhi, khi)], ((1.0 - dx) * dy * dz * c));
-  atomicAdd(&charge[at(ilo, jlo, khi)], ((1.0 - dx) * (1.0 - dy) * dz * c));
-  atomicAdd(&charge[at(ilo, jhi, klo)], ((1.0 - dx) * dy * (1.0 - dz) * c));
-  atomicAdd(&charge[at(ilo, jlo, klo)], ((1.0 - dx) * (1.0 - dy) * (1.0 - dz) * c));
-}
-
-void launch_charge_tril(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                        const double* q, double zmagic, double* charge) {
-  if (natoms <= 0) return;
-  k_charge_tril<<<(natoms + 127) / 128, 128, 0, s>>>(G, natoms, xyz, q, zmagic, charge);
-}
-
 // ---------------------------------------------------------------------------
 // bcfl mdh: bcflnew (src/mg/vpmg.c:3289-3367, packUnpack 3220-3287).  One
 // thread per stored face value sums, over all atoms in atom order, the
@@ -769,11 +738,242 @@ void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double
   k_qf_point_final<<<1, 256, 0, s>>>(part, nb, out);
 }
 
-void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                        const double* q, double zmagic, double* charge) {
-  if (natoms <= 0) return;
-  k_charge_spl2<<<(natoms + 127) / 128, 128, 0, s>>>(G, natoms, xyz, q, zmagic, charge);
+// ---------------------------------------------------------------------------
+// Deterministic charge spreading.  Atoms inside the method's acceptance band
+// are binned by the 8^3 tile of grid points that holds floor(position / h);
+// an atom's stencil (floor - 1 .. ceil + 1 per axis) reaches at most the
+// neighbouring tiles.  One CTA per tile gathers the atoms of the 27 bins
+// around it, sorts them by atom index and adds their contributions point by
+// point in that order, each term the reference's expression.  A tile with
+// more than kChCap candidates (far denser than any molecule) runs in passes
+// over windows of kChCap consecutive atom indices, which keeps the order.
+// ---------------------------------------------------------------------------
+constexpr int kChTile = 8;
+constexpr int kChCap = 512;
+constexpr int kChThreads = 128;
+
+// KIND 2: bspline2 (fillcoChargeSpline2), KIND 1: trilinear
+template <int KIND>
+__device__ __forceinline__ bool charge_in_band(const FillGeom& G, double ax, double ay,
+                                               double az) {
+  if (KIND == 2)
+    return !((ax <= (G.xmin[0] - G.h[0])) || (ax >= (G.xmax[0] + G.h[0])) ||
+             (ay <= (G.xmin[1] - G.h[1])) || (ay >= (G.xmax[1] + G.h[1])) ||
+             (az <= (G.xmin[2] - G.h[2])) || (az >= (G.xmax[2] + G.h[2])));
+  return !((ax <= G.xmin[0]) || (ax >= G.xmax[0]) || (ay <= G.xmin[1]) ||
+           (ay >= G.xmax[1]) || (az <= G.xmin[2]) || (az >= G.xmax[2]));
 }
+
+__device__ __forceinline__ int charge_tile_axis(double f, int ntile) {
+  const int fl = (int)floor(f);
+  const int t = fl >= 0 ? fl / kChTile : -1;
+  return min(max(t, 0), ntile - 1);
+}
+
+template <int KIND>
+__device__ __forceinline__ int charge_tile(const FillGeom& G, const int* nt, const double* xyz,
+                                           int a) {
+  const double fi = (xyz[3 * a] - G.xmin[0]) / G.h[0];
+  const double fj = (xyz[3 * a + 1] - G.xmin[1]) / G.h[1];
+  const double fk = (xyz[3 * a + 2] - G.xmin[2]) / G.h[2];
+  return (charge_tile_axis(fk, nt[2]) * nt[1] + charge_tile_axis(fj, nt[1])) * nt[0] +
+         charge_tile_axis(fi, nt[0]);
+}
+
+struct ChargeTiles {
+  int n[3];
+};
+
+template <int KIND>
+__global__ void k_chtile_count(FillGeom G, ChargeTiles T, int natoms,
+                               const double* __restrict__ xyz, int* count) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  if (!charge_in_band<KIND>(G, xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2])) return;
+  atomicAdd(count + charge_tile<KIND>(G, T.n, xyz, a), 1);
+}
+
+template <int KIND>
+__global__ void k_chtile_fill(FillGeom G, ChargeTiles T, int natoms,
+                              const double* __restrict__ xyz, int* fillpos, int* atoms) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  if (!charge_in_band<KIND>(G, xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2])) return;
+  atoms[atomicAdd(fillpos + charge_tile<KIND>(G, T.n, xyz, a), 1)] = a;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kChThreads) k_charge_gather(
+    FillGeom G, ChargeTiles T, int natoms, const double* __restrict__ xyz,
+    const double* __restrict__ q, double zmagic, const int* __restrict__ start,
+    const int* __restrict__ atoms, double* charge) {
+  // thread t owns the points (i, j) = (t % 8, (t / 8) % 8) of planes
+  // t / 64 + 2 r of the tile, r = 0..3
+  constexpr int PPT = kChTile * kChTile * kChTile / kChThreads;
+  __shared__ int cand[kChCap], sorted[kChCap];
+  __shared__ double cf[3][kChCap];  // fi, fj, fk
+  __shared__ double cq[kChCap];     // q zmagic / (hx hy hz)
+  __shared__ int cb[6][kChCap];     // stencil bounds per axis (lo, hi)
+  __shared__ int ncand, total;
+  const int tx = blockIdx.x % T.n[0], ty = (blockIdx.x / T.n[0]) % T.n[1];
+  const int tz = blockIdx.x / (T.n[0] * T.n[1]);
+  const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz;
+  const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  const int i = tx * kChTile + threadIdx.x % kChTile;
+  const int j = ty * kChTile + (threadIdx.x / kChTile) % kChTile;
+  const int kb = tz * kChTile + threadIdx.x / (kChTile * kChTile);
+  if (threadIdx.x == 0) total = 0;
+  __syncthreads();
+  // threads 0..26 own one neighbour bin each
+  int b0 = 0, b1 = 0;
+  if (threadIdx.x < 27) {
+    const int bx = tx + threadIdx.x % 3 - 1, by = ty + (threadIdx.x / 3) % 3 - 1,
+              bz = tz + threadIdx.x / 9 - 1;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < T.n[0] && by < T.n[1] && bz < T.n[2]) {
+      const int b = (bz * T.n[1] + by) * T.n[0] + bx;
+      b0 = start[b];
+      b1 = start[b + 1];
+      if (b1 > b0) atomicAdd(&total, b1 - b0);
+    }
+  }
+  __syncthreads();
+  const int tot = total;
+  double acc[PPT];
+#pragma unroll
+  for (int r = 0; r < PPT; r++) acc[r] = 0.0;
+  const int npass = tot <= kChCap ? (tot > 0 ? 1 : 0) : (natoms + kChCap - 1) / kChCap;
+  for (int pass = 0; pass < npass; pass++) {
+    const int wlo = npass == 1 ? 0 : pass * kChCap;
+    const int whi = npass == 1 ? natoms : min(natoms, wlo + kChCap);
+    if (threadIdx.x == 0) ncand = 0;
+    __syncthreads();
+    for (int e = b0; e < b1; e++) {
+      const int a = atoms[e];
+      if (a >= wlo && a < whi) cand[atomicAdd(&ncand, 1)] = a;
+    }
+    __syncthreads();
+    const int nc = ncand;
+    // rank sort by atom index (the indices are distinct)
+    for (int e = threadIdx.x; e < nc; e += kChThreads) {
+      const int key = cand[e];
+      int rank = 0;
+      for (int f = 0; f < nc; f++) rank += cand[f] < key;
+      sorted[rank] = key;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nc; e += kChThreads) {
+      const int a = sorted[e];
+      const double px = xyz[3 * a] - G.xmin[0], py = xyz[3 * a + 1] - G.xmin[1],
+                   pz = xyz[3 * a + 2] - G.xmin[2];
+      const double fi = px / hx, fj = py / hy, fk = pz / hz;
+      cq[e] = q[a] * zmagic / (hx * hy * hz);
+      cf[0][e] = fi;
+      cf[1][e] = fj;
+      cf[2][e] = fk;
+      if (KIND == 2) {
+        // the loop bounds of fillcoChargeSpline2 (vpmg.c:5207-5224)
+        cb[0][e] = max((int)floor(fi) - 1, 0);
+        cb[1][e] = min((int)ceil(fi) + 1, nx - 1);
+        cb[2][e] = max((int)floor(fj) - 1, 0);
+        cb[3][e] = min((int)ceil(fj) + 1, ny - 1);
+        cb[4][e] = max((int)floor(fk) - 1, 0);
+        cb[5][e] = min((int)ceil(fk) + 1, nz - 1);
+      } else {
+        cb[0][e] = (int)floor(fi);
+        cb[1][e] = (int)ceil(fi);
+        cb[2][e] = (int)floor(fj);
+        cb[3][e] = (int)ceil(fj);
+        cb[4][e] = (int)floor(fk);
+        cb[5][e] = (int)ceil(fk);
+      }
+    }
+    __syncthreads();
+    if (i < nx && j < ny) {
+      for (int e = 0; e < nc; e++) {
+        if (KIND == 2) {
+          if (i < cb[0][e] || i > cb[1][e] || j < cb[2][e] || j > cb[3][e]) continue;
+          const double c = cq[e], fk = cf[2][e];
+          const double mx = bspline2(1.5 + ((double)i - cf[0][e]));
+          const double my = bspline2(1.5 + ((double)j - cf[1][e]));
+#pragma unroll
+          for (int r = 0; r < PPT; r++) {
+            const int k = kb + 2 * r;
+            if (k < cb[4][e] || k > cb[5][e]) continue;
+            const double mz = bspline2(1.5 + ((double)k - fk));
+            acc[r] += (c * mx * my * mz);
+          }
+        } else {
+          const int ilo = cb[0][e], ihi = cb[1][e], jlo = cb[2][e], jhi = cb[3][e];
+          const int klo = cb[4][e], khi = cb[5][e];
+          if ((i != ihi && i != ilo) || (j != jhi && j != jlo)) continue;
+          const double c = cq[e];
+          const double dx = cf[0][e] - (double)(ilo), dy = cf[1][e] - (double)(jlo),
+                       dz = cf[2][e] - (double)(klo);
+#pragma unroll
+          for (int r = 0; r < PPT; r++) {
+            const int k = kb + 2 * r;
+            if (k != khi && k != klo) continue;
+            double v = acc[r];
+            // the eight corner terms in the reference's statement order
+            if (i == ihi && j == jhi && k == khi) v += (dx * dy * dz * c);
+            if (i == ihi && j == jlo && k == khi) v += (dx * (1.0 - dy) * dz * c);
+            if (i == ihi && j == jhi && k == klo) v += (dx * dy * (1.0 - dz) * c);
+            if (i == ihi && j == jlo && k == klo) v += (dx * (1.0 - dy) * (1.0 - dz) * c);
+            if (i == ilo && j == jhi && k == khi) v += ((1.0 - dx) * dy * dz * c);
+            if (i == ilo && j == jlo && k == khi) v += ((1.0 - dx) * (1.0 - dy) * dz * c);
+            if (i == ilo && j == jhi && k == klo) v += ((1.0 - dx) * dy * (1.0 - dz) * c);
+            if (i == ilo && j == jlo && k == klo)
+              v += ((1.0 - dx) * (1.0 - dy) * (1.0 - dz) * c);
+            acc[r] = v;
+          }
+        }
+      }
+    }
+    __syncthreads();  // the next pass refills the candidate arrays
+  }
+  if (i < nx && j < ny)
+#pragma unroll
+    for (int r = 0; r < PPT; r++) {
+      const int k = kb + 2 * r;
+      if (k < nz) charge[G.g.idx(i, j, k)] = acc[r];
+    }
+}
+
+size_t charge_tile_count(const Grid& g) {
+  return (size_t)((g.nx + kChTile - 1) / kChTile) * ((g.ny + kChTile - 1) / kChTile) *
+         ((g.nz + kChTile - 1) / kChTile);
+}
+
+// kind 2: bspline2, 1: trilinear.  count, start, fillpos: charge_tile_count + 1
+// ints; atoms: natoms ints.  Every point of the map is written.
+void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, const double* xyz,
+                   const double* q, double zmagic, int* count, int* start, int* fillpos,
+                   int* atoms, double* charge) {
+  ChargeTiles T;
+  T.n[0] = (G.g.nx + kChTile - 1) / kChTile;
+  T.n[1] = (G.g.ny + kChTile - 1) / kChTile;
+  T.n[2] = (G.g.nz + kChTile - 1) / kChTile;
+  const int nt = T.n[0] * T.n[1] * T.n[2];
+  const int nb = std::max(1, (natoms + 255) / 256);
+  cudaMemsetAsync(count, 0, sizeof(int) * nt, s);
+  if (natoms > 0) {
+    if (kind == 2) k_chtile_count<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
+    else k_chtile_count<1><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
+  }
+  k_scan_single<<<1, 1024, 0, s>>>(count, nt, start);
+  cudaMemcpyAsync(fillpos, start, sizeof(int) * nt, cudaMemcpyDeviceToDevice, s);
+  if (natoms > 0) {
+    if (kind == 2) k_chtile_fill<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
+    else k_chtile_fill<1><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
+  }
+  if (kind == 2)
+    k_charge_gather<2><<<nt, kChThreads, 0, s>>>(G, T, natoms, xyz, q, zmagic, start, atoms,
+                                                 charge);
+  else
+    k_charge_gather<1><<<nt, kChThreads, 0, s>>>(G, T, natoms, xyz, q, zmagic, start, atoms,
+                                                 charge);
+}
+
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                             const double* r, double srad, double epsp, double* epsx,
                             double* epsy, double* epsz) {
@@ -796,18 +996,24 @@ void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const doub
 }
 size_t sas_nbr_ints(int natoms) { return (size_t)natoms * (kNbrCap + 1); }
 
-void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
-                const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, int* nbr, unsigned* list,
-                int* npts, double* epsx, double* epsy, double* epsz) {
+void launch_sas_test(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
+                     const double* r, const double* ref, int nref, double srad,
+                     const int* start, const int* sorted, int* nbr, unsigned* list, int* npts) {
   const long long tot = (long long)natoms * nref;
   if (tot <= 0) return;
   cudaMemsetAsync(npts, 0, sizeof(int), s);
   int* ncount = nbr + (size_t)natoms * kNbrCap;
   k_sas_nbr<<<(natoms + 7) / 8, 256, 0, s>>>(C, natoms, xyz, r, srad, start, sorted, nbr, ncount);
-  k_sas_test<<<dim3((nref + 255) / 256, std::min(natoms, 65535)), 256, 0, s>>>(C, natoms, xyz, r, ref, nref,
-                                                              srad, start, sorted, nbr, ncount,
-                                                              list, npts);
+  k_sas_test<<<dim3((nref + 255) / 256, std::min(natoms, 65535)), 256, 0, s>>>(
+      C, natoms, xyz, r, ref, nref, srad, start, sorted, nbr, ncount, list, npts);
+}
+
+void launch_sas_mark(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                     const double* r, const double* ref, int nref, double srad, double epsw,
+                     const unsigned* list, const int* npts, double* epsx, double* epsy,
+                     double* epsz) {
+  const long long tot = (long long)natoms * nref;
+  if (tot <= 0) return;
   static const int nblocks = [] {
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
@@ -824,8 +1030,10 @@ void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms
                                 epsz);
 }
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
-                   const double* a3, double* epsx, double* epsy, double* epsz) {
-  k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, a1, a2, a3, epsx, epsy, epsz);
+                   const double* a3, double v0, double v1, double* epsx, double* epsy,
+                   double* epsz) {
+  InvPair inv{v0, 1.0 / v0, v1, 1.0 / v1};
+  k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, a1, a2, a3, inv, epsx, epsy, epsz);
 }
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* q, double* terms, double* mom, const double* xf,

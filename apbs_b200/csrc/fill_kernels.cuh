@@ -39,8 +39,13 @@ struct MdhArgs {
   double pre1;    // e_c / (4 pi eps0 eps_w k_B T) * 1e10
   double xkappa;  // 1/A
 };
-void launch_charge_tril(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                        const double* q, double zmagic, double* charge);
+// charge map by fillcoChargeSpline2 (kind 2) or fillcoChargeSpline1 (kind
+// 1), every point written, each point's terms added in atom order.  count,
+// start and fillpos hold charge_tile_count(g) + 1 ints, atoms natoms ints.
+size_t charge_tile_count(const Grid& g);
+void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, const double* xyz,
+                   const double* q, double zmagic, int* count, int* start, int* fillpos,
+                   int* atoms, double* charge);
 void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz, const double* q,
                 const double* r);
 // sum over atoms of the trilinearly interpolated potential x charge (part:
@@ -54,8 +59,6 @@ void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz,
 void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                      const double* q, const double* u, double* part, double* out,
                      const double* box = nullptr);
-void launch_charge_spl2(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                        const double* q, double zmagic, double* charge);
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                             const double* r, double srad, double epsp, double* epsx,
                             double* epsy, double* epsz);
@@ -65,12 +68,20 @@ void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const doub
                        int* count, int* start, int* fillpos, int* cell_of, int* sorted);
 // ints of the per-atom excluder lists launch_sas needs (nbr)
 size_t sas_nbr_ints(int natoms);
-void launch_sas(cudaStream_t s, const FillGeom& G, const CellGrid& C, int natoms,
-                const double* xyz, const double* r, const double* ref, int nref, double srad,
-                double epsw, const int* start, const int* sorted, int* nbr, unsigned* list,
-                int* npts, double* epsx, double* epsy, double* epsz);
+// accessible SAS points into list (atom * nref + point), their count into *npts
+void launch_sas_test(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
+                     const double* r, const double* ref, int nref, double srad,
+                     const int* start, const int* sorted, int* nbr, unsigned* list, int* npts);
+// probe spheres of the *npts accessible points of list reset the dielectric
+// maps to epsw
+void launch_sas_mark(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
+                     const double* r, const double* ref, int nref, double srad, double epsw,
+                     const unsigned* list, const int* npts, double* epsx, double* epsy,
+                     double* epsz);
+// the 9-point harmonic smoothing of maps a1..a3 whose values are mostly v0 or v1
 void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
-                   const double* a3, double* epsx, double* epsy, double* epsz);
+                   const double* a3, double v0, double v1, double* epsx, double* epsy,
+                   double* epsz);
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* q, double* terms, double* mom, const double* xf, const double* yf,
                 const double* zf, double* gx, double* gy, double* gz);

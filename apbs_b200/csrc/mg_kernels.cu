@@ -29,9 +29,8 @@ __global__ void k_build_fine(Grid g, const double* __restrict__ xf,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const double hzm1 = zf[k] - zf[k - 1], hz = zf[k + 1] - zf[k];
     const double hym1 = yf[j] - yf[j - 1], hy = yf[j + 1] - yf[j];
     const double hxm1 = xf[i] - xf[i - 1], hx = xf[i + 1] - xf[i];
@@ -149,9 +148,8 @@ __global__ void __launch_bounds__(128) k_galerkin(Grid gf, Op fine, Grid gc,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int I = 1 + (int)(q % (nx - 2));
-    const int J = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int K = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int I, J, K;
+    interior_ijk(q, nx, ny, I, J, K);
     // couplings to coarse boundary points are zero (P vanishes there)
     const bool okx[3] = {I - 1 >= 1, true, I + 1 <= nx - 2};
     const bool oky[3] = {J - 1 >= 1, true, J + 1 <= ny - 2};
@@ -276,9 +274,8 @@ __global__ void k_interp_axpy(Grid gc, const double* __restrict__ xc, Grid gf, d
   const double h = 0.5, qq = 0.25, e = 0.125;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
     const int oi = i & 1, oj = j & 1, ok = k & 1;
 #define XC(a, b, c) xc[gc.idx(a, b, c)]
@@ -426,9 +423,8 @@ __global__ void k_resid(Grid g, Op op, const double* __restrict__ cc,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     if (op.nop == 4) {
       r[id] = sum7(op, g, x, id, fc[id]) - (op.c[OC][id] + cc[id]) * x[id];
@@ -453,9 +449,8 @@ __global__ void k_matvec(Grid g, Op op, const double* __restrict__ cc,
   const size_t sx = 1, sy = nx, sz = (size_t)nx * ny;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     if (op.nop == 4) {
       y[id] = -op.c[ON][id] * x[id + sy] - op.c[ON][id - sy] * x[id - sy] -
@@ -872,9 +867,8 @@ __global__ void k_copy_interior(Grid g, const double* __restrict__ x, double* y)
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     y[id] = x[id];
   }
@@ -891,9 +885,8 @@ __global__ void k_axpy_interior(Grid g, const double* a_dev, double a_host,
   const double a = a_dev ? a_dev[0] : a_host;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     y[id] += a * x[id];
   }
@@ -922,9 +915,8 @@ __global__ void k_reduce_partial(Grid g, const double* __restrict__ x,
   double acc = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     acc += (MODE == 0) ? fabs(x[id]) : x[id] * y[id];
   }
@@ -969,9 +961,8 @@ __global__ void k_band_build(Grid g, Op op, double* abd, int m, int lda) {
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     double* col = abd + q * (size_t)lda;  // column jj = q+1
     // abd(kk, jj) with kk = off + m + 1 (1-based) -> col[off + m]
     auto put = [&](int off, double v) { col[off + m] = v; };
@@ -1711,9 +1702,8 @@ __global__ void k_nresid(Grid g, Op op, const double* __restrict__ cc,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const double w = cvec_point(ions, cc[id], x[id], false);
     r[id] = sum7(op, g, x, id, fc[id]) - op.c[OC][id] * x[id] - w;
@@ -1738,9 +1728,8 @@ __global__ void k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
   double acc = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const double c = cc[id], xv = x[id];
     double w, dw;
@@ -1770,9 +1759,8 @@ __global__ void k_xpay_interior(Grid g, const double* __restrict__ x, double a,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     out[id] = x[id] + a * y[id];
   }

@@ -21,7 +21,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "gs7_rb_bulk.cuh"
+#include "gs7_rb.cuh"
 #include "mixed.cuh"
 #include "solver_internal.cuh"
 
@@ -96,7 +96,6 @@ struct MixedState {
   // the dense coarsest inverse runs on the solver's side stream: forked after
   // the coarsest Helmholtz term is in place, done when dense_ev completes
   cudaEvent_t dense_fork, dense_ev;
-  int* d_err;  // set by a bulk-staged fine sweep whose copies did not complete
 };
 
 namespace {
@@ -302,9 +301,8 @@ __global__ void k_resid_f32(Grid g, OpF o, const float* __restrict__ cc,
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const float nb = (o.nop == 4) ? nb7(o, g, x, id) : nb27(o, g, x, id);
     r[id] = fc[id] + nb - (o.c[OC][id] + cc[id]) * x[id];
@@ -425,9 +423,8 @@ __global__ void k_interp_axpy_f32(Grid gc, const float* __restrict__ xc, Grid gf
   const float xdamp = (float)(num[0] / den[0]);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
     const int oi = i & 1, oj = j & 1, ok = k & 1;
     float w = 0.f;
@@ -460,9 +457,8 @@ __global__ void k_damp_dots(Grid g, OpF o, const float* __restrict__ cc,
   double an = 0.0, ad = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const float nb = (o.nop == 4) ? nb7(o, g, x, id) : nb27(o, g, x, id);
     const float xv = x[id];
@@ -507,9 +503,8 @@ __global__ void k_resid64_to32(Grid g, Op op, const double* __restrict__ cc,
   double acc = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const double r = fc[id] + op.c[ON][id] * x[id + sy] + op.c[ON][id - sy] * x[id - sy] +
                      op.c[OE][id] * x[id + 1] + op.c[OE][id - 1] * x[id - 1] +
@@ -528,9 +523,8 @@ __global__ void k_add_corr(Grid g, const float* __restrict__ e, double* x) {
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % (nx - 2));
-    const int j = 1 + (int)((q / (nx - 2)) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)(nx - 2) * (ny - 2)));
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     x[id] += (double)e[id];
   }
@@ -1286,25 +1280,20 @@ Gs7Rb<float> rb_f32(const MLevel& F, const float* d32, const int* tune) {
 }
 
 // The fine-level FP32 smoothing: tune[11] red-black sweeps, then (r given)
-// the residual.  tune[5] 2 and 3 run single-pass sweeps out of place
-// (x -> xs -> x ...; after an odd count xs is copied back), 3 with the
-// operands staged by the bulk-copy engine; otherwise one launch per colour.
-// k counts the kernels launched.
+// the residual.  tune[5] == 2 runs single-pass sweeps out of place
+// (x -> xs -> x ...; after an odd count xs is copied back); otherwise one
+// launch per colour.  k counts the kernels launched.
 cudaError_t gs7_f32(cudaStream_t st, const MLevel& F, float* x, float* r, int first_parity,
-                    float* xs, const float* d32, const int* tune, int* err, long long& k) {
-  const int mode = tune[5];
+                    float* xs, const float* d32, const int* tune, long long& k) {
   const int nsweep = tune[11];
-  if ((mode == 2 || mode == 3) && xs && d32 && (F.g.nx & 1) && (F.g.ny & 1)) {
+  if (tune[5] == 2 && xs && d32 && (F.g.nx & 1) && (F.g.ny & 1)) {
     Gs7Rb<float> a = rb_f32(F, d32, tune);
     float* buf[2] = {x, xs};
     cudaError_t e = cudaSuccess;
     for (int sw = 0; sw < nsweep && e == cudaSuccess; sw++) {
       a.xin = buf[sw & 1];
       a.xout = buf[(sw + 1) & 1];
-      e = cudaErrorNotSupported;
-      if (mode == 3) e = launch_gs7_rb_bulk<float>(st, a, first_parity, tune[12] & 15, err);
-      if (e == cudaErrorNotSupported)  // the windows do not fit shared memory
-        e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
+      e = launch_gs7_rb<float>(st, a, first_parity, tune[12]);
       k++;
     }
     if (e == cudaSuccess && (nsweep & 1))
@@ -1405,7 +1394,6 @@ void mixed_destroy(MixedState* m) {
   if (m->d_flag) cudaFree(m->d_flag);
   if (m->dense_fork) cudaEventDestroy(m->dense_fork);
   if (m->dense_ev) cudaEventDestroy(m->dense_ev);
-  if (m->d_err) cudaFree(m->d_err);
   delete m;
 }
 
@@ -1421,8 +1409,7 @@ int mixed_setup_from(pmgb_solver* s, int lo) {
   cudaStream_t st = s->stream;
   CKM(cudaEventCreateWithFlags(&m->dense_fork, cudaEventDisableTiming));
   CKM(cudaEventCreateWithFlags(&m->dense_ev, cudaEventDisableTiming));
-  CKM(cudaMalloc((void**)&m->d_err, sizeof(int)));
-  CKM(cudaMemset(m->d_err, 0, sizeof(int)));
+
   // levels shared with the FP64 hierarchy
   int nl = 0;
   m->zero_cc = (lo > 0);
@@ -1684,7 +1671,7 @@ int mixed_set_cc(pmgb_solver* s, int newton, int defer_check = 0) {
   // the FP32 Helmholtz terms of all levels in one launch
   conv.flush();
   MLevel& F = m->lev[0];
-  if (m->d32 && s->tune[PMGB_TUNE_GS7_COLOUR_PASSES] >= 2) {
+  if (m->d32 && s->tune[PMGB_TUNE_GS7_COLOUR_PASSES] == 2) {
     // the FP32 single-pass sweep's divisor
     k_diag_f32<<<blocks_for(F.g.n()), kThreads, 0, st>>>(F.g, F.op[OC], F.cc, m->d32);
     note_launches(1);
@@ -1778,7 +1765,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
   const OpF fo = opf(F);
   const size_t fint = (size_t)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   CKM(cudaMemsetAsync(F.x, 0, F.g.n() * sizeof(float), st));
-  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, m->d32, s->tune, m->d_err, k) != cudaSuccess) {
+  if (gs7_f32(st, F, F.x, m->r, 1, m->xs, m->d32, s->tune, k) != cudaSuccess) {
     set_error("FP32 fine smoother launch failed");
     return 0;
   }
@@ -1820,8 +1807,7 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
-      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, m->d32, s->tune, m->d_err, k) !=
-          cudaSuccess) {
+      if (gs7_f32(st, F, F.x, nullptr, 0, m->xs, m->d32, s->tune, k) != cudaSuccess) {
         set_error("FP32 fine smoother launch failed");
         return 0;
       }
@@ -1841,8 +1827,6 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
 int read_scal(pmgb_solver* s, int slot, double* v) {
   CKM(cudaMemcpyAsync(v, s->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   MixedState* m = s->mixed;
-  int bulk_err = 0;
-  if (m) CKM(cudaMemcpyAsync(&bulk_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   int info = 0;
   const int check = m && m->info_pending;
   if (check) {
@@ -1850,11 +1834,6 @@ int read_scal(pmgb_solver* s, int slot, double* v) {
     CKM(cudaMemcpyAsync(&info, m->dinfo, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   }
   CKM(cudaStreamSynchronize(s->stream));
-  if (bulk_err) {
-    cudaMemsetAsync(m->d_err, 0, sizeof(int), s->stream);
-    set_error("mixed: a staged copy of the FP32 fine sweep did not complete");
-    return 0;
-  }
   if (check) {
     m->info_pending = 0;
     if (info != 0) {
@@ -1953,8 +1932,8 @@ int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes) {
 }
 
 // One FP32 single-pass sweep for kernel timing: 28 B per point per sweep
-// (6 FP32 arrays read, x read and written once); bulk selects the
-// bulk-staged kernel.  mixed_prepare_sweep makes the divisor first.
+// (6 FP32 arrays read, x read and written once).  mixed_prepare_sweep makes
+// the divisor first.
 int mixed_prepare_sweep(pmgb_solver* s) {
   if (!mixed_setup(s) || !mixed_refresh(s)) return 0;
   MixedState* m = s->mixed;
@@ -1968,30 +1947,18 @@ int mixed_prepare_sweep(pmgb_solver* s) {
   return 1;
 }
 
-int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes, int bulk) {
+int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes) {
   MixedState* m = s->mixed;
   MLevel& F = m->lev[0];
   Gs7Rb<float> a = rb_f32(F, m->d32, s->tune);
   a.xin = F.x; a.xout = m->xs;
-  const cudaError_t e = bulk ? launch_gs7_rb_bulk<float>(s->stream, a, 1, s->tune[12] & 15,
-                                                         m->d_err)
-                             : launch_gs7_rb<float>(s->stream, a, 1, s->tune[12]);
+  const cudaError_t e = launch_gs7_rb<float>(s->stream, a, 1, s->tune[12]);
   if (e != cudaSuccess) {
     set_error("FP32 sweep launch failed");
     return 0;
   }
   *bytes = 28.0 * (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   return 1;
-}
-
-// the bulk sweep's error flag: 1 if a wait gave up since the last call
-int mixed_bulk_error(pmgb_solver* s) {
-  if (!s->mixed) return 0;
-  int v = 0;
-  cudaMemcpyAsync(&v, s->mixed->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
-  cudaMemsetAsync(s->mixed->d_err, 0, sizeof(int), s->stream);
-  cudaStreamSynchronize(s->stream);
-  return v;
 }
 
 // The coarse tail alone, for kernel timing.  Algorithmic bytes per tail

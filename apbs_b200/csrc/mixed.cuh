@@ -17,8 +17,7 @@ int newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed);
 void set_error(const char* fmt, ...);
 int mixed_time_gs7(pmgb_solver* s, int parity, double* bytes);
 int mixed_prepare_sweep(pmgb_solver* s);
-int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes, int bulk);
-int mixed_bulk_error(pmgb_solver* s);
+int mixed_time_gs7_sweep(pmgb_solver* s, double* bytes);
 int mixed_time_tail(pmgb_solver* s, double* bytes);
 // FP64 path, LPBE: exact-to-round-off solve of the FP64 coarsest level
 // (FP64 refinement over FP32 V-cycles of extra Galerkin levels).

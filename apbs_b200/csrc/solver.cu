@@ -535,6 +535,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->focus_w);
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
   dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->sas_nbr); dfree(s->d_ref); dfree(s->atom_terms);
+  dfree(s->ch_count); dfree(s->ch_start); dfree(s->ch_fill); dfree(s->ch_atoms);
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   free_maps(s);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
@@ -613,6 +614,15 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   if (p.bcfl == PMGB_BCFL_SDH &&
       !grow(&s->atom_terms, &s->terms_alloc, 13 * (size_t)natoms, st))
     return 0;
+  if (!uses_charge_map(s)) {
+    const size_t nt = charge_tile_count(s->g) + 1;
+    size_t a1 = s->ch_tiles_alloc, a2 = s->ch_tiles_alloc, a3 = s->ch_tiles_alloc;
+    if (!grow(&s->ch_count, &a1, nt, st) || !grow(&s->ch_start, &a2, nt, st) ||
+        !grow(&s->ch_fill, &a3, nt, st) ||
+        !grow(&s->ch_atoms, &s->ch_atoms_alloc, (size_t)std::max(natoms, 1), st))
+      return 0;
+    s->ch_tiles_alloc = std::min(a1, std::min(a2, a3));
+  }
   CK(cudaEventRecord(s->ev[0], st));
   CK(cudaMemsetAsync(s->d_npts, 0, sizeof(int), st));
   // The charge map and the sdh/mdh boundary values depend on the atoms only:
@@ -637,13 +647,10 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     // the charge map is read below (fillcoChargeMap)
     CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
   } else {
-    CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), sd));
-    if (p.chgm == PMGB_CHGM_TRIL)
-      launch_charge_tril(sd, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
-    else
-      launch_charge_spl2(sd, s->G, natoms, s->d_xyz, s->d_q, s->zmagic, s->charge);
+    launch_charge(sd, p.chgm == PMGB_CHGM_TRIL ? 1 : 2, s->G, natoms, s->d_xyz, s->d_q,
+                  s->zmagic, s->ch_count, s->ch_start, s->ch_fill, s->ch_atoms, s->charge);
+    note_launches(4);
   }
-  note_launches(1);
   if (side_bc && !side_boundary(s, sd)) return 0;
   // with coefficient maps the operator is never a plain Laplacian
   // (Vpmg_fillco, vpmg.c:5354-5361)
@@ -661,12 +668,16 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
                        s->epsx, s->epsy, s->epsz);
     note_launches(1);
   } else if (!islap) {
-    // dielectric (fillcoCoefMolDielNoSmooth)
-    launch_fill_value(st, s->epsx, n, p.sdie);
-    launch_fill_value(st, s->epsy, n, p.sdie);
-    launch_fill_value(st, s->epsz, n, p.sdie);
-    launch_mark_atoms_diel(st, s->G, natoms, s->d_xyz, s->d_r, p.srad, p.pdie, s->epsx,
-                           s->epsy, s->epsz);
+    // dielectric (fillcoCoefMolDielNoSmooth); with smoothing the unsmoothed
+    // maps are built in the scratch arrays and smoothed into epsx/y/z
+    const int smol = p.srfm == PMGB_SRFM_SMOL;
+    double* ex = smol ? s->tmp3 : s->epsx;
+    double* ey = smol ? s->tmp3 + n : s->epsy;
+    double* ez = smol ? s->tmp3 + 2 * n : s->epsz;
+    launch_fill_value(st, ex, n, p.sdie);
+    launch_fill_value(st, ey, n, p.sdie);
+    launch_fill_value(st, ez, n, p.sdie);
+    launch_mark_atoms_diel(st, s->G, natoms, s->d_xyz, s->d_r, p.srad, p.pdie, ex, ey, ez);
     note_launches(4);
     if (p.srad > 1.0e-9) {
       // Vacc_storeParms sphere density with the Vclist probe radius
@@ -722,20 +733,15 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
       }
       if (!grow(&s->sas_list, &s->sas_list_alloc, npairs, st)) return 0;
       if (!grow(&s->sas_nbr, &s->sas_nbr_alloc, sas_nbr_ints(natoms), st)) return 0;
-      launch_sas(st, s->G, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
-                 s->cell_start, s->cell_sorted, s->sas_nbr, s->sas_list, s->d_npts, s->epsx,
-                 s->epsy,
-                 s->epsz);
-      note_launches(3);
+      launch_sas_test(st, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, s->cell_start,
+                      s->cell_sorted, s->sas_nbr, s->sas_list, s->d_npts);
+      note_launches(2);
+      launch_sas_mark(st, s->G, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
+                      s->sas_list, s->d_npts, ex, ey, ez);
+      note_launches(1);
     }
-    if (p.srfm == PMGB_SRFM_SMOL) {
-      CK(cudaMemcpyAsync(s->tmp3, s->epsx, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemcpyAsync(s->tmp3 + n, s->epsy, n * sizeof(double), cudaMemcpyDeviceToDevice,
-                         st));
-      CK(cudaMemcpyAsync(s->tmp3 + 2 * n, s->epsz, n * sizeof(double),
-                         cudaMemcpyDeviceToDevice, st));
-      launch_smooth(st, s->g, s->tmp3, s->tmp3 + n, s->tmp3 + 2 * n, s->epsx, s->epsy,
-                    s->epsz);
+    if (smol) {
+      launch_smooth(st, s->g, ex, ey, ez, p.pdie, p.sdie, s->epsx, s->epsy, s->epsz);
       note_launches(1);
     }
     // ion accessibility (fillcoCoefMolIon)
@@ -1482,7 +1488,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
     return 0;
   }
   if ((which == PMGB_K_GS7_FP32 || which == PMGB_K_VCYCLE_TAIL ||
-       which == PMGB_K_GS7_SWEEP_FP32 || which == PMGB_K_GS7_BULK_FP32) &&
+       which == PMGB_K_GS7_SWEEP_FP32) &&
       s->precision != PMGB_MIXED) {
     set_error("pmgb_time_kernel: kernel %d belongs to the mixed-precision path", which);
     return 0;
@@ -1491,9 +1497,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
   Level& F = s->lev[0];
   const double fint = (double)(F.g.nx - 2) * (F.g.ny - 2) * (F.g.nz - 2);
   double b = 0.0;
-  if ((which == PMGB_K_GS7_SWEEP_FP32 || which == PMGB_K_GS7_BULK_FP32) &&
-      !mixed_prepare_sweep(s))
-    return 0;
+  if (which == PMGB_K_GS7_SWEEP_FP32 && !mixed_prepare_sweep(s)) return 0;
   CK(cudaStreamSynchronize(st));
   CK(cudaEventRecord(s->ev[6], st));
   for (int r = 0; r < reps; r++) {
@@ -1544,8 +1548,7 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
         b = 56.0 * fint;
         break;
       case PMGB_K_GS7_SWEEP_FP32:
-      case PMGB_K_GS7_BULK_FP32:
-        if (!mixed_time_gs7_sweep(s, &b, which == PMGB_K_GS7_BULK_FP32)) return 0;
+        if (!mixed_time_gs7_sweep(s, &b)) return 0;
         break;
       default:
         set_error("pmgb_time_kernel: unknown kernel %d", which);
@@ -1555,10 +1558,6 @@ extern "C" int pmgb_time_kernel(pmgb_solver* s, int which, int reps, double* ms,
   CK(cudaEventRecord(s->ev[7], st));
   CK(cudaEventSynchronize(s->ev[7]));
   CK(cudaGetLastError());
-  if (which == PMGB_K_GS7_BULK_FP32 && mixed_bulk_error(s)) {
-    set_error("pmgb_time_kernel: a staged copy of the bulk sweep did not complete");
-    return 0;
-  }
   *ms = elapsed_ms(s->ev[6], s->ev[7]) / reps;
   *bytes = b;
   note_launches(reps);

@@ -28,7 +28,6 @@ MIXED = 1
 K_GS7_FP64, K_GS27_WAVE, K_RESID_FP64, K_GS7_FP32, K_CG_COARSE = 0, 1, 2, 3, 4
 K_VCYCLE_TAIL = 7
 K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
-K_GS7_BULK_FP64, K_GS7_BULK_FP32 = 10, 11
 DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX, DX_DIELY, DX_DIELZ = range(6)
 MAP_DIELX, MAP_DIELY, MAP_DIELZ, MAP_KAPPA, MAP_CHARGE, MAP_POT = range(6)
 TUNE_MIXED_CHEBYSHEV = 0

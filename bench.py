@@ -507,7 +507,6 @@ def main():
     smoothers = {}
     for nm, sv, k in (("k_gs7_rb<double>", solvers["fp64"], vpmg.K_GS7_SWEEP_FP64),
                       ("k_gs7_rb<float>", solvers["mixed"], vpmg.K_GS7_SWEEP_FP32),
-                      ("k_gs7_rb_bulk<float>", solvers["mixed"], vpmg.K_GS7_BULK_FP32),
                       ("k_gs7_colour", solvers["fp64"], vpmg.K_GS7_FP64),
                       ("k_gs7_f32", solvers["mixed"], vpmg.K_GS7_FP32)):
         ms_k, b_k = sv.time_kernel(k, 20)

@@ -210,8 +210,6 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_K_VCYCLE_TAIL 7    /* mixed: coarse-level V-cycle tail (one cluster kernel) */
 #define PMGB_K_GS7_SWEEP_FP64 8 /* fine-level 7-point GS, one full sweep in one pass, FP64 */
 #define PMGB_K_GS7_SWEEP_FP32 9 /* the same, FP32 (mixed) */
-#define PMGB_K_GS7_BULK_FP64 10 /* the full sweep with its operands staged by bulk copies, FP64 */
-#define PMGB_K_GS7_BULK_FP32 11 /* the same, FP32 (mixed) */
 
 /* Launch-shape tunables.  pmgb_set_tuning sets the process-wide defaults a
  * calculation copies when it is created; pmgb_solver_set_tuning changes one
@@ -231,9 +229,7 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
                                           above 512 unknowns */
 #define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
                                           kernel, FP32 one launch per colour), 1 = one launch
-                                          per colour, 2 = single-pass sweeps in FP32 too,
-                                          3 = single-pass sweeps with the operands staged in
-                                          shared memory by bulk copies (FP32) */
+                                          per colour, 2 = single-pass sweeps in FP32 too */
 #define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 8) */
 #define PMGB_TUNE_GS27_CLUSTER_MID 7   /* the same as key 2 for levels with 28-59 interior
                                           points per axis (0 = 8) */
