@@ -1746,8 +1746,11 @@ __global__ void k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
 void launch_nresid_nrm1(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                         const double* x, double* r, IonTable ions, double* part,
                         double* out_dev, double* cp) {
+  // about two points per thread (up to four times the usual partial count,
+  // which the scratch holds): enough warps in flight to cover the loads
+  // around the exponentials
   const size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
-  const int nb = (int)reduce_parts(nint);
+  const int nb = (int)std::max<size_t>(1, std::min<size_t>(4 * 1184, (nint + 511) / 512));
   k_nresid_nrm<<<nb, kRedThreads, 0, s>>>(g, op, cc, fc, x, r, ions, part, cp);
   k_reduce_final<<<1, kRedThreads, 0, s>>>(part, nb, out_dev);
 }

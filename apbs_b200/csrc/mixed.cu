@@ -1846,7 +1846,7 @@ int read_scal(pmgb_solver* s, int slot, double* v) {
 
 // Refinement loop on (A + cc) x = f, all FP64 vectors on the fine level:
 // stop when ||f - (A+cc)x||_1 / rsden <= errtol (rsden = ||f||_1, or 1 for
-// the Newton inner solve).
+// the Newton inner solve, istop0, which starts from x64 = 0).
 int refine(pmgb_solver* s, int newton, const double* cc64, const double* fc64, double* x64,
            double errtol, int itmax, int istop0, int* iters_out) {
   MixedState* m = s->mixed;
@@ -1854,11 +1854,20 @@ int refine(pmgb_solver* s, int newton, const double* cc64, const double* fc64, d
   const Grid g = s->g;
   const size_t fint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
   const int nb = (int)reduce_parts(fint);
-  // initial residual (x64 as given) -> FP32 rhs and its norm
-  k_resid64_to32<<<nb, 256, 0, st>>>(g, s->lev[0].ops(), cc64, fc64, x64, m->lev[0].w0,
-                                     s->part);
-  k_sum_parts<<<1, 256, 0, st>>>(s->part, nb, s->scal + S_RSNRM);
-  note_launches(2);
+  if (istop0) {
+    // the Newton inner solve starts from x64 = 0, where the residual is f
+    // itself (f + 0 - 0): its FP32 copy is the V-cycle's rhs, and its norm
+    // is not needed
+    ConvQueue conv(st);
+    conv.add(fc64, m->lev[0].w0, g.n());
+    conv.flush();
+  } else {
+    // initial residual (x64 as given) -> FP32 rhs and its norm
+    k_resid64_to32<<<nb, 256, 0, st>>>(g, s->lev[0].ops(), cc64, fc64, x64, m->lev[0].w0,
+                                       s->part);
+    k_sum_parts<<<1, 256, 0, st>>>(s->part, nb, s->scal + S_RSNRM);
+    note_launches(2);
+  }
   double rsden = 1.0, rsnrm = 0.0;
   if (!istop0) {
     launch_nrm1(st, g, fc64, s->part + 2368, s->scal + S_RSDEN);
