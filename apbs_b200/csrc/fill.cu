@@ -12,8 +12,9 @@
 namespace pmgb {
 
 // ---------------------------------------------------------------------------
-// Charge: fillcoChargeSpline2 + bspline2 (vpmg.c:5091-5248) and the
-// trilinear fillcoChargeSpline1 (vpmg.c:4986-5121), gathered per tile of grid
+// Charge: fillcoChargeSpline2 + bspline2 (vpmg.c:5091-5248), the trilinear
+// fillcoChargeSpline1 (vpmg.c:4986-5121) and the 5th-order B-spline of
+// fillcoPermanentMultipole with atomic charges (vpmg.c:6835-7000), gathered per tile of grid
 // points (k_charge_gather below) so that every point adds its atoms'
 // contributions in atom order, as the reference's atom loop does: the map is
 // the reference's bit for bit and the same on every run.
@@ -742,7 +743,8 @@ void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double
 // Deterministic charge spreading.  Atoms inside the method's acceptance band
 // are binned by the 8^3 tile of grid points that holds floor(position / h);
 // an atom's stencil (floor - 1 .. ceil + 1 per axis) reaches at most the
-// neighbouring tiles.  One CTA per tile gathers the atoms of the 27 bins
+// neighbouring tiles (the 5th-order B-spline's floor - 2 .. ceil + 2 too).
+// One CTA per tile gathers the atoms of the 27 bins
 // around it, sorts them by atom index and adds their contributions point by
 // point in that order, each term the reference's expression.  A tile with
 // more than kChCap candidates (far denser than any molecule) runs in passes
@@ -752,10 +754,15 @@ constexpr int kChTile = 8;
 constexpr int kChCap = 512;
 constexpr int kChThreads = 128;
 
-// KIND 2: bspline2 (fillcoChargeSpline2), KIND 1: trilinear
+// KIND 2: bspline2 (fillcoChargeSpline2), KIND 1: trilinear, KIND 4: 5th-order
+// B-spline (fillcoPermanentMultipole)
 template <int KIND>
 __device__ __forceinline__ bool charge_in_band(const FillGeom& G, double ax, double ay,
                                                double az) {
+  if (KIND == 4)
+    return !((ax <= (G.xmin[0] - 2 * G.h[0])) || (ax >= (G.xmax[0] + 2 * G.h[0])) ||
+             (ay <= (G.xmin[1] - 2 * G.h[1])) || (ay >= (G.xmax[1] + 2 * G.h[1])) ||
+             (az <= (G.xmin[2] - 2 * G.h[2])) || (az >= (G.xmax[2] + 2 * G.h[2])));
   if (KIND == 2)
     return !((ax <= (G.xmin[0] - G.h[0])) || (ax >= (G.xmax[0] + G.h[0])) ||
              (ay <= (G.xmin[1] - G.h[1])) || (ay >= (G.xmax[1] + G.h[1])) ||
@@ -866,11 +873,20 @@ __global__ void __launch_bounds__(kChThreads) k_charge_gather(
       const double px = xyz[3 * a] - G.xmin[0], py = xyz[3 * a + 1] - G.xmin[1],
                    pz = xyz[3 * a + 2] - G.xmin[2];
       const double fi = px / hx, fj = py / hy, fk = pz / hz;
-      cq[e] = q[a] * zmagic / (hx * hy * hz);
+      // fillcoPermanentMultipole scales by f = zmagic / (hx hy hzed) first
+      cq[e] = KIND == 4 ? q[a] * (zmagic / (hx * hy * hz)) : q[a] * zmagic / (hx * hy * hz);
       cf[0][e] = fi;
       cf[1][e] = fj;
       cf[2][e] = fk;
-      if (KIND == 2) {
+      if (KIND == 4) {
+        // the loop bounds of fillcoPermanentMultipole (vpmg.c:6937-6965)
+        cb[0][e] = max((int)floor(fi) - 2, 0);
+        cb[1][e] = min((int)ceil(fi) + 2, nx - 1);
+        cb[2][e] = max((int)floor(fj) - 2, 0);
+        cb[3][e] = min((int)ceil(fj) + 2, ny - 1);
+        cb[4][e] = max((int)floor(fk) - 2, 0);
+        cb[5][e] = min((int)ceil(fk) + 2, nz - 1);
+      } else if (KIND == 2) {
         // the loop bounds of fillcoChargeSpline2 (vpmg.c:5207-5224)
         cb[0][e] = max((int)floor(fi) - 1, 0);
         cb[1][e] = min((int)ceil(fi) + 1, nx - 1);
@@ -890,7 +906,29 @@ __global__ void __launch_bounds__(kChThreads) k_charge_gather(
     __syncthreads();
     if (i < nx && j < ny) {
       for (int e = 0; e < nc; e++) {
-        if (KIND == 2) {
+        if (KIND == 4) {
+          if (i < cb[0][e] || i > cb[1][e] || j < cb[2][e] || j > cb[3][e]) continue;
+          const double c = cq[e], fk = cf[2][e];
+          const double mi = (2.5 + ((double)(i) - (cf[0][e])));
+          const double mj = (2.5 + ((double)(j) - (cf[1][e])));
+          const double mx = bspline4(mi), dmx = dbspline4(mi), d2mx = d2bspline4(mi);
+          const double my = bspline4(mj), dmy = dbspline4(mj), d2my = d2bspline4(mj);
+          // the dipole and quadrupole terms of the reference's expression,
+          // with the zero moments of plain atomic charges
+          const double ux = 0.0, uy = 0.0, uz = 0.0, qxx = 0.0, qyx = 0.0, qyy = 0.0,
+                       qzx = 0.0, qzy = 0.0, qzz = 0.0;
+#pragma unroll
+          for (int r = 0; r < PPT; r++) {
+            const int k = kb + 2 * r;
+            if (k < cb[4][e] || k > cb[5][e]) continue;
+            const double mk = (2.5 + ((double)(k) - (fk)));
+            const double mz = bspline4(mk), dmz = dbspline4(mk), d2mz = d2bspline4(mk);
+            acc[r] += mx * my * mz * c - dmx * my * mz * ux - mx * dmy * mz * uy -
+                      mx * my * dmz * uz + d2mx * my * mz * qxx + dmx * dmy * mz * qyx +
+                      mx * d2my * mz * qyy + dmx * my * dmz * qzx + mx * dmy * dmz * qzy +
+                      mx * my * d2mz * qzz;
+          }
+        } else if (KIND == 2) {
           if (i < cb[0][e] || i > cb[1][e] || j < cb[2][e] || j > cb[3][e]) continue;
           const double c = cq[e], fk = cf[2][e];
           const double mx = bspline2(1.5 + ((double)i - cf[0][e]));
@@ -944,7 +982,7 @@ size_t charge_tile_count(const Grid& g) {
          ((g.nz + kChTile - 1) / kChTile);
 }
 
-// kind 2: bspline2, 1: trilinear.  count, start, fillpos: charge_tile_count + 1
+// kind 2: bspline2, 1: trilinear, 4: 5th-order B-spline.  count, start, fillpos: charge_tile_count + 1
 // ints; atoms: natoms ints.  Every point of the map is written.
 void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, const double* xyz,
                    const double* q, double zmagic, int* count, int* start, int* fillpos,
@@ -957,16 +995,21 @@ void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, cons
   const int nb = std::max(1, (natoms + 255) / 256);
   cudaMemsetAsync(count, 0, sizeof(int) * nt, s);
   if (natoms > 0) {
-    if (kind == 2) k_chtile_count<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
+    if (kind == 4) k_chtile_count<4><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
+    else if (kind == 2) k_chtile_count<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
     else k_chtile_count<1><<<nb, 256, 0, s>>>(G, T, natoms, xyz, count);
   }
   k_scan_single<<<1, 1024, 0, s>>>(count, nt, start);
   cudaMemcpyAsync(fillpos, start, sizeof(int) * nt, cudaMemcpyDeviceToDevice, s);
   if (natoms > 0) {
-    if (kind == 2) k_chtile_fill<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
+    if (kind == 4) k_chtile_fill<4><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
+    else if (kind == 2) k_chtile_fill<2><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
     else k_chtile_fill<1><<<nb, 256, 0, s>>>(G, T, natoms, xyz, fillpos, atoms);
   }
-  if (kind == 2)
+  if (kind == 4)
+    k_charge_gather<4><<<nt, kChThreads, 0, s>>>(G, T, natoms, xyz, q, zmagic, start, atoms,
+                                                 charge);
+  else if (kind == 2)
     k_charge_gather<2><<<nt, kChThreads, 0, s>>>(G, T, natoms, xyz, q, zmagic, start, atoms,
                                                  charge);
   else

@@ -1,8 +1,88 @@
 // Kernel declarations of the coefficient-map fill (fill.cu).
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace pmgb {
+
+// the 5th-order B-spline and its first two derivatives (bspline4,
+// dbspline4, d2bspline4, vpmg.c:6731-6822)
+__device__ __forceinline__ double bspline4(double x) {
+  const double one6 = 1.0 / 6.0, one8 = 1.0 / 8.0, one24 = 1.0 / 24.0;
+  const double thirteen24 = 13.0 / 24.0, fourtyseven24 = 47.0 / 24.0,
+               seventeen24 = 17.0 / 24.0;
+  double m, m2;
+  if ((x > 0.0) && (x <= 1.0)) {
+    m = x * x;
+    return one24 * m * m;
+  } else if ((x > 1.0) && (x <= 2.0)) {
+    m = x - 1.0;
+    m2 = m * m;
+    return -one8 + one6 * x + m2 * (0.25 + one6 * m - one6 * m2);
+  } else if ((x > 2.0) && (x <= 3.0)) {
+    m = x - 2.0;
+    m2 = m * m;
+    return -thirteen24 + 0.5 * x + m2 * (-0.25 - 0.5 * m + 0.25 * m2);
+  } else if ((x > 3.0) && (x <= 4.0)) {
+    m = x - 3.0;
+    m2 = m * m;
+    return fourtyseven24 - 0.5 * x + m2 * (-0.25 + 0.5 * m - one6 * m2);
+  } else if ((x > 4.0) && (x <= 5.0)) {
+    m = x - 4.0;
+    m2 = m * m;
+    return seventeen24 - one6 * x + m2 * (0.25 - one6 * m + one24 * m2);
+  }
+  return 0.0;
+}
+__device__ __forceinline__ double dbspline4(double x) {
+  const double one6 = 1.0 / 6.0, one3 = 1.0 / 3.0, two3 = 2.0 / 3.0, thirteen6 = 13.0 / 6.0;
+  double m, m2;
+  if ((x > 0.0) && (x <= 1.0)) {
+    m2 = x * x;
+    return one6 * x * m2;
+  } else if ((x > 1.0) && (x <= 2.0)) {
+    m = x - 1.0;
+    m2 = m * m;
+    return -one3 + 0.5 * x + m2 * (0.5 - two3 * m);
+  } else if ((x > 2.0) && (x <= 3.0)) {
+    m = x - 2.0;
+    m2 = m * m;
+    return 1.5 - 0.5 * x + m2 * (-1.5 + m);
+  } else if ((x > 3.0) && (x <= 4.0)) {
+    m = x - 3.0;
+    m2 = m * m;
+    return 1.0 - 0.5 * x + m2 * (1.5 - two3 * m);
+  } else if ((x > 4.0) && (x <= 5.0)) {
+    m = x - 4.0;
+    m2 = m * m;
+    return -thirteen6 + 0.5 * x + m2 * (-0.5 + one6 * m);
+  }
+  return 0.0;
+}
+__device__ __forceinline__ double d2bspline4(double x) {
+  double m, m2;
+  if ((x > 0.0) && (x <= 1.0)) {
+    return 0.5 * x * x;
+  } else if ((x > 1.0) && (x <= 2.0)) {
+    m = x - 1.0;
+    m2 = m * m;
+    return -0.5 + x - 2.0 * m2;
+  } else if ((x > 2.0) && (x <= 3.0)) {
+    m = x - 2.0;
+    m2 = m * m;
+    return 5.5 - 3.0 * x + 3.0 * m2;
+  } else if ((x > 3.0) && (x <= 4.0)) {
+    m = x - 3.0;
+    m2 = m * m;
+    return -9.5 + 3.0 * x - 2.0 * m2;
+  } else if ((x > 4.0) && (x <= 5.0)) {
+    m = x - 4.0;
+    m2 = m * m;
+    return 4.5 - x + 0.5 * m2;
+  }
+  return 0.0;
+}
 
 struct FillGeom {
   Grid g;
@@ -39,8 +119,8 @@ struct MdhArgs {
   double pre1;    // e_c / (4 pi eps0 eps_w k_B T) * 1e10
   double xkappa;  // 1/A
 };
-// charge map by fillcoChargeSpline2 (kind 2) or fillcoChargeSpline1 (kind
-// 1), every point written, each point's terms added in atom order.  count,
+// charge map by fillcoChargeSpline2 (kind 2), fillcoChargeSpline1 (kind 1)
+// or fillcoPermanentMultipole's charges (kind 4), every point written, each point's terms added in atom order.  count,
 // start and fillpos hold charge_tile_count(g) + 1 ints, atoms natoms ints.
 size_t charge_tile_count(const Grid& g);
 void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, const double* xyz,
@@ -89,7 +169,10 @@ void launch_ccf(cudaStream_t s, size_t n, const double* kappa, double zkappa2, d
 // srfm spl2/spl4 kappa and dielectric maps (fillcoCoefSpline, fillcoCoefSpline4), spline.cu
 void launch_spline_fill(cudaStream_t st, int order, const FillGeom& G, int natoms,
                         const double* xyz, const double* r, double irad, double win,
-                        double ionmask, double epsp, double epsw, double* kappa, double* epsx,
-                        double* epsy, double* epsz);
+                        double ionmask, double epsp, double epsw, const double* coef3,
+                        double* kappa, double* epsx, double* epsy, double* epsz);
+// srfm spl3: 18 window-polynomial coefficients per atom (spline.cu)
+void spline3_table(int natoms, const double* r, double irad, double win,
+                   std::vector<double>& tab);
 
 }  // namespace pmgb

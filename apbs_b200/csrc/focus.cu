@@ -143,10 +143,11 @@ extern "C" int pmgb_focus(pmgb_solver* fine, pmgb_solver* coarse, int calc_energ
     return 0;
   }
   // the coarse charge energy outside the fine box: a volume sum of the
-  // charge map (spl2, or a charge map) or a point sum at the atoms (spl0)
-  const int coarse_point_qf = coarse->p.chgm == PMGB_CHGM_TRIL && !uses_charge_map(coarse);
+  // charge map (spl2, or a charge map) or a point sum at the atoms (spl0, spl4)
+  const int coarse_point_qf = coarse->p.chgm != PMGB_CHGM_SPL2 && !uses_charge_map(coarse);
   if (calc_energy && coarse_point_qf && (coarse->natoms <= 0 || !coarse->d_xyz)) {
-    set_error("pmgb_focus: chgm spl0 needs the coarse calculation's atom list (pmgb_fillco)");
+    set_error("pmgb_focus: chgm spl0/spl4 needs the coarse calculation's atom list "
+              "(pmgb_fillco)");
     return 0;
   }
   if (!coarse->solved) {

@@ -250,13 +250,14 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
     set_error("pmgb_create: unsupported grid %dx%dx%d nlev %d", p.nx, p.ny, p.nz, p.nlev);
     return 0;
   }
-  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL) {
-    set_error("pmgb_create: chgm %d not implemented (spl0 and spl2 are)", p.chgm);
+  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL && p.chgm != PMGB_CHGM_SPL4) {
+    set_error("pmgb_create: chgm %d not implemented (spl0, spl2 and spl4 are)", p.chgm);
     return 0;
   }
   if (p.srfm != PMGB_SRFM_MOL && p.srfm != PMGB_SRFM_SMOL && p.srfm != PMGB_SRFM_SPL2 &&
-      p.srfm != PMGB_SRFM_SPL4) {
-    set_error("pmgb_create: srfm %d not implemented (mol, smol, spl2 and spl4 are)", p.srfm);
+      p.srfm != PMGB_SRFM_SPL3 && p.srfm != PMGB_SRFM_SPL4) {
+    set_error("pmgb_create: srfm %d not implemented (mol, smol, spl2, spl3 and spl4 are)",
+              p.srfm);
     return 0;
   }
   if (p.nion > 8) {
@@ -536,6 +537,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->cell_count); dfree(s->cell_start); dfree(s->cell_fillpos); dfree(s->cell_of);
   dfree(s->cell_sorted); dfree(s->sas_list); dfree(s->sas_nbr); dfree(s->d_ref); dfree(s->atom_terms);
   dfree(s->ch_count); dfree(s->ch_start); dfree(s->ch_fill); dfree(s->ch_atoms);
+  dfree(s->d_spl3);
   dfree(s->a_xyz); dfree(s->a_q); dfree(s->a_r);
   free_maps(s);
   for (int i = 0; i < 8; i++) cudaEventDestroy(s->ev[i]);
@@ -647,7 +649,8 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
     // the charge map is read below (fillcoChargeMap)
     CK(cudaMemsetAsync(s->charge, 0, n * sizeof(double), st));
   } else {
-    launch_charge(sd, p.chgm == PMGB_CHGM_TRIL ? 1 : 2, s->G, natoms, s->d_xyz, s->d_q,
+    launch_charge(sd, p.chgm == PMGB_CHGM_TRIL ? 1 : (p.chgm == PMGB_CHGM_SPL4 ? 4 : 2), s->G,
+                  natoms, s->d_xyz, s->d_q,
                   s->zmagic, s->ch_count, s->ch_start, s->ch_fill, s->ch_atoms, s->charge);
     note_launches(4);
   }
@@ -658,14 +661,25 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
   const int islap = !coef_maps && (s->ionstr < 1.0e-12) && (fabs(p.pdie - p.sdie) < 1.0e-12);
   if (coef_maps) {
     // the maps are read below (fillcoCoefMap)
-  } else if (!islap && (p.srfm == PMGB_SRFM_SPL2 || p.srfm == PMGB_SRFM_SPL4)) {
+  } else if (!islap && (p.srfm == PMGB_SRFM_SPL2 || p.srfm == PMGB_SRFM_SPL3 ||
+                         p.srfm == PMGB_SRFM_SPL4)) {
     // spline surface: kappa and the dielectric maps together
     // (fillcoCoefSpline, fillcoCoefSpline4)
     const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
-    launch_spline_fill(st, p.srfm == PMGB_SRFM_SPL4 ? 4 : 2, s->G, natoms, s->d_xyz, s->d_r,
-                       s->maxIonRadius,
-                       (p.swin > 0.0) ? p.swin : 0.3, ionmask, p.pdie, p.sdie, s->kappa,
-                       s->epsx, s->epsy, s->epsz);
+    const double win = (p.swin > 0.0) ? p.swin : 0.3;
+    const double* coef3 = nullptr;
+    if (p.srfm == PMGB_SRFM_SPL3) {
+      // the 5th-order window polynomials per atom, made on the host with the
+      // reference's pow() (spline3_table)
+      std::vector<double> tab;
+      spline3_table(natoms, h_r, s->maxIonRadius, win, tab);
+      if (!grow(&s->d_spl3, &s->spl3_alloc, tab.size(), st)) return 0;
+      CK(cudaMemcpyAsync(s->d_spl3, tab.data(), sizeof(double) * tab.size(),
+                         cudaMemcpyHostToDevice, st));
+      coef3 = s->d_spl3;
+    }
+    launch_spline_fill(st, p.srfm, s->G, natoms, s->d_xyz, s->d_r, s->maxIonRadius, win,
+                       ionmask, p.pdie, p.sdie, coef3, s->kappa, s->epsx, s->epsy, s->epsz);
     note_launches(1);
   } else if (!islap) {
     // dielectric (fillcoCoefMolDielNoSmooth); with smoothing the unsmoothed
@@ -1169,7 +1183,11 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
   if (rsden == 0.0) rsden = 1.0;
   rsnrm = rsden;
   s->reslog.push_back(rsnrm / rsden);
-  if (!nresid_norm(s, F.x, s->nw_r0, &xnorm_old)) return 0;
+  // the residual of the current iterate is the next Jacobian system's
+  // right-hand side: it is written there directly where no damping trial
+  // can replace it, else copied from the kept trial
+  if (!nresid_norm(s, F.x, F.rhs, &xnorm_old)) return 0;
+  int rhs_ready = 1;
   int iters = 0, idamp = 1;
   // work vectors of the damping loop: trial iterate and residual, and the
   // best ones kept; "keep" is a swap of the two pairs (no copies)
@@ -1180,8 +1198,11 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
     // Vgetjac (newtond.c:550-598).  Only the fine right-hand side is used:
     // every coarse level's right-hand side is the restricted residual of
     // the V-cycle itself.
-    launch_copy_interior(st, F.g, r0, F.rhs);
-    note_launches(1);
+    if (!rhs_ready) {
+      launch_copy_interior(st, F.g, r0, F.rhs);
+      note_launches(1);
+    }
+    rhs_ready = 0;
     if (!cp_ready) {
       launch_dcvec(st, F.g, F.cc, F.x, F.cp, s->ions);
       note_launches(1);
@@ -1237,8 +1258,9 @@ int pmgb::newton_driver(pmgb_solver* s, double errtol, int itmax, int mixed) {
       launch_axpy_interior(st, F.g, nullptr, 1.0, F.xt, F.x);
       note_launches(1);
       // the residual pass also gives c'(x) for the next Jacobian
-      if (!nresid_norm(s, F.x, r0, &xnorm_new, F.cp)) return 0;
+      if (!nresid_norm(s, F.x, F.rhs, &xnorm_new, F.cp)) return 0;
       cp_ready = 1;
+      rhs_ready = 1;
       xnorm_old = xnorm_new;
     }
     rsnrm = xnorm_new;
@@ -1377,10 +1399,11 @@ extern "C" int pmgb_energy(pmgb_solver* s, double* energy_kT) {
   CK(cudaStreamSynchronize(st));
   const pmgb_params& p = s->p;
   double qf = sums[0] * p.hx * p.hy * p.hz / s->zmagic;
-  if (p.chgm == PMGB_CHGM_TRIL && !uses_charge_map(s)) {
-    // Vpmg_qfEnergyPoint (vpmg.c:1704-1789): charges at the atoms
+  if (p.chgm != PMGB_CHGM_SPL2 && !uses_charge_map(s)) {
+    // Vpmg_qfEnergyPoint (vpmg.c:1704-1789): charges at the atoms (every
+    // discretisation but spl2 without a charge map, Vpmg_qfEnergy 1692-1699)
     if (s->natoms <= 0 || !s->d_xyz) {
-      set_error("pmgb_energy: chgm spl0 needs the atom list (pmgb_fillco)");
+      set_error("pmgb_energy: chgm spl0/spl4 needs the atom list (pmgb_fillco)");
       return 0;
     }
     launch_qf_point(st, s->G, s->natoms, s->d_xyz, s->d_q, s->lev[0].x, s->part,

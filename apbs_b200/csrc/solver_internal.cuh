@@ -116,6 +116,9 @@ struct pmgb_solver {
   int* sas_nbr;        // per-atom lists of possible excluders, then their counts
   size_t sas_nbr_alloc;
   size_t sas_list_alloc;
+  // srfm spl3: the per-atom window polynomials (spline3_table)
+  double* d_spl3;
+  size_t spl3_alloc;
   // atoms binned by tile of grid points for the charge gather
   int *ch_count, *ch_start, *ch_fill, *ch_atoms;
   size_t ch_tiles_alloc, ch_atoms_alloc;

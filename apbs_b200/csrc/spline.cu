@@ -1,7 +1,8 @@
-// Spline-based molecular surfaces (srfm spl2, spl4) and the forces on the atoms.
+// Spline-based molecular surfaces (srfm spl2, spl3, spl4) and the forces on the atoms.
 //
-// Surface: fillcoCoefSpline (src/mg/vpmg.c:4631-4854); fillcoCoefSpline4
-// (7052-7366) is the same with a 7th-order polynomial on the window.  kappa, epsx, epsy
+// Surface: fillcoCoefSpline (src/mg/vpmg.c:4631-4854); fillcoCoefSpline3
+// (7525-7840) and fillcoCoefSpline4 (7052-7366) are the same with a 5th- and a
+// 7th-order polynomial on the window.  kappa, epsx, epsy
 // and epsz start at 1 everywhere; for every on-mesh atom with a positive
 // radius, in atom order, each grid point inside the atom's search box has
 // its values multiplied by the cubic spline accessibility of the point (0
@@ -18,8 +19,8 @@
 // reference's expressions, so each point sees the same factors in the same
 // order and the maps are bitwise equal.
 //
-// Forces: Vpmg_qfForce (vpmg.c:5862-5904 with qfForceSpline1 5906-6041 and
-// qfForceSpline2 6043-6154), Vpmg_dbForce (5605-5860) and Vpmg_ibForce
+// Forces: Vpmg_qfForce (vpmg.c:5862-5904 with qfForceSpline1 5906-6041,
+// qfForceSpline2 6043-6154 and qfForceSpline4 6156-6272), Vpmg_dbForce (5605-5860) and Vpmg_ibForce
 // (5440-5603) with Vacc_splineAccGradAtomNorm (src/generic/vacc.c:314-373).
 // One thread per atom walks the reference's loops in their order, so each
 // sum is taken in the reference's order.
@@ -50,6 +51,7 @@ struct SplineArgs {
   double win;       // spline window
   double ionmask;   // 1 if the ionic strength is positive
   double epsp, epsw;
+  const double* c3;  // spl3: spline3_table's 18 coefficients per atom
   double *kappa, *epsx, *epsy, *epsz;
 };
 
@@ -57,6 +59,7 @@ struct SplAtom {
   double pos[3];  // position relative to the grid origin
   double arad;
   int box[6];     // imin, imax, jmin, jmax, kmin, kmax
+  int idx;        // atom index
 };
 
 constexpr int kBX = 8, kBY = 8, kBZ = 8;        // grid points per CTA block
@@ -75,6 +78,7 @@ __device__ __forceinline__ bool spline_atom(const SplineArgs& A, int a, SplAtom&
   if (!(arad > kPmgSmall)) return false;
   for (int d = 0; d < 3; d++) s.pos[d] = apos[d] - G.xmin[d];
   s.arad = arad;
+  s.idx = a;
   const double itot = A.irad + arad + A.win;
   const double stot = arad + A.win;
   const double rtot = (itot > stot) ? itot : stot;
@@ -125,8 +129,20 @@ __device__ __forceinline__ double spline7_value(const double* c, double sm, doub
   return value;
 }
 
-// ORDER 2: cubic window (srfm spl2, fillcoCoefSpline); ORDER 4: 7th-order
-// polynomial (srfm spl4, fillcoCoefSpline4, vpmg.c:7052-7366)
+// the 5th-order accessibility of fillcoCoefSpline3 at distance sm (sm2 as the
+// reference forms it for that map), clamped to [0, 1]
+__device__ __forceinline__ double spline5_value(const double* c, double sm, double sm2) {
+  const double sm3 = sm2 * sm, sm4 = sm3 * sm, sm5 = sm4 * sm;
+  double value = c[0] + c[1] * sm + c[2] * sm2 + c[3] * sm3 + c[4] * sm4 + c[5] * sm5;
+  if (value > 1.0) value = 1.0;
+  else if (value < 0.0) value = 0.0;
+  return value;
+}
+
+// ORDER 2: cubic window (srfm spl2, fillcoCoefSpline); ORDER 3: 5th-order
+// polynomial (srfm spl3, fillcoCoefSpline3, vpmg.c:7525-7840) with the
+// per-atom coefficients of spline3_table; ORDER 4: 7th-order polynomial
+// (srfm spl4, fillcoCoefSpline4, vpmg.c:7052-7366)
 template <int ORDER>
 __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
   __shared__ SplAtom cand[kSplCap];
@@ -170,6 +186,8 @@ __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
             const double dist = sqrt(dist2);
             if (ORDER == 2) {
               kap[p] *= spline_value(dist, arad + A.irad, win, w2i, w3i);
+            } else if (ORDER == 3) {
+              kap[p] *= spline5_value(A.c3 + 18 * (size_t)s.idx + 6, dist, dist2);
             } else {
               double c[8];
               spline7_coef(A.irad + arad, win, c);
@@ -185,6 +203,8 @@ __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
             const double dist = sqrt(dist2);
             if (ORDER == 2) {
               ex[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else if (ORDER == 3) {
+              ex[p] *= spline5_value(A.c3 + 18 * (size_t)s.idx, dist, dist * dist);
             } else {
               double c[8];
               spline7_coef(arad, win, c);
@@ -200,6 +220,8 @@ __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
             const double dist = sqrt(dist2);
             if (ORDER == 2) {
               ey[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else if (ORDER == 3) {
+              ey[p] *= spline5_value(A.c3 + 18 * (size_t)s.idx, dist, dist * dist);
             } else {
               double c[8];
               spline7_coef(arad, win, c);
@@ -215,6 +237,8 @@ __global__ void __launch_bounds__(kSplThreads) k_spline_fill(SplineArgs A) {
             const double dist = sqrt(dist2);
             if (ORDER == 2) {
               ez[p] *= spline_value(dist, arad, win, w2i, w3i);
+            } else if (ORDER == 3) {
+              ez[p] *= spline5_value(A.c3 + 18 * (size_t)s.idx, dist, dist2);
             } else {
               double c[8];
               spline7_coef(arad, win, c);
@@ -282,7 +306,8 @@ struct ForceArgs {
   const double *epsx, *epsy, *epsz, *kappa;
   int chgm;         // PMGB_CHGM_*
   int boundary;     // compute the dielectric and ionic boundary forces
-  int order;        // surface: 2 = spl2, 4 = spl4 (Vpmg_splineSelect)
+  int order;        // surface: 2 = spl2, 3 = spl3, 4 = spl4 (Vpmg_splineSelect)
+  const double* c3; // spl3: spline3_table's coefficients
   int nonlin;
   double win, irad, srad, epsp, epsw, zkappa2, izmagic, ionstr;
   int nion;
@@ -363,6 +388,30 @@ __device__ __forceinline__ void spline_grad4(const double* center, double win, d
   for (int d = 0; d < 3; d++) grad[d] = -(mygrad / mychi) * ((center[d] - apos[d]) / dist);
 }
 
+// the same for the 5th-order polynomial (Vacc_splineAccGradAtomNorm3,
+// vacc.c:1097-1180); c: the atom's coefficients for this inflation
+__device__ __forceinline__ void spline_grad3(const double* center, double win, double infrad,
+                                             const double* apos, double radius, const double* c,
+                                             double* grad) {
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (!(radius > 0.0)) return;
+  const double arad = radius + infrad;
+  const double d0 = apos[0] - center[0], d1 = apos[1] - center[1], d2 = apos[2] - center[2];
+  const double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  double mychi, mygrad;
+  if (dist < (arad - win)) return;
+  else if (dist > (arad + win)) return;
+  else if ((fabs(dist - (arad - win)) < kVSmall) || (fabs(dist - (arad + win)) < kVSmall)) return;
+  else {
+    const double sm = dist, sm2 = sm * sm, sm3 = sm2 * sm, sm4 = sm3 * sm, sm5 = sm4 * sm;
+    mychi = c[0] + c[1] * sm + c[2] * sm2 + c[3] * sm3 + c[4] * sm4 + c[5] * sm5;
+    mygrad = c[1] + 2.0 * c[2] * sm + 3.0 * c[3] * sm2 + 4.0 * c[4] * sm3 + 5.0 * c[5] * sm4;
+    if (mychi <= 0.0) return;
+    else if (mychi > 1.0) mychi = 1.0;
+  }
+  for (int d = 0; d < 3; d++) grad[d] = -(mygrad / mychi) * ((center[d] - apos[d]) / dist);
+}
+
 // Vcap_exp (src/generic/vcap.c:59-73)
 __device__ __forceinline__ double cap_exp(double x) {
   if (x > kExpMax) return exp(kExpMax);
@@ -370,10 +419,15 @@ __device__ __forceinline__ double cap_exp(double x) {
   return exp(x);
 }
 
-__device__ __forceinline__ void surf_grad(const ForceArgs& A, const double* center,
+// infrad is 0 (dielectric) or the largest ion radius (ion accessibility),
+// which picks the spl3 coefficient set of atom a
+__device__ __forceinline__ void surf_grad(const ForceArgs& A, int a, const double* center,
                                           double infrad, const double* apos, double radius,
                                           double* grad) {
   if (A.order == 4) spline_grad4(center, A.win, infrad, apos, radius, grad);
+  else if (A.order == 3)
+    spline_grad3(center, A.win, infrad, apos, radius,
+                 A.c3 + 18 * (size_t)a + (infrad == 0.0 ? 0 : 12), grad);
   else spline_grad(center, A.win, infrad, apos, radius, grad);
 }
 
@@ -438,6 +492,8 @@ __global__ void k_forces(ForceArgs A) {
           }
         }
       }
+    } else if (A.chgm == PMGB_CHGM_SPL4) {
+      // handled below: qfForceSpline4 has no partition test
     } else if (!((apos[0] <= xmin) || (apos[0] >= xmax) || (apos[1] <= ymin) ||
                  (apos[1] >= ymax) || (apos[2] <= zmin) || (apos[2] >= zmax))) {
       // trilinear charges (qfForceSpline1)
@@ -480,6 +536,37 @@ __global__ void k_forces(ForceArgs A) {
       }
     }
   }
+  if (A.chgm == PMGB_CHGM_SPL4 &&
+      !((apos[0] <= (xmin + 2 * hx)) || (apos[0] >= (xmax - 2 * hx)) ||
+        (apos[1] <= (ymin + 2 * hy)) || (apos[1] >= (ymax - 2 * hy)) ||
+        (apos[2] <= (zmin + 2 * hzed)) || (apos[2] >= (zmax - 2 * hzed)))) {
+    // qfForceSpline4 (vpmg.c:6156-6272): the field of the 5th-order B-spline
+    // charge at the atom, times its charge
+    const double ifloat = (apos[0] - xmin) / hx;
+    const double jfloat = (apos[1] - ymin) / hy;
+    const double kfloat = (apos[2] - zmin) / hzed;
+    const int ip2 = min((int)ceil(ifloat) + 2, nx - 1), im2 = max((int)floor(ifloat) - 2, 0);
+    const int jp2 = min((int)ceil(jfloat) + 2, ny - 1), jm2 = max((int)floor(jfloat) - 2, 0);
+    const int kp2 = min((int)ceil(kfloat) + 2, nz - 1), km2 = max((int)floor(kfloat) - 2, 0);
+    double e[3] = {0.0, 0.0, 0.0};
+    for (int ii = im2; ii <= ip2; ii++) {
+      const double mi = (2.5 + ((double)(ii) - (ifloat)));
+      const double mx = bspline4(mi), dmx = dbspline4(mi);
+      for (int jj = jm2; jj <= jp2; jj++) {
+        const double mj = (2.5 + ((double)(jj) - (jfloat)));
+        const double my = bspline4(mj), dmy = dbspline4(mj);
+        for (int kk = km2; kk <= kp2; kk++) {
+          const double mk = (2.5 + ((double)(kk) - (kfloat)));
+          const double mz = bspline4(mk), dmz = dbspline4(mk);
+          const double f = u[IJK(ii, jj, kk)];
+          e[0] += f * dmx * my * mz / hx;
+          e[1] += f * mx * dmy * mz / hy;
+          e[2] += f * mx * my * dmz / hzed;
+        }
+      }
+    }
+    for (int d = 0; d < 3; d++) out[d] = e[d] * charge;
+  }
   if (!A.boundary || part_id == 0.0) {
     A.status[a] = status;
     return;
@@ -509,27 +596,27 @@ __global__ void k_forces(ForceArgs A) {
               double gpos[3], dHx[3], dHy[3], dHz[3], dHxm[3], dHym[3], dHzm[3];
               gpos[0] = (i + 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hxijk = (A.epsx[IJK(i, j, k)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHx);
+              surf_grad(A, a, gpos, 0., apos, radius, dHx);
               for (int l = 0; l < 3; l++) dHx[l] *= Hxijk;
               gpos[0] = i * hx + xmin; gpos[1] = (j + 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hyijk = (A.epsy[IJK(i, j, k)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHy);
+              surf_grad(A, a, gpos, 0., apos, radius, dHy);
               for (int l = 0; l < 3; l++) dHy[l] *= Hyijk;
               gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k + 0.5) * hzed + zmin;
               const double Hzijk = (A.epsz[IJK(i, j, k)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHz);
+              surf_grad(A, a, gpos, 0., apos, radius, dHz);
               for (int l = 0; l < 3; l++) dHz[l] *= Hzijk;
               gpos[0] = (i - 0.5) * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hxim1jk = (A.epsx[IJK(i - 1, j, k)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHxm);
+              surf_grad(A, a, gpos, 0., apos, radius, dHxm);
               for (int l = 0; l < 3; l++) dHxm[l] *= Hxim1jk;
               gpos[0] = i * hx + xmin; gpos[1] = (j - 0.5) * hy + ymin; gpos[2] = k * hzed + zmin;
               const double Hyijm1k = (A.epsy[IJK(i, j - 1, k)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHym);
+              surf_grad(A, a, gpos, 0., apos, radius, dHym);
               for (int l = 0; l < 3; l++) dHym[l] *= Hyijm1k;
               gpos[0] = i * hx + xmin; gpos[1] = j * hy + ymin; gpos[2] = (k - 0.5) * hzed + zmin;
               const double Hzijkm1 = (A.epsz[IJK(i, j, k - 1)] - A.epsp) * depsi;
-              surf_grad(A, gpos, 0., apos, radius, dHzm);
+              surf_grad(A, a, gpos, 0., apos, radius, dHzm);
               for (int l = 0; l < 3; l++) dHzm[l] *= Hzijkm1;
               const double u0 = u[IJK(i, j, k)];
               const double dbFmag = u0;
@@ -583,7 +670,7 @@ __global__ void k_forces(ForceArgs A) {
             gpos[0] = i * hx + xmin;
             gpos[1] = j * hy + ymin;
             gpos[2] = k * hzed + zmin;
-            surf_grad(A, gpos, A.irad, apos, radius, tgrad);
+            surf_grad(A, a, gpos, A.irad, apos, radius, tgrad);
             const double uv = u[IJK(i, j, k)], kv = A.kappa[IJK(i, j, k)];
             double fmag;
             if (A.nonlin) {
@@ -607,8 +694,8 @@ __global__ void k_forces(ForceArgs A) {
 
 void launch_spline_fill(cudaStream_t st, int order, const FillGeom& G, int natoms,
                         const double* xyz, const double* r, double irad, double win,
-                        double ionmask, double epsp, double epsw, double* kappa, double* epsx,
-                        double* epsy, double* epsz) {
+                        double ionmask, double epsp, double epsw, const double* coef3,
+                        double* kappa, double* epsx, double* epsy, double* epsz) {
   SplineArgs A;
   A.G = G;
   A.natoms = natoms;
@@ -619,13 +706,52 @@ void launch_spline_fill(cudaStream_t st, int order, const FillGeom& G, int natom
   A.ionmask = ionmask;
   A.epsp = epsp;
   A.epsw = epsw;
+  A.c3 = coef3;
   A.kappa = kappa;
   A.epsx = epsx;
   A.epsy = epsy;
   A.epsz = epsz;
   dim3 grid((G.g.nx + kBX - 1) / kBX, (G.g.ny + kBY - 1) / kBY, (G.g.nz + kBZ - 1) / kBZ);
   if (order == 4) k_spline_fill<4><<<grid, kSplThreads, 0, st>>>(A);
+  else if (order == 3) k_spline_fill<3><<<grid, kSplThreads, 0, st>>>(A);
   else k_spline_fill<2><<<grid, kSplThreads, 0, st>>>(A);
+}
+
+// The window polynomials of fillcoCoefSpline3 (vpmg.c:7590-7641) and
+// Vacc_splineAccGradAtomNorm3 (vacc.c:1118-1143) for window [b, e]:
+// c_k / (e - b)^5 with the reference's expressions and its pow().
+static void spline3_poly(double b, double e, double* c) {
+  const double e2 = e * e;
+  const double b2 = b * b, b3 = b2 * b, b4 = b3 * b, b5 = b4 * b;
+  const double denom = pow((e - b), 5.0);
+  c[0] = (-10.0 * e2 * b3 + 5.0 * e * b4 - b5) / denom;
+  c[1] = (30.0 * e2 * b2) / denom;
+  c[2] = (-30.0 * (e2 * b + e * b2)) / denom;
+  c[3] = (10.0 * (e2 + 4.0 * e * b + b2)) / denom;
+  c[4] = (-15.0 * (e + b)) / denom;
+  c[5] = 6.0 / denom;
+}
+
+// Per atom, 18 coefficients: [0, 6) the dielectric window (radius +- win),
+// used by the eps maps and by the dielectric-boundary gradient; [6, 12) what
+// fillcoCoefSpline3 multiplies kappa by: the dielectric coefficients divided
+// once more by the ion window's (e - b)^5 (vpmg.c:7630-7641 assign
+// ic0 = c0/denom ... after c0..c5 were divided already, so the ion window's
+// own polynomial is never used there); [12, 18) the ion window's own
+// polynomial (radius + irad +- win), used by the ionic-boundary gradient.
+void spline3_table(int natoms, const double* r, double irad, double win,
+                   std::vector<double>& tab) {
+  tab.assign(18 * (size_t)natoms, 0.0);
+  for (int a = 0; a < natoms; a++) {
+    double* t = tab.data() + 18 * (size_t)a;
+    const double arad = r[a];
+    spline3_poly(arad - win, arad + win, t);
+    const double bi = irad + arad - win, ei = irad + arad + win;
+    const double idenom = pow((ei - bi), 5.0);
+    for (int k = 0; k < 6; k++) t[6 + k] = t[k] / idenom;
+    const double ar = arad + irad;
+    spline3_poly(ar - win, ar + win, t + 12);
+  }
 }
 
 }  // namespace pmgb
@@ -641,11 +767,13 @@ extern "C" int pmgb_forces(pmgb_solver* s, double* qf, double* db, double* ib) {
   const pmgb_params& p = s->p;
   const int natoms = s->natoms;
   const int boundary = (db || ib) ? 1 : 0;
-  if (boundary && p.srfm != PMGB_SRFM_SPL2 && p.srfm != PMGB_SRFM_SPL4) {
-    set_error("pmgb_forces: the boundary forces need srfm spl2 or spl4 (spline-based surfaces)");
+  if (boundary && p.srfm != PMGB_SRFM_SPL2 && p.srfm != PMGB_SRFM_SPL3 &&
+      p.srfm != PMGB_SRFM_SPL4) {
+    set_error("pmgb_forces: the boundary forces need srfm spl2, spl3 or spl4 (spline-based "
+              "surfaces)");
     return 0;
   }
-  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL) {
+  if (p.chgm != PMGB_CHGM_SPL2 && p.chgm != PMGB_CHGM_TRIL && p.chgm != PMGB_CHGM_SPL4) {
     set_error("pmgb_forces: chgm %d has no charge-field force", p.chgm);
     return 0;
   }
@@ -672,7 +800,8 @@ extern "C" int pmgb_forces(pmgb_solver* s, double* qf, double* db, double* ib) {
   A.kappa = s->kappa;
   A.chgm = p.chgm;
   A.boundary = boundary;
-  A.order = (p.srfm == PMGB_SRFM_SPL4) ? 4 : 2;
+  A.order = (p.srfm == PMGB_SRFM_SPL4) ? 4 : (p.srfm == PMGB_SRFM_SPL3 ? 3 : 2);
+  A.c3 = s->d_spl3;
   A.nonlin = p.nonlin;
   A.win = (p.swin > 0.0) ? p.swin : 0.3;
   A.irad = s->maxIonRadius;

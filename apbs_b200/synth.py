@@ -20,8 +20,8 @@ from dataclasses import dataclass
 import numpy as np
 
 PMGB_MAXION = 8
-SRFM_MOL, SRFM_SMOL, SRFM_SPL2, SRFM_SPL4 = 0, 1, 2, 4
-CHGM_TRIL, CHGM_SPL2 = 0, 1
+SRFM_MOL, SRFM_SMOL, SRFM_SPL2, SRFM_SPL3, SRFM_SPL4 = 0, 1, 2, 3, 4
+CHGM_TRIL, CHGM_SPL2, CHGM_SPL4 = 0, 1, 2
 BCFL_ZERO, BCFL_SDH, BCFL_MDH, BCFL_FOCUS, BCFL_MAP = 0, 1, 2, 4, 6
 
 

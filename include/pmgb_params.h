@@ -19,10 +19,13 @@
 #define PMGB_SRFM_MOL 0
 #define PMGB_SRFM_SMOL 1
 #define PMGB_SRFM_SPL2 2   /* cubic-spline surface (fillcoCoefSpline) */
+#define PMGB_SRFM_SPL3 3   /* 5th-order polynomial surface (fillcoCoefSpline3) */
 #define PMGB_SRFM_SPL4 4   /* 7th-order polynomial surface (fillcoCoefSpline4) */
 /* Charge method codes (Vchrg_Meth, src/generic/vhal.h:231-234). */
 #define PMGB_CHGM_TRIL 0   /* chgm spl0: trilinear to the 8 nearest points */
 #define PMGB_CHGM_SPL2 1
+#define PMGB_CHGM_SPL4 2   /* chgm spl4: 5th-order B-spline to 6^3 points
+                              (fillcoPermanentMultipole with atomic charges) */
 /* Boundary condition codes (Vbcfl, src/generic/vhal.h:208-216). */
 #define PMGB_BCFL_ZERO 0
 #define PMGB_BCFL_SDH 1
@@ -37,7 +40,7 @@ typedef struct pmgb_params {
     double center[3];       /* grid centre in Angstrom ("gcent") */
     int nonlin;             /* 0 = lpbe, 1 = npbe */
     int srfm;               /* PMGB_SRFM_* */
-    int chgm;               /* PMGB_CHGM_TRIL (spl0) or PMGB_CHGM_SPL2 */
+    int chgm;               /* PMGB_CHGM_TRIL (spl0), _SPL2 or _SPL4 */
     int bcfl;               /* PMGB_BCFL_* */
     double pdie;            /* solute dielectric */
     double sdie;            /* solvent dielectric */

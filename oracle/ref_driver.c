@@ -106,7 +106,7 @@ static MGparm *make_mgparm(const pmgb_params *p) {
  *          [6] t_energy (seconds) [7] qf [8] diel [9] qm (kT, NPBE only)
  *   reslog (out, optional) relative residual of every progress message
  *   forces (out, optional) 9 doubles per atom: Vpmg_qfForce, Vpmg_dbForce,
- *          Vpmg_ibForce (kT/A), the last two for srfm spl2 only
+ *          Vpmg_ibForce (kT/A), the last two for the spline surfaces only
  *   fstatus (out, optional) per atom, 1 if both boundary forces succeeded
  * Returns 1 on success (Vpmg convention), 0 on failure.
  */
@@ -223,7 +223,8 @@ static int run_impl(const pmgb_params *p, int natoms, const double *xyz,
         for (i = 0; i < natoms; i++) {
             int rcf = 1;
             Vpmg_qfForce(pmg, forces + 9 * (size_t)i, i, (Vchrg_Meth)p->chgm);
-            if (p->srfm == PMGB_SRFM_SPL2 || p->srfm == PMGB_SRFM_SPL4) {
+            if (p->srfm == PMGB_SRFM_SPL2 || p->srfm == PMGB_SRFM_SPL3 ||
+                p->srfm == PMGB_SRFM_SPL4) {
                 rcf &= Vpmg_dbForce(pmg, forces + 9 * (size_t)i + 3, i, (Vsurf_Meth)p->srfm);
                 rcf &= Vpmg_ibForce(pmg, forces + 9 * (size_t)i + 6, i, (Vsurf_Meth)p->srfm);
             } else {

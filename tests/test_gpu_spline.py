@@ -1,5 +1,7 @@
-"""Spline-based surfaces (srfm spl2 and spl4: fillcoCoefSpline,
-fillcoCoefSpline4) and the per-atom forces (Vpmg_qfForce, Vpmg_dbForce,
+"""Spline-based surfaces (srfm spl2, spl3 and spl4: fillcoCoefSpline,
+fillcoCoefSpline3, fillcoCoefSpline4), the charge discretisations (chgm
+spl0, spl2 and spl4: fillcoChargeSpline1/2, fillcoPermanentMultipole with
+atomic charges) and the per-atom forces (Vpmg_qfForce, Vpmg_dbForce,
 Vpmg_ibForce) on the device against the reference compiled from source
 (oracle/_ref): the kappa and dielectric maps bitwise, the potential and
 energy to 1e-9, every force component to 1e-8 of the largest force of its
@@ -34,8 +36,19 @@ def _cases():
     p4.swin = 0.4
     p5 = synth.mg_manual(65, 0.5, m1.center(), srfm=synth.SRFM_SPL4, ions=IONS)
     p6 = synth.mg_manual(57, 0.5, m3.center(), srfm=synth.SRFM_SPL4, npbe=True, ions=IONS)
-    return [("lpbe65", m1, p1), ("npbe65", m1, p2), ("lpbe_box_spl0", m3, p3),
-            ("lpbe49_noions_swin04", m3, p4), ("lpbe65_spl4", m1, p5), ("npbe57_spl4", m3, p6)]
+    p7 = synth.mg_manual(65, 0.5, m1.center(), srfm=synth.SRFM_SPL3, ions=IONS)
+    p8 = synth.mg_manual(57, 0.5, m3.center(), srfm=synth.SRFM_SPL3, npbe=True, ions=IONS)
+    p9 = synth.mg_manual(49, 0.55, m3.center(), srfm=synth.SRFM_SPL3, ions=())
+    p9.swin = 0.4
+    p10 = synth.mg_manual(65, 0.5, m1.center(), srfm=synth.SRFM_SPL2, ions=IONS)
+    p10.chgm = synth.CHGM_SPL4
+    p11 = synth.mg_manual(57, 0.5, m3.center(), srfm=synth.SRFM_SPL4, npbe=True, ions=IONS)
+    p11.chgm = synth.CHGM_SPL4
+    return [("lpbe65_chgm_spl4", m1, p10), ("npbe57_spl4_chgm_spl4", m3, p11),
+            ("lpbe65", m1, p1), ("npbe65", m1, p2), ("lpbe_box_spl0", m3, p3),
+            ("lpbe49_noions_swin04", m3, p4), ("lpbe65_spl4", m1, p5), ("npbe57_spl4", m3, p6),
+            ("lpbe65_spl3", m1, p7), ("npbe57_spl3", m3, p8),
+            ("lpbe49_spl3_noions_swin04", m3, p9)]
 
 
 CASES = _cases()
