@@ -42,15 +42,17 @@ CANDIDATES = {
         TUNE_GS27_PLANES: [0, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
-        TUNE_GS7_SWEEP_SHAPE: [2, 0x12, 0x01, 0x31],
-        TUNE_GS7_SWEEP_KCHUNK: [8, 6, 12, 18],
+        TUNE_GS7_SWEEP_SHAPE: [0x12, 0x11, 0x02, 0x21],
+        TUNE_GS7_SWEEP_KCHUNK: [10, 8, 12, 6],
     },
     MIXED: {
         TUNE_MIXED_CHEBYSHEV: [2, 0, 4],
         TUNE_TAIL_MAX_POINTS: [70000, 20000, 5000],
-        TUNE_MIXED_FINE_SWEEPS: [2, 1, 3],
+        TUNE_MIXED_FINE_SWEEPS: [2, 1, 3, 4],
         TUNE_MIXED_COARSE_SWEEPS: [2, 1, 3],
         TUNE_GS7_COLOUR_PASSES: [0, 2],
+        TUNE_GS7_SWEEP_SHAPE: [0x12, 0x21, 0x11],
+        TUNE_GS7_SWEEP_KCHUNK: [10, 6, 8],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
     },
 }

@@ -73,7 +73,9 @@ __device__ __forceinline__ T rb_update(T f, T n1, T xn, T n0, T xs, T e1, T xe, 
     return (f + (n1 * xn + n0 * xs + e1 * xe + e0 * xw + d0 * xd + u1 * xu)) / dg;
 }
 
-template <typename T, int C1, int NT>
+// Q pair slots per thread (E = NT Q): the slot loops are unrolled so the
+// loads of all of a thread's slots are in flight together.
+template <typename T, int C1, int NT, int Q>
 __global__ void __launch_bounds__(NT) k_gs7_rb(Gs7Rb<T> a) {
   constexpr int C2 = 1 - C1;
   extern __shared__ __align__(16) unsigned char rb_smem[];
@@ -96,7 +98,9 @@ __global__ void __launch_bounds__(NT) k_gs7_rb(Gs7Rb<T> a) {
     const int m0 = rb_base(k, S, c0, nx);
     const int lo = k * S, hi = lo + S;
     const bool boundary_plane = (k == 0) || (k == a.nz - 1);
-    for (int e = threadIdx.x; e < E; e += NT) {
+#pragma unroll
+    for (int r = 0; r < Q; r++) {
+      const int e = threadIdx.x + r * NT;
       const int p = 2 * (m0 + e) + C1;
       T v = T(0);
       if (!boundary_plane && p >= lo && p < hi) {
@@ -125,7 +129,9 @@ __global__ void __launch_bounds__(NT) k_gs7_rb(Gs7Rb<T> a) {
     const int dU = m0 + (C2 - C1 + S) / 2 - rb_base(k + 1, S, c0, nx);
     const int lo = k * S + c0, hi = k * S + c1e;
     T* __restrict__ xo = a.xout;
-    for (int e = threadIdx.x; e < E; e += NT) {
+#pragma unroll
+    for (int r = 0; r < Q; r++) {
+      const int e = threadIdx.x + r * NT;
       const int m = m0 + e;
       const int p2 = 2 * m + C2;
       const int p1 = 2 * m + C1;
@@ -169,29 +175,40 @@ inline int gs7_rb_core(int nx, int S, int slots) {
   return core > S ? ((S + 1) & ~1) : core;
 }
 
-template <typename T, int NT>
-inline cudaError_t launch_gs7_rb_nt(cudaStream_t st, Gs7Rb<T> a, int c1, int q) {
-  a.E = NT * q;
+template <typename T, int NT, int Q>
+inline cudaError_t launch_gs7_rb_q(cudaStream_t st, Gs7Rb<T> a, int c1) {
+  a.E = NT * Q;
   a.core = gs7_rb_core(a.nx, a.S, a.E);
   if (a.core == 0) return cudaErrorInvalidValue;
   const size_t smem = (size_t)3 * a.E * sizeof(T);
   const dim3 grid((a.S + a.core - 1) / a.core, (a.nz - 2 + a.kchunk - 1) / a.kchunk);
   if (c1) {
     static const cudaError_t attr = cudaFuncSetAttribute(
-        k_gs7_rb<T, 1, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_gs7_rb<T, 1, NT, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     if (attr != cudaSuccess) return attr;
-    k_gs7_rb<T, 1, NT><<<grid, NT, smem, st>>>(a);
+    k_gs7_rb<T, 1, NT, Q><<<grid, NT, smem, st>>>(a);
   } else {
     static const cudaError_t attr = cudaFuncSetAttribute(
-        k_gs7_rb<T, 0, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_gs7_rb<T, 0, NT, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     if (attr != cudaSuccess) return attr;
-    k_gs7_rb<T, 0, NT><<<grid, NT, smem, st>>>(a);
+    k_gs7_rb<T, 0, NT, Q><<<grid, NT, smem, st>>>(a);
   }
   return cudaGetLastError();
 }
 
+template <typename T, int NT>
+inline cudaError_t launch_gs7_rb_nt(cudaStream_t st, const Gs7Rb<T>& a, int c1, int q) {
+  switch (q) {
+    case 1: return launch_gs7_rb_q<T, NT, 1>(st, a, c1);
+    case 2: return launch_gs7_rb_q<T, NT, 2>(st, a, c1);
+    case 3: return launch_gs7_rb_q<T, NT, 3>(st, a, c1);
+    case 4: return launch_gs7_rb_q<T, NT, 4>(st, a, c1);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // shape: bits 0-3 threads per CTA (0: 256, 1: 512, 2: 1024), bits 4-7 pair
-// slots per thread (0: 2); a CTA's widened range is threads x slots pairs
+// slots per thread (1-4, 0: 2); a CTA's widened range is threads x slots pairs
 template <typename T>
 inline cudaError_t launch_gs7_rb(cudaStream_t st, const Gs7Rb<T>& a, int c1, int shape) {
   const int nt = shape & 15, q = ((shape >> 4) & 15) ? ((shape >> 4) & 15) : 2;

@@ -372,7 +372,7 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {2, 0, 0, 0, 0, 0, 8, 0, 70000, 0, 2, 2, 2, 0, 0, 0};
+int g_tune[16] = {2, 0, 0, 0, 0, 0, 10, 0, 70000, 0, 2, 2, 0x12, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,

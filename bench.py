@@ -396,8 +396,8 @@ def main():
             ids = [k for k, n in autotune.KEY_NAMES.items() if n == key]
             if not ids:
                 raise SystemExit("--tune: unknown key %r" % key)
-            s.set_tuning(ids[0], int(val))
-            tuned[name][ids[0]] = int(val)
+            s.set_tuning(ids[0], int(val, 0))
+            tuned[name][ids[0]] = int(val, 0)
         s.set_stream(stream.cuda_stream)
         solvers[name] = s
 
@@ -488,7 +488,13 @@ def main():
     # headline stream
     peak, peak_kind = peak_hbm()
     if args.headline == "mixed":
-        kern, kname, ksolver = vpmg.K_GS7_FP32, "k_gs7_f32", solvers["mixed"]
+        # the fine smoother the tuned calculation runs: FP32 single-pass
+        # sweeps or one launch per colour
+        ksolver = solvers["mixed"]
+        if ksolver.get_tuning(vpmg.TUNE_GS7_COLOUR_PASSES) == 2:
+            kern, kname = vpmg.K_GS7_SWEEP_FP32, "k_gs7_rb<float>"
+        else:
+            kern, kname = vpmg.K_GS7_FP32, "k_gs7_f32"
     else:
         kern, kname, ksolver = vpmg.K_GS27_WAVE, "k_gs27_wave", solvers["fp64"]
     ms, nbytes = ksolver.time_kernel(kern, 10)

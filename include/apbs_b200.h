@@ -230,7 +230,7 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
                                           kernel, FP32 one launch per colour), 1 = one launch
                                           per colour, 2 = single-pass sweeps in FP32 too */
-#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 8) */
+#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 10) */
 #define PMGB_TUNE_GS27_CLUSTER_MID 7   /* the same as key 2 for levels with 28-59 interior
                                           points per axis (0 = 8) */
 #define PMGB_TUNE_TAIL_MAX_POINTS 8    /* mixed: largest level (interior points) run inside
@@ -243,8 +243,9 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_MIXED_FINE_SWEEPS 11 /* mixed: red-black sweeps on the fine level (default 2) */
 #define PMGB_TUNE_GS7_SWEEP_SHAPE 12 /* single-pass sweep launch shape: bits 0-3 threads per
                                           CTA (0 = 256, 1 = 512, 2 = 1024), bits 4-7 pair
-                                          slots per thread (0 = 2); a CTA owns a flat range
-                                          of 2 x (slots - nx - 3) points of each plane */
+                                          slots per thread (1-4, 0 = 2); a CTA owns a flat range
+                                          of 2 x (slots - nx - 3) points of each plane;
+                                          default 0x12: 1024 threads, 1 slot */
 #define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
                                           synchronised with its neighbour planes on every
                                           level whose planes fit on the device, 1 = one
