@@ -39,6 +39,7 @@ DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
 # candidate values per key; the first value of each list is the default
 CANDIDATES = {
     FP64: {
+        vpmg.TUNE_GS27_LAG: [6, 4, 8, 12],
         TUNE_GS27_PLANES: [0, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
@@ -58,6 +59,7 @@ CANDIDATES = {
 }
 
 KEY_NAMES = {TUNE_GS27_CLUSTER: "gs27_cluster", TUNE_GS27_CLUSTER_MID: "gs27_cluster_mid",
+             vpmg.TUNE_GS27_LAG: "gs27_lag",
              TUNE_GS27_PLANES: "gs27_planes",
              TUNE_GS7_COLOUR_PASSES: "gs7_colour_passes", TUNE_GS7_SWEEP_KCHUNK: "gs7_sweep_kchunk",
              TUNE_TAIL_MAX_POINTS: "tail_max_points", TUNE_MC_COOPERATIVE: "mc_cooperative",

@@ -372,7 +372,7 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {2, 0, 0, 0, 0, 0, 10, 0, 70000, 0, 2, 2, 0x12, 0, 0, 0};
+int g_tune[16] = {2, 6, 0, 0, 0, 0, 10, 0, 70000, 0, 2, 2, 0x12, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
@@ -568,16 +568,23 @@ __global__ void k_gs27_wave(Grid g, Op op, const double* __restrict__ cc,
 // The same wavefront schedule with one CTA per interior plane k, synchronised
 // point to point instead of by a barrier over all CTAs.
 //
-// A step's items on plane k read values of planes k-1, k and k+1 only, so a
-// CTA may start step s once its two neighbour planes have finished step s-1;
-// each CTA publishes the number of steps it has finished in a counter.  A CTA
-// then runs at most one step ahead of its neighbours and never starts step s+1
-// before they have finished step s, so every value a step reads was written
-// in an earlier step and no value is overwritten before the step that reads
-// it, exactly as with the barrier: the iterates are bitwise those of
-// k_gs27_wave.  Spreading the planes over up to all SMs (one CTA each, a
-// cooperative launch so that all are resident together) divides the
-// per-step work that bounds the one-cluster kernel by the number of planes.
+// A step's items on plane k read values of planes k-1, k and k+1 only; each
+// CTA publishes the number of steps it has finished in a counter.  Successive
+// half-sweeps run wlag wavefronts apart (wlag >= 4; the residual wlag after
+// the last).  A point of half-sweep p reads, on the lower plane, values of
+// half-sweep p written one wavefront earlier, and on the upper plane values
+// of half-sweep p-1 written up to wlag-3 wavefronts earlier; so a CTA may
+// start step s once the lower neighbour has finished step s-1 and the upper
+// one step s-wlag+3.  Every value a step reads was written in an earlier
+// step, and no value is overwritten before the step that reads it (a
+// neighbour that would overwrite it waits for this plane first): the
+// iterates are bitwise those of k_gs27_wave whatever the lag, and with wlag
+// above 4 a plane may run ahead of the plane above it, so the planes
+// pipeline instead of moving in lockstep.  tests/test_gs27_wave_deps.py
+// checks both claims on adversarial interleavings.  Spreading the planes
+// over up to all SMs (one CTA each, a cooperative launch so that all are
+// resident together) divides the per-step work that bounds the one-cluster
+// kernel by the number of planes.
 //
 // The counters of a level are never reset between launches: every CTA of a
 // launch finishes all steps (after a wait that ran out it records the
@@ -646,13 +653,13 @@ template <bool POLL_ALL>
 __global__ void __launch_bounds__(kPlanesThreads, 1)
     k_gs27_planes(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ fc,
                   double* x, double* r, int nhalf, int first_parity, int do_resid,
-                  unsigned* counters, int* err) {
+                  unsigned* counters, int* err, int wlag) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t sy = nx, sz = (size_t)nx * ny;
   const int tmin = 1 + 2 * 1, tmax = (ny - 2) + 2 * (nz - 2);
   const int nphase = nhalf + (do_resid ? 1 : 0);
-  const int resid_lag = kWaveLag * (nhalf - 1) + 4;
-  const int last_start = do_resid ? resid_lag : kWaveLag * (nhalf - 1);
+  const int resid_lag = wlag * nhalf;
+  const int last_start = do_resid ? resid_lag : wlag * (nhalf - 1);
   const int nsteps = (tmax - tmin + 1) + last_start;
   const int hr = (nx - 1) / 2;
   const int c = blockIdx.x, k = 1 + c;  // this CTA's plane
@@ -670,7 +677,7 @@ __global__ void __launch_bounds__(kPlanesThreads, 1)
   auto item_of = [&](int s, size_t& id) -> int {
     int m = threadIdx.x;
     for (int ph = 0; ph < nphase; ph++) {
-      const int lag = (ph < nhalf) ? kWaveLag * ph : resid_lag;
+      const int lag = (ph < nhalf) ? wlag * ph : resid_lag;
       const int t = tmin + s - lag;
       const int j = t - 2 * k;
       if (t < tmin || t > tmax || j < 1 || j > ny - 2) continue;
@@ -696,15 +703,22 @@ __global__ void __launch_bounds__(kPlanesThreads, 1)
   Coef27 C;
   if (kind) load_coef27(op, cc, fc, id, sy, sz, C);
   volatile int* verr = err;
-  // waits for the neighbour planes to finish step s-1 (every thread or only
-  // thread 0); once any CTA has given up, nobody waits any more
+  // waits for the lower neighbour plane to finish step s-1 and the upper
+  // one step s-wlag+3 (every thread or only thread 0); the last counter
+  // value seen of each is kept, so a neighbour known to be far enough ahead
+  // costs no read; once any CTA has given up, nobody waits any more
+  unsigned seen[2] = {base, base};
   auto wait_neighbours = [&](int s) {
-    const unsigned need = base + (unsigned)s;
     const unsigned long long t0 = global_ns();
-    for (int nb = -1; nb <= 1; nb += 2) {
-      if (c + nb < 0 || c + nb >= ncta) continue;
-      const unsigned* f = counters + c + nb;
-      while ((int)(ld_acquire(f) - need) < 0) {
+    for (int side = 0; side < 2; side++) {
+      const int nb = side == 0 ? c - 1 : c + 1;
+      if (nb < 0 || nb >= ncta) continue;
+      const unsigned need = base + (unsigned)(side == 0 ? s : s - wlag + 4);
+      if ((int)(seen[side] - need) >= 0) continue;
+      const unsigned* f = counters + nb;
+      for (;;) {
+        seen[side] = ld_acquire(f);
+        if ((int)(seen[side] - need) >= 0) break;
         if (failed_sh || *verr) {
           failed_sh = 1;
           return;
@@ -769,14 +783,16 @@ int wave_planes_fit(Grid g) {
 
 int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, double* r, int nsweep, int first_parity, unsigned* counters,
-                       int* err, int poll_all) {
+                       int* err, int poll_all, int wlag) {
   int nhalf = 2 * nsweep;
   int do_resid = (r != nullptr) ? 1 : 0;
   const int hr = (g.nx - 1) / 2;
   const int items = nhalf * hr + (do_resid ? g.nx - 2 : 0);
   if (items > kPlanesThreads) return 0;
   const int threads = std::max(64, (items + 31) / 32 * 32);
-  void* args[] = {&g, &op, &cc, &fc, &x, &r, &nhalf, &first_parity, &do_resid, &counters, &err};
+  if (wlag < 4) wlag = 4;
+  void* args[] = {&g, &op, &cc, &fc, &x, &r,   &nhalf, &first_parity,
+                  &do_resid, &counters, &err, &wlag};
   void* fn = poll_all ? (void*)k_gs27_planes<true> : (void*)k_gs27_planes<false>;
   return cudaLaunchCooperativeKernel(fn, dim3(g.nz - 2), dim3(threads), args, 0, s) ==
          cudaSuccess;

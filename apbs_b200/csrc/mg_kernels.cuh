@@ -54,9 +54,10 @@ constexpr int kWavePlanesMax = 1024;
 constexpr int kWaveCounterBase = 16;  // words before level 0's counters
 constexpr size_t kWaveWords = kWaveCounterBase + 16 * (size_t)kWavePlanesMax;
 int wave_planes_fit(Grid g);
+// wlag: wavefronts between successive half-sweeps (>= 4)
 int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                        double* x, double* r, int nsweep, int first_parity, unsigned* counters,
-                       int* err, int poll_all);
+                       int* err, int poll_all, int wlag);
 int launch_gs27_wave(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, int nsweep, int first_parity, Gs27Plan plan);
 

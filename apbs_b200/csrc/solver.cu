@@ -991,7 +991,7 @@ static int gs27_smooth(pmgb_solver* s, cudaStream_t st, int l, const double* cc,
     return launch_gs27_planes(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
                               s->d_wave + kWaveCounterBase + (size_t)l * kWavePlanesMax,
                               reinterpret_cast<int*>(s->d_wave),
-                              s->tune[PMGB_TUNE_GS27_PLANES_POLL]);
+                              s->tune[PMGB_TUNE_GS27_PLANES_POLL], s->tune[PMGB_TUNE_GS27_LAG]);
   }
   return launch_gs27_wave(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity, s->plan[l]);
 }
@@ -1597,6 +1597,10 @@ extern "C" int pmgb_set_tuning(int key, int value) {
     set_error("pmgb_set_tuning: sweeps must be 1..4");
     return 0;
   }
+  if (key == PMGB_TUNE_GS27_LAG && (value < 4 || value > 64)) {
+    set_error("pmgb_set_tuning: the wavefront lag must be 4..64");
+    return 0;
+  }
   g_tune[key] = value;
   return 1;
 }
@@ -1619,6 +1623,10 @@ extern "C" int pmgb_solver_set_tuning(pmgb_solver* s, int key, int value) {
   if (key == PMGB_TUNE_CG_CLUSTER && value != 0 && value != 1 && value != 4 && value != 8 &&
       value != 16) {
     set_error("pmgb_solver_set_tuning: CG cluster must be 0, 1, 4, 8 or 16");
+    return 0;
+  }
+  if (key == PMGB_TUNE_GS27_LAG && (value < 4 || value > 64)) {
+    set_error("pmgb_solver_set_tuning: the wavefront lag must be 4..64");
     return 0;
   }
   if (s->tune[key] == value) return 1;

@@ -31,6 +31,7 @@ K_GS7_SWEEP_FP64, K_GS7_SWEEP_FP32 = 8, 9
 DX_POT, DX_CHARGE, DX_KAPPA, DX_DIELX, DX_DIELY, DX_DIELZ = range(6)
 MAP_DIELX, MAP_DIELY, MAP_DIELZ, MAP_KAPPA, MAP_CHARGE, MAP_POT = range(6)
 TUNE_MIXED_CHEBYSHEV = 0
+TUNE_GS27_LAG = 1
 TUNE_GS27_CLUSTER = 2
 TUNE_BAND_ALWAYS = 4
 TUNE_GS7_COLOUR_PASSES = 5

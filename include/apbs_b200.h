@@ -221,7 +221,10 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
                                           8-colour Gauss-Seidel (PMGB_TUNE_MIXED_COARSE_SWEEPS
                                           sweeps), K > 0 = Jacobi-preconditioned Chebyshev of
                                           degree K (rounded up to even) */
-/* keys 1 and 3 are not used */
+#define PMGB_TUNE_GS27_LAG 1          /* plane-parallel GS27: wavefronts between successive
+                                          half-sweeps (>= 4, default 6); a larger lag lets a
+                                          plane run ahead of the plane above it */
+/* key 3 is not used */
 #define PMGB_TUNE_GS27_CLUSTER 2       /* CTAs per cluster of the ordered GS27 on levels with
                                           >= 60 interior points per axis (0 = device max) */
 #define PMGB_TUNE_BAND_ALWAYS 4        /* 1: FP64 LPBE coarsest level always by the banded

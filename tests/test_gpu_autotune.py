@@ -7,7 +7,7 @@ import pytest
 
 from apbs_b200 import autotune, synth
 from apbs_b200.vpmg import (FP64, MIXED, TUNE_GS27_CLUSTER, TUNE_GS27_CLUSTER_MID,
-                            TUNE_GS27_PLANES, TUNE_GS27_PLANES_POLL, TUNE_GS7_COLOUR_PASSES,
+                            TUNE_GS27_LAG, TUNE_GS27_PLANES, TUNE_GS27_PLANES_POLL, TUNE_GS7_COLOUR_PASSES,
                             TUNE_GS7_SWEEP_KCHUNK, TUNE_GS7_SWEEP_SHAPE,
                             TUNE_TAIL_MAX_POINTS, Vpmg, get_tuning)
 
@@ -24,13 +24,16 @@ def _solve(p, m, prec, tune):
 
 
 def test_fp64_launch_shapes_do_not_change_the_solve():
-    """The plane-parallel and one-cluster GS27 wavefronts, cluster sizes and
+    """The plane-parallel and one-cluster GS27 wavefronts, the plane
+    wavefront's lag between half-sweeps (4 is lockstep), cluster sizes and
     fine-smoother shapes: bitwise the same FP64 solve (NPBE, 129^3: GS27 on
     the 65^3, 33^3 and 17^3 levels)."""
     m = synth.cluster(400, 11.0, seed=12, net_charge=2.0)
     p = synth.mg_manual(129, 0.4, m.center(), npbe=True, ions=((1, 0.1, 2.0), (-1, 0.1, 2.0)))
     e0, u0, h0 = _solve(p, m, FP64, {})
-    for tune in ({TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2}, {TUNE_GS27_PLANES_POLL: 1},
+    for tune in ({TUNE_GS27_LAG: 4}, {TUNE_GS27_LAG: 5}, {TUNE_GS27_LAG: 12},
+                 {TUNE_GS27_LAG: 16, TUNE_GS27_PLANES_POLL: 1},
+                 {TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2}, {TUNE_GS27_PLANES_POLL: 1},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER: 4},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER_MID: 16},
                  {TUNE_GS7_SWEEP_KCHUNK: 3}, {TUNE_GS7_SWEEP_KCHUNK: 32},
