@@ -365,19 +365,11 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    from apbs_b200 import replicas
+    if world > 1:
+        max_over_ranks, sum_over_ranks = replicas.torch_reducers(dist, dev)
+    else:
+        max_over_ranks = sum_over_ranks = (lambda x: x)
 
     results = {}
     potentials = {}
@@ -428,11 +420,12 @@ def main():
         if sampler:
             clocks = sampler.stop()
         lat = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-        total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+        rate, total_ms = replicas.aggregate(args.steps, ev[0].elapsed_time(ev[-1]),
+                                            max_over_ranks, sum_over_ranks)
         st = s.stats()
         potentials[name] = s.u
         results[name] = {
-            "solves_per_s": sum_over_ranks(args.steps) / (total_ms / 1e3),
+            "solves_per_s": rate,
             "ms_per_step": total_ms / args.steps,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "energy_kT": e, "vcycles": st["vcycles"], "newton_iters": st["newton_iters"],
@@ -475,8 +468,9 @@ def main():
             s.potential_into(h_u_np)
         ev1.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e = {"value": sum_over_ranks(args.steps) / (e2e_ms / 1e3), "unit": "solves/s",
+    e2e_rate, e2e_ms = replicas.aggregate(args.steps, ev0.elapsed_time(ev1), max_over_ranks,
+                                          sum_over_ranks)
+    e2e = {"value": e2e_rate, "unit": "solves/s",
            "h2d_bytes_per_step": int(8 * (h_xyz.numel() + h_q.numel() + h_r.numel())),
            "d2h_bytes_per_step": int(8 + 8 * h_u.numel()),
            "returns": "energy (8 B) and the potential grid (nx*ny*nz doubles) to pinned "
