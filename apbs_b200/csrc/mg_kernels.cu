@@ -1735,7 +1735,9 @@ void launch_nresid(cudaStream_t s, Grid g, Op op, const double* cc, const double
 // k_nresid fused with the 1-norm of r (the partial sums of k_reduce_partial
 // with the same grid and traversal, so the norm is the same bits) and, when
 // cp is not null, c'(x) on the interior (the update of k_dcvec)
-__global__ void k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
+// at most 48 registers: five 256-thread CTAs per SM keep enough loads in
+// flight around the exponentials (76 registers allowed three)
+__global__ void __launch_bounds__(256, 5) k_nresid_nrm(Grid g, Op op, const double* __restrict__ cc,
                              const double* __restrict__ fc, const double* __restrict__ x,
                              double* r, IonTable ions, double* part, double* cp) {
   __shared__ double sh[32];
@@ -1846,7 +1848,7 @@ __device__ __forceinline__ double pvec_at(const EnergyArgs& a, int i, int j, int
   return v;
 }
 
-__global__ void k_energy_partial(EnergyArgs a, double* part) {
+__global__ void __launch_bounds__(256, 5) k_energy_partial(EnergyArgs a, double* part) {
   __shared__ double sh[32];
   const Grid g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
