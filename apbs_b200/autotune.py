@@ -44,7 +44,7 @@ CANDIDATES = {
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
         TUNE_GS7_SWEEP_SHAPE: [0x12, 0x11, 0x02, 0x21],
-        TUNE_GS7_SWEEP_KCHUNK: [10, 8, 12, 6],
+        TUNE_GS7_SWEEP_KCHUNK: [0, 8, 10, 12],
     },
     MIXED: {
         TUNE_MIXED_CHEBYSHEV: [2, 0, 4],
@@ -53,7 +53,7 @@ CANDIDATES = {
         TUNE_MIXED_COARSE_SWEEPS: [2, 1, 3],
         TUNE_GS7_COLOUR_PASSES: [0, 2],
         TUNE_GS7_SWEEP_SHAPE: [0x12, 0x21, 0x11],
-        TUNE_GS7_SWEEP_KCHUNK: [10, 6, 8],
+        TUNE_GS7_SWEEP_KCHUNK: [0, 6, 8],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
     },
 }

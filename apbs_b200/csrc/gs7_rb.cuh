@@ -38,6 +38,8 @@
 // another.  All offsets are 32-bit (the host keeps grids below 2^31 bytes).
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace pmgb {
@@ -54,7 +56,7 @@ struct Gs7Rb {
   int nx, S, nz;  // row length, plane size nx*ny, planes
   int core;       // core points of a CTA per plane (even)
   int E;          // pair slots of the widened range (shared-memory ring width)
-  int kchunk;     // planes per CTA
+  int kchunk;     // planes per CTA (0: as many chunks as fill the resident CTA slots)
 };
 
 // pair slot e of plane k covers flat indices 2 (base(k) + e) and 2 (base(k) + e) + 1
@@ -175,12 +177,38 @@ inline int gs7_rb_core(int nx, int S, int slots) {
   return core > S ? ((S + 1) & ~1) : core;
 }
 
+// CTAs of one instance resident on the device at once (SMs x CTAs per SM)
+template <typename T, int C1, int NT, int Q>
+inline int gs7_rb_slots(size_t smem) {
+  static const int slots = [smem] {
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_gs7_rb<T, C1, NT, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         96 * 1024);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs7_rb<T, C1, NT, Q>, NT,
+                                                      smem) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    return sms * per_sm;
+  }();
+  return slots;
+}
+
 template <typename T, int NT, int Q>
 inline cudaError_t launch_gs7_rb_q(cudaStream_t st, Gs7Rb<T> a, int c1) {
   a.E = NT * Q;
   a.core = gs7_rb_core(a.nx, a.S, a.E);
   if (a.core == 0) return cudaErrorInvalidValue;
   const size_t smem = (size_t)3 * a.E * sizeof(T);
+  if (a.kchunk <= 0) {
+    // one wave: as many plane chunks per flat range as the resident CTA
+    // slots allow (the last wave of an uneven split leaves SMs idle)
+    const int nranges = (a.S + a.core - 1) / a.core;
+    const int slots = gs7_rb_slots<T, 0, NT, Q>(smem);
+    const int nchunks = std::max(1, slots / nranges);
+    a.kchunk = std::max(1, (a.nz - 2 + nchunks - 1) / nchunks);
+  }
   const dim3 grid((a.S + a.core - 1) / a.core, (a.nz - 2 + a.kchunk - 1) / a.kchunk);
   if (c1) {
     static const cudaError_t attr = cudaFuncSetAttribute(
@@ -212,7 +240,7 @@ inline cudaError_t launch_gs7_rb_nt(cudaStream_t st, const Gs7Rb<T>& a, int c1, 
 template <typename T>
 inline cudaError_t launch_gs7_rb(cudaStream_t st, const Gs7Rb<T>& a, int c1, int shape) {
   const int nt = shape & 15, q = ((shape >> 4) & 15) ? ((shape >> 4) & 15) : 2;
-  if (a.kchunk < 1 || (a.nx & 1) == 0 || (a.S & 1) == 0 ||
+  if (a.kchunk < 0 || (a.nx & 1) == 0 || (a.S & 1) == 0 ||
       (double)a.S * a.nz * sizeof(T) >= 2147483647.0)
     return cudaErrorInvalidValue;
   switch (nt) {

@@ -372,7 +372,7 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   }
 }
 
-int g_tune[16] = {2, 6, 0, 0, 0, 0, 10, 0, 70000, 0, 2, 2, 0x12, 0, 0, 0};
+int g_tune[16] = {2, 6, 0, 0, 0, 0, 0, 0, 70000, 0, 2, 2, 0x12, 0, 0, 0};
 
 int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const double* fc,
                        const double* xin, double* xout, int first_parity, int kchunk,
@@ -381,7 +381,7 @@ int launch_gs7_sweep64(cudaStream_t s, Grid g, Op op, const double* diag, const 
   a.oE = op.c[OE]; a.oN = op.c[ON]; a.uC = op.c[UC];
   a.D = diag; a.f = fc; a.xin = xin; a.xout = xout;
   a.nx = g.nx; a.S = g.nx * g.ny; a.nz = g.nz;
-  a.kchunk = kchunk > 0 ? kchunk : 8;
+  a.kchunk = kchunk;  // 0: sized to the resident CTA slots
   return launch_gs7_rb<double>(s, a, first_parity, shape) == cudaSuccess;
 }
 

@@ -1274,7 +1274,7 @@ Gs7Rb<float> rb_f32(const MLevel& F, const float* d32, const int* tune) {
   a.oE = F.op[OE]; a.oN = F.op[ON]; a.uC = F.op[UC];
   a.D = d32; a.f = F.w0;
   a.nx = F.g.nx; a.S = F.g.nx * F.g.ny; a.nz = F.g.nz;
-  a.kchunk = tune[6] > 0 ? tune[6] : 8;
+  a.kchunk = tune[6];  // 0: sized to the resident CTA slots
   a.xin = nullptr; a.xout = nullptr;
   return a;
 }

@@ -233,7 +233,8 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
 #define PMGB_TUNE_GS7_COLOUR_PASSES 5  /* fine smoother: 0 = default (FP64 single-pass sweep
                                           kernel, FP32 one launch per colour), 1 = one launch
                                           per colour, 2 = single-pass sweeps in FP32 too */
-#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep (default 10) */
+#define PMGB_TUNE_GS7_SWEEP_KCHUNK 6   /* planes per CTA of the single-pass sweep; 0 (default)
+                                          = as many chunks as fill the resident CTA slots */
 #define PMGB_TUNE_GS27_CLUSTER_MID 7   /* the same as key 2 for levels with 28-59 interior
                                           points per axis (0 = 8) */
 #define PMGB_TUNE_TAIL_MAX_POINTS 8    /* mixed: largest level (interior points) run inside

@@ -36,7 +36,7 @@ def test_fp64_launch_shapes_do_not_change_the_solve():
                  {TUNE_GS27_PLANES: 1}, {TUNE_GS27_PLANES: 2}, {TUNE_GS27_PLANES_POLL: 1},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER: 4},
                  {TUNE_GS27_PLANES: 1, TUNE_GS27_CLUSTER_MID: 16},
-                 {TUNE_GS7_SWEEP_KCHUNK: 3}, {TUNE_GS7_SWEEP_KCHUNK: 32},
+                 {TUNE_GS7_SWEEP_KCHUNK: 3}, {TUNE_GS7_SWEEP_KCHUNK: 32}, {TUNE_GS7_SWEEP_KCHUNK: 0},
                  {TUNE_GS7_SWEEP_SHAPE: 0x01}, {TUNE_GS7_SWEEP_SHAPE: 0x12},
                  {TUNE_GS7_SWEEP_SHAPE: 0x41}, {TUNE_GS7_COLOUR_PASSES: 1}):
         e, u, h = _solve(p, m, FP64, tune)
