@@ -798,6 +798,290 @@ int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const do
          cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// The same schedule, one CTA per interior plane, with the CTA's plane and its
+// two neighbour planes held in shared memory and every update passed to the
+// neighbour planes through a mailbox in global memory instead of by step
+// counters.
+//
+// The GS update of point (i, j, k) in half-sweep q goes into the CTA's own
+// copy and into mailbox slot (k, q, j, m) as two 64-bit words, each holding
+// one 32-bit half of the value beside the launch's tag.  A reader polls the
+// slot until both tags are the launch's: the value validates itself, so no
+// fence and no counter lies between one plane's update and the neighbour's
+// use of it.  Every slot is written once per launch, so nothing is
+// overwritten before it is read, and the tags of earlier launches never
+// match.
+//
+// A CTA copies a neighbour's updates into its copy of that plane at the step
+// that first needs them: half-sweep q at row j takes row j+1 of the lower
+// plane's half-sweep q (finished one wavefront earlier) and row j+1 of the
+// upper plane's half-sweep q-1 (finished wlag-3 wavefronts earlier), and at
+// j = 1 row 1 of both too.  The rows a step reads then hold exactly the
+// values the sequential order reads (the lower plane swept by this
+// half-sweep, the upper one by the earlier ones), and the rows a step
+// changes lie at least two rows from those any other half-sweep reads in
+// that step or the one before, so one block barrier per step orders
+// everything.  The iterates are bitwise those of k_gs27_wave whatever the
+// order in which the planes run; tests/test_gs27_wave_deps.py runs this rule
+// on adversarial interleavings.
+//
+// The counters hold the launch count of each plane (the tag is that plus
+// one); a CTA writes its plane back to x at the end, after both neighbours
+// have read theirs (with two or more half-sweeps a CTA waits on both
+// neighbours' updates before it finishes).  A wait that runs out is counted
+// in *err like the counter kernel's.
+// ---------------------------------------------------------------------------
+constexpr int kMailThreads = 384;
+constexpr int kMailPoll = 2;     // mailbox slots one thread polls per step, at most
+constexpr int kMailHalfMax = 4;  // half-sweeps per launch the mailbox holds
+
+__device__ __forceinline__ void mail_put(unsigned long long* p, double v, unsigned tag) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  const unsigned long long hi = (unsigned long long)tag << 32;
+  asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p),
+               "l"((b & 0xffffffffull) | hi), "l"((b >> 32) | hi)
+               : "memory");
+}
+__device__ __forceinline__ void mail_load(const unsigned long long* p, unsigned long long& w0,
+                                          unsigned long long& w1) {
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(p));
+}
+
+size_t mail_words(Grid g) {
+  const size_t hr = (g.nx - 1) / 2;
+  return 2 * (size_t)(g.nz - 2) * kMailHalfMax * (g.ny - 2) * hr;
+}
+static size_t mail_smem(Grid g) { return 3 * (size_t)g.nx * g.ny * sizeof(double); }
+
+__global__ void __launch_bounds__(kMailThreads, 1)
+    k_gs27_mail(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ fc,
+                double* x, double* r, int nhalf, int first_parity, int do_resid,
+                unsigned* counters, int* err, int wlag, unsigned long long* mail) {
+  extern __shared__ double pl[];  // planes k-1, k, k+1 of x, nx*ny each
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int pn = nx * ny;
+  const size_t sy = nx, sz = (size_t)pn;
+  const int tmin = 1 + 2 * 1, tmax = (ny - 2) + 2 * (nz - 2);
+  const int nphase = nhalf + (do_resid ? 1 : 0);
+  const int resid_lag = wlag * nhalf;
+  const int last_start = do_resid ? resid_lag : wlag * (nhalf - 1);
+  const int nsteps = (tmax - tmin + 1) + last_start;
+  const int hr = (nx - 1) / 2;
+  const int c = blockIdx.x, k = 1 + c;
+  const int ncta = gridDim.x;
+  double* P0 = pl;
+  double* P1 = pl + pn;
+  double* P2 = pl + 2 * pn;
+  __shared__ unsigned tag_sh;
+  __shared__ volatile int failed_sh;
+  if (threadIdx.x == 0) {
+    tag_sh = counters[c] + 1u;
+    failed_sh = 0;
+  }
+  {
+    // the three planes are contiguous in x; asynchronous 8-byte copies keep
+    // all of them in flight at once
+    const double* src = x + (size_t)(k - 1) * pn;
+    for (int e = threadIdx.x; e < 3 * pn; e += blockDim.x) {
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(pl + e);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + e)
+                   : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  }
+  __syncthreads();
+  const unsigned tag = tag_sh;
+  auto slot = [&](int plane_c, int q, int j, int m) -> unsigned long long* {
+    return mail + 2 * ((((size_t)plane_c * nhalf + q) * (ny - 2) + (j - 1)) * hr + m);
+  };
+  auto colour_i = [&](int j, int kk, int q, int m) -> int {
+    const int parity = (first_parity + q) & 1;
+    return 1 + (((1 + j + kk) & 1) != parity) + 2 * m;
+  };
+  // this thread's item of step s: 0 = none, 1 = GS update, 2 = residual;
+  // j, i, the half-sweep q and the slot m
+  auto item_of = [&](int s, int& j, int& i, int& q, int& m) -> int {
+    int rem = threadIdx.x;
+    for (int ph = 0; ph < nphase; ph++) {
+      const int lag = (ph < nhalf) ? wlag * ph : resid_lag;
+      const int t = tmin + s - lag;
+      const int jj = t - 2 * k;
+      if (t < tmin || t > tmax || jj < 1 || jj > ny - 2) continue;
+      const int cnt = (ph < nhalf) ? hr : (nx - 2);
+      if (rem >= cnt) {
+        rem -= cnt;
+        continue;
+      }
+      j = jj;
+      q = ph;
+      m = rem;
+      if (ph < nhalf) {
+        i = colour_i(jj, k, ph, rem);
+        return (i > nx - 2) ? 0 : 1;
+      }
+      i = 1 + rem;
+      return 2;
+    }
+    return 0;
+  };
+  // the mailbox slots this thread polls: thread group G = tid / hr takes the
+  // lower plane's half-sweep G (G < nhalf) or the upper plane's half-sweep
+  // G - nhalf, slot tid % hr, of row j+1 and, at j = 1, of row 1 too
+  const int grp = threadIdx.x / hr, gm = threadIdx.x - grp * hr;
+  const int pside = grp < nhalf ? 0 : 1;
+  const int pq = grp - pside * nhalf;
+  const int pph = pside == 0 ? pq : pq + 1;
+  const int pnb = pside == 0 ? c - 1 : c + 1;
+  const bool poller = grp < 2 * nhalf && pnb >= 0 && pnb < ncta && pph < nphase;
+  const int plag = (pph < nhalf) ? wlag * pph : resid_lag;
+  const unsigned long long* pp[kMailPoll];
+  double* dp[kMailPoll];
+  auto polls_of = [&](int s) -> unsigned {
+    unsigned pend = 0;
+    pp[0] = pp[1] = nullptr;
+    dp[0] = dp[1] = nullptr;
+    if (!poller) return 0;
+    const int t = tmin + s - plag;
+    const int j = t - 2 * k;
+    if (t < tmin || t > tmax || j < 1 || j > ny - 2) return 0;
+#pragma unroll
+    for (int pass = 0; pass < kMailPoll; pass++) {
+      const int jj = pass == 0 ? j + 1 : 1;
+      if (pass == 0 ? (jj > ny - 2) : (j != 1)) continue;
+      const int i = colour_i(jj, k - 1 + 2 * pside, pq, gm);
+      if (i > nx - 2) continue;
+      pp[pass] = slot(pnb, pq, jj, gm);
+      dp[pass] = (pside == 0 ? P0 : P2) + jj * nx + i;
+      pend |= 1u << pass;
+    }
+    return pend;
+  };
+  volatile int* verr = err;
+  int j = 0, i = 0, q = 0, m = 0;
+  int kind = (nsteps > 0) ? item_of(0, j, i, q, m) : 0;
+  Coef27 C;
+  if (kind) load_coef27(op, cc, fc, g.idx(i, j, k), sy, sz, C);
+  for (int s = 0; s < nsteps; s++) {
+    unsigned pend = polls_of(s);
+    if (pend) {
+      const unsigned long long t0 = global_ns();
+      int spins = 0;
+      while (pend) {
+        unsigned long long w[kMailPoll][2];
+#pragma unroll
+        for (int n = 0; n < kMailPoll; n++)
+          if (pend & (1u << n)) mail_load(pp[n], w[n][0], w[n][1]);
+#pragma unroll
+        for (int n = 0; n < kMailPoll; n++) {
+          if ((pend & (1u << n)) && (unsigned)(w[n][0] >> 32) == tag &&
+              (unsigned)(w[n][1] >> 32) == tag) {
+            *dp[n] =
+                __longlong_as_double((long long)((w[n][1] << 32) | (w[n][0] & 0xffffffffull)));
+            pend &= ~(1u << n);
+          }
+        }
+        if (pend && (++spins & 15) == 0) {
+          if (failed_sh || *verr) {
+            failed_sh = 1;
+            break;
+          }
+          if ((long long)(global_ns() - t0) > kWaveWaitNs) {
+            failed_sh = 1;
+            atomicAdd(err, 1);
+            break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (kind) {
+      const int o = j * nx + i;
+      const double* Xd = P0 + o;
+      const double* Xo = P1 + o;
+      const double* Xu = P2 + o;
+      const double tO = +C.o[0] * Xo[nx] + C.o[1] * Xo[-nx] + C.o[2] * Xo[1] +
+                        C.o[3] * Xo[-1] + C.o[4] * Xo[nx + 1] + C.o[5] * Xo[nx - 1] +
+                        C.o[6] * Xo[-nx + 1] + C.o[7] * Xo[-nx - 1];
+      const double tU = +C.u[0] * Xu[0] + C.u[1] * Xu[nx] + C.u[2] * Xu[-nx] +
+                        C.u[3] * Xu[1] + C.u[4] * Xu[-1] + C.u[5] * Xu[nx + 1] +
+                        C.u[6] * Xu[nx - 1] + C.u[7] * Xu[-nx + 1] + C.u[8] * Xu[-nx - 1];
+      const double tD = +C.d[0] * Xd[0] + C.d[1] * Xd[nx] + C.d[2] * Xd[-nx] +
+                        C.d[3] * Xd[1] + C.d[4] * Xd[-1] + C.d[5] * Xd[nx + 1] +
+                        C.d[6] * Xd[nx - 1] + C.d[7] * Xd[-nx + 1] + C.d[8] * Xd[-nx - 1];
+      if (kind == 1) {
+        const double v = (C.f + (tO + tU + tD)) / (C.oc + C.cc);
+        P1[o] = v;
+        mail_put(slot(c, q, j, m), v, tag);
+      } else {
+        r[g.idx(i, j, k)] = C.f + tO + tU + tD - (C.oc + C.cc) * Xo[0];
+      }
+    }
+    // the next step's coefficients do not depend on this step: fetch them
+    // while the neighbour planes finish
+    const int nkind = (s + 1 < nsteps) ? item_of(s + 1, j, i, q, m) : 0;
+    if (nkind) load_coef27(op, cc, fc, g.idx(i, j, k), sy, sz, C);
+    kind = nkind;
+  }
+  __syncthreads();
+  double* dst = x + (size_t)k * pn;
+  for (int e = threadIdx.x; e < pn; e += blockDim.x) {
+    const int jj = e / nx, ii = e - jj * nx;
+    if (jj >= 1 && jj <= ny - 2 && ii >= 1 && ii <= nx - 2) __stcg(dst + e, P1[e]);
+  }
+  if (threadIdx.x == 0) counters[c] = tag;
+}
+
+int wave_mail_fit(Grid g) {
+  static int dev_smem = -1, sms = 0;
+  if (dev_smem < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int planes = g.nz - 2;
+  const int hr = (g.nx - 1) / 2;
+  const int items = kMailHalfMax * hr + (g.nx - 2);
+  const int pollers = 2 * kMailHalfMax * hr;
+  const size_t smem = mail_smem(g);
+  return planes >= 2 && planes <= kWavePlanesMax && planes <= sms && items <= kMailThreads &&
+         pollers <= kMailThreads && smem + 1024 <= (size_t)dev_smem;
+}
+
+int launch_gs27_mail(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                     double* x, double* r, int nsweep, int first_parity, unsigned* counters,
+                     int* err, int wlag, unsigned long long* mail) {
+  int nhalf = 2 * nsweep;
+  int do_resid = (r != nullptr) ? 1 : 0;
+  if (!mail || nhalf < 2 || nhalf > kMailHalfMax || !wave_mail_fit(g)) return 0;
+  const int hr = (g.nx - 1) / 2;
+  const int items = nhalf * hr + (do_resid ? g.nx - 2 : 0);
+  int threads = std::max(items, 2 * nhalf * hr);
+  threads = std::max(64, (threads + 31) / 32 * 32);
+  if (threads > kMailThreads) return 0;
+  const size_t smem = mail_smem(g);
+  static size_t smem_set = 0;
+  if (smem > smem_set) {
+    if (cudaFuncSetAttribute(k_gs27_mail, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return 0;
+    smem_set = smem;
+  }
+  int per_sm = 0, sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gs27_mail, threads, smem) !=
+          cudaSuccess ||
+      per_sm * sms < g.nz - 2)
+    return 0;
+  if (wlag < 4) wlag = 4;
+  void* args[] = {&g, &op, &cc, &fc, &x, &r, &nhalf, &first_parity, &do_resid,
+                  &counters, &err, &wlag, &mail};
+  return cudaLaunchCooperativeKernel((void*)k_gs27_mail, dim3(g.nz - 2), dim3(threads), args,
+                                     smem, s) == cudaSuccess;
+}
+
 int mg_init() {
   cudaError_t e = cudaFuncSetAttribute(k_gs27_wave<16>,
                                        cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

@@ -60,6 +60,16 @@ int launch_gs27_planes(cudaStream_t s, Grid g, Op op, const double* cc, const do
                        int* err, int poll_all, int wlag);
 int launch_gs27_wave(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                      double* x, double* r, int nsweep, int first_parity, Gs27Plan plan);
+// The same schedule with each CTA's plane and its neighbours in shared
+// memory and updates passed through a self-validating mailbox (mail_words(g)
+// 64-bit words per level, zeroed whenever the level's counters restart);
+// wave_mail_fit: three planes fit in one CTA's shared memory and the level's
+// planes on the device.  Returns 0 (nothing launched) where it does not fit.
+size_t mail_words(Grid g);
+int wave_mail_fit(Grid g);
+int launch_gs27_mail(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
+                     double* x, double* r, int nsweep, int first_parity, unsigned* counters,
+                     int* err, int wlag, unsigned long long* mail);
 
 // ---- BLAS-1 on interior points -------------------------------------------
 void launch_zero(cudaStream_t s, double* x, size_t n);

@@ -239,6 +239,14 @@ Gs27Plan plan_for(Grid g, const int* tune) {
 // ===========================================================================
 static int set_geometry(pmgb_solver* s);
 
+// Restarts the wavefront step counters of every level and zeroes the
+// mailboxes with them (a mailbox tag is a counter value plus one, so old
+// slots must not outlive the counters they were tagged from).
+static void wave_reset(pmgb_solver* s, cudaStream_t st) {
+  if (s->d_wave) cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), st);
+  if (s->d_mail) cudaMemsetAsync(s->d_mail, 0, s->mail_total * sizeof(unsigned long long), st);
+}
+
 extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver** out) {
   *out = nullptr;
   if (!params) {
@@ -347,6 +355,22 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
   if (ok) ok &= (cudaMalloc(&s->d_npts, sizeof(int)) == cudaSuccess);
   if (ok) ok &= (cudaMalloc(&s->d_wave, kWaveWords * sizeof(unsigned)) == cudaSuccess);
   if (ok) ok &= (cudaMemset(s->d_wave, 0, kWaveWords * sizeof(unsigned)) == cudaSuccess);
+  // mailboxes for the levels the ordered GS27 smooths (all but the
+  // coarsest) where the shared-memory plane wavefront fits
+  s->mail_total = 0;
+  for (int l = 0; l < 12; l++) {
+    s->mail_off[l] = -1;
+    if (l >= 1 && l < s->nlev - 1 && wave_mail_fit(s->lev[l].g)) {
+      s->mail_off[l] = (long long)s->mail_total;
+      s->mail_total += mail_words(s->lev[l].g);
+    }
+  }
+  if (ok && s->mail_total) {
+    ok &= (cudaMalloc(&s->d_mail, s->mail_total * sizeof(unsigned long long)) == cudaSuccess);
+    if (ok)
+      ok &= (cudaMemset(s->d_mail, 0, s->mail_total * sizeof(unsigned long long)) ==
+             cudaSuccess);
+  }
   if (ok) ok &= (cudaMalloc(&s->d_opptrs, sizeof(double*) * 14 * 16) == cudaSuccess);
   if (ok) {
     // the operator arrays never move, so the pointer table is written once
@@ -407,7 +431,7 @@ static int set_geometry(pmgb_solver* s) {
     cudaStream_t st = s->stream;
     // plane counts per level change with the grid: restart the wavefront
     // step counters so every level's counters start equal
-    if (s->d_wave) cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), st);
+    wave_reset(s, st);
     CK(cudaMemcpyAsync(s->xf, xf.data(), sizeof(double) * p.nx, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->yf, yf.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(s->zf, zf.data(), sizeof(double) * p.nz, cudaMemcpyHostToDevice, st));
@@ -531,6 +555,7 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   dfree(s->dg[0]); dfree(s->dg[1]);
   dfree(s->nw_r0); dfree(s->nw_ws); dfree(s->nw_keepx); dfree(s->nw_keepr);
   dfree(s->part); dfree(s->scal); dfree(s->d_iters); dfree(s->d_info); dfree(s->d_npts); dfree(s->d_wave); dfree(s->d_forces);
+  if (s->d_mail) cudaFree(s->d_mail);
   dfree(s->d_opptrs);
   dfree(s->band);
   dfree(s->focus_w);
@@ -986,6 +1011,15 @@ int pmgb::solver_build(pmgb_solver* s) { return build_ops(s); }
 static int gs27_smooth(pmgb_solver* s, cudaStream_t st, int l, const double* cc,
                        const double* fc, double* x, double* r, int first_parity) {
   const Level& L = s->lev[l];
+  if (s->tune[PMGB_TUNE_GS27_PLANES] == 0 && s->mail_off[l] >= 0 &&
+      launch_gs27_mail(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
+                       s->d_wave + kWaveCounterBase + (size_t)l * kWavePlanesMax,
+                       reinterpret_cast<int*>(s->d_wave), s->tune[PMGB_TUNE_GS27_LAG],
+                       s->d_mail + s->mail_off[l])) {
+    s->wave_used = 1;
+    return 1;
+  }
+  (void)cudaGetLastError();  // a refused launch above leaves no error behind
   if (s->tune[PMGB_TUNE_GS27_PLANES] != 1 && wave_planes_fit(L.g)) {
     s->wave_used = 1;
     return launch_gs27_planes(st, L.g, L.ops(), cc, fc, x, r, 2, first_parity,
@@ -1288,7 +1322,7 @@ static int wave_check(pmgb_solver* s) {
   CK(cudaStreamSynchronize(s->stream));
   if (nerr) {
     // the counters of the levels may now disagree: restart them all
-    CK(cudaMemsetAsync(s->d_wave, 0, kWaveWords * sizeof(unsigned), s->stream));
+    wave_reset(s, s->stream);
     CK(cudaStreamSynchronize(s->stream));
     set_error("%d bounded device waits ran out (gs27 plane wavefront)", nerr);
     return 0;

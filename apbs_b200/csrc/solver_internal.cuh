@@ -135,6 +135,12 @@ struct pmgb_solver {
   size_t forces_alloc;
   unsigned* d_wave;
   int wave_used;  // the plane kernel has been launched or captured (stays set)
+  // mailboxes of the shared-memory plane wavefront: level l's starts at word
+  // mail_off[l] (levels it does not fit have none: mail_off[l] = -1); zeroed
+  // with the step counters
+  unsigned long long* d_mail;
+  long long mail_off[12];
+  size_t mail_total;
   double* atom_terms;  // 13 x natoms sdh moment terms
   size_t terms_alloc;
   // focusing: faces set from a coarse solution, energies outside the domain

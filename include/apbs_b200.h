@@ -250,10 +250,14 @@ int pmgb_solve_molecule(const pmgb_params *params, int precision, int natoms,
                                           slots per thread (1-4, 0 = 2); a CTA owns a flat range
                                           of 2 x (slots - nx - 3) points of each plane;
                                           default 0x12: 1024 threads, 1 slot */
-#define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (or 2) = one CTA per plane
-                                          synchronised with its neighbour planes on every
-                                          level whose planes fit on the device, 1 = one
-                                          cluster with a barrier per wavefront everywhere */
+#define PMGB_TUNE_GS27_PLANES 13      /* ordered GS27: 0 (default) = one CTA per plane
+                                          holding its plane and both neighbours in shared
+                                          memory, updates passed through a mailbox, on
+                                          levels where three planes fit (else as 2);
+                                          2 = one CTA per plane synchronised with its
+                                          neighbour planes by step counters on every level
+                                          whose planes fit on the device; 1 = one cluster
+                                          with a barrier per wavefront everywhere */
 #define PMGB_TUNE_CG_CLUSTER 14       /* coarsest-level CG of the FP64 NPBE path: CTAs per
                                           cluster of the slab kernel (0 = smallest that fits;
                                           4, 8 or 16); 1 = the strided cluster kernel that

@@ -19,6 +19,12 @@ plane's earlier half-sweep LAG - 3 steps back, a read of a lower neighbour
 its current half-sweep one step back, and every anti-dependence (a value a
 plane still has to read in its old state) is covered by the neighbour's own
 wait on this plane.
+
+The second half models the shared-memory variant (k_gs27_mail): every CTA
+works on its own copies of planes k-1, k and k+1 and takes its neighbours'
+updates from a mailbox at the step that first needs them.  Free-running
+interleavings give the lockstep iterates and residual bit for bit, never
+deadlock, and no plane is written back before both neighbours loaded it.
 """
 import random
 
@@ -166,3 +172,106 @@ def test_lag_changes_nothing():
         if ref is None:
             ref = (x, r)
         assert np.array_equal(x, ref[0]) and np.array_equal(r, ref[1])
+
+
+# --- the shared-memory plane wavefront with a mailbox (k_gs27_mail) --------
+# Each plane's CTA holds copies of planes k-1, k, k+1 loaded at its start; an
+# update of half-sweep q, row j goes into its own copy and into mailbox slot
+# (k, q, j).  At a step, half-sweep q at row j first takes row j+1 of the
+# lower plane's half-sweep q and of the upper plane's half-sweep q-1 (and row
+# 1 of both when j = 1); a CTA may run the step once every slot it takes
+# exists.  At its end a CTA writes its plane back.
+
+def mail_takes(s, k, nz, ny, nhalf, do_resid, lag, tmin, tmax, resid_lag):
+    """Mailbox rows (plane, q, row) that plane k's step s takes."""
+    out = []
+    for ph in range(nhalf + (1 if do_resid else 0)):
+        t = tmin + s - (lag * ph if ph < nhalf else resid_lag)
+        j = t - 2 * k
+        if t < tmin or t > tmax or j < 1 or j > ny - 2:
+            continue
+        for kn, q in ((k - 1, ph), (k + 1, ph - 1)):
+            if kn < 1 or kn > nz - 2 or q < 0 or q >= nhalf:
+                continue
+            if j + 1 <= ny - 2:
+                out.append((kn, q, j + 1))
+            if j == 1:
+                out.append((kn, q, 1))
+    return out
+
+
+def mail_run(x0, w, d, f, prm, nz, nsteps, pick):
+    nx, ny, nhalf, do_resid, fp, lag, tmin, tmax, resid_lag = prm
+    xg = x0.copy()  # x in global memory
+    r = np.zeros_like(x0)
+    planes = list(range(1, nz - 1))
+    local = {}  # plane -> its CTA's copy of planes k-1..k+1 (a 3-plane array)
+    mail = {}
+    done = {k: 0 for k in planes}
+    finished = set()
+    while len(finished) < len(planes):
+        ready = []
+        for k in planes:
+            s = done[k]
+            if k in finished:
+                continue
+            if s == nsteps or all(key in mail for key in
+                                  mail_takes(s, k, nz, ny, nhalf, do_resid, lag, tmin, tmax,
+                                             resid_lag)):
+                ready.append(k)
+        assert ready, "deadlock"
+        k = pick(ready, done)
+        s = done[k]
+        if s == 0 and k not in local:
+            local[k] = xg[k - 1:k + 2].copy()
+        if s == nsteps:
+            # the plane goes back to x only after both neighbours loaded theirs
+            for kn in (k - 1, k + 1):
+                assert kn < 1 or kn > nz - 2 or kn in local
+            xg[k] = local[k][1]
+            finished.add(k)
+            continue
+        L = local[k]
+        for kn, q, jj in mail_takes(s, k, nz, ny, nhalf, do_resid, lag, tmin, tmax, resid_lag):
+            for i, v in mail[(kn, q, jj)]:
+                L[1 + (kn - k), jj, i] = v
+        # one plane's step on its copy: the same arithmetic as step()
+        pend = []
+        for ph, j, ii in items(s, k, nx, ny, nhalf, do_resid, fp, lag, tmin, tmax, resid_lag):
+            row = []
+            for i in ii:
+                acc = 0.0
+                for qq, (di, dj, dk) in enumerate(OFFS):
+                    acc += w[qq, k, j, i] * L[1 + dk, j + dj, i + di]
+                if ph < nhalf:
+                    v = (f[k, j, i] + acc) / d[k, j, i]
+                    pend.append((j, i, v))
+                    row.append((i, v))
+                else:
+                    r[k, j, i] = f[k, j, i] + acc - d[k, j, i] * L[1, j, i]
+            if ph < nhalf:
+                mail[(k, ph, j)] = row
+        for j, i, v in pend:
+            L[1, j, i] = v
+        done[k] += 1
+    return xg, r
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(9, 9, 9), (11, 7, 13), (13, 13, 9), (7, 5, 5)])
+@pytest.mark.parametrize("nhalf,do_resid", [(2, True), (4, True), (4, False), (2, False)])
+@pytest.mark.parametrize("lag", [4, 6, 9])
+def test_mailbox_planes_equal_lockstep(nx, ny, nz, nhalf, do_resid, lag):
+    x0, w, d, f = make(nx, ny, nz, seed=nx * 5 + nz + lag + nhalf)
+    tmin, tmax, resid_lag, nsteps = schedule(ny, nz, nhalf, do_resid, lag)
+    prm = (nx, ny, nhalf, do_resid, 0, lag, tmin, tmax, resid_lag)
+    xt, rt = lockstep(x0, w, d, f, prm, nz, nsteps)
+    rng = random.Random(nx * ny + nz + lag)
+    pickers = [lambda ready, done: rng.choice(ready),
+               lambda ready, done: max(ready, key=lambda k: (done[k], k)),
+               lambda ready, done: min(ready, key=lambda k: (done[k], -k)),
+               lambda ready, done: max(ready)]
+    for pick in pickers:
+        x, r = mail_run(x0, w, d, f, prm, nz, nsteps, pick)
+        assert np.array_equal(x, xt)
+        if do_resid:
+            assert np.array_equal(r, rt)
