@@ -40,7 +40,7 @@ DEFAULT_TABLE = os.path.join(HERE, "tuning", "b200.json")
 CANDIDATES = {
     FP64: {
         vpmg.TUNE_GS27_LAG: [6, 4, 8, 12],
-        TUNE_GS27_PLANES: [0, 1],
+        TUNE_GS27_PLANES: [0, 2, 1],
         TUNE_GS27_CLUSTER_MID: [0, 4, 16],
         TUNE_GS7_COLOUR_PASSES: [0, 1],
         TUNE_GS7_SWEEP_SHAPE: [0x12, 0x11, 0x02, 0x21],
