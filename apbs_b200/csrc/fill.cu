@@ -42,11 +42,11 @@ __device__ __forceinline__ double off2_rn(double pos, double h, double f) {
 // markSphere (vpmg.c:6444-6491) for one sphere on one (possibly staggered)
 // grid, executed by the calling thread group.
 // ---------------------------------------------------------------------------
+template <typename T>
 __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double cy, double cz,
                                                   Grid g, double hx, double hy, double hz,
                                                   double xmin, double ymin, double zmin,
-                                                  double* array, double markVal, int lane,
-                                                  int nlanes) {
+                                                  T* array, T markVal, int lane, int nlanes) {
   const double posx = cx - xmin, posy = cy - ymin, posz = cz - zmin;
   const double rtot2 = __dmul_rn(rtot, rtot);
   const double xr = rtot + 0.5 * hx, yr = rtot + 0.5 * hy, zr = rtot + 0.5 * hz;
@@ -68,7 +68,7 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
     const double dx2 = off2_rn(posx, hx, fi);
     const double dy2 = off2_rn(posy, hy, fj);
     if (__dadd_rn(dx2, dy2) > rtot2) continue;
-    double* col = array + g.idx(ii, jj, 0);
+    T* col = array + g.idx(ii, jj, 0);
     const size_t sz = (size_t)g.nx * g.ny;
     for (int kk = kmin; kk <= kmax; kk++) {
       const double dz2 = off2_rn(posz, hz, (double)kk);
@@ -83,11 +83,18 @@ __global__ void k_fill_value(double* a, size_t n, double v) {
     a[q] = v;
 }
 
-// Atom spheres of fillcoCoefMolDielNoSmooth (vpmg.c:4390-4446): one block per
-// atom, the three staggered dielectric grids marked with epsp.
+// The dielectric maps of fillcoCoefMolDielNoSmooth (vpmg.c:4390-4496) take only
+// two values, epsw and epsp, so they are built as one byte per point per
+// staggered grid (0 = epsw, 1 = epsp) in the reference's order -- all epsw,
+// the inflated atom spheres set to epsp, the probe spheres at accessible
+// surface points back to epsw -- and written as doubles once, smoothed or
+// not (k_diel_maps, k_smooth): an eighth of the bytes for the fill, the
+// scattered marking and the smoothing's reads, the same maps bit for bit.
+//
+// Atom spheres (vpmg.c:4390-4446): one block per atom, the three staggered
+// grids marked 1.
 __global__ void k_mark_atoms_diel(FillGeom G, int natoms, const double* __restrict__ xyz,
-                                  const double* __restrict__ r, double srad, double epsp,
-                                  double* epsx, double* epsy, double* epsz) {
+                                  const double* __restrict__ r, double srad, DielMask M) {
   const int a = blockIdx.x;
   if (a >= natoms) return;
   const double ax = xyz[3 * a], ay = xyz[3 * a + 1], az = xyz[3 * a + 2], arad = r[a];
@@ -96,12 +103,13 @@ __global__ void k_mark_atoms_diel(FillGeom G, int natoms, const double* __restri
     return;
   if (!(arad > 1.0e-9)) return;
   const double hx = G.h[0], hy = G.h[1], hz = G.h[2];
+  const unsigned char one = 1;
   mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx),
-                    G.xmin[1], G.xmin[2], epsx, epsp, threadIdx.x, blockDim.x);
+                    G.xmin[1], G.xmin[2], M.m[0], one, threadIdx.x, blockDim.x);
   mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, G.xmin[0],
-                    (G.xmin[1] + 0.5 * hy), G.xmin[2], epsy, epsp, threadIdx.x, blockDim.x);
+                    (G.xmin[1] + 0.5 * hy), G.xmin[2], M.m[1], one, threadIdx.x, blockDim.x);
   mark_sphere_group(arad + srad, ax, ay, az, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
-                    (G.xmin[2] + 0.5 * hz), epsz, epsp, threadIdx.x, blockDim.x);
+                    (G.xmin[2] + 0.5 * hz), M.m[2], one, threadIdx.x, blockDim.x);
 }
 
 // Ion accessibility of fillcoCoefMolIon (vpmg.c:4237-4333).
@@ -345,14 +353,13 @@ __global__ void __launch_bounds__(256) k_sas_test(
 }
 
 // Probe spheres around accessible SAS points reset the three dielectric
-// grids to epsw (vpmg.c:4456-4496).  One warp per listed surface point; the
+// grids to epsw, byte 0 (vpmg.c:4456-4496).  One warp per listed surface point; the
 // grid is sized for the device and strides over the list, whose length the
 // test pass left in *npts.
 __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
                            const double* __restrict__ r, const double* __restrict__ ref,
-                           int nref, double srad, double epsw, const unsigned* __restrict__ list,
-                           const int* __restrict__ npts, double* epsx, double* epsy,
-                           double* epsz) {
+                           int nref, double srad, const unsigned* __restrict__ list,
+                           const int* __restrict__ npts, DielMask M) {
   const int n = *npts;
   const int lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -363,30 +370,33 @@ __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
     double px, py, pz;
     sas_point(xyz, r, ref, (int)(tid / (unsigned)nref), (int)(tid % (unsigned)nref), srad, px,
               py, pz);
+    const unsigned char zero = 0;
     mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
-                      G.xmin[2], epsx, epsw, lane, 32);
+                      G.xmin[2], M.m[0], zero, lane, 32);
     mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
-                      G.xmin[2], epsy, epsw, lane, 32);
+                      G.xmin[2], M.m[1], zero, lane, 32);
     mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
-                      (G.xmin[2] + 0.5 * hz), epsz, epsw, lane, 32);
+                      (G.xmin[2] + 0.5 * hz), M.m[2], zero, lane, 32);
   }
 }
 
-// 9-point harmonic-mean smoothing, fillcoCoefMolDielSmooth (vpmg.c:4500-4628).
-// a1..a3 are the unsmoothed maps.  Their values are the two dielectric
-// constants v0 and v1 almost everywhere, so 1 / a comes from a table of the
-// two reciprocals (the same correctly rounded quotients) with a division
-// only for any other value.
+// 9-point harmonic-mean smoothing, fillcoCoefMolDielSmooth (vpmg.c:4500-4628),
+// of the maps the byte maps describe: 1 / a is 1/epsp or 1/epsw (the correctly
+// rounded quotients, as 1.0 / a gives them).
 struct InvPair {
-  double v0, r0, v1, r1;
-  __device__ __forceinline__ double operator()(double a) const {
-    return a == v0 ? r0 : (a == v1 ? r1 : 1.0 / a);
+  const unsigned char* m0;
+  const unsigned char* m1;
+  const unsigned char* m2;
+  double rp, rw;
+  __device__ __forceinline__ double operator()(const unsigned char* m, size_t q) const {
+    return __ldg(m + q) ? rp : rw;
   }
 };
 
-__global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __restrict__ a2,
-                         const double* __restrict__ a3, InvPair inv, double* epsx, double* epsy,
-                         double* epsz) {
+__global__ void k_smooth(Grid g, InvPair inv, double* epsx, double* epsy, double* epsz) {
+  const unsigned char* a1 = inv.m0;
+  const unsigned char* a2 = inv.m1;
+  const unsigned char* a3 = inv.m2;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t n = g.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
@@ -394,50 +404,61 @@ __global__ void k_smooth(Grid g, const double* __restrict__ a1, const double* __
     const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
     double frac;
     int np;
-    frac = inv(a1[q]);
-    frac += inv(a2[q]);
-    frac += inv(a3[q]);
+    frac = inv(a1, q);
+    frac += inv(a2, q);
+    frac += inv(a3, q);
     np = 3;
-    if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k)]); np += 1; }
-    if (k > 0) { frac += inv(a3[g.idx(i, j, k - 1)]); np += 1; }
+    if (j > 0) { frac += inv(a2, g.idx(i, j - 1, k)); np += 1; }
+    if (k > 0) { frac += inv(a3, g.idx(i, j, k - 1)); np += 1; }
     if (i < (nx - 1)) {
-      frac += inv(a2[g.idx(i + 1, j, k)]);
-      frac += inv(a3[g.idx(i + 1, j, k)]);
+      frac += inv(a2, g.idx(i + 1, j, k));
+      frac += inv(a3, g.idx(i + 1, j, k));
       np += 2;
-      if (j > 0) { frac += inv(a2[g.idx(i + 1, j - 1, k)]); np += 1; }
-      if (k > 0) { frac += inv(a3[g.idx(i + 1, j, k - 1)]); np += 1; }
+      if (j > 0) { frac += inv(a2, g.idx(i + 1, j - 1, k)); np += 1; }
+      if (k > 0) { frac += inv(a3, g.idx(i + 1, j, k - 1)); np += 1; }
     }
     epsx[q] = np / frac;
 
-    frac = inv(a2[q]);
-    frac += inv(a1[q]);
-    frac += inv(a3[q]);
+    frac = inv(a2, q);
+    frac += inv(a1, q);
+    frac += inv(a3, q);
     np = 3;
-    if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k)]); np += 1; }
-    if (k > 0) { frac += inv(a3[g.idx(i, j, k - 1)]); np += 1; }
+    if (i > 0) { frac += inv(a1, g.idx(i - 1, j, k)); np += 1; }
+    if (k > 0) { frac += inv(a3, g.idx(i, j, k - 1)); np += 1; }
     if (j < (ny - 1)) {
-      frac += inv(a1[g.idx(i, j + 1, k)]);
-      frac += inv(a3[g.idx(i, j + 1, k)]);
+      frac += inv(a1, g.idx(i, j + 1, k));
+      frac += inv(a3, g.idx(i, j + 1, k));
       np += 2;
-      if (i > 0) { frac += inv(a1[g.idx(i - 1, j + 1, k)]); np += 1; }
-      if (k > 0) { frac += inv(a3[g.idx(i, j + 1, k - 1)]); np += 1; }
+      if (i > 0) { frac += inv(a1, g.idx(i - 1, j + 1, k)); np += 1; }
+      if (k > 0) { frac += inv(a3, g.idx(i, j + 1, k - 1)); np += 1; }
     }
     epsy[q] = np / frac;
 
-    frac = inv(a3[q]);
-    frac += inv(a1[q]);
-    frac += inv(a2[q]);
+    frac = inv(a3, q);
+    frac += inv(a1, q);
+    frac += inv(a2, q);
     np = 3;
-    if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k)]); np += 1; }
-    if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k)]); np += 1; }
+    if (i > 0) { frac += inv(a1, g.idx(i - 1, j, k)); np += 1; }
+    if (j > 0) { frac += inv(a2, g.idx(i, j - 1, k)); np += 1; }
     if (k < (nz - 1)) {
-      frac += inv(a1[g.idx(i, j, k + 1)]);
-      frac += inv(a2[g.idx(i, j, k + 1)]);
+      frac += inv(a1, g.idx(i, j, k + 1));
+      frac += inv(a2, g.idx(i, j, k + 1));
       np += 2;
-      if (i > 0) { frac += inv(a1[g.idx(i - 1, j, k + 1)]); np += 1; }
-      if (j > 0) { frac += inv(a2[g.idx(i, j - 1, k + 1)]); np += 1; }
+      if (i > 0) { frac += inv(a1, g.idx(i - 1, j, k + 1)); np += 1; }
+      if (j > 0) { frac += inv(a2, g.idx(i, j - 1, k + 1)); np += 1; }
     }
     epsz[q] = np / frac;
+  }
+}
+
+// The unsmoothed maps (srfm mol) from the byte maps.
+__global__ void k_diel_maps(size_t n, DielMask M, double epsp, double epsw, double* epsx,
+                            double* epsy, double* epsz) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+       q += (size_t)gridDim.x * blockDim.x) {
+    epsx[q] = M.m[0][q] ? epsp : epsw;
+    epsy[q] = M.m[1][q] ? epsp : epsw;
+    epsz[q] = M.m[2][q] ? epsp : epsw;
   }
 }
 
@@ -1018,10 +1039,9 @@ void launch_charge(cudaStream_t s, int kind, const FillGeom& G, int natoms, cons
 }
 
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                            const double* r, double srad, double epsp, double* epsx,
-                            double* epsy, double* epsz) {
+                            const double* r, double srad, const DielMask& M) {
   if (natoms <= 0) return;
-  k_mark_atoms_diel<<<natoms, 256, 0, s>>>(G, natoms, xyz, r, srad, epsp, epsx, epsy, epsz);
+  k_mark_atoms_diel<<<natoms, 256, 0, s>>>(G, natoms, xyz, r, srad, M);
 }
 void launch_mark_atoms_kappa(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                              const double* r, double irad, double* kappa) {
@@ -1052,9 +1072,8 @@ void launch_sas_test(cudaStream_t s, const CellGrid& C, int natoms, const double
 }
 
 void launch_sas_mark(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                     const double* r, const double* ref, int nref, double srad, double epsw,
-                     const unsigned* list, const int* npts, double* epsx, double* epsy,
-                     double* epsz) {
+                     const double* r, const double* ref, int nref, double srad,
+                     const unsigned* list, const int* npts, const DielMask& M) {
   const long long tot = (long long)natoms * nref;
   if (tot <= 0) return;
   static const int nblocks = [] {
@@ -1069,14 +1088,16 @@ void launch_sas_mark(cudaStream_t s, const FillGeom& G, int natoms, const double
   }();
   const long long want = (tot + 7) / 8;  // 8 warps per block
   const unsigned nb = (unsigned)std::min<long long>(nblocks, want);
-  k_sas_mark<<<nb, 256, 0, s>>>(G, xyz, r, ref, nref, srad, epsw, list, npts, epsx, epsy,
-                                epsz);
+  k_sas_mark<<<nb, 256, 0, s>>>(G, xyz, r, ref, nref, srad, list, npts, M);
 }
-void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
-                   const double* a3, double v0, double v1, double* epsx, double* epsy,
-                   double* epsz) {
-  InvPair inv{v0, 1.0 / v0, v1, 1.0 / v1};
-  k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, a1, a2, a3, inv, epsx, epsy, epsz);
+void launch_diel_maps(cudaStream_t s, Grid g, const DielMask& M, int smooth, double epsp,
+                      double epsw, double* epsx, double* epsy, double* epsz) {
+  if (smooth) {
+    InvPair inv{M.m[0], M.m[1], M.m[2], 1.0 / epsp, 1.0 / epsw};
+    k_smooth<<<blocks_for(g.n()), kThreads, 0, s>>>(g, inv, epsx, epsy, epsz);
+  } else {
+    k_diel_maps<<<blocks_for(g.n()), kThreads, 0, s>>>(g.n(), M, epsp, epsw, epsx, epsy, epsz);
+  }
 }
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* q, double* terms, double* mom, const double* xf,

@@ -139,9 +139,14 @@ void launch_mdh(cudaStream_t s, const MdhArgs& A, int natoms, const double* xyz,
 void launch_qf_point(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                      const double* q, const double* u, double* part, double* out,
                      const double* box = nullptr);
+// The three staggered dielectric grids as one byte per point: 1 = epsp,
+// 0 = epsw (the maps of fillcoCoefMolDielNoSmooth take no other value).
+struct DielMask {
+  unsigned char* m[3];
+};
+// inflated atom spheres set 1
 void launch_mark_atoms_diel(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                            const double* r, double srad, double epsp, double* epsx,
-                            double* epsy, double* epsz);
+                            const double* r, double srad, const DielMask& M);
 void launch_mark_atoms_kappa(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
                              const double* r, double irad, double* kappa);
 void launch_cell_build(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
@@ -152,16 +157,14 @@ size_t sas_nbr_ints(int natoms);
 void launch_sas_test(cudaStream_t s, const CellGrid& C, int natoms, const double* xyz,
                      const double* r, const double* ref, int nref, double srad,
                      const int* start, const int* sorted, int* nbr, unsigned* list, int* npts);
-// probe spheres of the *npts accessible points of list reset the dielectric
-// maps to epsw
+// probe spheres of the *npts accessible points of list set 0 (epsw)
 void launch_sas_mark(cudaStream_t s, const FillGeom& G, int natoms, const double* xyz,
-                     const double* r, const double* ref, int nref, double srad, double epsw,
-                     const unsigned* list, const int* npts, double* epsx, double* epsy,
-                     double* epsz);
-// the 9-point harmonic smoothing of maps a1..a3 whose values are mostly v0 or v1
-void launch_smooth(cudaStream_t s, Grid g, const double* a1, const double* a2,
-                   const double* a3, double v0, double v1, double* epsx, double* epsy,
-                   double* epsz);
+                     const double* r, const double* ref, int nref, double srad,
+                     const unsigned* list, const int* npts, const DielMask& M);
+// the dielectric maps from the byte maps: 9-point harmonic smoothing
+// (smooth) or the unsmoothed values
+void launch_diel_maps(cudaStream_t s, Grid g, const DielMask& M, int smooth, double epsp,
+                      double epsw, double* epsx, double* epsy, double* epsz);
 void launch_sdh(cudaStream_t s, const SdhArgs& A, int natoms, const double* xyz,
                 const double* q, double* terms, double* mom, const double* xf, const double* yf,
                 const double* zf, double* gx, double* gy, double* gz);

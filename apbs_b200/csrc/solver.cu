@@ -328,7 +328,12 @@ extern "C" int pmgb_create(const pmgb_params* params, int precision, pmgb_solver
   ok &= dalloc(&s->xf, p.nx) && dalloc(&s->yf, p.ny) && dalloc(&s->zf, p.nz) &&
         dalloc(&s->wx, p.nx) && dalloc(&s->wy, p.ny) && dalloc(&s->wz, p.nz) &&
         dalloc(&s->mom, 16);
-  ok &= dalloc(&s->tmp3, 3 * n);
+  // the dielectric byte maps (DielMask), 3 bytes per point
+  if (ok && cudaMalloc(&s->dmask, 3 * n) != cudaSuccess) {
+    set_error("cudaMalloc(%zu bytes) failed", 3 * n);
+    s->dmask = nullptr;
+    ok = 0;
+  }
   // hierarchy (Vbuildstr, src/pmgc/mgsubd.c:261-343)
   s->nlev = p.nlev;
   for (int l = 0; ok && l < s->nlev; l++) {
@@ -545,7 +550,8 @@ extern "C" void pmgb_destroy(pmgb_solver* s) {
   if (s->mixed) mixed_destroy(s->mixed);
   dfree(s->charge); dfree(s->epsx); dfree(s->epsy); dfree(s->epsz); dfree(s->kappa);
   dfree(s->ccf); dfree(s->gx); dfree(s->gy); dfree(s->gz); dfree(s->xf); dfree(s->yf);
-  dfree(s->zf); dfree(s->wx); dfree(s->wy); dfree(s->wz); dfree(s->mom); dfree(s->tmp3);
+  dfree(s->zf); dfree(s->wx); dfree(s->wy); dfree(s->wz); dfree(s->mom);
+  if (s->dmask) cudaFree(s->dmask);
   for (int l = 0; l < s->nlev; l++) {
     Level& L = s->lev[l];
     for (int c = 0; c < 14; c++) dfree(L.op[c]);
@@ -707,17 +713,14 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
                        ionmask, p.pdie, p.sdie, coef3, s->kappa, s->epsx, s->epsy, s->epsz);
     note_launches(1);
   } else if (!islap) {
-    // dielectric (fillcoCoefMolDielNoSmooth); with smoothing the unsmoothed
-    // maps are built in the scratch arrays and smoothed into epsx/y/z
+    // dielectric (fillcoCoefMolDielNoSmooth) as byte maps, then the maps
+    // from them, smoothed (fillcoCoefMolDielSmooth) or not
     const int smol = p.srfm == PMGB_SRFM_SMOL;
-    double* ex = smol ? s->tmp3 : s->epsx;
-    double* ey = smol ? s->tmp3 + n : s->epsy;
-    double* ez = smol ? s->tmp3 + 2 * n : s->epsz;
-    launch_fill_value(st, ex, n, p.sdie);
-    launch_fill_value(st, ey, n, p.sdie);
-    launch_fill_value(st, ez, n, p.sdie);
-    launch_mark_atoms_diel(st, s->G, natoms, s->d_xyz, s->d_r, p.srad, p.pdie, ex, ey, ez);
-    note_launches(4);
+    DielMask M;
+    for (int d = 0; d < 3; d++) M.m[d] = s->dmask + d * n;
+    CK(cudaMemsetAsync(s->dmask, 0, 3 * n, st));
+    launch_mark_atoms_diel(st, s->G, natoms, s->d_xyz, s->d_r, p.srad, M);
+    note_launches(1);
     if (p.srad > 1.0e-9) {
       // Vacc_storeParms sphere density with the Vclist probe radius
       const double clist_rad =
@@ -775,14 +778,12 @@ static int do_fill(pmgb_solver* s, const double* h_xyz, const double* h_r, int w
       launch_sas_test(st, C, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, s->cell_start,
                       s->cell_sorted, s->sas_nbr, s->sas_list, s->d_npts);
       note_launches(2);
-      launch_sas_mark(st, s->G, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad, p.sdie,
-                      s->sas_list, s->d_npts, ex, ey, ez);
+      launch_sas_mark(st, s->G, natoms, s->d_xyz, s->d_r, s->d_ref, nref, p.srad,
+                      s->sas_list, s->d_npts, M);
       note_launches(1);
     }
-    if (smol) {
-      launch_smooth(st, s->g, ex, ey, ez, p.pdie, p.sdie, s->epsx, s->epsy, s->epsz);
-      note_launches(1);
-    }
+    launch_diel_maps(st, s->g, M, smol, p.pdie, p.sdie, s->epsx, s->epsy, s->epsz);
+    note_launches(1);
     // ion accessibility (fillcoCoefMolIon)
     const double ionmask = (s->ionstr > 1.0e-12) ? 1.0 : 0.0;
     launch_fill_value(st, s->kappa, n, ionmask);

@@ -85,7 +85,7 @@ struct pmgb_solver {
   // maps
   double *charge, *epsx, *epsy, *epsz, *kappa, *ccf;
   double *gx, *gy, *gz, *xf, *yf, *zf, *wx, *wy, *wz, *mom;
-  double* tmp3;  // 3N scratch for smoothing
+  unsigned char* dmask;  // the dielectric byte maps (DielMask), 3N bytes
   // atoms (d_* point at the owned buffers a_* or at the caller's arrays)
   int natoms;
   double *d_xyz, *d_q, *d_r;
