@@ -507,11 +507,18 @@ extern "C" size_t pmgb_footprint(const pmgb_params* params, int precision, int n
   for (int l = 0; l < nlev; l++) nl[l] = (size_t)gx[l] * gy[l] * gz[l];
   const size_t n = nl[0];
   size_t d = 0;  // doubles
-  d += 6 * n + 3 * n + 3 * n + 4 * n;  // maps, smoothing scratch, w1-3, Newton vectors
+  d += 6 * n + 3 * n + 4 * n;  // maps, w1-3, Newton vectors
   d += 2 * ((size_t)p.ny * p.nz + (size_t)p.nx * p.nz + (size_t)p.nx * p.ny);
   d += 2 * (size_t)(p.nx + p.ny + p.nz) + 16 + 4 * 1184 + 64 + S_COUNT;
   for (int l = 0; l < nlev; l++) d += (size_t)((l == 0 ? 4 : 14) + 7) * nl[l];
   size_t bytes = d * sizeof(double);
+  bytes += 3 * n;  // the dielectric byte maps
+  // mailboxes of the shared-memory GS27 wavefront (levels whose three planes
+  // fit in a CTA's shared memory; an upper bound where the device says no)
+  for (int l = 1; l < nlev - 1; l++)
+    if ((size_t)3 * gx[l] * gy[l] * sizeof(double) + 1024 <= 232448)
+      bytes += 2 * sizeof(unsigned long long) * (size_t)(gz[l] - 2) * 4 * (gy[l] - 2) *
+               ((gx[l] - 1) / 2);
   // FP32 hierarchy from level lo, plus Galerkin levels down to <= 512 unknowns
   const int lo = (precision == PMGB_MIXED) ? 0 : nlev - 1;
   const size_t nc_int = (size_t)(gx[nlev - 1] - 2) * (gy[nlev - 1] - 2) * (gz[nlev - 1] - 2);
