@@ -852,15 +852,26 @@ size_t mail_words(Grid g) {
   const size_t hr = (g.nx - 1) / 2;
   return 2 * (size_t)(g.nz - 2) * kMailHalfMax * (g.ny - 2) * hr;
 }
-static size_t mail_smem(Grid g) { return 3 * (size_t)g.nx * g.ny * sizeof(double); }
+// shared memory of k_gs27_mail: three planes, each row split by the parity
+// of i into two runs of (nx + 1) / 2 values
+static size_t mail_smem(Grid g) {
+  return 3 * (size_t)2 * ((g.nx + 1) / 2) * g.ny * sizeof(double);
+}
 
 __global__ void __launch_bounds__(kMailThreads, 1)
     k_gs27_mail(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ fc,
                 double* x, double* r, int nhalf, int first_parity, int do_resid,
                 unsigned* counters, int* err, int wlag, unsigned long long* mail) {
-  extern __shared__ double pl[];  // planes k-1, k, k+1 of x, nx*ny each
+  // planes k-1, k, k+1 of x; each row as its even-i values then its odd-i
+  // values, so the points one warp updates (one colour of a row) and each of
+  // their stencil neighbours lie contiguously: two shared-memory wavefronts
+  // per warp load instead of four
+  extern __shared__ double pl[];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int pn = nx * ny;
+  const int H = (nx + 1) / 2;
+  const int ps = 2 * H * ny;  // doubles per plane in shared memory
+  auto sidx = [&](int i, int j) -> int { return (2 * j + (i & 1)) * H + (i >> 1); };
   const size_t sy = nx, sz = (size_t)pn;
   const int tmin = 1 + 2 * 1, tmax = (ny - 2) + 2 * (nz - 2);
   const int nphase = nhalf + (do_resid ? 1 : 0);
@@ -871,8 +882,8 @@ __global__ void __launch_bounds__(kMailThreads, 1)
   const int c = blockIdx.x, k = 1 + c;
   const int ncta = gridDim.x;
   double* P0 = pl;
-  double* P1 = pl + pn;
-  double* P2 = pl + 2 * pn;
+  double* P1 = pl + ps;
+  double* P2 = pl + 2 * ps;
   __shared__ unsigned tag_sh;
   __shared__ volatile int failed_sh;
   if (threadIdx.x == 0) {
@@ -884,7 +895,9 @@ __global__ void __launch_bounds__(kMailThreads, 1)
     // all of them in flight at once
     const double* src = x + (size_t)(k - 1) * pn;
     for (int e = threadIdx.x; e < 3 * pn; e += blockDim.x) {
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(pl + e);
+      const int p3 = e / pn, e2 = e - p3 * pn;
+      const int jj = e2 / nx, ii = e2 - jj * nx;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(pl + p3 * ps + sidx(ii, jj));
       asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + e)
                    : "memory");
     }
@@ -899,31 +912,29 @@ __global__ void __launch_bounds__(kMailThreads, 1)
     const int parity = (first_parity + q) & 1;
     return 1 + (((1 + j + kk) & 1) != parity) + 2 * m;
   };
-  // this thread's item of step s: 0 = none, 1 = GS update, 2 = residual;
-  // j, i, the half-sweep q and the slot m
+  // this thread's item: a fixed half-sweep (or the residual) and slot --
+  // threads [q hr, (q+1) hr) sweep half-sweep q, slot tid - q hr, threads
+  // from nhalf hr on the residual, point tid - nhalf hr -- at the row the
+  // step reaches: 0 = none, 1 = GS update, 2 = residual; j, i and, for a GS
+  // update, the slot m
+  const int iq = (int)threadIdx.x < nhalf * hr ? (int)threadIdx.x / hr : nhalf;
+  const int im = (int)threadIdx.x - iq * hr;
+  const bool iworker = iq < nhalf || (do_resid && im < nx - 2);
+  const int ilag = (iq < nhalf) ? wlag * iq : resid_lag;
   auto item_of = [&](int s, int& j, int& i, int& q, int& m) -> int {
-    int rem = threadIdx.x;
-    for (int ph = 0; ph < nphase; ph++) {
-      const int lag = (ph < nhalf) ? wlag * ph : resid_lag;
-      const int t = tmin + s - lag;
-      const int jj = t - 2 * k;
-      if (t < tmin || t > tmax || jj < 1 || jj > ny - 2) continue;
-      const int cnt = (ph < nhalf) ? hr : (nx - 2);
-      if (rem >= cnt) {
-        rem -= cnt;
-        continue;
-      }
-      j = jj;
-      q = ph;
-      m = rem;
-      if (ph < nhalf) {
-        i = colour_i(jj, k, ph, rem);
-        return (i > nx - 2) ? 0 : 1;
-      }
-      i = 1 + rem;
-      return 2;
+    if (!iworker) return 0;
+    const int t = tmin + s - ilag;
+    const int jj = t - 2 * k;
+    if (t < tmin || t > tmax || jj < 1 || jj > ny - 2) return 0;
+    j = jj;
+    q = iq;
+    m = im;
+    if (iq < nhalf) {
+      i = colour_i(jj, k, iq, im);
+      return (i > nx - 2) ? 0 : 1;
     }
-    return 0;
+    i = 1 + im;
+    return 2;
   };
   // the mailbox slots this thread polls: thread group G = tid / hr takes the
   // lower plane's half-sweep G (G < nhalf) or the upper plane's half-sweep
@@ -952,26 +963,34 @@ __global__ void __launch_bounds__(kMailThreads, 1)
       const int i = colour_i(jj, k - 1 + 2 * pside, pq, gm);
       if (i > nx - 2) continue;
       pp[pass] = slot(pnb, pq, jj, gm);
-      dp[pass] = (pside == 0 ? P0 : P2) + jj * nx + i;
+      dp[pass] = (pside == 0 ? P0 : P2) + sidx(i, jj);
       pend |= 1u << pass;
     }
     return pend;
   };
   volatile int* verr = err;
+  unsigned long long w[kMailPoll][2];
+  auto issue = [&](unsigned pend) {
+#pragma unroll
+    for (int n = 0; n < kMailPoll; n++)
+      if (pend & (1u << n)) mail_load(pp[n], w[n][0], w[n][1]);
+  };
   int j = 0, i = 0, q = 0, m = 0;
   int kind = (nsteps > 0) ? item_of(0, j, i, q, m) : 0;
   Coef27 C;
   if (kind) load_coef27(op, cc, fc, g.idx(i, j, k), sy, sz, C);
+  // A step's polls are issued one step early, right after the previous
+  // step's barrier, so that their round trip overlaps that step's update:
+  // a slot that is already written then costs no wait at all.  (A plane's
+  // own loop -- poll round trip plus update -- sets the period of the plane
+  // below every other, and so of the whole wavefront.)
+  unsigned pend = (nsteps > 0) ? polls_of(0) : 0u;
+  issue(pend);
   for (int s = 0; s < nsteps; s++) {
-    unsigned pend = polls_of(s);
     if (pend) {
       const unsigned long long t0 = global_ns();
       int spins = 0;
-      while (pend) {
-        unsigned long long w[kMailPoll][2];
-#pragma unroll
-        for (int n = 0; n < kMailPoll; n++)
-          if (pend & (1u << n)) mail_load(pp[n], w[n][0], w[n][1]);
+      for (;;) {
 #pragma unroll
         for (int n = 0; n < kMailPoll; n++) {
           if ((pend & (1u << n)) && (unsigned)(w[n][0] >> 32) == tag &&
@@ -981,7 +1000,8 @@ __global__ void __launch_bounds__(kMailThreads, 1)
             pend &= ~(1u << n);
           }
         }
-        if (pend && (++spins & 15) == 0) {
+        if (!pend) break;
+        if ((++spins & 15) == 0) {
           if (failed_sh || *verr) {
             failed_sh = 1;
             break;
@@ -992,29 +1012,39 @@ __global__ void __launch_bounds__(kMailThreads, 1)
             break;
           }
         }
+        issue(pend);
       }
     }
     __syncthreads();
+    // the next step's polls go out now (the slots they fill are rows no
+    // update of this step reads, and they are copied in only after it)
+    pend = (s + 1 < nsteps) ? polls_of(s + 1) : 0u;
+    issue(pend);
     if (kind) {
-      const int o = j * nx + i;
-      const double* Xd = P0 + o;
-      const double* Xo = P1 + o;
-      const double* Xu = P2 + o;
-      const double tO = +C.o[0] * Xo[nx] + C.o[1] * Xo[-nx] + C.o[2] * Xo[1] +
-                        C.o[3] * Xo[-1] + C.o[4] * Xo[nx + 1] + C.o[5] * Xo[nx - 1] +
-                        C.o[6] * Xo[-nx + 1] + C.o[7] * Xo[-nx - 1];
-      const double tU = +C.u[0] * Xu[0] + C.u[1] * Xu[nx] + C.u[2] * Xu[-nx] +
-                        C.u[3] * Xu[1] + C.u[4] * Xu[-1] + C.u[5] * Xu[nx + 1] +
-                        C.u[6] * Xu[nx - 1] + C.u[7] * Xu[-nx + 1] + C.u[8] * Xu[-nx - 1];
-      const double tD = +C.d[0] * Xd[0] + C.d[1] * Xd[nx] + C.d[2] * Xd[-nx] +
-                        C.d[3] * Xd[1] + C.d[4] * Xd[-1] + C.d[5] * Xd[nx + 1] +
-                        C.d[6] * Xd[nx - 1] + C.d[7] * Xd[-nx + 1] + C.d[8] * Xd[-nx - 1];
+      // the nine in-plane positions of the stencil (C: centre, N/S: j+-1,
+      // E/W: i+-1)
+      // (i +- 1 has the other parity: its run starts H further or H back,
+      // and its index in the run is i >> 1 or one less, plus the parity of i)
+      const int p = i & 1;
+      const int oC = sidx(i, j), oN = oC + 2 * H, oS = oC - 2 * H;
+      const int oE = oC + (1 - 2 * p) * H + p, oW = oE - 1;
+      const int oNE = oE + 2 * H, oNW = oW + 2 * H;
+      const int oSE = oE - 2 * H, oSW = oW - 2 * H;
+      const double tO = +C.o[0] * P1[oN] + C.o[1] * P1[oS] + C.o[2] * P1[oE] +
+                        C.o[3] * P1[oW] + C.o[4] * P1[oNE] + C.o[5] * P1[oNW] +
+                        C.o[6] * P1[oSE] + C.o[7] * P1[oSW];
+      const double tU = +C.u[0] * P2[oC] + C.u[1] * P2[oN] + C.u[2] * P2[oS] +
+                        C.u[3] * P2[oE] + C.u[4] * P2[oW] + C.u[5] * P2[oNE] +
+                        C.u[6] * P2[oNW] + C.u[7] * P2[oSE] + C.u[8] * P2[oSW];
+      const double tD = +C.d[0] * P0[oC] + C.d[1] * P0[oN] + C.d[2] * P0[oS] +
+                        C.d[3] * P0[oE] + C.d[4] * P0[oW] + C.d[5] * P0[oNE] +
+                        C.d[6] * P0[oNW] + C.d[7] * P0[oSE] + C.d[8] * P0[oSW];
       if (kind == 1) {
         const double v = (C.f + (tO + tU + tD)) / (C.oc + C.cc);
-        P1[o] = v;
+        P1[oC] = v;
         mail_put(slot(c, q, j, m), v, tag);
       } else {
-        r[g.idx(i, j, k)] = C.f + tO + tU + tD - (C.oc + C.cc) * Xo[0];
+        r[g.idx(i, j, k)] = C.f + tO + tU + tD - (C.oc + C.cc) * P1[oC];
       }
     }
     // the next step's coefficients do not depend on this step: fetch them
@@ -1027,7 +1057,7 @@ __global__ void __launch_bounds__(kMailThreads, 1)
   double* dst = x + (size_t)k * pn;
   for (int e = threadIdx.x; e < pn; e += blockDim.x) {
     const int jj = e / nx, ii = e - jj * nx;
-    if (jj >= 1 && jj <= ny - 2 && ii >= 1 && ii <= nx - 2) __stcg(dst + e, P1[e]);
+    if (jj >= 1 && jj <= ny - 2 && ii >= 1 && ii <= nx - 2) __stcg(dst + e, P1[sidx(ii, jj)]);
   }
   if (threadIdx.x == 0) counters[c] = tag;
 }
