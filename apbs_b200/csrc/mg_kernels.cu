@@ -471,6 +471,76 @@ void launch_matvec(cudaStream_t s, Grid g, Op op, const double* cc, const double
   k_matvec<<<blocks_for(nint), kThreads, 0, s>>>(g, op, cc, x, y);
 }
 
+// The two sums of the coarse-correction damping, <x, w0> and <x, (A + cc) x>
+// (Vmatvec and the two Vxdot of mgcsd.c:465-485), in one pass with A x formed
+// on the fly and never stored.  Each block writes its two partial sums; the
+// block that finishes last (a ticket on *done, reset by that block) adds
+// them in block order and writes num and den, so the result does not depend
+// on which block is last.
+constexpr int kDampThreads = 256;
+__global__ void __launch_bounds__(kDampThreads)
+    k_xdamp_sums(Grid g, Op op, const double* __restrict__ cc, const double* __restrict__ x,
+                 const double* __restrict__ w0, double* part, unsigned* done, double* num,
+                 double* den) {
+  __shared__ double sh[32];
+  __shared__ bool last;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
+  double a0 = 0.0, a1 = 0.0;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+       q += (size_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_ijk(q, nx, ny, i, j, k);
+    const size_t id = g.idx(i, j, k);
+    double ax;
+    if (op.nop == 4) {
+      const size_t sy = nx, sz = (size_t)nx * ny;
+      ax = -op.c[ON][id] * x[id + sy] - op.c[ON][id - sy] * x[id - sy] -
+           op.c[OE][id] * x[id + 1] - op.c[OE][id - 1] * x[id - 1] -
+           op.c[UC][id - sz] * x[id - sz] - op.c[UC][id] * x[id + sz] +
+           (op.c[OC][id] + cc[id]) * x[id];
+    } else {
+      double tO, tU, tD;
+      sum27<false>(op, g, x, id, tO, tU, tD);
+      ax = -tO - tU - tD + (op.c[OC][id] + cc[id]) * x[id];
+    }
+    a0 += x[id] * w0[id];
+    a1 += x[id] * ax;
+  }
+  const double s0 = block_sum<kDampThreads>(a0, sh);
+  const double s1 = block_sum<kDampThreads>(a1, sh);
+  const int nb = gridDim.x;
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s0;
+    part[nb + blockIdx.x] = s1;
+    __threadfence();
+    last = atomicAdd(done, 1u) == (unsigned)nb - 1u;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double b0 = 0.0, b1 = 0.0;
+  for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+    b0 += __ldcg(part + t);
+    b1 += __ldcg(part + nb + t);
+  }
+  const double n0 = block_sum<kDampThreads>(b0, sh);
+  const double d0 = block_sum<kDampThreads>(b1, sh);
+  if (threadIdx.x == 0) {
+    num[0] = n0;
+    den[0] = d0;
+    *done = 0u;
+  }
+}
+
+void launch_xdamp_sums(cudaStream_t s, Grid g, Op op, const double* cc, const double* x,
+                       const double* w0, double* part, unsigned* done, double* num,
+                       double* den) {
+  size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
+  const int nb = (int)reduce_parts(nint);
+  k_xdamp_sums<<<nb, kDampThreads, 0, s>>>(g, op, cc, x, w0, part, done, num, den);
+}
+
 // ===========================================================================
 // Ordered 27-point Gauss-Seidel, Vgsrb27x (src/pmgc/gsd.c:167-340).
 //

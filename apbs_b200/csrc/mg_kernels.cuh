@@ -35,6 +35,12 @@ extern int g_tune[16];
 void launch_resid(cudaStream_t s, Grid g, Op op, const double* cc, const double* fc,
                   const double* x, double* r);
 void launch_matvec(cudaStream_t s, Grid g, Op op, const double* cc, const double* x, double* y);
+// *num = <x, w0>, *den = <x, (A + cc) x> over the interior in one launch
+// (part: 2 * reduce_parts(interior) doubles; *done: a zero word the launch
+// leaves zero)
+void launch_xdamp_sums(cudaStream_t s, Grid g, Op op, const double* cc, const double* x,
+                       const double* w0, double* part, unsigned* done, double* num,
+                       double* den);
 
 // Ordered 27-point Gauss-Seidel: nsweep red-black sweeps (2*nsweep
 // half-sweeps) pipelined along wavefronts t = j + 2k, optionally followed by
@@ -52,6 +58,7 @@ int mg_init();
 // planes for one resident CTA each.
 constexpr int kWavePlanesMax = 1024;
 constexpr int kWaveCounterBase = 16;  // words before level 0's counters
+constexpr int kWaveDampTicket = 8;    // the word launch_xdamp_sums counts blocks in
 constexpr size_t kWaveWords = kWaveCounterBase + 16 * (size_t)kWavePlanesMax;
 int wave_planes_fit(Grid g);
 // wlag: wavefronts between successive half-sweeps (>= 4)

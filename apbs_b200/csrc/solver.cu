@@ -1108,12 +1108,12 @@ static int vcycle_body(pmgb_solver* s, int newton) {
   for (int l = nlev - 2; l >= 0; l--) {
     Level& C = s->lev[l + 1];
     Level& P = s->lev[l];
-    launch_matvec(st, C.g, C.ops(), CC(l + 1), X(l + 1), s->w2);
-    launch_dot(st, C.g, X(l + 1), C.w0, s->part, s->scal + S_XNUM_L + l);
-    launch_dot(st, C.g, X(l + 1), s->w2, s->part + 1184 * 2, s->scal + S_XDEN_L + l);
+    launch_xdamp_sums(st, C.g, C.ops(), CC(l + 1), X(l + 1), C.w0, s->part,
+                      s->d_wave + kWaveDampTicket, s->scal + S_XNUM_L + l,
+                      s->scal + S_XDEN_L + l);
     launch_interp_axpy(st, C.g, X(l + 1), P.g, X(l), s->scal + S_XNUM_L + l,
                        s->scal + S_XDEN_L + l);
-    k += 6;
+    k += 2;
     if (l == 0) {
       if (colour_passes) {
         for (int sw = 0; sw < 2; sw++) {
