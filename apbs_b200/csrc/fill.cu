@@ -77,6 +77,48 @@ __device__ __forceinline__ void mark_sphere_group(double rtot, double cx, double
   }
 }
 
+// The same marking by one warp with the squared z offsets of the sphere's
+// planes computed once (lane kk - kmin computes plane kk's into the warp's
+// dz2 buffer of 32 doubles) instead of once per column: the inner loop is
+// then the reference's two additions and its comparison.  Spheres more than
+// 32 planes thick use mark_sphere_group.
+template <typename T>
+__device__ __forceinline__ void mark_sphere_warp(double rtot, double cx, double cy, double cz,
+                                                 Grid g, double hx, double hy, double hz,
+                                                 double xmin, double ymin, double zmin,
+                                                 T* array, T markVal, int lane, double* dz2b) {
+  const double posx = cx - xmin, posy = cy - ymin, posz = cz - zmin;
+  const double rtot2 = __dmul_rn(rtot, rtot);
+  const double xr = rtot + 0.5 * hx, yr = rtot + 0.5 * hy, zr = rtot + 0.5 * hz;
+  const int imin = max(0, (int)ceil((posx - xr) / hx));
+  const int jmin = max(0, (int)ceil((posy - yr) / hy));
+  const int kmin = max(0, (int)ceil((posz - zr) / hz));
+  const int imax = min(g.nx - 1, (int)floor((posx + xr) / hx));
+  const int jmax = min(g.ny - 1, (int)floor((posy + yr) / hy));
+  const int kmax = min(g.nz - 1, (int)floor((posz + zr) / hz));
+  if (imax < imin || jmax < jmin || kmax < kmin) return;
+  const int nk = kmax - kmin + 1;
+  if (nk > 32) {
+    mark_sphere_group(rtot, cx, cy, cz, g, hx, hy, hz, xmin, ymin, zmin, array, markVal, lane,
+                      32);
+    return;
+  }
+  __syncwarp();  // the previous sphere's buffer is read by every lane
+  if (lane < nk) dz2b[lane] = off2_rn(posz, hz, (double)(kmin + lane));
+  __syncwarp();
+  const int ni = imax - imin + 1, nj = jmax - jmin + 1;
+  const size_t sz = (size_t)g.nx * g.ny;
+  for (int t = lane; t < ni * nj; t += 32) {
+    const int ii = imin + t % ni, jj = jmin + t / ni;
+    const double dx2 = off2_rn(posx, hx, (double)ii);
+    const double dy2 = off2_rn(posy, hy, (double)jj);
+    if (__dadd_rn(dx2, dy2) > rtot2) continue;
+    T* col = array + g.idx(ii, jj, 0);
+    for (int q = 0; q < nk; q++)
+      if (__dadd_rn(__dadd_rn(dz2b[q], dy2), dx2) <= rtot2) col[(kmin + q) * sz] = markVal;
+  }
+}
+
 __global__ void k_fill_value(double* a, size_t n, double v) {
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x)
@@ -360,6 +402,8 @@ __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
                            const double* __restrict__ r, const double* __restrict__ ref,
                            int nref, double srad, const unsigned* __restrict__ list,
                            const int* __restrict__ npts, DielMask M) {
+  __shared__ double dz2s[8][32];  // one buffer per warp of the 256-thread block
+  double* dz2b = dz2s[threadIdx.x >> 5];
   const int n = *npts;
   const int lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -371,12 +415,12 @@ __global__ void k_sas_mark(FillGeom G, const double* __restrict__ xyz,
     sas_point(xyz, r, ref, (int)(tid / (unsigned)nref), (int)(tid % (unsigned)nref), srad, px,
               py, pz);
     const unsigned char zero = 0;
-    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
-                      G.xmin[2], M.m[0], zero, lane, 32);
-    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
-                      G.xmin[2], M.m[1], zero, lane, 32);
-    mark_sphere_group(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
-                      (G.xmin[2] + 0.5 * hz), M.m[2], zero, lane, 32);
+    mark_sphere_warp(srad, px, py, pz, G.g, hx, hy, hz, (G.xmin[0] + 0.5 * hx), G.xmin[1],
+                     G.xmin[2], M.m[0], zero, lane, dz2b);
+    mark_sphere_warp(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], (G.xmin[1] + 0.5 * hy),
+                     G.xmin[2], M.m[1], zero, lane, dz2b);
+    mark_sphere_warp(srad, px, py, pz, G.g, hx, hy, hz, G.xmin[0], G.xmin[1],
+                     (G.xmin[2] + 0.5 * hz), M.m[2], zero, lane, dz2b);
   }
 }
 
