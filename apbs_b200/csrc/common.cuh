@@ -42,6 +42,22 @@ __device__ inline double warp_sum(double v) {
   return v;
 }
 
+// q -> (q % a, (q / a) % b, q / (a b)), with 32-bit divisions while q fits
+// (64-bit divisions are long instruction sequences in a grid-stride loop).
+__device__ __forceinline__ void split3(size_t q, int a, int b, int& x, int& y, int& z) {
+  if (q <= 0xffffffffull) {
+    const unsigned u = (unsigned)q, t = u / (unsigned)a, zz = t / (unsigned)b;
+    x = (int)(u - t * (unsigned)a);
+    y = (int)(t - zz * (unsigned)b);
+    z = (int)zz;
+  } else {
+    const size_t t = q / (size_t)a, zz = t / (size_t)b;
+    x = (int)(q - t * (size_t)a);
+    y = (int)(t - zz * (size_t)b);
+    z = (int)zz;
+  }
+}
+
 // Interior point q (i fastest) -> (i, j, k), 1-based interior indices, with
 // 32-bit divisions where the interior count allows (it does up to 1025^3).
 __device__ __forceinline__ void interior_ijk(size_t q, int nx, int ny, int& i, int& j, int& k) {

@@ -445,7 +445,8 @@ __global__ void k_smooth(Grid g, InvPair inv, double* epsx, double* epsy, double
   const size_t n = g.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
+    int i, j, k;
+    split3(q, nx, ny, i, j, k);
     double frac;
     int np;
     frac = inv(a1, q);

@@ -230,7 +230,8 @@ __global__ void k_restrict(Grid gf, const double* __restrict__ xin, Grid gc, dou
   const double h = 0.5, qq = 0.25, e = 0.125;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % cx), j = (int)((q / cx) % cy), k = (int)(q / ((size_t)cx * cy));
+    int i, j, k;
+    split3(q, cx, cy, i, j, k);
     if (i == 0 || j == 0 || k == 0 || i == cx - 1 || j == cy - 1 || k == cz - 1) {
       xout[q] = 0.0;
       continue;
@@ -362,9 +363,10 @@ __global__ void k_gs7_colour(Grid g, Op op, const double* __restrict__ cc,
   const size_t nslots = (size_t)hr * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nslots;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int m = (int)(q % hr);
-    const int j = 1 + (int)((q / hr) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)hr * (ny - 2)));
+    int m, j, k;
+    split3(q, hr, ny - 2, m, j, k);
+    j += 1;
+    k += 1;
     const int i = 1 + (((1 + j + k) & 1) != parity) + 2 * m;
     if (i > nx - 2) continue;
     const size_t id = g.idx(i, j, k);
@@ -396,9 +398,8 @@ __global__ void k_diag(Grid g, const double* __restrict__ oC, const double* __re
   const size_t n = g.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % g.nx);
-    const int j = (int)((q / g.nx) % g.ny);
-    const int k = (int)(q / ((size_t)g.nx * g.ny));
+    int i, j, k;
+    split3(q, g.nx, g.ny, i, j, k);
     const bool inner = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
     D[q] = inner ? oC[q] + cc[q] : 1.0;
   }
@@ -2199,7 +2200,8 @@ __global__ void k_fbound(Grid g, double* x, const double* __restrict__ gx,
   const size_t n = g.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
+    int i, j, k;
+    split3(q, nx, ny, i, j, k);
     if (k == 0) x[q] = gz[(size_t)j * nx + i];
     else if (k == nz - 1) x[q] = gz[((size_t)ny + j) * nx + i];
     else if (j == 0) x[q] = gy[(size_t)k * nx + i];
@@ -2240,7 +2242,8 @@ __global__ void __launch_bounds__(256, 5) k_energy_partial(EnergyArgs a, double*
   double qf = 0.0, diel = 0.0, qm = 0.0, nchop = 0.0;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
+    int i, j, k;
+    split3(q, nx, ny, i, j, k);
     const double pv = pvec_at(a, i, j, k);
     const double u = a.u[q];
     qf += (pv * u * a.charge[q]);

@@ -237,7 +237,8 @@ __global__ void k_cheb_step(Grid g, OpF o, const float* __restrict__ cc,
   const size_t nint = (size_t)ex * ey * (g.nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i0 = 1 + (int)(q % ex), j0 = 1 + (int)((q / ex) % ey), k0 = 1 + (int)(q / ((size_t)ex * ey));
+    int i0, j0, k0;
+    interior_ijk(q, g.nx, g.ny, i0, j0, k0);
     cheb_point(o, g, cc, f, xin, xout, d, g.idx(i0, j0, k0), alpha, beta);
   }
 }
@@ -252,7 +253,8 @@ __global__ void k_gersh(Grid g, OpF o, const float* __restrict__ cc, float* out)
   float mx = 0.0f;
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = 1 + (int)(q % ex), j = 1 + (int)((q / ex) % ey), k = 1 + (int)(q / ((size_t)ex * ey));
+    int i, j, k;
+    interior_ijk(q, g.nx, g.ny, i, j, k);
     const size_t id = g.idx(i, j, k);
     const float* const* c = o.c;
     float s = fabsf(c[ON][id]) + fabsf(c[ON][id - sy]) + fabsf(c[OE][id]) + fabsf(c[OE][id - 1]) +
@@ -284,9 +286,10 @@ __global__ void k_gs7_f32(Grid g, OpF o, const float* __restrict__ cc,
   const size_t nslots = (size_t)hr * (ny - 2) * (nz - 2);
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nslots;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int m = (int)(q % hr);
-    const int j = 1 + (int)((q / hr) % (ny - 2));
-    const int k = 1 + (int)(q / ((size_t)hr * (ny - 2)));
+    int m, j, k;
+    split3(q, hr, ny - 2, m, j, k);
+    j += 1;
+    k += 1;
     const int i = 1 + (((1 + j + k) & 1) != parity) + 2 * m;
     if (i > nx - 2) continue;
     const size_t id = g.idx(i, j, k);
@@ -396,7 +399,8 @@ __global__ void k_restrict_f32(Grid gf, const float* __restrict__ xin, Grid gc, 
   const size_t n = gc.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % cx), j = (int)((q / cx) % cy), k = (int)(q / ((size_t)cx * cy));
+    int i, j, k;
+    split3(q, cx, cy, i, j, k);
     if (i == 0 || j == 0 || k == 0 || i == cx - 1 || j == cy - 1 || k == cz - 1) {
       xout[q] = 0.f;
       continue;
@@ -1329,9 +1333,8 @@ __global__ void k_diag_f32(Grid g, const float* __restrict__ oC, const float* __
   const size_t n = g.n();
   for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
        q += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(q % g.nx);
-    const int j = (int)((q / g.nx) % g.ny);
-    const int k = (int)(q / ((size_t)g.nx * g.ny));
+    int i, j, k;
+    split3(q, g.nx, g.ny, i, j, k);
     const bool inner = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
     D[q] = inner ? oC[q] + cc[q] : 1.0f;
   }
