@@ -420,23 +420,58 @@ __global__ void k_restrict_f32(Grid gf, const float* __restrict__ xin, Grid gc, 
   }
 }
 
+// One thread per coarse cell (ii..ii+1, jj..jj+1, kk..kk+1): its eight corner
+// values, read once, give the interpolated correction of the up to eight fine
+// interior points 2ii+oi, 2jj+oj, 2kk+ok of the cell, each summed over the
+// corners it uses in the order of the per-point loop (c, then b, then a, from
+// 0), so the result is the per-point kernel's bit for bit with an eighth of
+// its loads and index arithmetic.
 __global__ void k_interp_axpy_f32(Grid gc, const float* __restrict__ xc, Grid gf, float* xf,
                                   const double* num, const double* den) {
-  const int nx = gf.nx, ny = gf.ny, nz = gf.nz;
-  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   const float xdamp = (float)(num[0] / den[0]);
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+  const int cx = gc.nx - 1, cy = gc.ny - 1, cz = gc.nz - 1;
+  const size_t ncell = (size_t)cx * cy * cz;
+  const size_t sy = gc.nx, sz = (size_t)gc.nx * gc.ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ncell;
        q += (size_t)gridDim.x * blockDim.x) {
-    int i, j, k;
-    interior_ijk(q, nx, ny, i, j, k);
-    const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
-    const int oi = i & 1, oj = j & 1, ok = k & 1;
-    float w = 0.f;
-    for (int c = 0; c <= ok; c++)
-      for (int b = 0; b <= oj; b++)
-        for (int a = 0; a <= oi; a++) w += xc[gc.idx(ii + a, jj + b, kk + c)];
-    w *= 1.f / (float)(1 << (oi + oj + ok));
-    xf[gf.idx(i, j, k)] += xdamp * w;
+    int ii, jj, kk;
+    split3(q, cx, cy, ii, jj, kk);
+    const size_t c0 = gc.idx(ii, jj, kk);
+    const float x000 = xc[c0], x100 = xc[c0 + 1], x010 = xc[c0 + sy], x110 = xc[c0 + sy + 1];
+    const float x001 = xc[c0 + sz], x101 = xc[c0 + sz + 1], x011 = xc[c0 + sz + sy];
+    const float x111 = xc[c0 + sz + sy + 1];
+#pragma unroll
+    for (int ok = 0; ok < 2; ok++) {
+      const int k = 2 * kk + ok;
+      if (k < 1 || k > gf.nz - 2) continue;
+#pragma unroll
+      for (int oj = 0; oj < 2; oj++) {
+        const int j = 2 * jj + oj;
+        if (j < 1 || j > gf.ny - 2) continue;
+#pragma unroll
+        for (int oi = 0; oi < 2; oi++) {
+          const int i = 2 * ii + oi;
+          if (i < 1 || i > gf.nx - 2) continue;
+          float w = 0.f;
+          w += x000;
+          if (oi) w += x100;
+          if (oj) {
+            w += x010;
+            if (oi) w += x110;
+          }
+          if (ok) {
+            w += x001;
+            if (oi) w += x101;
+            if (oj) {
+              w += x011;
+              if (oi) w += x111;
+            }
+          }
+          w *= 1.f / (float)(1 << (oi + oj + ok));
+          xf[gf.idx(i, j, k)] += xdamp * w;
+        }
+      }
+    }
   }
 }
 
@@ -1805,8 +1840,8 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
                 s->scal + S_XDEN_L + (l & 15));
       k += 2;
     }
-    const size_t pint = (size_t)(P.g.nx - 2) * (P.g.ny - 2) * (P.g.nz - 2);
-    k_interp_axpy_f32<<<blocks_for(pint), kThreads, 0, st>>>(
+    k_interp_axpy_f32<<<blocks_for((size_t)(C.g.nx - 1) * (C.g.ny - 1) * (C.g.nz - 1)),
+                        kThreads, 0, st>>>(
         C.g, C.x, P.g, P.x, s->scal + S_XNUM_L + (l & 15), s->scal + S_XDEN_L + (l & 15));
     k += 1;
     if (l == 0) {
