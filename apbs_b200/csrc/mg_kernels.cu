@@ -267,52 +267,69 @@ void launch_restrict(cudaStream_t s, Grid gf, const double* xin, Grid gc, double
 // with xdamp = <x_c, w0_c> / <x_c, A_c x_c> (src/pmgc/mgcsd.c:465-485).
 // Interior fine points only (Vxaxpy touches interior points).
 // ===========================================================================
+// One thread per coarse cell (ii..ii+1, jj..jj+1, kk..kk+1): its eight corner
+// values, read once, give the up to eight fine interior points 2ii+oi,
+// 2jj+oj, 2kk+ok of the cell, each with the reference's expression for its
+// parity case -- bitwise the per-point evaluation with an eighth of its loads
+// and index arithmetic.
 __global__ void k_interp_axpy(Grid gc, const double* __restrict__ xc, Grid gf, double* xf,
                               const double* num, const double* den) {
-  const int nx = gf.nx, ny = gf.ny, nz = gf.nz;
-  const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   const double xdamp = num[0] / den[0];
   const double h = 0.5, qq = 0.25, e = 0.125;
-  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nint;
+  const int cx = gc.nx - 1, cy = gc.ny - 1, cz = gc.nz - 1;
+  const size_t ncell = (size_t)cx * cy * cz;
+  const size_t sy = gc.nx, sz = (size_t)gc.nx * gc.ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < ncell;
        q += (size_t)gridDim.x * blockDim.x) {
-    int i, j, k;
-    interior_ijk(q, nx, ny, i, j, k);
-    const int ii = i >> 1, jj = j >> 1, kk = k >> 1;
-    const int oi = i & 1, oj = j & 1, ok = k & 1;
-#define XC(a, b, c) xc[gc.idx(a, b, c)]
-    double w;
-    if (!oi && !oj && !ok) {
-      w = XC(ii, jj, kk);
-    } else if (oi && !oj && !ok) {
-      w = h * XC(ii, jj, kk) + h * XC(ii + 1, jj, kk);
-    } else if (!oi && oj && !ok) {
-      w = h * XC(ii, jj, kk) + h * XC(ii, jj + 1, kk);
-    } else if (!oi && !oj && ok) {
-      w = h * XC(ii, jj, kk) + h * XC(ii, jj, kk + 1);
-    } else if (oi && oj && !ok) {
-      w = qq * XC(ii, jj, kk) + qq * XC(ii + 1, jj, kk) + qq * XC(ii, jj + 1, kk) +
-          qq * XC(ii + 1, jj + 1, kk);
-    } else if (oi && !oj && ok) {
-      w = qq * XC(ii, jj, kk) + qq * XC(ii + 1, jj, kk) + qq * XC(ii, jj, kk + 1) +
-          qq * XC(ii + 1, jj, kk + 1);
-    } else if (!oi && oj && ok) {
-      w = qq * XC(ii, jj, kk) + qq * XC(ii, jj + 1, kk) + qq * XC(ii, jj, kk + 1) +
-          qq * XC(ii, jj + 1, kk + 1);
-    } else {
-      w = +e * XC(ii, jj, kk) + e * XC(ii + 1, jj, kk) + e * XC(ii, jj + 1, kk) +
-          e * XC(ii + 1, jj + 1, kk) + e * XC(ii, jj, kk + 1) + e * XC(ii + 1, jj, kk + 1) +
-          e * XC(ii, jj + 1, kk + 1) + e * XC(ii + 1, jj + 1, kk + 1);
+    int ii, jj, kk;
+    split3(q, cx, cy, ii, jj, kk);
+    const size_t c0 = gc.idx(ii, jj, kk);
+    const double x000 = xc[c0], x100 = xc[c0 + 1], x010 = xc[c0 + sy], x110 = xc[c0 + sy + 1];
+    const double x001 = xc[c0 + sz], x101 = xc[c0 + sz + 1], x011 = xc[c0 + sz + sy];
+    const double x111 = xc[c0 + sz + sy + 1];
+#pragma unroll
+    for (int ok = 0; ok < 2; ok++) {
+      const int k = 2 * kk + ok;
+      if (k < 1 || k > gf.nz - 2) continue;
+#pragma unroll
+      for (int oj = 0; oj < 2; oj++) {
+        const int j = 2 * jj + oj;
+        if (j < 1 || j > gf.ny - 2) continue;
+#pragma unroll
+        for (int oi = 0; oi < 2; oi++) {
+          const int i = 2 * ii + oi;
+          if (i < 1 || i > gf.nx - 2) continue;
+          double w;
+          if (!oi && !oj && !ok) {
+            w = x000;
+          } else if (oi && !oj && !ok) {
+            w = h * x000 + h * x100;
+          } else if (!oi && oj && !ok) {
+            w = h * x000 + h * x010;
+          } else if (!oi && !oj && ok) {
+            w = h * x000 + h * x001;
+          } else if (oi && oj && !ok) {
+            w = qq * x000 + qq * x100 + qq * x010 + qq * x110;
+          } else if (oi && !oj && ok) {
+            w = qq * x000 + qq * x100 + qq * x001 + qq * x101;
+          } else if (!oi && oj && ok) {
+            w = qq * x000 + qq * x010 + qq * x001 + qq * x011;
+          } else {
+            w = +e * x000 + e * x100 + e * x010 + e * x110 + e * x001 + e * x101 + e * x011 +
+                e * x111;
+          }
+          const size_t id = gf.idx(i, j, k);
+          xf[id] += xdamp * w;
+        }
+      }
     }
-#undef XC
-    const size_t id = gf.idx(i, j, k);
-    xf[id] += xdamp * w;
   }
 }
 
 void launch_interp_axpy(cudaStream_t s, Grid gc, const double* xc, Grid gf, double* xf,
                         const double* num, const double* den) {
-  size_t nint = (size_t)(gf.nx - 2) * (gf.ny - 2) * (gf.nz - 2);
-  k_interp_axpy<<<blocks_for(nint), kThreads, 0, s>>>(gc, xc, gf, xf, num, den);
+  const size_t ncell = (size_t)(gc.nx - 1) * (gc.ny - 1) * (gc.nz - 1);
+  k_interp_axpy<<<blocks_for(ncell), kThreads, 0, s>>>(gc, xc, gf, xf, num, den);
 }
 
 // ===========================================================================
