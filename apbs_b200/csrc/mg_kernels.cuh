@@ -59,6 +59,7 @@ int mg_init();
 constexpr int kWavePlanesMax = 1024;
 constexpr int kWaveCounterBase = 16;  // words before level 0's counters
 constexpr int kWaveDampTicket = 8;    // the word launch_xdamp_sums counts blocks in
+constexpr int kWaveMixedDampTicket = 9;  // the same for the mixed path's damping sums
 constexpr size_t kWaveWords = kWaveCounterBase + 16 * (size_t)kWavePlanesMax;
 int wave_planes_fit(Grid g);
 // wlag: wavefronts between successive half-sweeps (>= 4)

@@ -486,11 +486,14 @@ __global__ void k_sum_parts(const double* __restrict__ part, int n, double* out)
 
 // The two sums of the interpolation damping on a coarse level, x.w0 and
 // x.((A + cc) x), in one pass over x: FP32 products (A + cc) x, FP64 sums,
-// partials per block (reduce_parts blocks) summed by k_sum_parts2.
+// partials per block (reduce_parts blocks) summed by the block that finishes
+// last (a ticket on *done, which it resets).
 __global__ void k_damp_dots(Grid g, OpF o, const float* __restrict__ cc,
                             const float* __restrict__ x, const float* __restrict__ w0,
-                            double* part_num, double* part_den) {
+                            double* part_num, double* part_den, unsigned* done, double* num,
+                            double* den) {
   __shared__ double sh[32];
+  __shared__ bool last;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const size_t nint = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
   double an = 0.0, ad = 0.0;
@@ -506,28 +509,37 @@ __global__ void k_damp_dots(Grid g, OpF o, const float* __restrict__ cc,
     ad += (double)xv * (double)ax;
   }
   const double tn = block_sum<256>(an, sh);
-  if (threadIdx.x == 0) part_num[blockIdx.x] = tn;
   const double td = block_sum<256>(ad, sh);
-  if (threadIdx.x == 0) part_den[blockIdx.x] = td;
-}
-
-// k_sum_parts of two partial arrays (blocks 0 and 1)
-__global__ void k_sum_parts2(const double* __restrict__ p0, const double* __restrict__ p1,
-                             int n, double* out0, double* out1) {
-  __shared__ double sh[32];
-  const double* part = blockIdx.x ? p1 : p0;
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
-  const double t = block_sum<256>(acc, sh);
-  if (threadIdx.x == 0) (blockIdx.x ? out1 : out0)[0] = t;
+  if (threadIdx.x == 0) {
+    part_num[blockIdx.x] = tn;
+    part_den[blockIdx.x] = td;
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (!last) return;
+  // the block that finishes last adds the partials in block order, as
+  // the separate two-block sum did: the same sums whichever block that is
+  __threadfence();
+  double bn = 0.0, bd = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+    bn += __ldcg(part_num + i);
+    bd += __ldcg(part_den + i);
+  }
+  const double sn = block_sum<256>(bn, sh);
+  const double sd = block_sum<256>(bd, sh);
+  if (threadIdx.x == 0) {
+    num[0] = sn;
+    den[0] = sd;
+    *done = 0u;
+  }
 }
 
 void damp_dots(cudaStream_t s, Grid g, OpF o, const float* cc, const float* x, const float* w0,
-               double* part, double* num, double* den) {
+               double* part, unsigned* done, double* num, double* den) {
   const size_t nint = (size_t)(g.nx - 2) * (g.ny - 2) * (g.nz - 2);
   const int nb = (int)reduce_parts(nint);
-  k_damp_dots<<<nb, 256, 0, s>>>(g, o, cc, x, w0, part, part + 2368);
-  k_sum_parts2<<<2, 256, 0, s>>>(part, part + 2368, nb, num, den);
+  k_damp_dots<<<nb, 256, 0, s>>>(g, o, cc, x, w0, part, part + 2368, done, num, den);
 }
 
 // FP64 fine residual r = f - (A + cc) x written as the FP32 V-cycle rhs,
@@ -1836,9 +1848,10 @@ int mixed_cycle_body(pmgb_solver* s, const double* cc64, const double* fc64, dou
     MLevel& C = m->lev[l + 1];
     MLevel& P = m->lev[l];
     if (l + 1 != tf || m->tail_first == 0) {
-      damp_dots(st, C.g, opf(C), C.cc, C.x, C.w0, s->part, s->scal + S_XNUM_L + (l & 15),
+      damp_dots(st, C.g, opf(C), C.cc, C.x, C.w0, s->part, s->d_wave + kWaveMixedDampTicket,
+                s->scal + S_XNUM_L + (l & 15),
                 s->scal + S_XDEN_L + (l & 15));
-      k += 2;
+      k += 1;
     }
     k_interp_axpy_f32<<<blocks_for((size_t)(C.g.nx - 1) * (C.g.ny - 1) * (C.g.nz - 1)),
                         kThreads, 0, st>>>(
